@@ -1,0 +1,319 @@
+#!/usr/bin/env python
+"""Throughput of the MD hot path on B200, one JSON line on rank 0.
+
+Workload (the 1M-molecule LJ configuration): FCC 64x64x64 unit cells
+(1,048,576 molecules), density 0.8442, T 0.722 (seeded Maxwell-Boltzmann),
+LJ 12-6 truncated and shifted at rc 2.5, skin 0.3, dt 0.005, NVE velocity
+Verlet with the reference's vmax rebuild criterion and tplot 100.  A "step"
+is one MD timestep of that system.  `value` is the precision form (FP32 pair
+forces, FP64 positions / velocities / sums); the plain FP64 drop-in is
+reported beside it.  Inputs are larger than L2: the neighbour list alone is
+~400 MB, so every step streams it from HBM.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+With N > 1 (torchrun) every rank advances its own replica of the system
+(replicas only: the hot path has no cross-replica exchange) and the timing is
+the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "molecule-steps/s (1M LJ), batched replica agg vs plain on same B200; p50/p99 latency"
+UNIT = "molecule-steps/s"
+NUNITS = (64, 64, 64)
+DENSITY, TEMP, RC, SKIN, DT, TPLOT = 0.8442, 0.722, 2.5, 0.3, 0.005, 100
+SEED = 0x466D6F6C + 1
+
+
+def alg_bytes_per_molecule_step(rn=RC + SKIN, rho=DENSITY):
+    """192 B of FP64 r, v, a read and written once, plus 4-byte half-list
+    indices: n_h = (2/3) pi r_n^3 rho."""
+    n_h = (2.0 / 3.0) * np.pi * rn ** 3 * rho
+    return 192.0 + 4.0 * n_h
+
+
+def workload_name():
+    return (f"LJ fluid, FCC {NUNITS[0]}x{NUNITS[1]}x{NUNITS[2]} units ({4 * int(np.prod(NUNITS)):,} molecules), "
+            f"rho {DENSITY}, T {TEMP}, rc {RC} shifted, skin {SKIN}, dt {DT}, NVE velocity Verlet")
+
+
+def make_state():
+    from flowmol_b200 import lattice
+    return lattice.lj_fluid(NUNITS, DENSITY, TEMP, SEED)
+
+
+def read_peaks():
+    try:
+        pk = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(pk["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """Per-launch DRAM bytes of the force kernel from the committed ncu
+    summary (None when no capture has been summarised yet)."""
+    p = os.path.join(ROOT, "profiles", "force_kernel_lj1m.json")
+    try:
+        return json.load(open(p)).get("dram_bytes_per_launch_full_size")
+    except Exception:
+        return None
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.device), "-lms", "100"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        sm, smax, reasons = [], [], set()
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1])); smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def run_form(api, torch, r, v, dom, precision, steps, warmup, dev, timing_pass=True):
+    """Device-resident throughput of one precision form."""
+    stream = torch.cuda.Stream(device=dev)
+    p = api.make_params(len(r), dom, RC, (SKIN,) * 3, DT, TPLOT, density=DENSITY, precision=precision)
+    s = api.MDSystem(p, stream=stream)
+    s.upload(r, v)
+    s.setup()
+    s.simulation_md(warmup, blocking=True)
+    s.records()
+    torch.cuda.synchronize(dev)
+    launches0 = s.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    out = {}
+    with Clocks(dev) as clk:
+        e0.record(stream)
+        s.simulation_md(steps, blocking=False)
+        e1.record(stream)
+        e1.synchronize()
+    s.sync()
+    out["ms"] = e0.elapsed_time(e1)
+    out["clocks"] = clk.summary()
+    out["launches"] = s.launch_count() - launches0
+    out["rebuilds"] = s.counters()["rebuilds"]
+    if timing_pass:
+        s.force_kernel_timing(True)
+        s.simulation_md(steps, blocking=True)
+        ms, nl = s.force_kernel_time()
+        s.force_kernel_timing(False)
+        out["force_ms_avg"] = ms / max(nl, 1)
+        out["force_launches"] = nl
+    out["records"] = s.records()
+    out["capacity"] = s.counters()["nlist_capacity"]
+    s.close()
+    return out
+
+
+def run_e2e(api, torch, r, v, dom, precision, steps, dev):
+    """Through the public API with host buffers: pinned upload, setup, steps,
+    download of the final state and the records, all inside the timed region."""
+    n = len(r)
+    rh = torch.from_numpy(np.ascontiguousarray(r)).pin_memory()
+    vh = torch.from_numpy(np.ascontiguousarray(v)).pin_memory()
+    ro = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+    vo = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+    ao = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+    p = api.make_params(n, dom, RC, (SKIN,) * 3, DT, TPLOT, density=DENSITY, precision=precision)
+    s = api.MDSystem(p)
+    torch.cuda.synchronize(dev)
+    import ctypes as C
+    dp = lambda t: C.cast(t.data_ptr(), C.POINTER(C.c_double))  # noqa: E731
+    t0 = time.perf_counter()
+    api.check(api.lib().fm_upload_state(s.h, n, dp(rh), dp(vh), None, None))
+    s.setup()
+    s.simulation_md(steps, blocking=True)
+    api.check(api.lib().fm_download_state(s.h, dp(ro), dp(vo), dp(ao), None))
+    recs = s.records()
+    t1 = time.perf_counter()
+    s.close()
+    h2d = 2 * n * 3 * 8
+    d2h = 3 * n * 3 * 8 + len(recs) * 80
+    return {"value": n * steps / (t1 - t0), "unit": UNIT, "h2d_bytes_per_step": h2d / steps,
+            "d2h_bytes_per_step": d2h / steps, "steps": steps, "seconds": t1 - t0}
+
+
+def cpu_baseline(r, v, dom, nsteps=8):
+    """The FP64 oracle (C restatement of the reference's routines, one
+    thread) on the same 1M system: setup excluded, nsteps timed."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    o = O.Oracle(r, v, dom, RC, (SKIN,) * 3, DT, TPLOT, density=DENSITY)
+    t0 = time.perf_counter()
+    o.setup()
+    t_setup = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    o.run_vv(nsteps)
+    dt = time.perf_counter() - t0
+    return {"value": len(r) * nsteps / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{len(r):,} molecules x {nsteps} velocity-Verlet steps from the FCC start "
+                      f"({o.rebuild_count} list rebuilds inside; setup {t_setup:.1f} s excluded)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        r, v, dom = make_state()
+        steps = max(2, min(args.steps, 8))
+        cb = cpu_baseline(r, v, dom, steps)
+        line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "impl": "reference",
+                "n_gpus": args.gpus, "steps": steps, "warmup": 0,
+                "ms_per_step": 1e3 * len(r) / cb["value"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": workload_name(), "molecules": len(r), "form": "oracle FP64 CPU restatement"},
+                "cpu_baseline": cb,
+                "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    from flowmol_b200 import api, build as fb
+    fb.build()
+    dev = local
+    torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", dev))
+    r, v, dom = make_state()
+    n = len(r)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    barrier()
+    f32 = run_form(api, torch, r, v, dom, api.PRECISION_FP32, args.steps, args.warmup, dev)
+    ms32 = max_over_ranks(f32["ms"])
+    barrier()
+    f64 = run_form(api, torch, r, v, dom, api.PRECISION_FP64, args.steps, args.warmup, dev)
+    ms64 = max_over_ranks(f64["ms"])
+    barrier()
+    e2e = None if args.no_e2e else run_e2e(api, torch, r, v, dom, api.PRECISION_FP32, args.steps, dev)
+    if e2e is not None:
+        e2e["value"] = world * n * args.steps / max_over_ranks(e2e["seconds"])
+    barrier()
+
+    if rank == 0:
+        value = world * n * args.steps / (ms32 * 1e-3)
+        peak, peak_kind = read_peaks()
+        b_alg = alg_bytes_per_molecule_step()
+        achieved = n * b_alg / (f32["force_ms_avg"] * 1e-3) / 1e9
+        traffic = profile_traffic()
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            cpu = cpu_baseline(r, v, dom)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64", "data": "synthetic",
+            "config": {"workload": workload_name(), "molecules": n, "replicas": world,
+                       "form": "precision: FP32 pair forces, FP64 r/v/a, FP64 compensated sums",
+                       "l2": "no flush: per-step working set (neighbour list ~%d MB + state) exceeds the 126 MB L2"
+                             % (n * f32["capacity"] * 4 // 2 ** 20),
+                       "rebuilds_in_timed_region": f32["rebuilds"], "parallelism": f"replicas x{world}"},
+            "forms": {
+                "fp32_forces": {"value": value, "ms_per_step": ms32 / args.steps,
+                                "force_kernel_ms": f32["force_ms_avg"]},
+                "fp64_plain": {"value": world * n * args.steps / (ms64 * 1e-3), "ms_per_step": ms64 / args.steps,
+                               "force_kernel_ms": f64["force_ms_avg"]},
+            },
+            "roofline": {"bound": "hbm", "kernel": "k_force (fused forces + move(2) + next move(1))",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": f"{peak_kind} hbm_gbs", "alg_bytes_per_molecule_step": b_alg,
+                         "traffic": traffic},
+            "clocks": f32["clocks"],
+            "gpu_launches": f32["launches"],
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,359 @@
+"""ctypes binding of libflowmol_b200.so (C ABI in include/flowmol_b200.h).
+
+``MDSystem`` exposes the reference's hot-path subroutines under their own
+names (simulation_move_particles_vv, messenger_updateborders,
+simulation_checkrebuild, linklist_deallocateall, sendmols, assign_to_cell,
+assign_to_neighbourlist, simulation_compute_forces,
+evaluate_macroscopic_properties) plus ``md_advance_vv`` and the fused
+``simulation_md`` loop, so a driver written against Flowmol's md.f90 reads
+the same.  Every call goes to the CUDA library; there is no CPU path, and a
+missing library raises at import of this module's first use.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libflowmol_b200.so")
+
+FM_OK = 0
+ERRORS = {1: "ARG", 2: "CUDA", 3: "FEWCELLS", 4: "ESCAPE", 5: "NLIST", 6: "PE", 7: "STATE", 8: "BOND",
+          9: "NODEVICE", 10: "IO"}
+
+FORCE_LIST_ALLPAIRS, FORCE_LIST_FULL, FORCE_LIST_HALF = 0, 2, 3
+PRECISION_FP64, PRECISION_FP32 = 0, 1
+
+
+class FmParams(C.Structure):
+    _fields_ = [
+        ("np", C.c_int32),
+        ("domain", C.c_double * 3),
+        ("density", C.c_double),
+        ("rcutoff", C.c_double),
+        ("delta_rneighbr", C.c_double * 3),
+        ("delta_t", C.c_double),
+        ("tplot", C.c_int32),
+        ("initialstep", C.c_int32),
+        ("simtime", C.c_double),
+        ("force_list", C.c_int32),
+        ("potential_flag", C.c_int32),
+        ("rebuild_criteria", C.c_int32),
+        ("fixed_rebuild", C.c_int32),
+        ("sLRC_flag", C.c_int32),
+        ("precision", C.c_int32),
+        ("k_c", C.c_double),
+        ("R_0", C.c_double),
+        ("nlist_capacity", C.c_int32),
+        ("threads_per_molecule", C.c_int32),
+    ]
+
+
+class FmMacro(C.Structure):
+    _fields_ = [
+        ("iter", C.c_int32), ("pad_", C.c_int32), ("simtime", C.c_double), ("vsum", C.c_double),
+        ("mv2sum", C.c_double), ("temperature", C.c_double), ("kinenergy", C.c_double),
+        ("potenergy", C.c_double), ("totenergy", C.c_double), ("pressure", C.c_double),
+        ("virial", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad_"}
+
+
+class FlowmolError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"FM_ERR_{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """Loads the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m flowmol_b200.build` "
+                              "(the MD path has no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        P = C.POINTER
+        h = C.c_void_p
+        sig = {
+            "fm_derive_geometry": [P(FmParams), P(C.c_int32), P(C.c_double), P(C.c_double), P(C.c_double),
+                                   P(C.c_double)],
+            "fm_global_domain": [P(C.c_int32), C.c_double, P(C.c_double)],
+            "fm_create": [P(FmParams), P(h)],
+            "fm_destroy": [h],
+            "fm_set_stream": [h, C.c_void_p],
+            "fm_upload_state": [h, C.c_int32, P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_int32)],
+            "fm_download_state": [h, P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_int32)],
+            "fm_upload_state_device": [h, C.c_int32, C.c_void_p, C.c_void_p],
+            "fm_download_state_device": [h, C.c_void_p, C.c_void_p, C.c_void_p],
+            "fm_setup": [h],
+            "fm_move_vv": [h, C.c_int32],
+            "fm_update_borders": [h, C.c_int32],
+            "fm_check_rebuild": [h, P(C.c_int32)],
+            "fm_linklist_deallocateall": [h],
+            "fm_sendmols": [h],
+            "fm_assign_to_cell": [h],
+            "fm_assign_to_neighbourlist": [h],
+            "fm_compute_forces": [h],
+            "fm_evaluate_macroscopic_properties": [h, P(FmMacro)],
+            "fm_set_iter": [h, C.c_int32],
+            "fm_get_iter": [h, P(C.c_int32)],
+            "fm_step": [h, C.c_int32, C.c_int32],
+            "fm_sync": [h],
+            "fm_get_records": [h, P(FmMacro), C.c_int32, P(C.c_int32)],
+            "fm_get_per_molecule": [h, P(C.c_double), P(C.c_double)],
+            "fm_get_pair_list": [h, P(C.c_int32), P(C.c_int32), P(C.c_int8), C.c_int64, P(C.c_int64)],
+            "fm_pair_digest": [h, P(C.c_uint64), P(C.c_int64)],
+            "fm_get_counters": [h, P(C.c_int64), P(C.c_int32), P(C.c_int32)],
+            "fm_last_error": [C.c_char_p, C.c_int32],
+            "fm_force_kernel_timing": [h, C.c_int32],
+            "fm_get_force_kernel_time": [h, P(C.c_double), P(C.c_int64)],
+            "fm_get_launch_count": [h, P(C.c_int64)],
+        }
+        for name, args in sig.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def exported_symbols():
+    """Names declared in include/flowmol_b200.h that the loaded library exports."""
+    L = lib()
+    out = []
+    hdr = os.path.join(os.path.dirname(_PKG), "include", "flowmol_b200.h")
+    import re
+    for name in re.findall(r"FM_API int (fm_\w+)\(", open(hdr).read()):
+        getattr(L, name)  # raises AttributeError when missing
+        out.append(name)
+    return out
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(512)
+    lib().fm_last_error(buf, 512)
+    return buf.value.decode(errors="replace")
+
+
+def check(rc):
+    if rc != FM_OK:
+        raise FlowmolError(rc, last_error())
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def make_params(np_, domain, rcutoff, delta_rneighbr=(0.3, 0.3, 0.3), delta_t=0.005, tplot=100,
+                density=None, initialstep=0, simtime=0.0, force_list=FORCE_LIST_HALF, potential_flag=0,
+                rebuild_criteria=0, fixed_rebuild=1, sLRC_flag=0, precision=PRECISION_FP64, k_c=30.0,
+                R_0=1.5, nlist_capacity=0, threads_per_molecule=0) -> FmParams:
+    p = FmParams()
+    p.np = int(np_)
+    for k in range(3):
+        p.domain[k] = float(domain[k])
+        p.delta_rneighbr[k] = float(delta_rneighbr[k])
+    p.density = float(density) if density is not None else np_ / float(np.prod(domain))
+    p.rcutoff = float(rcutoff)
+    p.delta_t = float(delta_t)
+    p.tplot = int(tplot)
+    p.initialstep = int(initialstep)
+    p.simtime = float(simtime)
+    p.force_list = int(force_list)
+    p.potential_flag = int(potential_flag)
+    p.rebuild_criteria = int(rebuild_criteria)
+    p.fixed_rebuild = int(fixed_rebuild)
+    p.sLRC_flag = int(sLRC_flag)
+    p.precision = int(precision)
+    p.k_c = float(k_c)
+    p.R_0 = float(R_0)
+    p.nlist_capacity = int(nlist_capacity)
+    p.threads_per_molecule = int(threads_per_molecule)
+    return p
+
+
+def derive_geometry(params: FmParams):
+    nc = (C.c_int32 * 3)()
+    cs = (C.c_double * 3)()
+    rn2, rc2, ps = C.c_double(), C.c_double(), C.c_double()
+    rc = lib().fm_derive_geometry(C.byref(params), nc, cs, C.byref(rn2), C.byref(rc2), C.byref(ps))
+    return rc, dict(ncells=list(nc), cellside=list(cs), rneighbr2=rn2.value, rcutoff2=rc2.value,
+                    potshift=ps.value)
+
+
+def global_domain(nunits, density):
+    n = (C.c_int32 * 3)(*[int(x) for x in nunits])
+    d = (C.c_double * 3)()
+    check(lib().fm_global_domain(n, float(density), d))
+    return np.array(list(d))
+
+
+class MDSystem:
+    """One simulation on the current CUDA device (a handle of the C ABI)."""
+
+    def __init__(self, params: FmParams, stream=None):
+        self.params = params
+        self.n = params.np
+        hp = C.c_void_p()
+        check(lib().fm_create(C.byref(params), C.byref(hp)))
+        self.h = hp
+        if stream is not None:
+            self.set_stream(stream)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().fm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream):
+        ptr = stream if isinstance(stream, int) else getattr(stream, "cuda_stream", 0)
+        check(lib().fm_set_stream(self.h, C.c_void_p(ptr)))
+
+    # ---- state ----
+    def upload(self, r, v, a=None, glob_no=None):
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        ap = None
+        if a is not None:
+            a = np.ascontiguousarray(a, dtype=np.float64)
+            ap = _dp(a)
+        gp = None
+        if glob_no is not None:
+            glob_no = np.ascontiguousarray(glob_no, dtype=np.int32)
+            gp = glob_no.ctypes.data_as(C.POINTER(C.c_int32))
+        check(lib().fm_upload_state(self.h, self.n, _dp(r), _dp(v), ap, gp))
+
+    def download(self):
+        r = np.empty((self.n, 3)); v = np.empty((self.n, 3)); a = np.empty((self.n, 3))
+        g = np.empty(self.n, np.int32)
+        check(lib().fm_download_state(self.h, _dp(r), _dp(v), _dp(a), g.ctypes.data_as(C.POINTER(C.c_int32))))
+        return r, v, a, g
+
+    # ---- reference subroutine mirrors (md.f90) ----
+    def setup(self):
+        check(lib().fm_setup(self.h))
+
+    def simulation_move_particles_vv(self, pass_num):
+        check(lib().fm_move_vv(self.h, int(pass_num)))
+
+    def messenger_updateborders(self, rebuild):
+        check(lib().fm_update_borders(self.h, int(rebuild)))
+
+    def simulation_checkrebuild(self) -> int:
+        r = C.c_int32()
+        check(lib().fm_check_rebuild(self.h, C.byref(r)))
+        return r.value
+
+    def linklist_deallocateall(self):
+        check(lib().fm_linklist_deallocateall(self.h))
+
+    def sendmols(self):
+        check(lib().fm_sendmols(self.h))
+
+    def sort_mols(self):
+        """SORT_FLAG 0: molecules keep their identity (the device re-orders by
+        cell internally, invisibly)."""
+
+    def assign_to_cell(self):
+        check(lib().fm_assign_to_cell(self.h))
+
+    def assign_to_neighbourlist(self):
+        check(lib().fm_assign_to_neighbourlist(self.h))
+
+    def simulation_compute_forces(self):
+        check(lib().fm_compute_forces(self.h))
+
+    def evaluate_macroscopic_properties(self):
+        m = FmMacro()
+        check(lib().fm_evaluate_macroscopic_properties(self.h, C.byref(m)))
+        return m.as_dict()
+
+    @property
+    def iter(self):
+        i = C.c_int32()
+        check(lib().fm_get_iter(self.h, C.byref(i)))
+        return i.value
+
+    @iter.setter
+    def iter(self, value):
+        check(lib().fm_set_iter(self.h, int(value)))
+
+    def md_advance_vv(self):
+        """One iteration, subroutine by subroutine (md.f90:143-163)."""
+        self.iter = self.iter + 1
+        self.simulation_move_particles_vv(1)
+        self.messenger_updateborders(0)
+        if self.simulation_checkrebuild():
+            self.linklist_deallocateall()
+            self.sendmols()
+            self.sort_mols()
+            self.assign_to_cell()
+            self.messenger_updateborders(1)
+            self.assign_to_neighbourlist()
+        self.simulation_compute_forces()
+        self.simulation_move_particles_vv(2)
+
+    def simulation_md(self, nsteps, blocking=True):
+        """The fused device loop over nsteps iterations."""
+        check(lib().fm_step(self.h, int(nsteps), 1 if blocking else 0))
+
+    def sync(self):
+        check(lib().fm_sync(self.h))
+
+    # ---- results ----
+    def records(self, cap=100000):
+        arr = (FmMacro * cap)()
+        n = C.c_int32()
+        check(lib().fm_get_records(self.h, arr, cap, C.byref(n)))
+        return [arr[k].as_dict() for k in range(n.value)]
+
+    def per_molecule(self):
+        pe = np.empty(self.n); vir = np.empty(self.n)
+        check(lib().fm_get_per_molecule(self.h, _dp(pe), _dp(vir)))
+        return pe, vir
+
+    def pair_list(self):
+        n = C.c_int64()
+        check(lib().fm_get_pair_list(self.h, None, None, None, 0, C.byref(n)))
+        o = np.empty(n.value, np.int32); p = np.empty(n.value, np.int32); c = np.empty(n.value, np.int8)
+        check(lib().fm_get_pair_list(self.h, o.ctypes.data_as(C.POINTER(C.c_int32)),
+                                     p.ctypes.data_as(C.POINTER(C.c_int32)),
+                                     c.ctypes.data_as(C.POINTER(C.c_int8)), n.value, C.byref(n)))
+        return o, p, c.astype(np.int32)
+
+    def pair_digest(self):
+        d = C.c_uint64(); n = C.c_int64()
+        check(lib().fm_pair_digest(self.h, C.byref(d), C.byref(n)))
+        return d.value, n.value
+
+    def force_kernel_timing(self, enable=True):
+        check(lib().fm_force_kernel_timing(self.h, 1 if enable else 0))
+
+    def force_kernel_time(self):
+        ms = C.c_double(); n = C.c_int64()
+        check(lib().fm_get_force_kernel_time(self.h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    def launch_count(self):
+        n = C.c_int64()
+        check(lib().fm_get_launch_count(self.h, C.byref(n)))
+        return n.value
+
+    def counters(self):
+        rb = C.c_int64(); cap = C.c_int32(); mx = C.c_int32()
+        check(lib().fm_get_counters(self.h, C.byref(rb), C.byref(cap), C.byref(mx)))
+        return dict(rebuilds=rb.value, nlist_capacity=cap.value, max_neighbours=mx.value)

@@ -1,0 +1,882 @@
+// fm_api.cu -- C ABI and host-side step driver of the B200 MD hot path.
+//
+// The driver mirrors md_advance_vv (md.f90:143-163): per iteration it queues
+// move(1), the rebuild decision, the (device-gated) rebuild pipeline, forces
+// and move(2), and the record reduction on tplot steps.  Move(2) of one
+// iteration and move(1) of the next are fused into the force kernel, so a
+// non-rebuild step is one force launch plus the small decision kernel and
+// the gated no-op rebuild launches.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "fm_common.cuh"
+#include "flowmol_b200.h"
+
+using fm::FmDev;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string &msg)
+{
+    g_last_error = msg;
+    return code;
+}
+
+#define FM_CUDA(call)                                                                              \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return fail(FM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));          \
+    } while (0)
+
+#define FM_TRY(call)                 \
+    do {                             \
+        int r_ = (call);             \
+        if (r_ != FM_OK) return r_;  \
+    } while (0)
+
+const double kPi = 3.14159265358979323846;
+
+inline double p3(double s) { return s * s * s; }
+inline double p6(double s) { double t = p3(s); return t * t; }
+inline double p12(double s) { double t = p6(s); return t * t; }
+
+}  // namespace
+
+struct fm_handle {
+    fm_params p{};
+    FmDev d{};
+    cudaStream_t st = nullptr;
+    int device = 0;
+    int iter = 0;
+    double simtime = 0.0;
+    int stage = 0;            // 0 created, 1 state uploaded, 2 forces valid, 3 broken
+    int tpm = 8;
+    double half_min_delta = 0.0;
+    double4 *tpos = nullptr;
+    int32_t *tuidx = nullptr;
+    int32_t *glob = nullptr;  // device: glob_no of upload index
+    std::vector<int32_t> glob_host;
+    double *stage3 = nullptr; // device staging, 3 arrays of (3, n)
+    // queued fused-loop range, kept so that a list overflow can be resumed
+    struct Range {
+        bool active = false;
+        int first_iter = 0;
+        int nsteps = 0;
+        std::vector<double> simtime_after;  // simtime after step k of the range
+    } q;
+    bool has_pe = false;
+    bool cells_valid = false;  // cell_start/perm describe the current slot order
+    bool list_valid = false;   // the neighbour list was built after the last re-order
+    // instrumentation
+    bool timing = false;
+    std::vector<cudaEvent_t> ev;
+    size_t ev_used = 0;
+    int64_t launches = 0;
+};
+
+// ---------------------------------------------------------------------------
+// geometry (setup_set_parameters.f90)
+// ---------------------------------------------------------------------------
+
+static int derive(const fm_params *p, int32_t nc[3], double cs[3], double *rn2, double *rc2, double *ps)
+{
+    if (!p) return fail(FM_ERR_ARG, "null params");
+    if (!(p->rcutoff > 0.0)) return fail(FM_ERR_ARG, "rcutoff must be > 0");
+    for (int k = 0; k < 3; k++)
+        if (!(p->domain[k] > 0.0)) return fail(FM_ERR_ARG, "domain must be > 0");
+    // rneighbr = rcutoff + mean(delta) (set_parameters_cells :1858-1859)
+    double rneighbr = p->rcutoff + (p->delta_rneighbr[0] + p->delta_rneighbr[1] + p->delta_rneighbr[2]) / 3.0;
+    double rneighbr2 = rneighbr * rneighbr;
+    if (p->potential_flag == 1 && rneighbr < p->R_0) rneighbr2 = p->R_0 * p->R_0;  // :1865-1869
+    for (int k = 0; k < 3; k++) nc[k] = (int32_t)std::floor(p->domain[k] / (p->rcutoff + p->delta_rneighbr[k]));
+    *rn2 = rneighbr2;
+    *rc2 = p->rcutoff * p->rcutoff;
+    *ps = 4.0 * (1.0 / p12(p->rcutoff) - 1.0 / p6(p->rcutoff));  // :1222
+    bool few = nc[0] < 3 || nc[1] < 3 || nc[2] < 3;
+    for (int k = 0; k < 3; k++) cs[k] = nc[k] > 0 ? p->domain[k] / (double)nc[k] : p->domain[k];
+    if (few) return fail(FM_ERR_FEWCELLS, "domain should have at least 3 cells in x, y and z");
+    return FM_OK;
+}
+
+extern "C" int fm_derive_geometry(const fm_params *p, int32_t ncells[3], double cellsidelength[3],
+                                  double *rneighbr2, double *rcutoff2, double *potshift)
+{
+    if (!ncells || !cellsidelength || !rneighbr2 || !rcutoff2 || !potshift) return fail(FM_ERR_ARG, "null output");
+    return derive(p, ncells, cellsidelength, rneighbr2, rcutoff2, potshift);
+}
+
+extern "C" int fm_global_domain(const int32_t nunits[3], double density, double domain[3])
+{
+    if (!nunits || !domain || !(density > 0.0)) return fail(FM_ERR_ARG, "bad arguments");
+    for (int k = 0; k < 3; k++) domain[k] = (double)nunits[k] / std::pow(density / 4.0, 1.0 / 3.0);
+    return FM_OK;
+}
+
+extern "C" int fm_last_error(char *buf, int32_t len)
+{
+    if (!buf || len <= 0) return FM_ERR_ARG;
+    std::snprintf(buf, (size_t)len, "%s", g_last_error.c_str());
+    return FM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// allocation
+// ---------------------------------------------------------------------------
+
+template <typename T>
+static int dalloc(T **ptr, size_t count)
+{
+    *ptr = nullptr;
+    if (count == 0) count = 1;
+    FM_CUDA(cudaMalloc((void **)ptr, count * sizeof(T)));
+    return FM_OK;
+}
+
+static void release(fm_handle *h)
+{
+    for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
+    h->ev.clear();
+    FmDev &d = h->d;
+    void *ptrs[] = {d.pos0, d.pos1, d.vx, d.vy, d.vz, d.ax, d.ay, d.az, d.slot_of, d.tvx, d.tvy, d.tvz,
+                    d.tax, d.tay, d.taz, d.cell_of, d.cell_count, d.cell_start, d.perm, d.nbr, d.nnbr,
+                    d.pe, d.vir, d.partial, d.rec, d.sc, h->tpos, h->tuidx, h->glob, h->stage3};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    d = FmDev{};
+    h->tpos = nullptr; h->tuidx = nullptr; h->glob = nullptr; h->stage3 = nullptr;
+}
+
+static int pick_tpm(const fm_params &p, double expected_full)
+{
+    if (p.threads_per_molecule > 0) {
+        int t = p.threads_per_molecule;
+        if (t != 1 && t != 2 && t != 4 && t != 8 && t != 16) return -1;
+        return t;
+    }
+    // about 8-12 candidates per lane keeps the lanes of a group busy while the
+    // shuffle reduction stays short
+    if (expected_full > 96) return 8;
+    if (expected_full > 40) return 4;
+    if (expected_full > 16) return 2;
+    return 1;
+}
+
+static int round_up(int x, int m) { return ((x + m - 1) / m) * m; }
+
+static int alloc_nlist(fm_handle *h, int maxn)
+{
+    FmDev &d = h->d;
+    if (d.nbr) cudaFree(d.nbr);
+    d.nbr = nullptr;
+    d.maxn = maxn;
+    FM_TRY(dalloc(&d.nbr, (size_t)d.n * (size_t)maxn));
+    return FM_OK;
+}
+
+extern "C" int fm_create(const fm_params *p, fm_handle **out)
+{
+    if (!p || !out) return fail(FM_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (p->np <= 0 || p->np > fm::MAX_MOLECULES) return fail(FM_ERR_ARG, "np out of range (1 .. 2^26-1)");
+    if (p->tplot <= 0) return fail(FM_ERR_ARG, "tplot must be > 0");
+    if (!(p->delta_t > 0.0)) return fail(FM_ERR_ARG, "delta_t must be > 0");
+    if (p->force_list != 0 && p->force_list != 2 && p->force_list != 3)
+        return fail(FM_ERR_ARG, "force_list must be 0, 2 or 3");
+    if (p->precision != FM_PRECISION_FP64 && p->precision != FM_PRECISION_FP32)
+        return fail(FM_ERR_ARG, "precision must be FM_PRECISION_FP64 or FM_PRECISION_FP32");
+    if (p->potential_flag != 0) return fail(FM_ERR_ARG, "potential_flag 1 (FENE) is served by fm_poly_* handles");
+    if (p->rebuild_criteria != 0 && p->rebuild_criteria != 1)
+        return fail(FM_ERR_ARG, "rebuild_criteria must be 0 (vmax) or 1 (fixed)");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(FM_ERR_NODEVICE, "no CUDA device");
+
+    int32_t nc[3];
+    double cs[3], rn2, rc2, ps;
+    int grc = derive(p, nc, cs, &rn2, &rc2, &ps);
+    if (grc != FM_OK && !(grc == FM_ERR_FEWCELLS && p->force_list == 0)) return grc;
+
+    fm_handle *h = new fm_handle();
+    h->p = *p;
+    FM_CUDA(cudaGetDevice(&h->device));
+    FmDev &d = h->d;
+    d.n = p->np;
+    for (int k = 0; k < 3; k++) {
+        d.L[k] = p->domain[k];
+        d.hd[k] = 0.5 * p->domain[k];
+        d.cs[k] = cs[k];
+        d.nc[k] = p->force_list == 0 ? 1 : nc[k];
+        d.ne[k] = d.nc[k] + 2;
+    }
+    d.ncell = d.ne[0] * d.ne[1] * d.ne[2];
+    d.rc2 = rc2;
+    d.rn2 = rn2;
+    d.dt = p->delta_t;
+    d.half_dt = 0.5 * p->delta_t;
+    d.half_dt2 = 0.5 * (p->delta_t * p->delta_t);
+    d.potshift = ps;
+    d.density = p->density > 0.0 ? p->density : (double)p->np / (p->domain[0] * p->domain[1] * p->domain[2]);
+    if (p->sLRC_flag) {  // setup_set_parameters.f90:1226-1238
+        d.pot_slrc = 8.0 * kPi * d.density * (1.0 / (9.0 * std::pow(p->rcutoff, 9)) - 1.0 / (3.0 * p3(p->rcutoff)));
+        d.p_slrc = 8.0 * kPi * std::pow(d.density, 2.0) *
+                   (4.0 / (9.0 * std::pow(p->rcutoff, 9)) - 2.0 / (3.0 * p3(p->rcutoff)));
+    }
+    d.tplot = p->tplot;
+    d.precision = p->precision;
+    double dmin = std::min(p->delta_rneighbr[0], std::min(p->delta_rneighbr[1], p->delta_rneighbr[2]));
+    h->half_min_delta = 0.5 * dmin;
+
+    double rho = (double)p->np / (p->domain[0] * p->domain[1] * p->domain[2]);
+    double expected = 4.0 / 3.0 * kPi * std::pow(std::sqrt(rn2), 3) * std::max(rho, 0.25);
+    int tpm = pick_tpm(*p, expected);
+    if (tpm < 0) { delete h; return fail(FM_ERR_ARG, "threads_per_molecule must be 0, 1, 2, 4, 8 or 16"); }
+    h->tpm = tpm;
+    int maxn = p->nlist_capacity > 0 ? p->nlist_capacity : round_up((int)std::ceil(1.3 * expected) + 16, 8);
+
+    const size_t n = (size_t)d.n;
+    int rc = FM_OK;
+#define FM_ALLOC(ptr, cnt)                                   \
+    if (rc == FM_OK) rc = dalloc(&(ptr), (size_t)(cnt));
+    FM_ALLOC(d.pos0, n) FM_ALLOC(d.pos1, n)
+    FM_ALLOC(d.vx, n) FM_ALLOC(d.vy, n) FM_ALLOC(d.vz, n)
+    FM_ALLOC(d.ax, n) FM_ALLOC(d.ay, n) FM_ALLOC(d.az, n)
+    FM_ALLOC(d.tvx, n) FM_ALLOC(d.tvy, n) FM_ALLOC(d.tvz, n)
+    FM_ALLOC(d.tax, n) FM_ALLOC(d.tay, n) FM_ALLOC(d.taz, n)
+    FM_ALLOC(d.slot_of, n) FM_ALLOC(h->tuidx, n) FM_ALLOC(h->tpos, n) FM_ALLOC(h->glob, n)
+    FM_ALLOC(d.cell_of, n) FM_ALLOC(d.perm, n) FM_ALLOC(d.nnbr, n)
+    FM_ALLOC(d.cell_count, d.ncell) FM_ALLOC(d.cell_start, d.ncell + 1)
+    FM_ALLOC(d.pe, n) FM_ALLOC(d.vir, n)
+    FM_ALLOC(h->stage3, 9 * n)
+    int nb = std::max(std::max(fm::force_blocks(d.n, 16), fm::all_pairs_blocks(d.n)), fm::macro_blocks(d.n));
+    FM_ALLOC(d.partial, (size_t)nb * fm::RS_N)
+    d.rec_cap = 4096;
+    FM_ALLOC(d.rec, d.rec_cap)
+    FM_ALLOC(d.sc, 1)
+#undef FM_ALLOC
+    if (rc == FM_OK && p->force_list != 0) rc = alloc_nlist(h, maxn);
+    if (rc != FM_OK) {
+        std::string msg = g_last_error;
+        release(h);
+        delete h;
+        return fail(rc, msg);
+    }
+    d.nblocks_force = fm::force_blocks(d.n, h->tpm);
+    cudaMemset(d.cell_count, 0, sizeof(int32_t) * (size_t)d.ncell);
+    cudaMemset(d.cell_start, 0, sizeof(int32_t) * (size_t)(d.ncell + 1));
+    cudaMemset(d.nnbr, 0, sizeof(int32_t) * n);
+    cudaMemset(d.pe, 0, sizeof(double) * n);
+    cudaMemset(d.vir, 0, sizeof(double) * n);
+    cudaMemset(d.sc, 0, sizeof(fm::FmScalars));
+    fm::launch_reset_scalars(d, nullptr);
+    FM_CUDA(cudaGetLastError());
+    FM_CUDA(cudaDeviceSynchronize());
+    h->iter = p->initialstep;
+    h->simtime = p->simtime;
+    *out = h;
+    return FM_OK;
+}
+
+extern "C" int fm_destroy(fm_handle *h)
+{
+    if (!h) return FM_OK;
+    cudaStreamSynchronize(h->st);
+    release(h);
+    delete h;
+    return FM_OK;
+}
+
+extern "C" int fm_set_stream(fm_handle *h, void *stream)
+{
+    if (!h) return fail(FM_ERR_ARG, "null handle");
+    h->st = (cudaStream_t)stream;
+    return FM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// state transfer
+// ---------------------------------------------------------------------------
+
+static int begin_state(fm_handle *h, int32_t n)
+{
+    if (!h) return fail(FM_ERR_ARG, "null handle");
+    if (n != h->d.n) return fail(FM_ERR_ARG, "n differs from the np the handle was created with");
+    h->q.active = false;
+    h->cells_valid = false;
+    h->list_valid = false;
+    h->iter = h->p.initialstep;
+    h->simtime = h->p.simtime;
+    h->d.nblocks_force = fm::force_blocks(h->d.n, h->tpm);
+    fm::launch_reset_scalars(h->d, h->st);
+    FM_CUDA(cudaMemsetAsync(h->d.cell_count, 0, sizeof(int32_t) * (size_t)h->d.ncell, h->st));
+    return FM_OK;
+}
+
+static int set_glob(fm_handle *h, const int32_t *glob_no)
+{
+    const int n = h->d.n;
+    h->glob_host.resize((size_t)n);
+    for (int i = 0; i < n; i++) h->glob_host[(size_t)i] = glob_no ? glob_no[i] : i + 1;
+    FM_CUDA(cudaMemcpyAsync(h->glob, h->glob_host.data(), sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice, h->st));
+    return FM_OK;
+}
+
+extern "C" int fm_upload_state(fm_handle *h, int32_t n, const double *r, const double *v, const double *a,
+                               const int32_t *glob_no)
+{
+    FM_TRY(begin_state(h, n));
+    if (!r || !v) return fail(FM_ERR_ARG, "r and v are required");
+    const size_t bytes = sizeof(double) * 3 * (size_t)n;
+    double *dr = h->stage3, *dv = h->stage3 + 3 * (size_t)n, *da = h->stage3 + 6 * (size_t)n;
+    FM_CUDA(cudaMemcpyAsync(dr, r, bytes, cudaMemcpyHostToDevice, h->st));
+    FM_CUDA(cudaMemcpyAsync(dv, v, bytes, cudaMemcpyHostToDevice, h->st));
+    if (a) FM_CUDA(cudaMemcpyAsync(da, a, bytes, cudaMemcpyHostToDevice, h->st));
+    fm::launch_scatter_state(h->d, dr, dv, a ? da : nullptr, h->st);
+    FM_TRY(set_glob(h, glob_no));
+    FM_CUDA(cudaGetLastError());
+    FM_CUDA(cudaStreamSynchronize(h->st));
+    h->stage = 1;
+    return FM_OK;
+}
+
+extern "C" int fm_upload_state_device(fm_handle *h, int32_t n, const double *d_r, const double *d_v)
+{
+    FM_TRY(begin_state(h, n));
+    if (!d_r || !d_v) return fail(FM_ERR_ARG, "r and v are required");
+    fm::launch_scatter_state(h->d, d_r, d_v, nullptr, h->st);
+    FM_TRY(set_glob(h, nullptr));
+    FM_CUDA(cudaGetLastError());
+    h->stage = 1;
+    return FM_OK;
+}
+
+extern "C" int fm_download_state(fm_handle *h, double *r, double *v, double *a, int32_t *glob_no)
+{
+    if (!h) return fail(FM_ERR_ARG, "null handle");
+    if (h->stage < 1) return fail(FM_ERR_STATE, "no state uploaded");
+    const size_t n = (size_t)h->d.n;
+    const size_t bytes = sizeof(double) * 3 * n;
+    double *dr = h->stage3, *dv = h->stage3 + 3 * n, *da = h->stage3 + 6 * n;
+    fm::launch_gather_state(h->d, r ? dr : nullptr, v ? dv : nullptr, a ? da : nullptr, nullptr, nullptr, nullptr,
+                            h->st);
+    if (r) FM_CUDA(cudaMemcpyAsync(r, dr, bytes, cudaMemcpyDeviceToHost, h->st));
+    if (v) FM_CUDA(cudaMemcpyAsync(v, dv, bytes, cudaMemcpyDeviceToHost, h->st));
+    if (a) FM_CUDA(cudaMemcpyAsync(a, da, bytes, cudaMemcpyDeviceToHost, h->st));
+    FM_CUDA(cudaGetLastError());
+    FM_CUDA(cudaStreamSynchronize(h->st));
+    if (glob_no) std::memcpy(glob_no, h->glob_host.data(), sizeof(int32_t) * n);
+    return FM_OK;
+}
+
+extern "C" int fm_download_state_device(fm_handle *h, double *d_r, double *d_v, double *d_a)
+{
+    if (!h) return fail(FM_ERR_ARG, "null handle");
+    if (h->stage < 1) return fail(FM_ERR_STATE, "no state uploaded");
+    fm::launch_gather_state(h->d, d_r, d_v, d_a, nullptr, nullptr, nullptr, h->st);
+    FM_CUDA(cudaGetLastError());
+    return FM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// device status
+// ---------------------------------------------------------------------------
+
+static int read_scalars(fm_handle *h, fm::FmScalars *s)
+{
+    FM_CUDA(cudaMemcpyAsync(s, h->d.sc, sizeof(*s), cudaMemcpyDeviceToHost, h->st));
+    FM_CUDA(cudaStreamSynchronize(h->st));
+    return FM_OK;
+}
+
+static int status_error(fm_handle *h, const fm::FmScalars &s)
+{
+    char buf[256];
+    if (s.status & fm::ST_ESCAPE) {
+        std::snprintf(buf, sizeof buf, "molecule escaped the cell grid at iteration %d", s.fail_iter);
+        h->stage = 3;
+        return fail(FM_ERR_ESCAPE, buf);
+    }
+    if (s.status & fm::ST_PE) {
+        std::snprintf(buf, sizeof buf, "max(potenergymol) > 10000 at iteration %d", s.fail_iter);
+        h->stage = 3;
+        return fail(FM_ERR_PE, buf);
+    }
+    if (s.status & fm::ST_BOND) {
+        std::snprintf(buf, sizeof buf, "polymer bond beyond R_0 at iteration %d", s.fail_iter);
+        h->stage = 3;
+        return fail(FM_ERR_BOND, buf);
+    }
+    if (s.status & fm::ST_NLIST) {
+        std::snprintf(buf, sizeof buf, "neighbour list overflow at iteration %d (%d > %d)", s.fail_iter, s.max_nbr,
+                      h->d.maxn);
+        h->stage = 3;
+        return fail(FM_ERR_NLIST, buf);
+    }
+    return FM_OK;
+}
+
+// Grows the neighbour list to fit the largest list seen, clears the overflow
+// bit and rebuilds the list from the (frozen) current cells.
+static int grow_nlist(fm_handle *h, const fm::FmScalars &s, int iter)
+{
+    int want = round_up((int)std::ceil(1.2 * s.max_nbr) + 8, 8);
+    if ((size_t)want * (size_t)h->d.n > ((size_t)1 << 34)) return status_error(h, s);
+    FM_TRY(alloc_nlist(h, want));
+    fm::FmScalars t = s;
+    t.status = 0u;
+    t.fail_iter = -1;
+    t.max_nbr = 0;
+    FM_CUDA(cudaMemcpyAsync(h->d.sc, &t, sizeof t, cudaMemcpyHostToDevice, h->st));
+    fm::launch_build_nlist(h->d, 0, iter, h->st);
+    FM_CUDA(cudaGetLastError());
+    return FM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// pieces of the step
+// ---------------------------------------------------------------------------
+
+static void queue_cells(fm_handle *h, int wrap, int gated)
+{
+    const FmDev &d = h->d;
+    fm::launch_wrap_bin(d, wrap, 1, gated, h->iter, h->st);
+    fm::launch_scan_cells(d, gated, h->st);
+    fm::launch_scatter(d, gated, h->st);
+    fm::launch_reorder(d, gated, h->tpos, h->tuidx, h->st);
+    h->launches += 6;
+}
+
+static cudaEvent_t next_event(fm_handle *h)
+{
+    if (h->ev_used == h->ev.size()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+        h->ev.push_back(e);
+    }
+    return h->ev[h->ev_used++];
+}
+
+static void queue_force(fm_handle *h, int record, int mode)
+{
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (h->timing) {
+        e0 = next_event(h);
+        e1 = next_event(h);
+        if (e0) cudaEventRecord(e0, h->st);
+    }
+    if (h->p.force_list == 0) {
+        FmDev d = h->d;
+        d.nblocks_force = fm::all_pairs_blocks(d.n);
+        fm::launch_all_pairs(d, record, mode, h->st);
+    } else {
+        fm::launch_force(h->d, record, mode, h->tpm, h->st);
+    }
+    if (e1) cudaEventRecord(e1, h->st);
+    h->launches += 1;
+}
+
+static void queue_record(fm_handle *h, int iter, double simtime)
+{
+    FmDev d = h->d;
+    d.nblocks_force = h->p.force_list == 0 ? fm::all_pairs_blocks(d.n) : fm::force_blocks(d.n, h->tpm);
+    fm::launch_record(d, iter, simtime, h->st);
+    h->launches += 1;
+}
+
+extern "C" int fm_setup(fm_handle *h)
+{
+    if (!h) return fail(FM_ERR_ARG, "null handle");
+    if (h->stage < 1) return fail(FM_ERR_STATE, "fm_setup before fm_upload_state");
+    if (h->p.force_list != 0) {
+        queue_cells(h, 0, 0);
+        fm::launch_build_nlist(h->d, 0, h->iter, h->st);
+    }
+    const int record = (h->iter % h->p.tplot) == 0;
+    queue_force(h, record, 0);
+    if (record) queue_record(h, h->iter, h->simtime);
+    FM_CUDA(cudaGetLastError());
+    fm::FmScalars s;
+    FM_TRY(read_scalars(h, &s));
+    if (s.status & fm::ST_NLIST && !(s.status & (fm::ST_FATAL & ~fm::ST_NLIST))) {
+        FM_TRY(grow_nlist(h, s, h->iter));
+        queue_force(h, record, 0);
+        if (record) queue_record(h, h->iter, h->simtime);
+        FM_TRY(read_scalars(h, &s));
+    }
+    FM_TRY(status_error(h, s));
+    h->has_pe = record;
+    h->cells_valid = h->list_valid = h->p.force_list != 0;
+    h->stage = 2;
+    return FM_OK;
+}
+
+// Queues iterations [first, first + nsteps) of md_advance_vv, starting at
+// `phase` 0 (move(1)) or 1 (forces) of the first iteration.
+static int queue_steps(fm_handle *h, int first, int nsteps, int phase, const std::vector<double> &simtime_after,
+                       int range_offset)
+{
+    const fm_params &p = h->p;
+    bool fused_move1 = false;  // the previous force kernel already did move(1)
+    for (int s = 0; s < nsteps; s++) {
+        const int it = first + s;
+        h->iter = it;
+        if (!(s == 0 && phase == 1)) {
+            if (!fused_move1) { fm::launch_move1(h->d, h->st); h->launches += 1; }
+            fm::launch_decide(h->d, it, fused_move1 ? 1 : 0, p.rebuild_criteria, p.fixed_rebuild,
+                              h->half_min_delta, h->st);
+            h->launches += 1;
+            if (p.force_list != 0) {
+                queue_cells(h, 1, 1);
+                fm::launch_build_nlist(h->d, 1, it, h->st);
+                h->launches += 1;
+            } else {
+                fm::launch_wrap_bin(h->d, 1, 0, 1, it, h->st);
+                h->launches += 1;
+            }
+        }
+        const int record = (it % p.tplot) == 0;
+        const int last = s == nsteps - 1;
+        queue_force(h, record, last ? 1 : 2);
+        fused_move1 = !last;
+        h->simtime = simtime_after[(size_t)(range_offset + s)];
+        if (record) queue_record(h, it, h->simtime);
+    }
+    FM_CUDA(cudaGetLastError());
+    return FM_OK;
+}
+
+// Waits for the queued range; resumes it once per overflow after growing the
+// neighbour list.
+static int finish_range(fm_handle *h)
+{
+    for (int attempt = 0; attempt < 8; attempt++) {
+        fm::FmScalars s;
+        FM_TRY(read_scalars(h, &s));
+        if (!(s.status & fm::ST_FATAL)) {
+            h->q.active = false;
+            return FM_OK;
+        }
+        if (!h->q.active || (s.status & (fm::ST_FATAL & ~fm::ST_NLIST))) {
+            h->q.active = false;
+            return status_error(h, s);
+        }
+        const int f = s.fail_iter;
+        const int off = f - h->q.first_iter;
+        if (off < 0 || off >= h->q.nsteps) return status_error(h, s);
+        FM_TRY(grow_nlist(h, s, f));
+        FM_TRY(queue_steps(h, f, h->q.nsteps - off, 1, h->q.simtime_after, off));
+    }
+    return fail(FM_ERR_NLIST, "neighbour list kept overflowing");
+}
+
+extern "C" int fm_step(fm_handle *h, int32_t nsteps, int32_t blocking)
+{
+    if (!h) return fail(FM_ERR_ARG, "null handle");
+    if (h->stage != 2) return fail(FM_ERR_STATE, "fm_step needs fm_setup (or a failed state was not re-uploaded)");
+    if (h->p.force_list != 0 && !(h->cells_valid && h->list_valid))
+        return fail(FM_ERR_STATE, "fm_step needs current cell and neighbour lists (call fm_setup)");
+    if (nsteps < 0) return fail(FM_ERR_ARG, "nsteps < 0");
+    if (nsteps == 0) return FM_OK;
+    if (h->q.active) FM_TRY(finish_range(h));
+    const int first = h->iter + 1;
+    h->q.active = true;
+    h->q.first_iter = first;
+    h->q.nsteps = nsteps;
+    h->q.simtime_after.resize((size_t)nsteps);
+    double t = h->simtime;
+    for (int s = 0; s < nsteps; s++) {
+        t = t + h->p.delta_t;  // simtime = simtime + delta_t (simulation_move_particles_vv.f90:191)
+        h->q.simtime_after[(size_t)s] = t;
+    }
+    FM_TRY(queue_steps(h, first, nsteps, 0, h->q.simtime_after, 0));
+    for (int s = 0; s < nsteps; s++)
+        if (((first + s) % h->p.tplot) == 0) h->has_pe = true;
+    if (blocking) return finish_range(h);
+    return FM_OK;
+}
+
+extern "C" int fm_sync(fm_handle *h)
+{
+    if (!h) return fail(FM_ERR_ARG, "null handle");
+    if (h->q.active) return finish_range(h);
+    fm::FmScalars s;
+    FM_TRY(read_scalars(h, &s));
+    return status_error(h, s);
+}
+
+// ---------------------------------------------------------------------------
+// subroutine-by-subroutine mirrors
+// ---------------------------------------------------------------------------
+
+static int ready(fm_handle *h, int min_stage)
+{
+    if (!h) return fail(FM_ERR_ARG, "null handle");
+    if (h->stage == 3) return fail(FM_ERR_STATE, "state is broken; re-upload it");
+    if (h->stage < min_stage) return fail(FM_ERR_STATE, "call order: upload, setup, then step");
+    if (h->q.active) FM_TRY(finish_range(h));
+    return FM_OK;
+}
+
+extern "C" int fm_move_vv(fm_handle *h, int32_t pass_num)
+{
+    FM_TRY(ready(h, 1));
+    if (pass_num == 1) {
+        fm::launch_move1(h->d, h->st);
+    } else if (pass_num == 2) {
+        fm::launch_move2(h->d, h->st);
+        h->simtime = h->simtime + h->p.delta_t;
+    } else {
+        return fail(FM_ERR_ARG, "pass_num must be 1 or 2");
+    }
+    FM_CUDA(cudaGetLastError());
+    return FM_OK;
+}
+
+extern "C" int fm_update_borders(fm_handle *h, int32_t rebuild)
+{
+    (void)rebuild;
+    return ready(h, 1);
+}
+
+extern "C" int fm_linklist_deallocateall(fm_handle *h) { return ready(h, 1); }
+
+extern "C" int fm_check_rebuild(fm_handle *h, int32_t *rebuild)
+{
+    FM_TRY(ready(h, 1));
+    if (!rebuild) return fail(FM_ERR_ARG, "null output");
+    FM_CUDA(cudaMemsetAsync(&h->d.sc->vmax2, 0, sizeof(unsigned long long), h->st));
+    fm::launch_vmax(h->d, h->st);
+    fm::launch_decide(h->d, h->iter, 0, h->p.rebuild_criteria, h->p.fixed_rebuild, h->half_min_delta, h->st);
+    FM_CUDA(cudaGetLastError());
+    fm::FmScalars s;
+    FM_TRY(read_scalars(h, &s));
+    FM_TRY(status_error(h, s));
+    *rebuild = s.rebuild;
+    return FM_OK;
+}
+
+extern "C" int fm_sendmols(fm_handle *h)
+{
+    FM_TRY(ready(h, 1));
+    fm::launch_wrap_bin(h->d, 1, 0, 0, h->iter, h->st);
+    FM_CUDA(cudaGetLastError());
+    return FM_OK;
+}
+
+extern "C" int fm_assign_to_cell(fm_handle *h)
+{
+    FM_TRY(ready(h, 1));
+    if (h->p.force_list == 0) return FM_OK;
+    queue_cells(h, 0, 0);
+    FM_CUDA(cudaGetLastError());
+    fm::FmScalars s;
+    FM_TRY(read_scalars(h, &s));
+    FM_TRY(status_error(h, s));
+    h->cells_valid = true;
+    h->list_valid = false;
+    return FM_OK;
+}
+
+extern "C" int fm_assign_to_neighbourlist(fm_handle *h)
+{
+    FM_TRY(ready(h, 1));
+    if (h->p.force_list == 0) return FM_OK;
+    if (!h->cells_valid) return fail(FM_ERR_STATE, "assign_to_neighbourlist needs assign_to_cell first");
+    fm::launch_build_nlist(h->d, 0, h->iter, h->st);
+    FM_CUDA(cudaGetLastError());
+    fm::FmScalars s;
+    FM_TRY(read_scalars(h, &s));
+    if ((s.status & fm::ST_NLIST) && !(s.status & (fm::ST_FATAL & ~fm::ST_NLIST))) {
+        FM_TRY(grow_nlist(h, s, h->iter));
+        FM_TRY(read_scalars(h, &s));
+    }
+    FM_TRY(status_error(h, s));
+    h->list_valid = true;
+    return FM_OK;
+}
+
+extern "C" int fm_compute_forces(fm_handle *h)
+{
+    FM_TRY(ready(h, 1));
+    if (h->p.force_list != 0 && !(h->cells_valid && h->list_valid))
+        return fail(FM_ERR_STATE, "compute_forces needs assign_to_cell and assign_to_neighbourlist first");
+    const int record = (h->iter % h->p.tplot) == 0;
+    queue_force(h, record, 0);
+    FM_CUDA(cudaGetLastError());
+    if (record) h->has_pe = true;
+    if (h->stage < 2) h->stage = 2;
+    return FM_OK;
+}
+
+extern "C" int fm_evaluate_macroscopic_properties(fm_handle *h, fm_macro *out)
+{
+    FM_TRY(ready(h, 2));
+    if (!out) return fail(FM_ERR_ARG, "null output");
+    FmDev d = h->d;
+    d.nblocks_force = fm::macro_blocks(d.n);
+    fm::launch_macro_partials(d, h->st);
+    fm::launch_record(d, h->iter, h->simtime, h->st);
+    FM_CUDA(cudaGetLastError());
+    fm::FmScalars s;
+    FM_TRY(read_scalars(h, &s));
+    FM_TRY(status_error(h, s));
+    int slot = (s.nrec_pending - 1 + d.rec_cap) % d.rec_cap;
+    static_assert(sizeof(fm::FmRecord) == sizeof(fm_macro), "record layout");
+    FM_CUDA(cudaMemcpyAsync(out, d.rec + slot, sizeof(fm_macro), cudaMemcpyDeviceToHost, h->st));
+    FM_CUDA(cudaStreamSynchronize(h->st));
+    return FM_OK;
+}
+
+extern "C" int fm_set_iter(fm_handle *h, int32_t iter)
+{
+    FM_TRY(ready(h, 0));
+    h->iter = iter;
+    return FM_OK;
+}
+
+extern "C" int fm_get_iter(fm_handle *h, int32_t *iter)
+{
+    if (!h || !iter) return fail(FM_ERR_ARG, "null argument");
+    *iter = h->iter;
+    return FM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// results
+// ---------------------------------------------------------------------------
+
+extern "C" int fm_get_records(fm_handle *h, fm_macro *out, int32_t cap, int32_t *n)
+{
+    if (!h || !n) return fail(FM_ERR_ARG, "null argument");
+    if (h->q.active) FM_TRY(finish_range(h));
+    fm::FmScalars s;
+    FM_TRY(read_scalars(h, &s));
+    const int rc_cap = h->d.rec_cap;
+    int pending = s.nrec_pending;
+    int avail = std::min(pending, rc_cap);
+    int take = std::min(avail, cap > 0 ? cap : 0);
+    std::vector<fm::FmRecord> rows((size_t)rc_cap);
+    if (take > 0) {
+        FM_CUDA(cudaMemcpyAsync(rows.data(), h->d.rec, sizeof(fm::FmRecord) * (size_t)rc_cap, cudaMemcpyDeviceToHost,
+                                h->st));
+        FM_CUDA(cudaStreamSynchronize(h->st));
+        int oldest = pending - avail;
+        for (int k = 0; k < take; k++) std::memcpy(&out[k], &rows[(size_t)((oldest + k) % rc_cap)], sizeof(fm_macro));
+    }
+    int zero = 0;
+    FM_CUDA(cudaMemcpyAsync(&h->d.sc->nrec_pending, &zero, sizeof zero, cudaMemcpyHostToDevice, h->st));
+    FM_CUDA(cudaStreamSynchronize(h->st));
+    *n = take;
+    return FM_OK;
+}
+
+extern "C" int fm_get_per_molecule(fm_handle *h, double *pe, double *vir)
+{
+    FM_TRY(ready(h, 2));
+    const size_t n = (size_t)h->d.n;
+    double *dpe = h->stage3, *dvir = h->stage3 + n;
+    fm::launch_gather_state(h->d, nullptr, nullptr, nullptr, nullptr, dpe, dvir, h->st);
+    if (pe) FM_CUDA(cudaMemcpyAsync(pe, dpe, sizeof(double) * n, cudaMemcpyDeviceToHost, h->st));
+    if (vir) FM_CUDA(cudaMemcpyAsync(vir, dvir, sizeof(double) * n, cudaMemcpyDeviceToHost, h->st));
+    FM_CUDA(cudaStreamSynchronize(h->st));
+    return FM_OK;
+}
+
+extern "C" int fm_get_pair_list(fm_handle *h, int32_t *owner, int32_t *partner, int8_t *code, int64_t cap,
+                                int64_t *n_out)
+{
+    FM_TRY(ready(h, 1));
+    if (!n_out) return fail(FM_ERR_ARG, "null output");
+    if (h->p.force_list == 0) { *n_out = 0; return FM_OK; }
+    const size_t n = (size_t)h->d.n;
+    std::vector<int32_t> nnbr(n), slot(n), nbr(n * (size_t)h->d.maxn);
+    FM_CUDA(cudaMemcpyAsync(nnbr.data(), h->d.nnbr, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, h->st));
+    FM_CUDA(cudaMemcpyAsync(slot.data(), h->d.slot_of, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, h->st));
+    FM_CUDA(cudaMemcpyAsync(nbr.data(), h->d.nbr, sizeof(int32_t) * nbr.size(), cudaMemcpyDeviceToHost, h->st));
+    FM_CUDA(cudaStreamSynchronize(h->st));
+    int64_t k = 0;
+    for (size_t i = 0; i < n; i++) {
+        for (int q = 0; q < nnbr[i]; q++) {
+            int32_t e = nbr[i * (size_t)h->d.maxn + (size_t)q];
+            int32_t j = e & fm::NB_INDEX_MASK;
+            int c6 = (int)((uint32_t)e >> fm::NB_SHIFT_BITS);
+            int sx = (c6 & 3) - 1, sy = ((c6 >> 2) & 3) - 1, sz = ((c6 >> 4) & 3) - 1;
+            if (k < cap) {
+                if (owner) owner[k] = h->glob_host[(size_t)slot[i]];
+                if (partner) partner[k] = h->glob_host[(size_t)slot[(size_t)j]];
+                if (code) code[k] = (int8_t)((sx + 1) + 3 * (sy + 1) + 9 * (sz + 1));
+            }
+            k++;
+        }
+    }
+    *n_out = k;
+    return FM_OK;
+}
+
+extern "C" int fm_pair_digest(fm_handle *h, uint64_t *digest, int64_t *npairs)
+{
+    FM_TRY(ready(h, 1));
+    if (!digest || !npairs) return fail(FM_ERR_ARG, "null output");
+    if (h->p.force_list == 0) { *digest = 0; *npairs = 0; return FM_OK; }
+    FM_CUDA(cudaMemsetAsync(&h->d.sc->digest, 0, sizeof(uint64_t) + sizeof(int64_t), h->st));
+    fm::launch_pair_digest(h->d, h->glob, h->st);
+    FM_CUDA(cudaGetLastError());
+    fm::FmScalars s;
+    FM_TRY(read_scalars(h, &s));
+    *digest = s.digest;
+    *npairs = s.digest_n;
+    return FM_OK;
+}
+
+extern "C" int fm_get_counters(fm_handle *h, int64_t *rebuilds, int32_t *cap, int32_t *max_nbr)
+{
+    FM_TRY(ready(h, 0));
+    fm::FmScalars s;
+    FM_TRY(read_scalars(h, &s));
+    if (rebuilds) *rebuilds = s.rebuilds;
+    if (cap) *cap = h->d.maxn;
+    if (max_nbr) *max_nbr = s.max_nbr;
+    return FM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// instrumentation
+// ---------------------------------------------------------------------------
+
+extern "C" int fm_force_kernel_timing(fm_handle *h, int32_t enable)
+{
+    if (!h) return fail(FM_ERR_ARG, "null handle");
+    h->timing = enable != 0;
+    h->ev_used = 0;
+    return FM_OK;
+}
+
+extern "C" int fm_get_force_kernel_time(fm_handle *h, double *ms, int64_t *launches)
+{
+    if (!h || !ms || !launches) return fail(FM_ERR_ARG, "null argument");
+    FM_CUDA(cudaStreamSynchronize(h->st));
+    double tot = 0.0;
+    for (size_t k = 0; k + 1 < h->ev_used; k += 2) {
+        float t = 0.f;
+        FM_CUDA(cudaEventElapsedTime(&t, h->ev[k], h->ev[k + 1]));
+        tot += (double)t;
+    }
+    *ms = tot;
+    *launches = (int64_t)(h->ev_used / 2);
+    h->ev_used = 0;
+    return FM_OK;
+}
+
+extern "C" int fm_get_launch_count(fm_handle *h, int64_t *launches)
+{
+    if (!h || !launches) return fail(FM_ERR_ARG, "null argument");
+    *launches = h->launches;
+    return FM_OK;
+}

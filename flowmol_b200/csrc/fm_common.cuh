@@ -1,0 +1,125 @@
+// fm_common.cuh -- device data layout and kernel launch interface of the
+// B200 MD hot path (single system).  Host code (fm_api.cu) owns an FmSystem;
+// kernels (fm_kernels.cu) receive an FmDev by value.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace fm {
+
+// ---- status word bits (FmScalars::status) -------------------------------
+// A set FATAL bit freezes the step loop: every later kernel returns at entry,
+// so the device state stays exactly as it was when the fault was detected.
+enum : uint32_t {
+    ST_ESCAPE = 1u << 0,    // molecule binned outside the extended cell grid
+    ST_NLIST = 1u << 1,     // a neighbour list needed more than maxn slots
+    ST_PE = 1u << 2,        // per-molecule PE above 10000 on a record step
+    ST_BOND = 1u << 3,      // FENE bond at or beyond R_0
+    ST_FATAL = ST_ESCAPE | ST_NLIST | ST_PE | ST_BOND,
+};
+
+// Device-resident scalars of the step loop (one per system).
+struct FmScalars {
+    double rmax;              // simulation_checkrebuild.f90 `rmax` (save variable)
+    unsigned long long vmax2; // bits of max |v|^2 (non-negative doubles order like u64)
+    int32_t rebuild;          // decision for the current iteration
+    int32_t pset;             // which position buffer is current
+    uint32_t status;          // ST_* bits
+    int32_t fail_iter;        // iteration at which a FATAL bit was first set
+    int32_t max_nbr;          // largest neighbour count seen at the last build
+    int32_t escape_slot;      // a molecule that escaped (internal slot)
+    int64_t rebuilds;         // rebuilds performed
+    uint64_t digest;          // pair-set digest (test hook)
+    int64_t digest_n;
+    int32_t nrec_pending;     // record rows written since the host last read
+    int32_t pad_;
+};
+
+// Partial sums of one record step, one row per force-kernel block.
+enum { RS_PE = 0, RS_VIR, RS_MV2, RS_VSUM, RS_PEMAX, RS_N };
+
+// Record row layout in device memory (matches fm_macro on the host).
+struct FmRecord {
+    int32_t iter;
+    int32_t pad_;
+    double simtime, vsum, mv2sum, temperature, kinenergy, potenergy, totenergy, pressure, virial;
+};
+
+// Everything a kernel needs, passed by value.
+struct FmDev {
+    // geometry and constants
+    int n;                 // real molecules
+    double L[3], hd[3], cs[3];
+    int nc[3];             // interior cells per axis
+    int ne[3];             // extended cells per axis (nc + 2)
+    int ncell;             // ne[0]*ne[1]*ne[2]
+    double rc2, rn2, dt, potshift, half_dt, half_dt2;
+    double density, pot_slrc, p_slrc;
+    int tplot;
+    int maxn;              // neighbour slots per molecule
+    int precision;
+    // positions (double-buffered: pos[sc->pset] is current)
+    double4 *pos0, *pos1;
+    // velocities, accelerations (SoA)
+    double *vx, *vy, *vz, *ax, *ay, *az;
+    int32_t *slot_of;      // internal slot -> upload index (the molecule's identity)
+    // reorder scratch
+    double *tvx, *tvy, *tvz, *tax, *tay, *taz;
+    // cells (extended grid, x fastest)
+    int32_t *cell_of;      // per molecule (old order) cell id
+    int32_t *cell_count;   // ncell
+    int32_t *cell_start;   // ncell + 1
+    int32_t *perm;         // new slot -> old slot
+    // neighbour list: nbr[i*maxn + k] = j | (sx+1)<<26 | (sy+1)<<28 | (sz+1)<<30
+    int32_t *nbr;
+    int32_t *nnbr;
+    // per-molecule PE / virial (record steps)
+    double *pe, *vir;
+    // record partials [nblocks][RS_N] and finished rows
+    double *partial;
+    int nblocks_force;
+    FmRecord *rec;
+    int rec_cap;
+    FmScalars *sc;
+};
+
+__host__ __device__ inline double4 *cur_pos(const FmDev &d, int pset) { return pset ? d.pos1 : d.pos0; }
+
+// Neighbour entry encoding.
+constexpr int NB_SHIFT_BITS = 26;
+constexpr int32_t NB_INDEX_MASK = (1 << NB_SHIFT_BITS) - 1;
+constexpr int MAX_MOLECULES = NB_INDEX_MASK;
+
+// ---- kernel launchers (fm_kernels.cu) -----------------------------------
+// All launchers enqueue on `st` and never synchronise.
+void launch_reset_scalars(const FmDev &d, cudaStream_t st);
+void launch_move1(const FmDev &d, cudaStream_t st);          // pass 1 in place + vmax2
+void launch_move2(const FmDev &d, cudaStream_t st);          // pass 2 in place
+void launch_vmax(const FmDev &d, cudaStream_t st);           // vmax2 of current v
+void launch_decide(const FmDev &d, int iter, int flip, int rebuild_criteria, int fixed_rebuild,
+                   double half_min_delta, cudaStream_t st);
+// Rebuild pipeline; gated = 1 makes each kernel a no-op unless sc->rebuild.
+void launch_wrap_bin(const FmDev &d, int wrap, int bin, int gated, int iter, cudaStream_t st);
+void launch_scan_cells(const FmDev &d, int gated, cudaStream_t st);
+void launch_scatter(const FmDev &d, int gated, cudaStream_t st);
+void launch_reorder(const FmDev &d, int gated, double4 *tpos, int32_t *tuidx, cudaStream_t st);
+void launch_build_nlist(const FmDev &d, int gated, int iter, cudaStream_t st);
+// Forces: mode 0 forces only, 1 forces + move(2), 2 forces + move(2) + next move(1).
+void launch_force(const FmDev &d, int record, int mode, int tpm, cudaStream_t st);
+void launch_record(const FmDev &d, int iter, double simtime, cudaStream_t st);
+void launch_all_pairs(const FmDev &d, int record, int mode, cudaStream_t st);
+// Record partials straight from the per-molecule arrays (PE, virial) and the
+// current velocities, for the subroutine-by-subroutine path.
+void launch_macro_partials(const FmDev &d, cudaStream_t st);
+int macro_blocks(int n);
+void launch_pair_digest(const FmDev &d, const int32_t *glob_of_upload, cudaStream_t st);
+int force_blocks(int n, int tpm);
+int all_pairs_blocks(int n);
+// Layout conversion between the reference's (3,n) column-major arrays and
+// the device layout; `order` maps upload index -> slot.
+void launch_scatter_state(const FmDev &d, const double *r3, const double *v3, const double *a3,
+                          cudaStream_t st);
+void launch_gather_state(const FmDev &d, double *r3, double *v3, double *a3, int32_t *gid,
+                         double *pe, double *vir, cudaStream_t st);
+
+}  // namespace fm

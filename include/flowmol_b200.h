@@ -1,0 +1,227 @@
+/*
+ * flowmol_b200.h -- C ABI of the B200 (sm_100a) per-timestep MD hot path.
+ *
+ * Every entry point replaces one Fortran subroutine (or the fused loop) of
+ * Flowmol's velocity-Verlet step (md.f90:143-163, md_advance_vv).  The
+ * reference subroutines take no arguments and talk through module globals;
+ * here the module state lives in an opaque handle whose arrays sit in device
+ * memory.  All functions return 0 on success or one of the FM_ERR_* codes; a
+ * message is available from fm_last_error().  Nothing aborts the host process
+ * (the reference's error_abort -> MPI_Abort, messenger.MPI.f90:3376-3410,
+ * becomes a return code).  Plain C types only: callable from Fortran through
+ * iso_c_binding, from Python through ctypes, from C/C++ directly.
+ *
+ * Threading: a handle is used by one host thread at a time; all its device
+ * work is ordered on one CUDA stream (fm_set_stream).  Different handles may
+ * be driven from different threads.
+ */
+#ifndef FLOWMOL_B200_H
+#define FLOWMOL_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define FM_API __attribute__((visibility("default")))
+#else
+#define FM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define FM_OK 0
+#define FM_ERR_ARG 1            /* invalid argument */
+#define FM_ERR_CUDA 2           /* CUDA runtime failure (message has the CUDA error) */
+#define FM_ERR_FEWCELLS 3       /* fewer than 3 cells per axis (setup_set_parameters.f90:1891-1896) */
+#define FM_ERR_ESCAPE 4         /* molecule outside the cell grid (linklist.f90:2664-2673) */
+#define FM_ERR_NLIST 5          /* neighbour list needs more capacity than the cap allows */
+#define FM_ERR_PE 6             /* max per-molecule PE > 10000 (simulation_record.f90:1271-1283) */
+#define FM_ERR_STATE 7          /* call made in the wrong order (e.g. step before setup) */
+#define FM_ERR_BOND 8           /* polymer bond stretched beyond R_0 (setup_set_parameters.f90:352) */
+#define FM_ERR_NODEVICE 9       /* no CUDA device / library not built for this GPU */
+#define FM_ERR_IO 10            /* restart or input file could not be read or written */
+
+/* ---- enumerations mirroring the reference's input flags ------------- */
+#define FM_FORCE_LIST_ALLPAIRS 0   /* FORCE_LIST 0: LJ all pairs, minimum image */
+#define FM_FORCE_LIST_FULL 2       /* FORCE_LIST 2: full neighbour list */
+#define FM_FORCE_LIST_HALF 3       /* FORCE_LIST 3: half (Newton-3) list, the reference default */
+#define FM_PRECISION_FP64 0        /* plain FP64 drop-in */
+#define FM_PRECISION_FP32 1        /* FP32 pair forces, FP64 r/v/a, FP64 compensated sums */
+
+/*
+ * Parameters of one simulation (the hot-path subset of the reference's
+ * input keywords, setup_read_input.f90).  Derived quantities -- halfdomain,
+ * rneighbr2, ncells, cellsidelength, potshift, long-range corrections -- are
+ * computed by the library with the reference's formulas
+ * (setup_set_parameters.f90:1099-1245, 1848-1903).
+ */
+typedef struct fm_params {
+    int32_t np;                   /* molecules (globalnp on one rank) */
+    double domain[3];             /* box lengths (globaldomain) */
+    double density;               /* DENSITY: used in pressure and sLRC */
+    double rcutoff;               /* RCUTOFF */
+    double delta_rneighbr[3];     /* DELTA_RNEIGHBR (skin per axis) */
+    double delta_t;               /* DELTA_T */
+    int32_t tplot;                /* TPLOT: record / forced-rebuild period */
+    int32_t initialstep;          /* iteration number of the uploaded state */
+    double simtime;               /* simulated time of the uploaded state */
+    int32_t force_list;           /* FORCE_LIST: 0, 2 or 3 */
+    int32_t potential_flag;       /* POTENTIAL_FLAG: 0 LJ, 1 FENE polymer */
+    int32_t rebuild_criteria;     /* REBUILD_CRITERIA: 0 vmax (Rapaport), 1 fixed */
+    int32_t fixed_rebuild;        /* FIXED_REBUILD period when rebuild_criteria = 1 */
+    int32_t sLRC_flag;            /* SLRC_FLAG: long-range corrections on PE and P */
+    int32_t precision;            /* FM_PRECISION_* */
+    double k_c, R_0;              /* FENE_INFO spring constant and maximum extension */
+    int32_t nlist_capacity;       /* neighbours per molecule reserved; 0 = automatic */
+    int32_t threads_per_molecule; /* force kernel lanes per molecule; 0 = autotuned */
+} fm_params;
+
+/* Macroscopic properties of one record step, the columns of
+ * results/macroscopic_properties (parallel_io.MPI2.f90:4589-4646) plus the
+ * virial sum (simulation_record.f90:1205-1314). */
+typedef struct fm_macro {
+    int32_t iter;
+    int32_t pad_;
+    double simtime;
+    double vsum;        /* sum of m v over all components */
+    double mv2sum;      /* sum of m v^2 */
+    double temperature; /* mv2sum / (3 N) */
+    double kinenergy;   /* 0.5 mv2sum / N */
+    double potenergy;   /* 0.5 sum PE_i / N + sLRC */
+    double totenergy;
+    double pressure;    /* rho/(3N) (mv2sum + virial/2) + P_sLRC */
+    double virial;      /* sum of per-molecule virials */
+} fm_macro;
+
+typedef struct fm_handle fm_handle;
+
+/* Geometry the reference derives from the parameters (no device needed):
+ * ncells = floor(domain/(rcutoff+delta)), cellsidelength = domain/ncells,
+ * rneighbr2 = (rcutoff + mean(delta))^2 with the FENE R_0 override, and
+ * potshift = 4(rc^-12 - rc^-6).  Replaces set_parameters_cells
+ * (setup_set_parameters.f90:1848-1903) and the potshift line (:1222).
+ * Returns FM_ERR_FEWCELLS where the reference aborts. */
+FM_API int fm_derive_geometry(const fm_params *p, int32_t ncells[3], double cellsidelength[3],
+                       double *rneighbr2, double *rcutoff2, double *potshift);
+
+/* Domain of an FCC start of nunits unit cells at a density
+ * (set_parameters_global_domain, setup_set_parameters.f90:1545-1580). */
+FM_API int fm_global_domain(const int32_t nunits[3], double density, double domain[3]);
+
+/* ---- lifetime ------------------------------------------------------- */
+/* Allocates device state for p->np molecules on the current CUDA device
+ * (set_parameters_allocate, setup_set_parameters.f90:1248-1376). */
+FM_API int fm_create(const fm_params *p, fm_handle **out);
+FM_API int fm_destroy(fm_handle *h);
+/* Orders all of the handle's device work on this cudaStream_t (NULL = the
+ * legacy default stream). */
+FM_API int fm_set_stream(fm_handle *h, void *cuda_stream);
+
+/* ---- state transfer ------------------------------------------------- */
+/* r, v (and optionally a) in the reference's column-major (3, n) layout,
+ * i.e. r[3*i + k] = r(k+1, i+1).  glob_no (1-based) may be NULL: molecules
+ * are then numbered 1..n in upload order.  The device copies are private to
+ * the handle; host buffers are only read during the call. */
+FM_API int fm_upload_state(fm_handle *h, int32_t n, const double *r, const double *v, const double *a,
+                    const int32_t *glob_no);
+/* Writes r, v, a (each may be NULL) back in upload order -- molecule i of
+ * the upload is row i here whatever order the device keeps internally.
+ * Blocks until the stream has drained. */
+FM_API int fm_download_state(fm_handle *h, double *r, double *v, double *a, int32_t *glob_no);
+/* Device pointers variant for callers that keep the state on the GPU:
+ * d_r/d_v are (3, n) column-major FP64 device arrays, read or written on the
+ * handle's stream without host staging. */
+FM_API int fm_upload_state_device(fm_handle *h, int32_t n, const double *d_r, const double *d_v);
+FM_API int fm_download_state_device(fm_handle *h, double *d_r, double *d_v, double *d_a);
+
+/* ---- the drop-in subroutine mirrors (md.f90:143-163) ------------------ */
+/* Initial cell binning, halo images, neighbour list, forces and record of
+ * the uploaded state: assign_to_cell, messenger_updateborders(1),
+ * assign_to_neighbourlist (md.f90:60-64) then simulation_compute_forces +
+ * evaluate_macroscopic_properties (setup_initial_record.f90:88-89). */
+FM_API int fm_setup(fm_handle *h);
+/* simulation_move_particles_vv(pass_num), NVE (simulation_move_particles_vv.f90:64-69,132-135). */
+FM_API int fm_move_vv(fm_handle *h, int32_t pass_num);
+/* messenger_updateborders(rebuild) (messenger.MPI.f90:594-627).  Periodic
+ * images are generated on the fly from their source molecule inside the
+ * list-build and force kernels (x_img = x_src +/- domain, the same FP64 add),
+ * so this call only validates the handle. */
+FM_API int fm_update_borders(fm_handle *h, int32_t rebuild);
+/* simulation_checkrebuild(rebuild) (simulation_checkrebuild.f90:17-148);
+ * writes the 0/1 decision (blocks on the stream). */
+FM_API int fm_check_rebuild(fm_handle *h, int32_t *rebuild);
+/* linklist_deallocateall (linklist.f90:2872-2964): lists are overwritten in
+ * place on the device, so this only validates the handle. */
+FM_API int fm_linklist_deallocateall(fm_handle *h);
+/* sendmols, single-rank form: periodic wrap r >= L/2 -> r-L, r < -L/2 -> r+L
+ * (messenger.serial.f90:961-1028; messenger.MPI.f90:1383-1424). */
+FM_API int fm_sendmols(fm_handle *h);
+/* assign_to_cell (linklist.f90:2645-2679) as a counting sort: histogram,
+ * exclusive scan, scatter.  Molecules are also re-ordered by cell on the
+ * device (invisible through fm_download_state). */
+FM_API int fm_assign_to_cell(fm_handle *h);
+/* assign_to_neighbourlist (linklist.f90:2710-2741) for FORCE_LIST 2/3: the
+ * pair set of assign_to_neighbourlist_halfint_opt (660-804) stored in both
+ * directions, built from shared-memory cell tiles. */
+FM_API int fm_assign_to_neighbourlist(fm_handle *h);
+/* simulation_compute_forces (simulation_compute_forces.f90:182-275): zeroes
+ * and recomputes a; per-molecule PE and virial when mod(iter,tplot) == 0. */
+FM_API int fm_compute_forces(fm_handle *h);
+/* evaluate_macroscopic_properties (simulation_record.f90:1205-1314) from the
+ * sums of the last force evaluation that recorded PE and virial. */
+FM_API int fm_evaluate_macroscopic_properties(fm_handle *h, fm_macro *out);
+/* Sets the iteration counter (the reference's module global iter). */
+FM_API int fm_set_iter(fm_handle *h, int32_t iter);
+FM_API int fm_get_iter(fm_handle *h, int32_t *iter);
+
+/* ---- the fused step loop -------------------------------------------- */
+/* Runs nsteps iterations of md_advance_vv (md.f90:143-163) on the device:
+ * move(1), rebuild check, [wrap, bin, list], forces, move(2), record.  The
+ * rebuild decision is taken on the device, so the host never waits inside
+ * the loop.  Returns after the work is queued unless blocking != 0; errors
+ * detected on the device (escape, list overflow that cannot be resized, PE
+ * blow-up) are reported by the next blocking call. */
+FM_API int fm_step(fm_handle *h, int32_t nsteps, int32_t blocking);
+/* Waits for queued work and returns the first device-side error, if any. */
+FM_API int fm_sync(fm_handle *h);
+
+/* ---- results -------------------------------------------------------- */
+/* Records (one per tplot step) produced since the previous call, oldest
+ * first.  *n receives how many were written (at most cap). */
+FM_API int fm_get_records(fm_handle *h, fm_macro *out, int32_t cap, int32_t *n);
+/* Per-molecule potenergymol and virialmol of the last recording force
+ * evaluation, in upload order. */
+FM_API int fm_get_per_molecule(fm_handle *h, double *potenergymol, double *virialmol);
+/* Neighbour pairs as (owner glob_no, partner glob_no, image code) triplets,
+ * image code = (sx+1) + 3(sy+1) + 9(sz+1) for the domain shift of the
+ * partner, 13 = no shift.  Both directions of every pair are listed.  *n is
+ * the total; at most cap triplets are written.  Test hook. */
+FM_API int fm_get_pair_list(fm_handle *h, int32_t *owner, int32_t *partner, int8_t *code, int64_t cap,
+                     int64_t *n);
+/* Order-independent 64-bit digest of the canonical pair set (a sum of
+ * mixed hashes of (min gid, max gid) for unshifted pairs and of
+ * (owner, partner, code) for image pairs); matches the oracle's digest of
+ * the reference half list. */
+FM_API int fm_pair_digest(fm_handle *h, uint64_t *digest, int64_t *npairs);
+/* Counters: rebuilds done, neighbour capacity in use, largest list seen. */
+FM_API int fm_get_counters(fm_handle *h, int64_t *rebuilds, int32_t *nlist_capacity, int32_t *max_neighbours);
+
+/* ---- instrumentation -------------------------------------------------- */
+/* When enabled, every force-kernel launch is bracketed by CUDA events on the
+ * handle's stream; fm_get_force_kernel_time returns the summed device time
+ * (ms) and the number of launches since it was last read. */
+FM_API int fm_force_kernel_timing(fm_handle *h, int32_t enable);
+FM_API int fm_get_force_kernel_time(fm_handle *h, double *ms, int64_t *launches);
+/* Kernels this handle has launched since creation. */
+FM_API int fm_get_launch_count(fm_handle *h, int64_t *launches);
+
+/* ---- errors --------------------------------------------------------- */
+/* Copies the message of the last failing call on this thread. */
+FM_API int fm_last_error(char *buf, int32_t len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FLOWMOL_B200_H */

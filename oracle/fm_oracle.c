@@ -1,0 +1,1099 @@
+/*
+ * fm_oracle.c -- CPU FP64 restatement of Flowmol's per-timestep MD hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker that the CUDA path in
+ * flowmol_b200/ is compared against.  It is linked only by tests/, by
+ * __graft_entry__.smoke() and by bench.py's CPU-baseline leg; the product
+ * library never calls it.
+ *
+ * Parity status: the reference (Fortran 90 + MPI) cannot be compiled in this
+ * environment (no gfortran, no MPI) and ships no golden force / pair-list
+ * vectors.  The geometry rules below are pinned against the values the
+ * reference printed into runs/Intrinsic_Interface/results/simulation_header;
+ * the restart format is pinned against src/reorder_restart/read_final_state.py
+ * run on runs/Intrinsic_Interface/initial_state.  Pair lists, forces, the
+ * integrator and the rebuild criterion are restated line by line from the
+ * Fortran cited at each function, but for those parts parity is UNPINNED by
+ * reference outputs (only analytic known-answer cases pin them).
+ *
+ * Numerics follow the reference build (gfortran -O3 -funroll-loops on x86-64,
+ * no -march, hence no FMA contraction): compile with -ffp-contract=off and
+ * without -ffast-math.  Array layout mirrors the Fortran modules: r, v, a are
+ * column-major (3, cap) so r[3*n+k] is r(k+1, n+1).  Molecule numbers inside
+ * the linked lists are 1-based like the reference; halo images occupy
+ * np+1 .. np+halo_np.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define ORC_OK 0
+#define ORC_ERR_ALLOC 1
+#define ORC_ERR_ESCAPE 2
+#define ORC_ERR_FEWCELLS 3
+#define ORC_ERR_BOND 4
+#define ORC_ERR_PARAM 5
+
+typedef struct orc {
+    /* ---- parameters (modules.f90 computational/physical constants) ---- */
+    int np, halo_np, cap, globalnp;
+    double domain[3], halfdomain[3], cellsidelength[3];
+    int ncells[3];
+    double rcutoff, rcutoff2, rneighbr2, delta_rneighbr[3], delta_t, potshift;
+    double density, potential_sLRC, pressure_sLRC;
+    int tplot, teval, iter;
+    int force_list;        /* 0 all pairs, 2 full list, 3 half list */
+    int rebuild_criteria;  /* 0 vmax, 1 fixed, 2 displacement */
+    int fixed_rebuild;
+    int integration_algorithm; /* 0 leap-frog, 1 velocity Verlet */
+    int potential_flag;    /* 0 LJ, 1 FENE polymer */
+    double k_c, R_0;
+    int max_funcy;
+    /* ---- state (arrays_MD) ---- */
+    double *r, *v, *a;        /* (3, cap) */
+    int *glob_no;             /* cap: identity carried to halo images */
+    int *halo_src;            /* cap: source molecule (1-based) of an image */
+    signed char *halo_shift;  /* (3, cap): -1/0/+1 domain shift of an image */
+    double *potenergymol, *virialmol, *potenergymol_POLY;
+    double *rdisp;            /* (3, np) displacement criterion */
+    /* polymer connectivity: chain/subchain/funcy/bin_bflag per molecule, bond(max_funcy, cap) */
+    int *chainID, *subchainID, *funcy;
+    int *bflag;               /* (4, cap) bin_bflag words */
+    int *bond;                /* (max_funcy, np) 1-based molecule numbers, 0 = empty */
+    int *bondcount;           /* np */
+    /* ---- cell linked lists (linklist.f90 cellinfo/node) ---- */
+    int ncell_tot;
+    int *cellnp, *cellhead;   /* (nc+2)^3 */
+    int *cn_molno, *cn_next;  /* node pool */
+    int cn_count, cn_cap;
+    /* ---- neighbour lists (linklist.f90 neighbrinfo) ---- */
+    int *Nlist, *nhead;       /* np */
+    int *nn_molno, *nn_next;
+    long nn_count, nn_cap;
+    /* ---- checkrebuild / record ---- */
+    double rmax, simtime;
+    double vsum, mv2sum, potenergysum, virial;
+    double kinenergy, potenergy, totenergy, temperature, pressure;
+    int rebuild_count;
+} orc;
+
+/* ------------------------------------------------------------------------ */
+/* setup_set_parameters.f90                                                  */
+/* ------------------------------------------------------------------------ */
+
+/* set_parameters_global_domain, initial_config_flag 0
+ * (setup_set_parameters.f90:1545-1580): L_i = n_i / (density/4)**(1/nd). */
+void orc_global_domain(const int nunits[3], double density, double domain_out[3],
+                       double unitsize_out[3], double *volume_out)
+{
+    double vol = 1.0;
+    for (int k = 0; k < 3; k++) {
+        domain_out[k] = (double)nunits[k] / pow(density / 4.0, 1.0 / 3.0);
+        vol = vol * domain_out[k];
+    }
+    for (int k = 0; k < 3; k++) unitsize_out[k] = domain_out[k] / (double)nunits[k];
+    *volume_out = vol;
+}
+
+/* set_parameters_cells (setup_set_parameters.f90:1848-1903).  Returns
+ * ORC_ERR_FEWCELLS where the reference aborts (fewer than 3 cells). */
+int orc_set_parameters_cells(const double domain[3], double rcutoff, const double delta[3],
+                             int potential_flag, double R_0, int ncells_out[3],
+                             double cellside_out[3], double *rneighbr2_out)
+{
+    double rneighbr = rcutoff + (delta[0] + delta[1] + delta[2]) / 3.0;
+    double rneighbr2 = rneighbr * rneighbr;
+    if (potential_flag == 1 && rneighbr < R_0) { /* FENE override, 1865-1869 */
+        rneighbr = R_0;
+        rneighbr2 = R_0 * R_0;
+    }
+    for (int k = 0; k < 3; k++) ncells_out[k] = (int)floor(domain[k] / (rcutoff + delta[k]));
+    *rneighbr2_out = rneighbr2;
+    if (ncells_out[0] < 3 || ncells_out[1] < 3 || ncells_out[2] < 3) return ORC_ERR_FEWCELLS;
+    for (int k = 0; k < 3; k++) cellside_out[k] = domain[k] / (double)ncells_out[k];
+    return ORC_OK;
+}
+
+/* Integer powers as gfortran -O3 expands x**n (repeated multiplication). */
+static inline double p3(double s) { return s * s * s; }
+static inline double p6(double s) { double t = p3(s); return t * t; }
+static inline double p12(double s) { double t = p6(s); return t * t; }
+
+/* LJ_accijmag / LJ_energy (setup_set_parameters.f90:105-135). */
+static inline double lj_accijmag(double s)
+{
+    double s2 = s * s, s4 = s2 * s2, s7 = s4 * s2 * s;
+    return 48.0 * (s7 - 0.5 * s4);
+}
+static inline double lj_energy(double s, double potshift)
+{
+    return 4.0 * (p6(s) - p3(s)) - potshift;
+}
+
+double orc_lj_accijmag(double invrij2) { return lj_accijmag(invrij2); }
+double orc_lj_energy(double invrij2, double potshift) { return lj_energy(invrij2, potshift); }
+/* potshift = 4(rc^-12 - rc^-6) (setup_set_parameters.f90:1222) */
+double orc_potshift(double rcutoff)
+{
+    return 4.0 * (1.0 / p12(rcutoff) - 1.0 / p6(rcutoff));
+}
+
+/* FENE_accijmag / FENE_energy (setup_set_parameters.f90:348-380). */
+static inline double fene_accijmag(double rij2, double k_c, double R_0)
+{
+    return -k_c / (1.0 - (rij2 / (R_0 * R_0)));
+}
+static inline double fene_energy(double rij2, double k_c, double R_0)
+{
+    return 0.5 * k_c * R_0 * R_0 * log(1.0 - (rij2 / (R_0 * R_0)));
+}
+
+/* ------------------------------------------------------------------------ */
+/* allocation                                                                */
+/* ------------------------------------------------------------------------ */
+
+static void *xcalloc(size_t n, size_t sz) { return calloc(n ? n : 1, sz); }
+
+void orc_free(orc *s);
+
+/* Creates a state for np molecules.  extralloc mirrors
+ * set_parameters_allocate (setup_set_parameters.f90:1248-1290): room for the
+ * halo images behind the real molecules. */
+orc *orc_create(int np, const double domain[3], double rcutoff, const double delta[3],
+                double delta_t, int tplot, int force_list, int potential_flag,
+                double k_c, double R_0, int rebuild_criteria, int fixed_rebuild,
+                double density, int sLRC_flag, int *err)
+{
+    orc *s = (orc *)xcalloc(1, sizeof(orc));
+    *err = ORC_OK;
+    if (!s) { *err = ORC_ERR_ALLOC; return NULL; }
+    s->np = np; s->globalnp = np;
+    for (int k = 0; k < 3; k++) {
+        s->domain[k] = domain[k];
+        s->halfdomain[k] = 0.5 * domain[k];
+        s->delta_rneighbr[k] = delta[k];
+    }
+    s->rcutoff = rcutoff;
+    s->rcutoff2 = rcutoff * rcutoff;
+    s->delta_t = delta_t;
+    s->tplot = tplot;
+    s->teval = tplot;
+    s->force_list = force_list;
+    s->potential_flag = potential_flag;
+    s->k_c = k_c; s->R_0 = R_0;
+    s->max_funcy = 4;
+    s->rebuild_criteria = rebuild_criteria;
+    s->fixed_rebuild = fixed_rebuild > 0 ? fixed_rebuild : 1;
+    s->integration_algorithm = 1;
+    s->density = density;
+    s->potshift = orc_potshift(rcutoff);
+    if (sLRC_flag) {
+        const double pi = 3.14159265358979323846;
+        s->potential_sLRC = 8.0 * pi * density * (1.0 / (9.0 * pow(rcutoff, 9)) - 1.0 / (3.0 * p3(rcutoff)));
+        s->pressure_sLRC = 8.0 * pi * (density * density) *
+                           (4.0 / (9.0 * pow(rcutoff, 9)) - 2.0 / (3.0 * p3(rcutoff)));
+    }
+    int rc = orc_set_parameters_cells(s->domain, rcutoff, delta, potential_flag, R_0,
+                                      s->ncells, s->cellsidelength, &s->rneighbr2);
+    if (rc != ORC_OK && force_list != 0) { *err = rc; orc_free(s); return NULL; }
+    if (rc != ORC_OK) { s->ncells[0] = s->ncells[1] = s->ncells[2] = 1; }
+    /* halo capacity: every boundary molecule may be imaged up to 7 times */
+    s->cap = np * 8 + 1024;
+    size_t cap = (size_t)s->cap;
+    s->r = (double *)xcalloc(3 * cap, sizeof(double));
+    s->v = (double *)xcalloc(3 * cap, sizeof(double));
+    s->a = (double *)xcalloc(3 * cap, sizeof(double));
+    s->glob_no = (int *)xcalloc(cap, sizeof(int));
+    s->halo_src = (int *)xcalloc(cap, sizeof(int));
+    s->halo_shift = (signed char *)xcalloc(3 * cap, 1);
+    s->potenergymol = (double *)xcalloc(cap, sizeof(double));
+    s->potenergymol_POLY = (double *)xcalloc(cap, sizeof(double));
+    s->virialmol = (double *)xcalloc(cap, sizeof(double));
+    s->chainID = (int *)xcalloc(cap, sizeof(int));
+    s->subchainID = (int *)xcalloc(cap, sizeof(int));
+    s->funcy = (int *)xcalloc(cap, sizeof(int));
+    s->bflag = (int *)xcalloc(4 * cap, sizeof(int));
+    s->bond = (int *)xcalloc((size_t)s->max_funcy * (size_t)np, sizeof(int));
+    s->bondcount = (int *)xcalloc((size_t)np, sizeof(int));
+    s->ncell_tot = (s->ncells[0] + 2) * (s->ncells[1] + 2) * (s->ncells[2] + 2);
+    s->cellnp = (int *)xcalloc((size_t)s->ncell_tot, sizeof(int));
+    s->cellhead = (int *)xcalloc((size_t)s->ncell_tot, sizeof(int));
+    s->cn_cap = s->cap;
+    s->cn_molno = (int *)xcalloc(cap, sizeof(int));
+    s->cn_next = (int *)xcalloc(cap, sizeof(int));
+    s->Nlist = (int *)xcalloc((size_t)np, sizeof(int));
+    s->nhead = (int *)xcalloc((size_t)np, sizeof(int));
+    s->nn_cap = (long)np * 16 + 1024;
+    s->nn_molno = (int *)xcalloc((size_t)s->nn_cap, sizeof(int));
+    s->nn_next = (int *)xcalloc((size_t)s->nn_cap, sizeof(int));
+    for (int n = 0; n < np; n++) s->glob_no[n] = n + 1;
+    if (!s->r || !s->v || !s->a || !s->nn_molno || !s->nn_next || !s->cn_molno) {
+        *err = ORC_ERR_ALLOC; orc_free(s); return NULL;
+    }
+    return s;
+}
+
+void orc_free(orc *s)
+{
+    if (!s) return;
+    free(s->r); free(s->v); free(s->a); free(s->glob_no); free(s->halo_src); free(s->halo_shift);
+    free(s->potenergymol); free(s->potenergymol_POLY); free(s->virialmol); free(s->rdisp);
+    free(s->chainID); free(s->subchainID); free(s->funcy); free(s->bflag); free(s->bond);
+    free(s->bondcount);
+    free(s->cellnp); free(s->cellhead); free(s->cn_molno); free(s->cn_next);
+    free(s->Nlist); free(s->nhead); free(s->nn_molno); free(s->nn_next);
+    free(s);
+}
+
+/* Accessors used by the ctypes wrapper. */
+double *orc_r(orc *s) { return s->r; }
+double *orc_v(orc *s) { return s->v; }
+double *orc_a(orc *s) { return s->a; }
+int *orc_glob_no(orc *s) { return s->glob_no; }
+double *orc_potenergymol(orc *s) { return s->potenergymol; }
+double *orc_virialmol(orc *s) { return s->virialmol; }
+int orc_np(orc *s) { return s->np; }
+int orc_halo_np(orc *s) { return s->halo_np; }
+int orc_iter(orc *s) { return s->iter; }
+void orc_set_iter(orc *s, int iter) { s->iter = iter; }
+void orc_set_integration_algorithm(orc *s, int ia) { s->integration_algorithm = ia; }
+double orc_rmax(orc *s) { return s->rmax; }
+int orc_rebuild_count(orc *s) { return s->rebuild_count; }
+void orc_geometry(orc *s, int ncells[3], double cellside[3], double *rneighbr2, double *rcutoff2,
+                  double *potshift)
+{
+    for (int k = 0; k < 3; k++) { ncells[k] = s->ncells[k]; cellside[k] = s->cellsidelength[k]; }
+    *rneighbr2 = s->rneighbr2; *rcutoff2 = s->rcutoff2; *potshift = s->potshift;
+}
+void orc_macro(orc *s, double out[9])
+{
+    out[0] = s->vsum; out[1] = s->mv2sum; out[2] = s->temperature; out[3] = s->kinenergy;
+    out[4] = s->potenergy; out[5] = s->totenergy; out[6] = s->pressure; out[7] = s->virial;
+    out[8] = s->potenergysum;
+}
+
+/* ------------------------------------------------------------------------ */
+/* linked lists (linklist.f90)                                               */
+/* ------------------------------------------------------------------------ */
+
+static inline int cidx(const orc *s, int i, int j, int k) /* 1-based cell indices */
+{
+    return (i - 1) + (s->ncells[0] + 2) * ((j - 1) + (s->ncells[1] + 2) * (k - 1));
+}
+
+/* linklist_deallocateall for the cell and neighbour lists
+ * (linklist.f90:2872-2964). */
+void orc_linklist_deallocateall(orc *s)
+{
+    if (s->potential_flag == 1) { /* linklist.f90:2889-2892 */
+        memset(s->bond, 0, sizeof(int) * (size_t)s->max_funcy * (size_t)s->np);
+        memset(s->bondcount, 0, sizeof(int) * (size_t)s->np);
+    }
+    memset(s->cellnp, 0, sizeof(int) * (size_t)s->ncell_tot);
+    memset(s->cellhead, 0, sizeof(int) * (size_t)s->ncell_tot);
+    s->cn_count = 0;
+    memset(s->Nlist, 0, sizeof(int) * (size_t)s->np);
+    memset(s->nhead, 0, sizeof(int) * (size_t)s->np);
+    s->nn_count = 0;
+}
+
+/* linklist_checkpush (linklist.f90:1596-1632): head insert. */
+static int checkpush(orc *s, int c, int molno)
+{
+    if (s->cn_count >= s->cn_cap) return ORC_ERR_ALLOC;
+    int node = ++s->cn_count; /* 1-based node id, 0 = null */
+    s->cn_molno[node - 1] = molno;
+    s->cn_next[node - 1] = s->cellnp[c] > 0 ? s->cellhead[c] : 0;
+    s->cellhead[c] = node;
+    s->cellnp[c] += 1;
+    return ORC_OK;
+}
+
+/* linklist_checkpushneighbr (linklist.f90:1636-1670): head insert into the
+ * list of molnoi. */
+static int checkpushneighbr(orc *s, int molnoi, int molnoj)
+{
+    if (s->nn_count >= s->nn_cap) {
+        long ncap = s->nn_cap * 2;
+        int *m = (int *)realloc(s->nn_molno, sizeof(int) * (size_t)ncap);
+        if (!m) return ORC_ERR_ALLOC;
+        s->nn_molno = m;
+        int *x = (int *)realloc(s->nn_next, sizeof(int) * (size_t)ncap);
+        if (!x) return ORC_ERR_ALLOC;
+        s->nn_next = x;
+        s->nn_cap = ncap;
+    }
+    long node = ++s->nn_count;
+    s->nn_molno[node - 1] = molnoj;
+    s->nn_next[node - 1] = s->Nlist[molnoi - 1] > 0 ? s->nhead[molnoi - 1] : 0;
+    s->nhead[molnoi - 1] = (int)node;
+    s->Nlist[molnoi - 1] += 1;
+    return ORC_OK;
+}
+
+static inline int node_molno(const orc *s, int node) { return s->cn_molno[node - 1]; }
+static inline int node_next(const orc *s, int node) { return s->cn_next[node - 1]; }
+
+/* assign_to_cell (linklist.f90:2645-2679).  A molecule whose cell falls
+ * outside 1..ncells+2 makes the reference abort ("escaped mol"). */
+int orc_assign_to_cell(orc *s)
+{
+    for (int n = 1; n <= s->np; n++) {
+        const double *rn = &s->r[3 * (size_t)(n - 1)];
+        int ic = (int)ceil((rn[0] + s->halfdomain[0]) / s->cellsidelength[0]) + 1;
+        int jc = (int)ceil((rn[1] + s->halfdomain[1]) / s->cellsidelength[1]) + 1;
+        int kc = (int)ceil((rn[2] + s->halfdomain[2]) / s->cellsidelength[2]) + 1;
+        if (ic < 1 || jc < 1 || kc < 1 || ic > s->ncells[0] + 2 || jc > s->ncells[1] + 2 ||
+            kc > s->ncells[2] + 2)
+            return ORC_ERR_ESCAPE;
+        int rc = checkpush(s, cidx(s, ic, jc, kc), n);
+        if (rc) return rc;
+    }
+    return ORC_OK;
+}
+
+/* assign_to_halocell (linklist.f90:2681-2706).  No escape check in the
+ * reference; an image that bins outside the grid is reported here instead of
+ * writing out of bounds. */
+static int assign_to_halocell(orc *s, int start, int finish)
+{
+    for (int n = start; n <= finish; n++) {
+        const double *rn = &s->r[3 * (size_t)(n - 1)];
+        int ic = (int)ceil((rn[0] + s->halfdomain[0]) / s->cellsidelength[0]) + 1;
+        int jc = (int)ceil((rn[1] + s->halfdomain[1]) / s->cellsidelength[1]) + 1;
+        int kc = (int)ceil((rn[2] + s->halfdomain[2]) / s->cellsidelength[2]) + 1;
+        if (ic < 1 || jc < 1 || kc < 1 || ic > s->ncells[0] + 2 || jc > s->ncells[1] + 2 ||
+            kc > s->ncells[2] + 2)
+            return ORC_ERR_ESCAPE;
+        int rc = checkpush(s, cidx(s, ic, jc, kc), n);
+        if (rc) return rc;
+    }
+    return ORC_OK;
+}
+
+/* ------------------------------------------------------------------------ */
+/* halo images, single-rank periodic form (messenger.serial.f90:278-770)     */
+/* ------------------------------------------------------------------------ */
+
+static int add_image(orc *s, int molno, int sx, int sy, int sz)
+{
+    int m = s->np + s->halo_np + 1; /* 1-based index of the new image */
+    if (m > s->cap) return ORC_ERR_ALLOC;
+    double *dst = &s->r[3 * (size_t)(m - 1)];
+    const double *src = &s->r[3 * (size_t)(molno - 1)];
+    dst[0] = src[0]; dst[1] = src[1]; dst[2] = src[2];
+    /* r(k,np+m) = r(k,np+m) +/- domain(k): one FP64 add per shifted axis */
+    if (sx) dst[0] = dst[0] + (double)sx * s->domain[0];
+    if (sy) dst[1] = dst[1] + (double)sy * s->domain[1];
+    if (sz) dst[2] = dst[2] + (double)sz * s->domain[2];
+    double *vd = &s->v[3 * (size_t)(m - 1)];
+    const double *vs = &s->v[3 * (size_t)(molno - 1)];
+    vd[0] = vs[0]; vd[1] = vs[1]; vd[2] = vs[2];
+    s->glob_no[m - 1] = s->glob_no[molno - 1];
+    s->halo_src[m - 1] = molno;
+    s->halo_shift[3 * (size_t)(m - 1) + 0] = (signed char)sx;
+    s->halo_shift[3 * (size_t)(m - 1) + 1] = (signed char)sy;
+    s->halo_shift[3 * (size_t)(m - 1) + 2] = (signed char)sz;
+    s->chainID[m - 1] = s->chainID[molno - 1];
+    s->subchainID[m - 1] = s->subchainID[molno - 1];
+    s->funcy[m - 1] = s->funcy[molno - 1];
+    for (int b = 0; b < 4; b++) s->bflag[4 * (size_t)(m - 1) + b] = s->bflag[4 * (size_t)(molno - 1) + b];
+    s->halo_np += 1;
+    return ORC_OK;
+}
+
+static int image_cell(orc *s, int i, int j, int k, int sx, int sy, int sz)
+{
+    int c = cidx(s, i, j, k);
+    int node = s->cellhead[c];
+    for (int n = 0; n < s->cellnp[c]; n++) {
+        int rc = add_image(s, node_molno(s, node), sx, sy, sz);
+        if (rc) return rc;
+        node = node_next(s, node);
+    }
+    return ORC_OK;
+}
+
+/* sign(1, x) in Fortran: +1 for x >= 0 */
+static inline int fsign1(int x) { return x >= 0 ? 1 : -1; }
+
+/* messenger_updateborders_quiescent (messenger.serial.f90:278-323) with
+ * updatefacedown/up (372-584), updateedge (589-710), updatecorners (715-770). */
+int orc_updateborders(orc *s, int rebuild)
+{
+    const int nx = s->ncells[0], ny = s->ncells[1], nz = s->ncells[2];
+    int rc;
+    s->halo_np = 0;
+    /* faces down (+domain) then up (-domain), x, y, z */
+    for (int ixyz = 0; ixyz < 3; ixyz++) {
+        for (int dir = 0; dir < 2; dir++) {
+            int sgn = dir == 0 ? +1 : -1;
+            if (ixyz == 0) {
+                int ic = dir == 0 ? 2 : nx + 1;
+                for (int jc = 2; jc <= ny + 1; jc++)
+                    for (int kc = 2; kc <= nz + 1; kc++)
+                        if ((rc = image_cell(s, ic, jc, kc, sgn, 0, 0))) return rc;
+            } else if (ixyz == 1) {
+                int jc = dir == 0 ? 2 : ny + 1;
+                for (int ic = 2; ic <= nx + 1; ic++)
+                    for (int kc = 2; kc <= nz + 1; kc++)
+                        if ((rc = image_cell(s, ic, jc, kc, 0, sgn, 0))) return rc;
+            } else {
+                int kc = dir == 0 ? 2 : nz + 1;
+                for (int ic = 2; ic <= nx + 1; ic++)
+                    for (int jc = 2; jc <= ny + 1; jc++)
+                        if ((rc = image_cell(s, ic, jc, kc, 0, 0, sgn))) return rc;
+            }
+        }
+    }
+    /* edges: updateedge(1,2) -> along z, (2,3) -> along x, (1,3) -> along y */
+    const int order[3] = {2, 0, 1};
+    for (int e = 0; e < 3; e++) {
+        int ixyz = order[e];
+        if (ixyz == 0) { /* edge1 over y, edge2 over z */
+            int e1[4] = {2, 2, ny + 1, ny + 1}, e2[4] = {2, nz + 1, 2, nz + 1};
+            for (int q = 0; q < 4; q++)
+                for (int ic = 2; ic <= nx + 1; ic++)
+                    if ((rc = image_cell(s, ic, e1[q], e2[q], 0, fsign1(ny - e1[q]), fsign1(nz - e2[q]))))
+                        return rc;
+        } else if (ixyz == 1) { /* edge1 over x, edge2 over z */
+            int e1[4] = {2, 2, nx + 1, nx + 1}, e2[4] = {2, nz + 1, 2, nz + 1};
+            for (int q = 0; q < 4; q++)
+                for (int jc = 2; jc <= ny + 1; jc++)
+                    if ((rc = image_cell(s, e1[q], jc, e2[q], fsign1(nx - e1[q]), 0, fsign1(nz - e2[q]))))
+                        return rc;
+        } else { /* edge1 over x, edge2 over y */
+            int e1[4] = {2, 2, nx + 1, nx + 1}, e2[4] = {2, ny + 1, 2, ny + 1};
+            for (int q = 0; q < 4; q++)
+                for (int kc = 2; kc <= nz + 1; kc++)
+                    if ((rc = image_cell(s, e1[q], e2[q], kc, fsign1(nx - e1[q]), fsign1(ny - e2[q]), 0)))
+                        return rc;
+        }
+    }
+    /* corners */
+    {
+        int ci[8] = {2, 2, 2, 2, nx + 1, nx + 1, nx + 1, nx + 1};
+        int cj[8] = {2, 2, ny + 1, ny + 1, 2, 2, ny + 1, ny + 1};
+        int ck[8] = {2, nz + 1, 2, nz + 1, 2, nz + 1, 2, nz + 1};
+        for (int q = 0; q < 8; q++)
+            if ((rc = image_cell(s, ci[q], cj[q], ck[q], fsign1(nx - ci[q]), fsign1(ny - cj[q]),
+                                 fsign1(nz - ck[q]))))
+                return rc;
+    }
+    if (rebuild == 1) return assign_to_halocell(s, s->np + 1, s->np + s->halo_np);
+    return ORC_OK;
+}
+
+/* Refresh image positions from their sources without re-walking the cells.
+ * Equivalent to messenger_updateborders(0) because the cell lists (and hence
+ * the image order) only change on rebuild. */
+void orc_refresh_halo(orc *s)
+{
+    for (int m = s->np + 1; m <= s->np + s->halo_np; m++) {
+        int src = s->halo_src[m - 1];
+        for (int k = 0; k < 3; k++) {
+            double x = s->r[3 * (size_t)(src - 1) + k];
+            int sh = s->halo_shift[3 * (size_t)(m - 1) + k];
+            if (sh) x = x + (double)sh * s->domain[k];
+            s->r[3 * (size_t)(m - 1) + k] = x;
+            s->v[3 * (size_t)(m - 1) + k] = s->v[3 * (size_t)(src - 1) + k];
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* polymer bond discovery (linklist.f90:2542-2584, modules.f90:597-610)      */
+/* ------------------------------------------------------------------------ */
+
+/* get_bondflag (modules.f90:602-610): subchain scID maps to word
+ * ceiling(scID/31) and bit mod(scID,31)-1 (bit 30 when that is -1), with
+ * intbits = bit_size(1)-1 = 31 (modules.f90:497). */
+static int get_bondflag(const orc *s, int i, int subj)
+{
+    int ipos = subj - 1;
+    int group = ipos / 31;
+    int expo = ipos % 31;
+    if (group < 0 || group > 3) return 0;
+    return (s->bflag[4 * (size_t)(i - 1) + group] >> expo) & 1;
+}
+
+static int check_update_adjacentbeadinfo(orc *s, int molnoi, int molnoj)
+{
+    if (s->chainID[molnoi - 1] != s->chainID[molnoj - 1] || s->chainID[molnoi - 1] == 0) return ORC_OK;
+    int bflag = get_bondflag(s, molnoi, s->subchainID[molnoj - 1]);
+    if (!bflag) return ORC_OK;
+    /* bond(bondcount+1, i) = j on both partners (linklist.f90:2556-2565); only
+     * the real molecules' rows are ever read by the force loop */
+    if (molnoi <= s->np) {
+        int bc = s->bondcount[molnoi - 1];
+        if (bc >= s->max_funcy) return ORC_ERR_BOND;
+        s->bond[(size_t)(molnoi - 1) * s->max_funcy + bc] = molnoj;
+        s->bondcount[molnoi - 1] = bc + 1;
+    }
+    if (molnoj <= s->np) {
+        int bc = s->bondcount[molnoj - 1];
+        if (bc >= s->max_funcy) return ORC_ERR_BOND;
+        s->bond[(size_t)(molnoj - 1) * s->max_funcy + bc] = molnoi;
+        s->bondcount[molnoj - 1] = bc + 1;
+    }
+    return ORC_OK;
+}
+
+/* ------------------------------------------------------------------------ */
+/* neighbour lists                                                           */
+/* ------------------------------------------------------------------------ */
+
+static inline double rij2_of(const orc *s, int mi, int mj, double rij[3])
+{
+    const double *ri = &s->r[3 * (size_t)(mi - 1)];
+    const double *rj = &s->r[3 * (size_t)(mj - 1)];
+    rij[0] = ri[0] - rj[0];
+    rij[1] = ri[1] - rj[1];
+    rij[2] = ri[2] - rj[2];
+    double d = 0.0;
+    d = d + rij[0] * rij[0];
+    d = d + rij[1] * rij[1];
+    d = d + rij[2] * rij[2];
+    return d;
+}
+
+/* calculate_cell_interactions_opt (linklist.f90:1118-1180): pairs between a
+ * halo cell range and its shifted neighbour, stored on molnoj's list. */
+static int cell_interactions_opt(orc *s, int is, int ie, int ish, int js, int je, int jsh, int ks,
+                                 int ke, int ksh)
+{
+    double rij[3];
+    int rc;
+    for (int kc = ks; kc <= ke; kc++)
+        for (int jc = js; jc <= je; jc++)
+            for (int ic = is; ic <= ie; ic++) {
+                int c = cidx(s, ic, jc, kc);
+                int c2 = cidx(s, ic + ish, jc + jsh, kc + ksh);
+                int oldi = s->cellhead[c];
+                for (int i = 0; i < s->cellnp[c]; i++) {
+                    int molnoi = node_molno(s, oldi);
+                    int oldj = s->cellhead[c2];
+                    for (int j = 0; j < s->cellnp[c2]; j++) {
+                        int molnoj = node_molno(s, oldj);
+                        oldj = node_next(s, oldj);
+                        double r2 = rij2_of(s, molnoi, molnoj, rij);
+                        if (s->potential_flag == 1)
+                            if ((rc = check_update_adjacentbeadinfo(s, molnoi, molnoj))) return rc;
+                        if (r2 < s->rneighbr2)
+                            if ((rc = checkpushneighbr(s, molnoj, molnoi))) return rc;
+                    }
+                    oldi = node_next(s, oldi);
+                }
+            }
+    return ORC_OK;
+}
+
+static const int ISH[13] = {1, 1, 0, -1, 0, 1, 1, 0, -1, -1, -1, 0, 1};
+static const int JSH[13] = {0, 1, 1, 1, 0, 0, 1, 1, 1, 0, -1, -1, -1};
+static const int KSH[13] = {0, 0, 0, 0, 1, 1, 1, 1, 1, 1, 1, 1, 1};
+
+/* assign_to_neighbourlist_halfint_opt (linklist.f90:660-804). */
+int orc_neighbourlist_halfint_opt(orc *s)
+{
+    const int nx = s->ncells[0], ny = s->ncells[1], nz = s->ncells[2];
+    double rij[3];
+    int rc;
+    memset(s->Nlist, 0, sizeof(int) * (size_t)s->np);
+    memset(s->nhead, 0, sizeof(int) * (size_t)s->np);
+    s->nn_count = 0;
+    for (int ic = 2; ic <= nx + 1; ic++)
+        for (int jc = 2; jc <= ny + 1; jc++)
+            for (int kc = 2; kc <= nz + 1; kc++) {
+                int c = cidx(s, ic, jc, kc);
+                int cellnp = s->cellnp[c];
+                int oldi = s->cellhead[c];
+                for (int i = 1; i <= cellnp; i++) { /* own cell, j after i */
+                    int molnoi = node_molno(s, oldi);
+                    int oldj = node_next(s, oldi);
+                    for (int j = i + 1; j <= cellnp; j++) {
+                        int molnoj = node_molno(s, oldj);
+                        oldj = node_next(s, oldj);
+                        if (molnoi == molnoj) continue;
+                        double r2 = rij2_of(s, molnoi, molnoj, rij);
+                        if (s->potential_flag == 1)
+                            if ((rc = check_update_adjacentbeadinfo(s, molnoi, molnoj))) return rc;
+                        if (r2 < s->rneighbr2)
+                            if ((rc = checkpushneighbr(s, molnoi, molnoj))) return rc;
+                    }
+                    oldi = node_next(s, oldi);
+                }
+                int oldihead = s->cellhead[c];
+                for (int k = 0; k < 13; k++) {
+                    int c2 = cidx(s, ic + ISH[k], jc + JSH[k], kc + KSH[k]);
+                    int oldi2 = oldihead;
+                    for (int i = 0; i < cellnp; i++) {
+                        int molnoi = node_molno(s, oldi2);
+                        int oldj = s->cellhead[c2];
+                        for (int j = 0; j < s->cellnp[c2]; j++) {
+                            int molnoj = node_molno(s, oldj);
+                            oldj = node_next(s, oldj);
+                            double r2 = rij2_of(s, molnoi, molnoj, rij);
+                            if (s->potential_flag == 1)
+                                if ((rc = check_update_adjacentbeadinfo(s, molnoi, molnoj))) return rc;
+                            if (r2 < s->rneighbr2)
+                                if ((rc = checkpushneighbr(s, molnoi, molnoj))) return rc;
+                        }
+                        oldi2 = node_next(s, oldi2);
+                    }
+                }
+            }
+    /* all_cell_interactions (linklist.f90:778-802): 27 sweeps from halo cells */
+    {
+        int x = nx, x1 = nx + 1, x2 = nx + 2, y = ny, y1 = ny + 1, y2 = ny + 2, z = nz, z1 = nz + 1;
+        const int imin[27] = {2, 1, 3, 2, 2, 1, 3, 3, 1, 1, 1, 1, 1, 1, x2, x2, x2, x2, 2, 2, 3, 2, 2, 3, 2, 3, 2};
+        const int imax[27] = {x1, x, x2, x1, x1, x, x2, x2, x, 1, 1, 1, 1, 1, x2, x2, x2, x2, x1, x, x1, x1, x, x1, x1, x1, x};
+        const int jmin[27] = {2, 2, 2, 1, 3, 1, 1, 3, 3, 2, 2, 1, 1, 3, 1, 2, 1, 3, 1, 1, 1, 1, 1, 1, y2, y2, y2};
+        const int jmax[27] = {y1, y1, y1, y, y2, y, y, y2, y2, y1, y1, y, y, y2, y, y1, y, y2, 1, 1, 1, 1, 1, 1, y2, y2, y2};
+        const int kmin[27] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 2, 2, 2, 2, 2, 2, 2, 2, 2, 2, 2, 2, 2, 2, 2, 2, 2, 2};
+        const int kmax[27] = {1, 1, 1, 1, 1, 1, 1, 1, 1, z1, z, z1, z, z, z1, z, z, z, z1, z1, z1, z, z, z, z, z, z};
+        const int shift[27] = {5, 6, 10, 8, 12, 7, 9, 11, 13, 1, 6, 2, 7, 13, 4, 10, 9, 11, 3, 2, 4, 8, 7, 9, 12, 11, 13};
+        for (int q = 0; q < 27; q++) {
+            int sh = shift[q] - 1;
+            if ((rc = cell_interactions_opt(s, imin[q], imax[q], ISH[sh], jmin[q], jmax[q], JSH[sh], kmin[q],
+                                            kmax[q], KSH[sh])))
+                return rc;
+        }
+    }
+    return ORC_OK;
+}
+
+/* assign_to_neighbourlist_allint (linklist.f90:181-263). */
+int orc_neighbourlist_allint(orc *s)
+{
+    double rij[3];
+    int rc;
+    memset(s->Nlist, 0, sizeof(int) * (size_t)s->np);
+    memset(s->nhead, 0, sizeof(int) * (size_t)s->np);
+    s->nn_count = 0;
+    for (int ic = 2; ic <= s->ncells[0] + 1; ic++)
+        for (int jc = 2; jc <= s->ncells[1] + 1; jc++)
+            for (int kc = 2; kc <= s->ncells[2] + 1; kc++) {
+                int c = cidx(s, ic, jc, kc);
+                int oldi = s->cellhead[c];
+                for (int i = 0; i < s->cellnp[c]; i++) {
+                    int molnoi = node_molno(s, oldi);
+                    for (int di = -1; di <= 1; di++)
+                        for (int dj = -1; dj <= 1; dj++)
+                            for (int dk = -1; dk <= 1; dk++) {
+                                int c2 = cidx(s, ic + di, jc + dj, kc + dk);
+                                int oldj = s->cellhead[c2];
+                                for (int j = 0; j < s->cellnp[c2]; j++) {
+                                    int molnoj = node_molno(s, oldj);
+                                    oldj = node_next(s, oldj);
+                                    if (molnoi == molnoj) continue;
+                                    double r2 = rij2_of(s, molnoi, molnoj, rij);
+                                    if (r2 < s->rneighbr2)
+                                        if ((rc = checkpushneighbr(s, molnoi, molnoj))) return rc;
+                                }
+                            }
+                    oldi = node_next(s, oldi);
+                }
+            }
+    return ORC_OK;
+}
+
+/* assign_to_neighbourlist (linklist.f90:2710-2741). */
+int orc_assign_to_neighbourlist(orc *s)
+{
+    if (s->force_list == 2) return orc_neighbourlist_allint(s);
+    if (s->force_list == 3) return orc_neighbourlist_halfint_opt(s);
+    return ORC_OK;
+}
+
+/* Exports the list as (owner, partner-source, shift-code) with 1-based
+ * glob_no identities; shift code = (sx+1) + 3(sy+1) + 9(sz+1), 13 = none. */
+long orc_pair_list(orc *s, int *owner, int *partner, int *code, long cap)
+{
+    long n = 0;
+    for (int i = 1; i <= s->np; i++) {
+        int node = s->nhead[i - 1];
+        for (int q = 0; q < s->Nlist[i - 1]; q++) {
+            int j = s->nn_molno[node - 1];
+            node = s->nn_next[node - 1];
+            if (n < cap) {
+                owner[n] = s->glob_no[i - 1];
+                if (j <= s->np) {
+                    partner[n] = s->glob_no[j - 1];
+                    code[n] = 13;
+                } else {
+                    const signed char *sh = &s->halo_shift[3 * (size_t)(j - 1)];
+                    partner[n] = s->glob_no[s->halo_src[j - 1] - 1];
+                    code[n] = (sh[0] + 1) + 3 * (sh[1] + 1) + 9 * (sh[2] + 1);
+                }
+            }
+            n++;
+        }
+    }
+    return n;
+}
+
+long orc_list_length(orc *s) { return s->nn_count; }
+
+/* ------------------------------------------------------------------------ */
+/* forces (simulation_compute_forces.f90)                                    */
+/* ------------------------------------------------------------------------ */
+
+static void zero_forces(orc *s)
+{
+    size_t tot = (size_t)(s->np + s->halo_np);
+    memset(s->a, 0, sizeof(double) * 3 * tot);
+    memset(s->potenergymol, 0, sizeof(double) * tot);
+    memset(s->potenergymol_POLY, 0, sizeof(double) * tot);
+    memset(s->virialmol, 0, sizeof(double) * tot);
+    s->virial = 0.0;
+}
+
+/* simulation_compute_forces_LJ_neigbr_halfint (:628-726). */
+static void forces_halfint(orc *s)
+{
+    const int rec = (s->iter % s->tplot) == 0;
+    const int tev = (s->iter % s->teval) == 0;
+    double rij[3];
+    for (int i = 1; i <= s->np; i++) {
+        int node = s->nhead[i - 1];
+        for (int q = 0; q < s->Nlist[i - 1]; q++) {
+            int j = s->nn_molno[node - 1];
+            node = s->nn_next[node - 1];
+            double r2 = rij2_of(s, i, j, rij);
+            if (r2 < s->rcutoff2) {
+                double inv = 1.0 / r2;
+                double acc = lj_accijmag(inv);
+                double *ai = &s->a[3 * (size_t)(i - 1)], *aj = &s->a[3 * (size_t)(j - 1)];
+                ai[0] = ai[0] + acc * rij[0] / 1.0;
+                ai[1] = ai[1] + acc * rij[1] / 1.0;
+                ai[2] = ai[2] + acc * rij[2] / 1.0;
+                aj[0] = aj[0] - acc * rij[0] / 1.0;
+                aj[1] = aj[1] - acc * rij[1] / 1.0;
+                aj[2] = aj[2] - acc * rij[2] / 1.0;
+                if (rec) {
+                    double e = lj_energy(inv, s->potshift);
+                    s->potenergymol[i - 1] += e;
+                    s->potenergymol[j - 1] += e;
+                    s->virialmol[i - 1] += acc * r2;
+                    s->virialmol[j - 1] += acc * r2;
+                } else if (tev) {
+                    s->virialmol[i - 1] += acc * r2;
+                    s->virialmol[j - 1] += acc * r2;
+                }
+            }
+        }
+    }
+}
+
+/* simulation_compute_forces_LJ_neigbr (:551-623): full list, i side only. */
+static void forces_full(orc *s)
+{
+    const int rec = (s->iter % s->tplot) == 0;
+    const int tev = (s->iter % s->teval) == 0;
+    double rij[3];
+    for (int i = 1; i <= s->np; i++) {
+        int node = s->nhead[i - 1];
+        for (int q = 0; q < s->Nlist[i - 1]; q++) {
+            int j = s->nn_molno[node - 1];
+            node = s->nn_next[node - 1];
+            double r2 = rij2_of(s, i, j, rij);
+            if (r2 < s->rcutoff2) {
+                double inv = 1.0 / r2;
+                double acc = lj_accijmag(inv);
+                double *ai = &s->a[3 * (size_t)(i - 1)];
+                ai[0] = ai[0] + acc * rij[0] / 1.0;
+                ai[1] = ai[1] + acc * rij[1] / 1.0;
+                ai[2] = ai[2] + acc * rij[2] / 1.0;
+                if (rec) {
+                    s->potenergymol[i - 1] += lj_energy(inv, s->potshift);
+                    s->virialmol[i - 1] += acc * r2;
+                } else if (tev) {
+                    s->virialmol[i - 1] += acc * r2;
+                }
+            }
+        }
+    }
+}
+
+/* simulation_compute_forces_LJ_AP (:280-341): all pairs, per-axis minimum
+ * image. */
+static void forces_AP(orc *s)
+{
+    const int rec = (s->iter % s->tplot) == 0;
+    const int tev = (s->iter % s->teval) == 0;
+    double rij[3];
+    for (int i = 1; i <= s->np; i++) {
+        const double *ri = &s->r[3 * (size_t)(i - 1)];
+        for (int j = i + 1; j <= s->np; j++) {
+            const double *rj = &s->r[3 * (size_t)(j - 1)];
+            double r2 = 0.0;
+            for (int k = 0; k < 3; k++) {
+                rij[k] = ri[k] - rj[k];
+                if (fabs(rij[k]) > s->halfdomain[k]) rij[k] = rij[k] - copysign(s->domain[k], rij[k]);
+                r2 = r2 + rij[k] * rij[k];
+            }
+            if (r2 < s->rcutoff2) {
+                double inv = 1.0 / r2;
+                double acc = lj_accijmag(inv);
+                double *ai = &s->a[3 * (size_t)(i - 1)], *aj = &s->a[3 * (size_t)(j - 1)];
+                for (int k = 0; k < 3; k++) {
+                    ai[k] = ai[k] + acc * rij[k] / 1.0;
+                    aj[k] = aj[k] - acc * rij[k] / 1.0;
+                }
+                if (rec) {
+                    double e = lj_energy(inv, s->potshift);
+                    s->potenergymol[i - 1] += e;
+                    s->potenergymol[j - 1] += e;
+                    s->virialmol[i - 1] += acc * r2;
+                    s->virialmol[j - 1] += acc * r2;
+                } else if (tev) {
+                    s->virialmol[i - 1] += acc * r2;
+                    s->virialmol[j - 1] += acc * r2;
+                }
+            }
+        }
+    }
+}
+
+/* simulation_compute_forces_poly (:731-789): bonded FENE, i side only. */
+static int forces_poly(orc *s)
+{
+    const int rec = (s->iter % s->tplot) == 0;
+    const int tev = (s->iter % s->teval) == 0;
+    double rij[3];
+    for (int i = 1; i <= s->np; i++) {
+        for (int b = 0; b < s->funcy[i - 1] && b < s->max_funcy; b++) {
+            int j = s->bond[(size_t)(i - 1) * s->max_funcy + b];
+            if (j == 0) continue;
+            double r2 = rij2_of(s, i, j, rij);
+            if (r2 >= s->R_0 * s->R_0) return ORC_ERR_BOND; /* polymer_bond_error */
+            double acc = fene_accijmag(r2, s->k_c, s->R_0);
+            double *ai = &s->a[3 * (size_t)(i - 1)];
+            ai[0] = ai[0] + acc * rij[0] / 1.0;
+            ai[1] = ai[1] + acc * rij[1] / 1.0;
+            ai[2] = ai[2] + acc * rij[2] / 1.0;
+            if (rec) {
+                s->potenergymol_POLY[i - 1] += fene_energy(r2, s->k_c, s->R_0);
+                s->virialmol[i - 1] += acc * r2;
+            } else if (tev) {
+                s->virialmol[i - 1] += acc * r2;
+            }
+        }
+    }
+    return ORC_OK;
+}
+
+/* simulation_compute_forces dispatcher (:182-275). */
+int orc_compute_forces(orc *s)
+{
+    zero_forces(s);
+    switch (s->force_list) {
+    case 0: forces_AP(s); break;
+    case 2: forces_full(s); break;
+    case 3: forces_halfint(s); break;
+    default: return ORC_ERR_PARAM;
+    }
+    if (s->potential_flag == 1) {
+        int rc = forces_poly(s);
+        if (rc) return rc;
+        for (int n = 0; n < s->np + s->halo_np; n++) s->potenergymol[n] += s->potenergymol_POLY[n];
+    }
+    return ORC_OK;
+}
+
+/* ------------------------------------------------------------------------ */
+/* integration (simulation_move_particles_vv.f90, NVE)                       */
+/* ------------------------------------------------------------------------ */
+
+void orc_move_vv(orc *s, int pass_num)
+{
+    const double dt = s->delta_t;
+    const double c = 0.5 * (dt * dt);
+    const double h = 0.5 * dt;
+    if (pass_num == 1) { /* :64-69 */
+        for (int n = 0; n < s->np; n++)
+            for (int k = 0; k < 3; k++) {
+                size_t q = 3 * (size_t)n + k;
+                s->r[q] = s->r[q] + dt * s->v[q] + c * s->a[q];
+                s->v[q] = s->v[q] + h * s->a[q];
+            }
+    } else { /* :132-135, simtime :191 */
+        for (int n = 0; n < s->np; n++)
+            for (int k = 0; k < 3; k++) {
+                size_t q = 3 * (size_t)n + k;
+                s->v[q] = s->v[q] + h * s->a[q];
+            }
+        s->simtime = s->simtime + dt;
+    }
+}
+
+/* simulation_move_particles_lfv NVE (simulation_move_particles_lfv.f90:81-92). */
+void orc_move_lfv(orc *s)
+{
+    const double dt = s->delta_t;
+    for (int n = 0; n < s->np; n++)
+        for (int k = 0; k < 3; k++) {
+            size_t q = 3 * (size_t)n + k;
+            s->v[q] = s->v[q] + dt * s->a[q];
+            s->r[q] = s->r[q] + dt * s->v[q];
+        }
+    s->simtime = s->simtime + dt;
+}
+
+/* ------------------------------------------------------------------------ */
+/* rebuild criterion (simulation_checkrebuild.f90:17-148)                    */
+/* ------------------------------------------------------------------------ */
+
+int orc_checkrebuild(orc *s)
+{
+    int rebuild = 0;
+    if (((s->iter + 1) % s->tplot) == 0) rebuild = 1; /* :34 */
+    double dmin = s->delta_rneighbr[0];
+    if (s->delta_rneighbr[1] < dmin) dmin = s->delta_rneighbr[1];
+    if (s->delta_rneighbr[2] < dmin) dmin = s->delta_rneighbr[2];
+    if (s->rebuild_criteria == 0) { /* :84-99 */
+        double vmax = 0.0;
+        for (int n = 0; n < s->np; n++) {
+            const double *vn = &s->v[3 * (size_t)n];
+            double m = 0.0;
+            m = m + vn[0] * vn[0];
+            m = m + vn[1] * vn[1];
+            m = m + vn[2] * vn[2];
+            if (n == 0 || m > vmax) vmax = m;
+        }
+        vmax = sqrt(vmax);
+        s->rmax = s->rmax + vmax * s->delta_t;
+        if (s->rmax > 0.5 * dmin) rebuild = 1;
+    } else if (s->rebuild_criteria == 1) { /* :101-103 */
+        if ((s->iter % s->fixed_rebuild) == 0) rebuild = 1;
+    } else { /* :105-121 */
+        if (!s->rdisp) s->rdisp = (double *)xcalloc(3 * (size_t)s->np, sizeof(double));
+        for (int n = 0; n < s->np; n++) {
+            int hit = 0;
+            for (int k = 0; k < 3; k++) {
+                size_t q = 3 * (size_t)n + k;
+                s->rdisp[q] = s->rdisp[q] + s->v[q] * s->delta_t;
+                if (fabs(s->rdisp[q]) > 0.5 * dmin) hit = 1;
+            }
+            if (hit) { rebuild = 1; break; }
+        }
+    }
+    if (rebuild) {
+        s->rmax = 0.0;
+        if (s->rebuild_criteria == 2 && s->rdisp) memset(s->rdisp, 0, sizeof(double) * 3 * (size_t)s->np);
+        s->rebuild_count++;
+    }
+    return rebuild;
+}
+
+/* ------------------------------------------------------------------------ */
+/* periodic wrap on rebuild (messenger.serial.f90:961-1028, in place)        */
+/* ------------------------------------------------------------------------ */
+
+void orc_sendmols(orc *s)
+{
+    for (int n = 0; n < s->np; n++)
+        for (int k = 0; k < 3; k++) {
+            size_t q = 3 * (size_t)n + k;
+            if (s->r[q] >= s->halfdomain[k]) s->r[q] = s->r[q] - s->domain[k];
+            if (s->r[q] < -s->halfdomain[k]) s->r[q] = s->r[q] + s->domain[k];
+        }
+}
+
+/* ------------------------------------------------------------------------ */
+/* record (simulation_record.f90:1205-1314)                                  */
+/* ------------------------------------------------------------------------ */
+
+void orc_evaluate_macroscopic_properties(orc *s)
+{
+    double vsum = 0.0, mv2sum = 0.0, pes = 0.0, vir = 0.0;
+    for (int n = 0; n < s->np; n++) pes = pes + s->potenergymol[n];
+    for (int n = 0; n < s->np; n++)
+        for (int k = 0; k < 3; k++) {
+            size_t q = 3 * (size_t)n + k;
+            double vel = s->v[q];
+            if (s->integration_algorithm == 0) vel = s->v[q] + 0.5 * s->a[q] * s->delta_t;
+            vsum = vsum + 1.0 * vel;
+            mv2sum = mv2sum + 1.0 * (vel * vel);
+        }
+    for (int n = 0; n < s->np; n++) vir = vir + s->virialmol[n];
+    double gnp = (double)s->globalnp;
+    s->vsum = vsum; s->mv2sum = mv2sum; s->potenergysum = pes; s->virial = vir;
+    s->kinenergy = (0.5 * mv2sum) / gnp;
+    s->potenergy = (0.5 * pes) / gnp + s->potential_sLRC;
+    s->totenergy = s->kinenergy + s->potenergy;
+    s->temperature = mv2sum / (3.0 * gnp);
+    s->pressure = (s->density / (gnp * 3.0)) * (mv2sum + vir / 2.0) + s->pressure_sLRC;
+}
+
+/* ------------------------------------------------------------------------ */
+/* driver (md.f90 setup_MD and md_advance_vv)                                */
+/* ------------------------------------------------------------------------ */
+
+/* setup: assign_to_cell, messenger_updateborders(1), assign_to_neighbourlist,
+ * then the initial force + record (setup_initial_record.f90:88-89). */
+int orc_setup(orc *s)
+{
+    int rc;
+    orc_linklist_deallocateall(s);
+    if (s->force_list != 0) {
+        if ((rc = orc_assign_to_cell(s))) return rc;
+        if ((rc = orc_updateborders(s, 1))) return rc;
+        if ((rc = orc_assign_to_neighbourlist(s))) return rc;
+    }
+    if ((rc = orc_compute_forces(s))) return rc;
+    if ((s->iter % s->tplot) == 0) orc_evaluate_macroscopic_properties(s);
+    return ORC_OK;
+}
+
+/* rebuild sequence (md.f90:150-157) with sort_mols disabled (SORT_FLAG 0). */
+int orc_rebuild(orc *s)
+{
+    int rc;
+    orc_linklist_deallocateall(s);
+    orc_sendmols(s);
+    if (s->force_list == 0) return ORC_OK;
+    if ((rc = orc_assign_to_cell(s))) return rc;
+    if ((rc = orc_updateborders(s, 1))) return rc;
+    return orc_assign_to_neighbourlist(s);
+}
+
+/* md_advance_vv (md.f90:143-163) for nsteps iterations; the record callback
+ * is replaced by storing the macroscopic properties of every tplot step into
+ * rec_out (9 doubles per record, see orc_macro) when non-null. */
+int orc_run_vv(orc *s, int nsteps, double *rec_out, int rec_cap, int *nrec)
+{
+    int rc;
+    *nrec = 0;
+    for (int st = 0; st < nsteps; st++) {
+        s->iter += 1;
+        orc_move_vv(s, 1);
+        if (s->force_list != 0 && (rc = orc_updateborders(s, 0))) return rc;
+        int rebuild = orc_checkrebuild(s);
+        if (rebuild && (rc = orc_rebuild(s))) return rc;
+        if ((rc = orc_compute_forces(s))) return rc;
+        orc_move_vv(s, 2);
+        if ((s->iter % s->tplot) == 0) {
+            orc_evaluate_macroscopic_properties(s);
+            if (rec_out && *nrec < rec_cap) {
+                double *o = &rec_out[10 * (size_t)(*nrec)];
+                o[0] = (double)s->iter;
+                orc_macro(s, o + 1);
+            }
+            (*nrec)++;
+        }
+    }
+    return ORC_OK;
+}
+
+/* Polymer metadata upload: chainID, subchainID, funcy, bin_bflag(4). */
+void orc_set_monomers(orc *s, const int *chain, const int *subchain, const int *funcy, const int *bflag)
+{
+    for (int n = 0; n < s->np; n++) {
+        s->chainID[n] = chain[n];
+        s->subchainID[n] = subchain[n];
+        s->funcy[n] = funcy[n];
+        for (int b = 0; b < 4; b++) s->bflag[4 * (size_t)n + b] = bflag[4 * (size_t)n + b];
+    }
+}

@@ -1,0 +1,251 @@
+"""ctypes wrapper over the CPU FP64 oracle (fm_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by ``__graft_entry__.smoke()``
+and by bench.py's CPU-baseline leg, and never by the product package.  Parity
+status: see the header of fm_oracle.c (geometry and restart format pinned by
+reference fixtures; forces and pair lists restated from the Fortran but
+unpinned by reference outputs).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "libfm_oracle.so")
+_lib = None
+
+ORC_ERRORS = {1: "allocation", 2: "escaped molecule", 3: "fewer than 3 cells",
+              4: "polymer bond error", 5: "bad parameter"}
+
+
+def build() -> str:
+    """Compiles the oracle with its Makefile (no-op when up to date)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB) or os.path.getmtime(_LIB) < os.path.getmtime(
+                os.path.join(_HERE, "fm_oracle.c")):
+            build()
+        L = C.CDLL(_LIB)
+        d3 = C.POINTER(C.c_double)
+        i3 = C.POINTER(C.c_int)
+        L.orc_create.restype = C.c_void_p
+        L.orc_create.argtypes = [C.c_int, d3, C.c_double, d3, C.c_double, C.c_int, C.c_int, C.c_int,
+                                 C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int, i3]
+        L.orc_free.argtypes = [C.c_void_p]
+        for name in ("orc_r", "orc_v", "orc_a", "orc_potenergymol", "orc_virialmol"):
+            getattr(L, name).restype = d3
+            getattr(L, name).argtypes = [C.c_void_p]
+        L.orc_glob_no.restype = i3
+        L.orc_glob_no.argtypes = [C.c_void_p]
+        for name in ("orc_np", "orc_halo_np", "orc_iter", "orc_rebuild_count", "orc_setup",
+                     "orc_rebuild", "orc_compute_forces", "orc_assign_to_cell",
+                     "orc_assign_to_neighbourlist", "orc_checkrebuild"):
+            getattr(L, name).restype = C.c_int
+            getattr(L, name).argtypes = [C.c_void_p]
+        L.orc_updateborders.restype = C.c_int
+        L.orc_updateborders.argtypes = [C.c_void_p, C.c_int]
+        L.orc_set_iter.argtypes = [C.c_void_p, C.c_int]
+        L.orc_set_integration_algorithm.argtypes = [C.c_void_p, C.c_int]
+        L.orc_rmax.restype = C.c_double
+        L.orc_rmax.argtypes = [C.c_void_p]
+        L.orc_move_vv.argtypes = [C.c_void_p, C.c_int]
+        L.orc_move_lfv.argtypes = [C.c_void_p]
+        L.orc_sendmols.argtypes = [C.c_void_p]
+        L.orc_linklist_deallocateall.argtypes = [C.c_void_p]
+        L.orc_evaluate_macroscopic_properties.argtypes = [C.c_void_p]
+        L.orc_macro.argtypes = [C.c_void_p, d3]
+        L.orc_geometry.argtypes = [C.c_void_p, i3, d3, d3, d3, d3]
+        L.orc_pair_list.restype = C.c_long
+        L.orc_pair_list.argtypes = [C.c_void_p, i3, i3, i3, C.c_long]
+        L.orc_list_length.restype = C.c_long
+        L.orc_list_length.argtypes = [C.c_void_p]
+        L.orc_run_vv.restype = C.c_int
+        L.orc_run_vv.argtypes = [C.c_void_p, C.c_int, d3, C.c_int, i3]
+        L.orc_global_domain.argtypes = [i3, C.c_double, d3, d3, d3]
+        L.orc_set_parameters_cells.restype = C.c_int
+        L.orc_set_parameters_cells.argtypes = [d3, C.c_double, d3, C.c_int, C.c_double, i3, d3, d3]
+        L.orc_lj_accijmag.restype = C.c_double
+        L.orc_lj_accijmag.argtypes = [C.c_double]
+        L.orc_lj_energy.restype = C.c_double
+        L.orc_lj_energy.argtypes = [C.c_double, C.c_double]
+        L.orc_potshift.restype = C.c_double
+        L.orc_potshift.argtypes = [C.c_double]
+        L.orc_set_monomers.argtypes = [C.c_void_p, i3, i3, i3, i3]
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _ip(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+class OracleError(RuntimeError):
+    pass
+
+
+def _check(rc):
+    if rc:
+        raise OracleError(ORC_ERRORS.get(rc, f"error {rc}"))
+
+
+def global_domain(nunits, density):
+    n = np.ascontiguousarray(nunits, dtype=np.int32)
+    dom = np.zeros(3); unit = np.zeros(3); vol = np.zeros(1)
+    lib().orc_global_domain(_ip(n), float(density), _dp(dom), _dp(unit), _dp(vol))
+    return dom, unit, float(vol[0])
+
+
+def cells(domain, rcutoff, delta, potential_flag=0, R_0=1.5):
+    d = np.ascontiguousarray(domain, dtype=np.float64)
+    dl = np.ascontiguousarray(delta, dtype=np.float64)
+    nc = np.zeros(3, np.int32); cs = np.zeros(3); rn2 = np.zeros(1)
+    rc = lib().orc_set_parameters_cells(_dp(d), float(rcutoff), _dp(dl), int(potential_flag), float(R_0),
+                                        _ip(nc), _dp(cs), _dp(rn2))
+    return rc, nc, cs, float(rn2[0])
+
+
+class Oracle:
+    """One FP64 CPU simulation state (single rank, fully periodic)."""
+
+    def __init__(self, r, v, domain, rcutoff, delta_rneighbr=(0.3, 0.3, 0.3), delta_t=0.005,
+                 tplot=100, force_list=3, potential_flag=0, k_c=30.0, R_0=1.5,
+                 rebuild_criteria=0, fixed_rebuild=1, density=None, sLRC_flag=0, iter0=0,
+                 integration_algorithm=1):
+        r = np.asarray(r, dtype=np.float64)
+        v = np.asarray(v, dtype=np.float64)
+        self.np_ = r.shape[0]
+        dom = np.ascontiguousarray(domain, dtype=np.float64)
+        dl = np.ascontiguousarray(delta_rneighbr, dtype=np.float64)
+        if density is None:
+            density = self.np_ / float(np.prod(dom))
+        err = C.c_int(0)
+        L = lib()
+        self.h = L.orc_create(self.np_, _dp(dom), float(rcutoff), _dp(dl), float(delta_t), int(tplot),
+                              int(force_list), int(potential_flag), float(k_c), float(R_0),
+                              int(rebuild_criteria), int(fixed_rebuild), float(density), int(sLRC_flag),
+                              C.byref(err))
+        if not self.h:
+            _check(err.value or 1)
+        self.domain = dom
+        self._r = np.ctypeslib.as_array(L.orc_r(self.h), shape=(self.np_ * 8 + 1024, 3))
+        self._v = np.ctypeslib.as_array(L.orc_v(self.h), shape=(self.np_ * 8 + 1024, 3))
+        self._a = np.ctypeslib.as_array(L.orc_a(self.h), shape=(self.np_ * 8 + 1024, 3))
+        self._r[:self.np_] = r
+        self._v[:self.np_] = v
+        L.orc_set_iter(self.h, int(iter0))
+        L.orc_set_integration_algorithm(self.h, int(integration_algorithm))
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            lib().orc_free(h)
+            self.h = None
+
+    # --- state ---
+    @property
+    def r(self):
+        return self._r[:self.np_].copy()
+
+    @property
+    def v(self):
+        return self._v[:self.np_].copy()
+
+    @property
+    def a(self):
+        return self._a[:self.np_].copy()
+
+    def set_state(self, r=None, v=None, a=None):
+        if r is not None:
+            self._r[:self.np_] = r
+        if v is not None:
+            self._v[:self.np_] = v
+        if a is not None:
+            self._a[:self.np_] = a
+
+    def set_monomers(self, chain, subchain, funcy, bflag):
+        c = np.ascontiguousarray(chain, np.int32)
+        s = np.ascontiguousarray(subchain, np.int32)
+        f = np.ascontiguousarray(funcy, np.int32)
+        b = np.ascontiguousarray(bflag, np.int32).reshape(-1)
+        lib().orc_set_monomers(self.h, _ip(c), _ip(s), _ip(f), _ip(b))
+
+    @property
+    def potenergymol(self):
+        return np.ctypeslib.as_array(lib().orc_potenergymol(self.h), shape=(self.np_,)).copy()
+
+    @property
+    def virialmol(self):
+        return np.ctypeslib.as_array(lib().orc_virialmol(self.h), shape=(self.np_,)).copy()
+
+    @property
+    def iter(self):
+        return lib().orc_iter(self.h)
+
+    @property
+    def halo_np(self):
+        return lib().orc_halo_np(self.h)
+
+    @property
+    def rebuild_count(self):
+        return lib().orc_rebuild_count(self.h)
+
+    def geometry(self):
+        nc = np.zeros(3, np.int32); cs = np.zeros(3)
+        rn2 = np.zeros(1); rc2 = np.zeros(1); ps = np.zeros(1)
+        lib().orc_geometry(self.h, _ip(nc), _dp(cs), _dp(rn2), _dp(rc2), _dp(ps))
+        return dict(ncells=nc, cellside=cs, rneighbr2=float(rn2[0]), rcutoff2=float(rc2[0]),
+                    potshift=float(ps[0]))
+
+    # --- subroutines ---
+    def setup(self):
+        _check(lib().orc_setup(self.h))
+
+    def rebuild(self):
+        _check(lib().orc_rebuild(self.h))
+
+    def compute_forces(self):
+        _check(lib().orc_compute_forces(self.h))
+
+    def move_vv(self, pass_num):
+        lib().orc_move_vv(self.h, int(pass_num))
+
+    def checkrebuild(self):
+        return lib().orc_checkrebuild(self.h)
+
+    def macro(self):
+        o = np.zeros(9)
+        lib().orc_macro(self.h, _dp(o))
+        keys = ("vsum", "mv2sum", "temperature", "kinenergy", "potenergy", "totenergy", "pressure",
+                "virial", "potenergysum")
+        return dict(zip(keys, o.tolist()))
+
+    def evaluate_macroscopic_properties(self):
+        lib().orc_evaluate_macroscopic_properties(self.h)
+        return self.macro()
+
+    def run_vv(self, nsteps, rec_cap=100000):
+        out = np.zeros((rec_cap, 10))
+        nrec = C.c_int(0)
+        _check(lib().orc_run_vv(self.h, int(nsteps), _dp(out), rec_cap, C.byref(nrec)))
+        return out[:min(nrec.value, rec_cap)]
+
+    def pair_list(self):
+        """(owner, partner, code) arrays, 1-based glob_no; code 13 = no image."""
+        n = lib().orc_list_length(self.h)
+        o = np.zeros(n, np.int32); p = np.zeros(n, np.int32); c = np.zeros(n, np.int32)
+        m = lib().orc_pair_list(self.h, _ip(o), _ip(p), _ip(c), n)
+        assert m == n
+        return o, p, c

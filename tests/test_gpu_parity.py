@@ -1,0 +1,225 @@
+"""Parity of the CUDA path (through the C ABI) with the FP64 CPU oracle.
+
+Tolerances:
+  * pair sets: bit-exact (FP64 distance test, no FMA, same image roundings);
+  * FP64 forces: |F_gpu - F_ref| <= 1e-12 * max(|F_ref|, 1), per molecule;
+  * FP32 pair forces: |F_gpu - F_ref| <= 1e-5 * max(|F_ref|, F_FLOOR32), per
+    molecule, F_FLOOR32 = 10 (the magnitude of one nearest-neighbour pair
+    force in the liquid; below it the relative error of a near-cancelling sum
+    is not meaningful);
+  * per-molecule PE and virial: 1e-12 (FP64) / 1e-5 (FP32) relative with a
+    floor of 1.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from flowmol_b200 import api, lattice
+from helpers import (WCA_RC, canonical_full, canonical_oracle, cfg1_state, digest_oracle, liquid_state,
+                     rel_err)
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+TOL32 = 1e-5
+F_FLOOR32 = 10.0
+
+
+def gpu_system(r, v, dom, rc, precision=0, tplot=10 ** 6, density=None, **kw):
+    p = api.make_params(len(r), dom, rc, tplot=tplot, precision=precision,
+                        density=density if density is not None else len(r) / float(np.prod(dom)), **kw)
+    s = api.MDSystem(p)
+    s.upload(r, v)
+    return s
+
+
+@pytest.fixture(scope="module")
+def liquid(gpu_lib):
+    # LJ rc 2.5 liquid at the large-config density, 2048 molecules, oracle-equilibrated
+    r, v, dom, o = liquid_state([8, 8, 8], 0.8442, 0.722, 2.5, steps=150)
+    return r, v, dom
+
+
+def test_cfg1_fcc_kat(gpu_lib):
+    r, v, dom = cfg1_state()
+    s = gpu_system(r, v, dom, WCA_RC, tplot=100)
+    s.setup()
+    _, _, a, _ = s.download()
+    assert np.all(a == 0.0), "FCC first shell lies beyond the WCA cutoff: forces must be exactly zero"
+    pe, vir = s.per_molecule()
+    assert np.all(pe == 0.0) and np.all(vir == 0.0)
+    own, par, code = s.pair_list()
+    assert np.all(np.bincount(own, minlength=len(r) + 1)[1:] == 12)
+    o = O.Oracle(r, v, dom, WCA_RC, tplot=100)
+    o.setup()
+    assert np.array_equal(canonical_full(own, par, code), canonical_oracle(*o.pair_list()))
+
+
+def test_pairs_forces_energies_fp64(liquid):
+    r, v, dom = liquid
+    o = O.Oracle(r, v, dom, 2.5, tplot=1, density=0.8442)
+    o.setup()
+    s = gpu_system(r, v, dom, 2.5, tplot=1, density=0.8442)
+    s.setup()
+    assert np.array_equal(canonical_full(*s.pair_list()), canonical_oracle(*o.pair_list()))
+    _, _, a, _ = s.download()
+    assert rel_err(a, o.a, 1.0).max() <= TOL64
+    pe, vir = s.per_molecule()
+    np.testing.assert_allclose(pe, o.potenergymol, rtol=TOL64, atol=TOL64)
+    np.testing.assert_allclose(vir, o.virialmol, rtol=TOL64, atol=TOL64)
+    m = s.records()[-1]
+    mo = o.macro()
+    for k in ("kinenergy", "potenergy", "pressure", "temperature", "virial"):
+        assert m[k] == pytest.approx(mo[k], rel=1e-12, abs=1e-12), k
+
+
+def test_fp32_forces_within_tolerance(liquid):
+    r, v, dom = liquid
+    o = O.Oracle(r, v, dom, 2.5, tplot=1, density=0.8442)
+    o.setup()
+    s = gpu_system(r, v, dom, 2.5, precision=api.PRECISION_FP32, tplot=1, density=0.8442)
+    s.setup()
+    assert np.array_equal(canonical_full(*s.pair_list()), canonical_oracle(*o.pair_list()))
+    _, _, a, _ = s.download()
+    err = rel_err(a, o.a, F_FLOOR32)
+    assert err.max() <= TOL32, err.max()
+    pe, vir = s.per_molecule()
+    assert (np.abs(pe - o.potenergymol) / np.maximum(np.abs(o.potenergymol), 1.0)).max() <= TOL32
+    assert (np.abs(vir - o.virialmol) / np.maximum(np.abs(o.virialmol), 1.0)).max() <= TOL32
+
+
+def test_trajectory_fp64_follows_oracle(liquid):
+    r, v, dom = liquid
+    nsteps, tplot = 300, 50
+    o = O.Oracle(r, v, dom, 2.5, tplot=tplot, density=0.8442)
+    o.setup()
+    recs_o = o.run_vv(nsteps)
+    s = gpu_system(r, v, dom, 2.5, tplot=tplot, density=0.8442)
+    s.setup()
+    s.records()
+    s.simulation_md(nsteps)
+    recs = s.records()
+    assert len(recs) == len(recs_o)
+    assert s.counters()["rebuilds"] == o.rebuild_count
+    for row, ro in zip(recs, recs_o):
+        assert row["iter"] == int(ro[0])
+        assert row["totenergy"] == pytest.approx(ro[6], rel=1e-10)
+        assert row["pressure"] == pytest.approx(ro[7], rel=1e-9)
+    rg, vg, _, _ = s.download()
+    np.testing.assert_allclose(rg, o.r, rtol=0, atol=1e-8)
+    np.testing.assert_allclose(vg, o.v, rtol=0, atol=1e-8)
+
+
+def test_subroutine_path_equals_fused_loop(liquid):
+    """md_advance_vv called subroutine by subroutine through the C ABI gives
+    bit-identical state to the fused device loop."""
+    r, v, dom = liquid
+    a_sys = gpu_system(r, v, dom, 2.5, tplot=40, density=0.8442)
+    a_sys.setup()
+    for _ in range(60):
+        a_sys.md_advance_vv()
+    b_sys = gpu_system(r, v, dom, 2.5, tplot=40, density=0.8442)
+    b_sys.setup()
+    b_sys.simulation_md(60)
+    ra, va, aa, _ = a_sys.download()
+    rb, vb, ab, _ = b_sys.download()
+    assert np.array_equal(ra, rb) and np.array_equal(va, vb) and np.array_equal(aa, ab)
+    assert a_sys.counters()["rebuilds"] == b_sys.counters()["rebuilds"]
+
+
+def test_all_pairs_matches_oracle(gpu_lib):
+    r, v, dom = lattice.lj_fluid([3, 3, 3], 0.8, 1.0, 7)
+    r = lattice.jitter(r, 0.08, 7, dom)
+    o = O.Oracle(r, v, dom, 2.5, force_list=0, tplot=1)
+    o.setup()
+    s = gpu_system(r, v, dom, 2.5, force_list=0, tplot=1)
+    s.setup()
+    _, _, a, _ = s.download()
+    assert rel_err(a, o.a, 1.0).max() <= TOL64
+    recs_o = o.run_vv(100)
+    s.simulation_md(100)
+    rg, _, _, _ = s.download()
+    np.testing.assert_allclose(rg, o.r, rtol=0, atol=1e-9)
+
+
+def test_nlist_overflow_is_resized_and_resumed(liquid):
+    r, v, dom = liquid
+    ref = gpu_system(r, v, dom, 2.5, tplot=25, density=0.8442)
+    ref.setup()
+    ref.simulation_md(80)
+    small = gpu_system(r, v, dom, 2.5, tplot=25, density=0.8442, nlist_capacity=8)
+    small.setup()
+    small.simulation_md(80)
+    assert small.counters()["nlist_capacity"] > 8
+    r1, v1, _, _ = ref.download()
+    r2, v2, _, _ = small.download()
+    assert np.array_equal(r1, r2) and np.array_equal(v1, v2)
+
+
+def test_escaped_molecule_is_an_error_code(gpu_lib):
+    r, v, dom = cfg1_state()
+    r = r.copy()
+    r[5] = [3.0 * dom[0], 0.0, 0.0]
+    s = gpu_system(r, v, dom, WCA_RC)
+    with pytest.raises(api.FlowmolError) as e:
+        s.setup()
+    assert e.value.code == 4
+
+
+def test_molecules_on_the_box_faces(gpu_lib):
+    """Molecules exactly at -L/2 bin into the low halo cell (reference
+    ceiling rule); the pair set still matches the oracle bit for bit."""
+    r, v, dom = cfg1_state()
+    r = r.copy()
+    r[0, 0] = -dom[0] / 2
+    r[1, 1] = -dom[1] / 2
+    r[2, 2] = -dom[2] / 2
+    o = O.Oracle(r, v, dom, WCA_RC, tplot=10 ** 6)
+    o.setup()
+    s = gpu_system(r, v, dom, WCA_RC)
+    s.setup()
+    assert np.array_equal(canonical_full(*s.pair_list()), canonical_oracle(*o.pair_list()))
+
+
+def test_cutoff_edge_ulps(gpu_lib):
+    """Pairs one ulp either side of rneighbr and rcutoff are classified like
+    the FP64 reference (strict `<`)."""
+    L = 20.0
+    rc = 2.5
+    rn = rc + 0.3
+    xs = []
+    for base in (rc, rn):
+        for d in (np.nextafter(base, 0.0), base, np.nextafter(base, 10.0)):
+            xs.append(d)
+    rows = []
+    for k, d in enumerate(xs):
+        y = -8.0 + 2.9 * k
+        rows += [[-d / 2, y, 0.0], [d / 2, y, 0.0]]
+    r = np.array(rows)
+    v = np.zeros_like(r)
+    o = O.Oracle(r, v, [L, L, L], rc, tplot=1)
+    o.setup()
+    s = gpu_system(r, v, [L, L, L], rc, tplot=1)
+    s.setup()
+    assert np.array_equal(canonical_full(*s.pair_list()), canonical_oracle(*o.pair_list()))
+    _, _, a, _ = s.download()
+    assert np.array_equal(a, o.a)
+
+
+def test_large_system_pair_digest_and_forces(gpu_lib):
+    """1,048,576 molecules (FCC 64^3, rho 0.8442, rc 2.5): the pair-set digest
+    equals the oracle's, and FP64 forces agree within 1e-12."""
+    r, v, dom = lattice.lj_fluid([64, 64, 64], 0.8442, 0.722, lattice.SEED_BASE + 2)
+    r = lattice.jitter(r, 0.04, 11, dom)
+    o = O.Oracle(r, v, dom, 2.5, tplot=1, density=0.8442)
+    o.setup()
+    dig_o = digest_oracle(*o.pair_list())
+    s = gpu_system(r, v, dom, 2.5, tplot=1, density=0.8442)
+    s.setup()
+    assert s.pair_digest() == dig_o
+    _, _, a, _ = s.download()
+    assert rel_err(a, o.a, 1.0).max() <= TOL64
+    s32 = gpu_system(r, v, dom, 2.5, tplot=1, density=0.8442, precision=api.PRECISION_FP32)
+    s32.setup()
+    _, _, a32, _ = s32.download()
+    assert rel_err(a32, o.a, F_FLOOR32).max() <= TOL32
