@@ -13,7 +13,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libflowmol_b200.so")
-SOURCES = ["fm_kernels.cu", "fm_api.cu"]
+SOURCES = ["fm_kernels.cu", "fm_api.cu", "fm_noalloc.cu"]
 HEADERS = ["fm_common.cuh"]
 
 NVCC_FLAGS = [

@@ -217,6 +217,28 @@ FM_API int fm_get_force_kernel_time(fm_handle *h, double *ms, int64_t *launches)
 /* Kernels this handle has launched since creation. */
 FM_API int fm_get_launch_count(fm_handle *h, int64_t *launches);
 
+/* ---- forces without device allocation -------------------------------- */
+/* No counterpart in the reference (Flowmol always owns its arrays).  For
+ * callers that cannot call cudaMalloc -- a host code whose device memory is
+ * all handed out by its own pool or framework, or a loop that must not take
+ * the device-wide synchronisation an allocation can imply -- this computes
+ * the same LJ forces, per-molecule PE and virial as fm_setup/fm_compute_forces
+ * for positions already on the device, without allocating: its scratch is one
+ * fixed __device__ array (about 3 MB, resident on every GPU that loads the
+ * library until exit) shared by all calls.  d_r, d_a are (3, n) column-major
+ * FP64 device arrays; d_potenergymol and d_virialmol (n) may be NULL.  Uses
+ * p->domain, rcutoff, delta_rneighbr, precision.  Limits: n <=
+ * FM_NOALLOC_MAX_MOLECULES and (ncells+2)^3 <= FM_NOALLOC_MAX_CELLS, else
+ * FM_ERR_ARG.  The first call on a device looks up the array's device
+ * address, so make it before any stream capture.  Calls that overlap on the
+ * GPU race on the shared scratch.  Blocks until the stream has drained. */
+#define FM_NOALLOC_MAX_MOLECULES 65536
+#define FM_NOALLOC_MAX_CELLS 32768
+FM_API int fm_compute_forces_noalloc(const fm_params *p, int32_t n, const double *d_r, double *d_a,
+                                     double *d_potenergymol, double *d_virialmol, void *cuda_stream);
+/* Message of the last failing fm_compute_forces_noalloc call on this thread. */
+FM_API int fm_noalloc_last_error(char *buf, int32_t len);
+
 /* ---- errors --------------------------------------------------------- */
 /* Copies the message of the last failing call on this thread. */
 FM_API int fm_last_error(char *buf, int32_t len);
