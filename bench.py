@@ -215,6 +215,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--profile-case", choices=["fp32", "fp64"], default=None,
+                    help="profiling workload: setup + 10 fused steps of the 1M system, no timing")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -243,6 +245,17 @@ def main():
     fb.build()
     dev = local
     torch.cuda.set_device(dev)
+    if args.profile_case:
+        r, v, dom = make_state()
+        prec = api.PRECISION_FP32 if args.profile_case == "fp32" else api.PRECISION_FP64
+        p = api.make_params(len(r), dom, RC, (SKIN,) * 3, DT, TPLOT, density=DENSITY, precision=prec)
+        s = api.MDSystem(p)
+        s.upload(r, v)
+        s.setup()
+        s.simulation_md(10, blocking=True)
+        print(json.dumps({"profile_case": args.profile_case, "molecules": len(r), **s.counters()}))
+        s.close()
+        return
     dist = None
     if world > 1:
         import datetime

@@ -81,6 +81,7 @@ struct fm_handle {
     std::vector<cudaEvent_t> ev;
     size_t ev_used = 0;
     int64_t launches = 0;
+    int expected_nbr = 0;  // (4/3) pi r_n^3 rho, rounded: the autotuner's key
 };
 
 // ---------------------------------------------------------------------------
@@ -147,7 +148,7 @@ static void release(fm_handle *h)
     h->ev.clear();
     FmDev &d = h->d;
     void *ptrs[] = {d.pos0, d.pos1, d.vx, d.vy, d.vz, d.ax, d.ay, d.az, d.slot_of, d.tvx, d.tvy, d.tvz,
-                    d.tax, d.tay, d.taz, d.cell_of, d.cell_count, d.cell_start, d.perm, d.nbr, d.nnbr,
+                    d.tax, d.tay, d.taz, d.cell_of, d.cell_count, d.cell_start, d.perm, d.tile_sum, d.nbr, d.nnbr,
                     d.pe, d.vir, d.partial, d.rec, d.sc, h->tpos, h->tuidx, h->glob, h->stage3};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -175,6 +176,7 @@ static int round_up(int x, int m) { return ((x + m - 1) / m) * m; }
 static int alloc_nlist(fm_handle *h, int maxn)
 {
     FmDev &d = h->d;
+    maxn = round_up(std::max(maxn, 8), 8);  // 16-byte aligned rows for the vector reads
     if (d.nbr) cudaFree(d.nbr);
     d.nbr = nullptr;
     d.maxn = maxn;
@@ -239,6 +241,7 @@ extern "C" int fm_create(const fm_params *p, fm_handle **out)
     int tpm = pick_tpm(*p, expected);
     if (tpm < 0) { delete h; return fail(FM_ERR_ARG, "threads_per_molecule must be 0, 1, 2, 4, 8 or 16"); }
     h->tpm = tpm;
+    h->expected_nbr = (int)std::lround(expected);
     int maxn = p->nlist_capacity > 0 ? p->nlist_capacity : round_up((int)std::ceil(1.3 * expected) + 16, 8);
 
     const size_t n = (size_t)d.n;
@@ -253,6 +256,7 @@ extern "C" int fm_create(const fm_params *p, fm_handle **out)
     FM_ALLOC(d.slot_of, n) FM_ALLOC(h->tuidx, n) FM_ALLOC(h->tpos, n) FM_ALLOC(h->glob, n)
     FM_ALLOC(d.cell_of, n) FM_ALLOC(d.perm, n) FM_ALLOC(d.nnbr, n)
     FM_ALLOC(d.cell_count, d.ncell) FM_ALLOC(d.cell_start, d.ncell + 1)
+    FM_ALLOC(d.tile_sum, fm::scan_tiles(d.ncell))
     FM_ALLOC(d.pe, n) FM_ALLOC(d.vir, n)
     FM_ALLOC(h->stage3, 9 * n)
     int nb = std::max(std::max(fm::force_blocks(d.n, 16), fm::all_pairs_blocks(d.n)), fm::macro_blocks(d.n));
@@ -450,7 +454,7 @@ static void queue_cells(fm_handle *h, int wrap, int gated)
     fm::launch_scan_cells(d, gated, h->st);
     fm::launch_scatter(d, gated, h->st);
     fm::launch_reorder(d, gated, h->tpos, h->tuidx, h->st);
-    h->launches += 6;
+    h->launches += 7;
 }
 
 static cudaEvent_t next_event(fm_handle *h)
@@ -490,6 +494,57 @@ static void queue_record(fm_handle *h, int iter, double simtime)
     h->launches += 1;
 }
 
+// Threads-per-molecule autotuner: times the force kernel (forces only, no
+// record) for TPM in {1, 2, 4, 8, 16} on the freshly built list and keeps the
+// fastest.  The choice is cached per (np, expected neighbours, precision) for
+// the process -- never per list capacity, which grows on overflow -- so handles
+// created with equal parameters run identical kernels and give bit-identical
+// results.
+#include <map>
+#include <mutex>
+#include <tuple>
+static std::mutex g_tune_mutex;
+static std::map<std::tuple<int, int, int>, int> g_tune_cache;
+
+static int autotune_tpm(fm_handle *h)
+{
+    if (h->p.threads_per_molecule > 0 || h->p.force_list == 0) return FM_OK;
+    const auto key = std::make_tuple(h->d.n, h->expected_nbr, h->d.precision);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mutex);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            h->tpm = it->second;
+            h->d.nblocks_force = fm::force_blocks(h->d.n, h->tpm);
+            return FM_OK;
+        }
+    }
+    cudaEvent_t e0, e1;
+    FM_CUDA(cudaEventCreate(&e0));
+    FM_CUDA(cudaEventCreate(&e1));
+    const int cands[5] = {1, 2, 4, 8, 16};
+    float best = 1e30f;
+    int best_tpm = h->tpm;
+    for (int t : cands) {
+        fm::launch_force(h->d, 0, 0, t, h->st);  // warm-up
+        cudaEventRecord(e0, h->st);
+        for (int rep = 0; rep < 3; rep++) fm::launch_force(h->d, 0, 0, t, h->st);
+        cudaEventRecord(e1, h->st);
+        cudaError_t err = cudaEventSynchronize(e1);
+        float ms = 0.f;
+        if (err == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+        if (err == cudaSuccess && ms < best) { best = ms; best_tpm = t; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    FM_CUDA(cudaGetLastError());
+    h->tpm = best_tpm;
+    h->d.nblocks_force = fm::force_blocks(h->d.n, h->tpm);
+    std::lock_guard<std::mutex> lk(g_tune_mutex);
+    g_tune_cache[key] = best_tpm;
+    return FM_OK;
+}
+
 extern "C" int fm_setup(fm_handle *h)
 {
     if (!h) return fail(FM_ERR_ARG, "null handle");
@@ -498,18 +553,20 @@ extern "C" int fm_setup(fm_handle *h)
         queue_cells(h, 0, 0);
         fm::launch_build_nlist(h->d, 0, h->iter, h->st);
     }
-    const int record = (h->iter % h->p.tplot) == 0;
-    queue_force(h, record, 0);
-    if (record) queue_record(h, h->iter, h->simtime);
     FM_CUDA(cudaGetLastError());
     fm::FmScalars s;
     FM_TRY(read_scalars(h, &s));
     if (s.status & fm::ST_NLIST && !(s.status & (fm::ST_FATAL & ~fm::ST_NLIST))) {
         FM_TRY(grow_nlist(h, s, h->iter));
-        queue_force(h, record, 0);
-        if (record) queue_record(h, h->iter, h->simtime);
         FM_TRY(read_scalars(h, &s));
     }
+    FM_TRY(status_error(h, s));
+    FM_TRY(autotune_tpm(h));
+    const int record = (h->iter % h->p.tplot) == 0;
+    queue_force(h, record, 0);
+    if (record) queue_record(h, h->iter, h->simtime);
+    FM_CUDA(cudaGetLastError());
+    FM_TRY(read_scalars(h, &s));
     FM_TRY(status_error(h, s));
     h->has_pe = record;
     h->cells_valid = h->list_valid = h->p.force_list != 0;

@@ -70,6 +70,7 @@ struct FmDev {
     int32_t *cell_count;   // ncell
     int32_t *cell_start;   // ncell + 1
     int32_t *perm;         // new slot -> old slot
+    int32_t *tile_sum;     // per scan tile (4096 cells)
     // neighbour list: nbr[i*maxn + k] = j | (sx+1)<<26 | (sy+1)<<28 | (sz+1)<<30
     int32_t *nbr;
     int32_t *nnbr;
@@ -114,6 +115,7 @@ void launch_macro_partials(const FmDev &d, cudaStream_t st);
 int macro_blocks(int n);
 void launch_pair_digest(const FmDev &d, const int32_t *glob_of_upload, cudaStream_t st);
 int force_blocks(int n, int tpm);
+int scan_tiles(int ncell);
 int all_pairs_blocks(int n);
 // Layout conversion between the reference's (3,n) column-major arrays and
 // the device layout; `order` maps upload index -> slot.

@@ -11,6 +11,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "fm_common.cuh"
 
 namespace fm {
@@ -31,12 +33,13 @@ __device__ __forceinline__ double norm2_rn(double x, double y, double z)
     return __dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z));
 }
 
-// Read-only gather of x, y, z of a double4 (one 32-byte sector).
+// Read-only gather of one double4 (32-byte aligned) as a single 256-bit load:
+// one L1 request per partner instead of two.
 __device__ __forceinline__ double4 ldg_pos(const double4 *p)
 {
-    const double2 xy = __ldg(reinterpret_cast<const double2 *>(p));
-    const double z = __ldg(reinterpret_cast<const double *>(p) + 2);
-    return make_double4(xy.x, xy.y, z, 0.0);
+    double4 r;
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(r.x), "=d"(r.y), "=d"(r.z), "=d"(r.w) : "l"(p));
+    return r;
 }
 
 template <typename T>
@@ -186,87 +189,120 @@ __device__ __forceinline__ int bin_axis(double x, double hd, double cs, int ne, 
 __global__ void k_wrap_bin(FmDev d, int wrap, int bin, int gated, int iter)
 {
     if (!gate(d, gated)) return;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= d.n) return;
     double4 *P = cur_pos(d, d.sc->pset);
-    double4 p = P[i];
-    if (wrap) {
-        double4 q = p;
-        if (q.x >= d.hd[0]) q.x = __dsub_rn(q.x, d.L[0]);
-        if (q.x < -d.hd[0]) q.x = __dadd_rn(q.x, d.L[0]);
-        if (q.y >= d.hd[1]) q.y = __dsub_rn(q.y, d.L[1]);
-        if (q.y < -d.hd[1]) q.y = __dadd_rn(q.y, d.L[1]);
-        if (q.z >= d.hd[2]) q.z = __dsub_rn(q.z, d.L[2]);
-        if (q.z < -d.hd[2]) q.z = __dadd_rn(q.z, d.L[2]);
-        if (q.x != p.x || q.y != p.y || q.z != p.z) P[i] = q;
-        p = q;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < d.n; i += gridDim.x * blockDim.x) {
+        double4 p = P[i];
+        if (wrap) {
+            double4 q = p;
+            if (q.x >= d.hd[0]) q.x = __dsub_rn(q.x, d.L[0]);
+            if (q.x < -d.hd[0]) q.x = __dadd_rn(q.x, d.L[0]);
+            if (q.y >= d.hd[1]) q.y = __dsub_rn(q.y, d.L[1]);
+            if (q.y < -d.hd[1]) q.y = __dadd_rn(q.y, d.L[1]);
+            if (q.z >= d.hd[2]) q.z = __dsub_rn(q.z, d.L[2]);
+            if (q.z < -d.hd[2]) q.z = __dadd_rn(q.z, d.L[2]);
+            if (q.x != p.x || q.y != p.y || q.z != p.z) P[i] = q;
+            p = q;
+        }
+        if (!bin) continue;
+        bool bad = false;
+        int cx = bin_axis(p.x, d.hd[0], d.cs[0], d.ne[0], bad);
+        int cy = bin_axis(p.y, d.hd[1], d.cs[1], d.ne[1], bad);
+        int cz = bin_axis(p.z, d.hd[2], d.cs[2], d.ne[2], bad);
+        if (bad) {
+            raise_status(d, ST_ESCAPE, iter);
+            d.sc->escape_slot = i;
+        }
+        int c = cx + d.ne[0] * (cy + d.ne[1] * cz);
+        d.cell_of[i] = c;
+        atomicAdd(&d.cell_count[c], 1);
     }
-    if (!bin) return;
-    bool bad = false;
-    int cx = bin_axis(p.x, d.hd[0], d.cs[0], d.ne[0], bad);
-    int cy = bin_axis(p.y, d.hd[1], d.cs[1], d.ne[1], bad);
-    int cz = bin_axis(p.z, d.hd[2], d.cs[2], d.ne[2], bad);
-    if (bad) {
-        raise_status(d, ST_ESCAPE, iter);
-        d.sc->escape_slot = i;
-    }
-    int c = cx + d.ne[0] * (cy + d.ne[1] * cz);
-    d.cell_of[i] = c;
-    atomicAdd(&d.cell_count[c], 1);
 }
 
-// Exclusive scan of the per-cell counts in one block; the counts are zeroed
-// so the scatter can reuse them as cursors.
+// Exclusive scan of the per-cell counts in two parallel passes over tiles of
+// SCAN_TILE cells: tile sums, then each tile adds the sum of the tiles before
+// it and scans itself.  The counts are zeroed so the scatter can reuse them
+// as cursors.
 constexpr int SCAN_THREADS = 1024;
-__global__ void __launch_bounds__(SCAN_THREADS) k_scan_cells(FmDev d, int gated)
+constexpr int SCAN_PER = 4;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_PER;
+
+__device__ __forceinline__ int block_excl_scan(int v, int *total)
 {
-    if (!gate(d, gated)) return;
-    __shared__ int wsum[32];
-    const int nc = d.ncell;
-    const int per = (nc + SCAN_THREADS - 1) / SCAN_THREADS;
-    const int b = threadIdx.x * per;
-    const int e = min(b + per, nc);
-    int local = 0;
-    for (int c = b; c < e; c++) local += d.cell_count[c];
-    // block exclusive scan of `local`
+    __shared__ int ws[SCAN_THREADS / 32];
     int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    int incl = local;
+    int incl = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         int t = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= o) incl += t;
     }
-    if (lane == 31) wsum[w] = incl;
+    if (lane == 31) ws[w] = incl;
     __syncthreads();
     if (w == 0) {
-        int v = wsum[lane];
-        int vi = v;
+        int x = lane < SCAN_THREADS / 32 ? ws[lane] : 0, xi = x;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            int t = __shfl_up_sync(0xffffffffu, vi, o);
-            if (lane >= o) vi += t;
+            int t = __shfl_up_sync(0xffffffffu, xi, o);
+            if (lane >= o) xi += t;
         }
-        wsum[lane] = vi - v;
+        if (lane < SCAN_THREADS / 32) ws[lane] = xi - x;
+        if (lane == SCAN_THREADS / 32 - 1) ws[SCAN_THREADS / 32 - 1] = xi - x, *total = xi;
     }
     __syncthreads();
-    int run = wsum[w] + incl - local;
-    for (int c = b; c < e; c++) {
-        int k = d.cell_count[c];
-        d.cell_start[c] = run;
-        d.cell_count[c] = 0;
-        run += k;
+    return ws[w] + incl - v;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_tiles(FmDev d, int gated)
+{
+    if (!gate(d, gated)) return;
+    __shared__ int tot;
+    const int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_PER;
+    int local = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_PER; k++)
+        if (base + k < d.ncell) local += d.cell_count[base + k];
+    block_excl_scan(local, &tot);
+    if (threadIdx.x == 0) d.tile_sum[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(FmDev d, int gated)
+{
+    if (!gate(d, gated)) return;
+    __shared__ int tot, prefix;
+    if (threadIdx.x < 32) {
+        int acc = 0;
+        for (int b = threadIdx.x; b < (int)blockIdx.x; b += 32) acc += d.tile_sum[b];
+        acc = warp_sum(acc);
+        if (threadIdx.x == 0) prefix = acc;
     }
-    if (threadIdx.x == SCAN_THREADS - 1) d.cell_start[nc] = run;
+    const int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_PER;
+    int cnt[SCAN_PER];
+    int local = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_PER; k++) {
+        cnt[k] = base + k < d.ncell ? d.cell_count[base + k] : 0;
+        local += cnt[k];
+    }
+    int run = block_excl_scan(local, &tot) + prefix;
+#pragma unroll
+    for (int k = 0; k < SCAN_PER; k++) {
+        if (base + k < d.ncell) {
+            d.cell_start[base + k] = run;
+            d.cell_count[base + k] = 0;
+        }
+        run += cnt[k];
+    }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) d.cell_start[d.ncell] = prefix + tot;
 }
 
 __global__ void k_scatter(FmDev d, int gated)
 {
     if (!gate(d, gated)) return;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= d.n) return;
-    int c = d.cell_of[i];
-    int slot = d.cell_start[c] + atomicAdd(&d.cell_count[c], 1);
-    d.perm[slot] = i;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < d.n; i += gridDim.x * blockDim.x) {
+        int c = d.cell_of[i];
+        int slot = d.cell_start[c] + atomicAdd(&d.cell_count[c], 1);
+        d.perm[slot] = i;
+    }
 }
 
 // Atomics make the in-cell order arbitrary; sorting each cell by old slot
@@ -274,19 +310,19 @@ __global__ void k_scatter(FmDev d, int gated)
 __global__ void k_sort_cells(FmDev d, int gated)
 {
     if (!gate(d, gated)) return;
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= d.ncell) return;
-    int b = d.cell_start[c], e = d.cell_start[c + 1];
-    for (int x = b + 1; x < e; x++) {
-        int key = d.perm[x];
-        int y = x - 1;
-        while (y >= b && d.perm[y] > key) {
-            d.perm[y + 1] = d.perm[y];
-            y--;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.ncell; c += gridDim.x * blockDim.x) {
+        int b = d.cell_start[c], e = d.cell_start[c + 1];
+        for (int x = b + 1; x < e; x++) {
+            int key = d.perm[x];
+            int y = x - 1;
+            while (y >= b && d.perm[y] > key) {
+                d.perm[y + 1] = d.perm[y];
+                y--;
+            }
+            d.perm[y + 1] = key;
         }
-        d.perm[y + 1] = key;
+        d.cell_count[c] = 0;  // leave counts zeroed for the next histogram
     }
-    d.cell_count[c] = 0;  // leave counts zeroed for the next histogram
 }
 
 // Gather into scratch in cell order, then copy back, so every array keeps
@@ -294,26 +330,26 @@ __global__ void k_sort_cells(FmDev d, int gated)
 __global__ void k_reorder_gather(FmDev d, int gated, double4 *tpos, int32_t *tuidx)
 {
     if (!gate(d, gated)) return;
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= d.n) return;
-    int o = d.perm[s];
     const double4 *P = cur_pos(d, d.sc->pset);
-    tpos[s] = P[o];
-    d.tvx[s] = d.vx[o]; d.tvy[s] = d.vy[o]; d.tvz[s] = d.vz[o];
-    d.tax[s] = d.ax[o]; d.tay[s] = d.ay[o]; d.taz[s] = d.az[o];
-    tuidx[s] = d.slot_of[o];
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < d.n; s += gridDim.x * blockDim.x) {
+        int o = d.perm[s];
+        tpos[s] = P[o];
+        d.tvx[s] = d.vx[o]; d.tvy[s] = d.vy[o]; d.tvz[s] = d.vz[o];
+        d.tax[s] = d.ax[o]; d.tay[s] = d.ay[o]; d.taz[s] = d.az[o];
+        tuidx[s] = d.slot_of[o];
+    }
 }
 
 __global__ void k_reorder_copy(FmDev d, int gated, const double4 *tpos, const int32_t *tuidx)
 {
     if (!gate(d, gated)) return;
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= d.n) return;
     double4 *P = cur_pos(d, d.sc->pset);
-    P[s] = tpos[s];
-    d.vx[s] = d.tvx[s]; d.vy[s] = d.tvy[s]; d.vz[s] = d.tvz[s];
-    d.ax[s] = d.tax[s]; d.ay[s] = d.tay[s]; d.az[s] = d.taz[s];
-    d.slot_of[s] = tuidx[s];
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < d.n; s += gridDim.x * blockDim.x) {
+        P[s] = tpos[s];
+        d.vx[s] = d.tvx[s]; d.vy[s] = d.tvy[s]; d.vz[s] = d.tvz[s];
+        d.ax[s] = d.tax[s]; d.ay[s] = d.tay[s]; d.az[s] = d.taz[s];
+        d.slot_of[s] = tuidx[s];
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -322,138 +358,163 @@ __global__ void k_reorder_copy(FmDev d, int gated, const double4 *tpos, const in
 //  1118-1180, stored in both directions)
 // ---------------------------------------------------------------------------
 
-constexpr int NB_THREADS = 32;
-constexpr int NB_STAGE = 192;
-
-struct Seg {
-    int start, count, code;  // code = (sx+1) | (sy+1)<<2 | (sz+1)<<4
-};
+constexpr int NB_WARPS = 4;                 // cells processed concurrently per block
+constexpr int NB_THREADS = 32 * NB_WARPS;
+constexpr int NB_STAGE = 128;               // staged candidates per warp
 
 __device__ __forceinline__ bool is_halo(int x, int ne) { return x == 0 || x == ne - 1; }
 
-// One block per extended cell.  The reference visits every pair of adjacent
-// cells of which at least one is interior exactly once (13 forward shifts
-// from interior cells + 27 sweeps from halo cells); a halo cell holds the
-// images of the opposite boundary cell (plus any real molecule that binned
-// onto it).  Here each molecule of cell c collects, from the 27 cells around
-// c that are not both halo with c, every candidate within rneighbr.
+// Neighbour list build, one warp per extended cell (grid-stride).
+//
+// The reference visits every pair of adjacent cells of which at least one is
+// interior exactly once (13 forward shifts from interior cells + 27 sweeps
+// from halo cells); a halo cell holds the images of the interior cell on the
+// far side (plus any real molecule that binned onto it).  Here each molecule
+// of cell c collects, from the 27 cells around c that are not both halo with
+// c, every candidate with r^2 < rneighbr^2 -- the same set, stored for both
+// partners.
+//
+// Lane q < 27 computes the segments of neighbour cell q (its real members and,
+// for a halo cell, the shifted images of its source); a warp prefix sum lays
+// the candidates out in the reference's visiting order (cell q ascending,
+// real before images, slot ascending).  Candidates are staged in shared
+// memory as FP64 image coordinates (x_src +/- L, one rounding, as the halo
+// copy) and as FP32 offsets from the cell's reference point.  Each lane owns
+// one molecule of the cell: an FP32 distance rejects candidates that are
+// certainly beyond r_n -- the FP32 error of r^2 is below 1e-5 cs^2 for
+// offsets within 1.5 cells, the margin is 1e-4 cs^2 -- and the survivors are
+// decided by the exact FP64 test (dx^2+dy^2)+dz^2 < rneighbr2.
 __global__ void __launch_bounds__(NB_THREADS) k_build_nlist(FmDev d, int gated, int iter)
 {
     if (!gate(d, gated)) return;
-    const int c = blockIdx.x;
-    const int cstart = d.cell_start[c];
-    const int ccount = d.cell_start[c + 1] - cstart;
-    if (ccount == 0) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ne0 = d.ne[0], ne1 = d.ne[1], ne2 = d.ne[2];
-    const int cx = c % ne0, cy = (c / ne0) % ne1, cz = c / (ne0 * ne1);
-    const bool chalo = is_halo(cx, ne0) || is_halo(cy, ne1) || is_halo(cz, ne2);
     const double4 *P = cur_pos(d, d.sc->pset);
-
-    __shared__ Seg segs[54];
-    __shared__ int nseg;
-    __shared__ double sx[NB_STAGE], sy[NB_STAGE], sz[NB_STAGE];
-    __shared__ int32_t se[NB_STAGE];
-
-    if (threadIdx.x == 0) {
-        int ns = 0;
-        for (int q = 0; q < 27; q++) {
-            int dx = q % 3 - 1, dy = (q / 3) % 3 - 1, dz = q / 9 - 1;
-            int x2 = cx + dx, y2 = cy + dy, z2 = cz + dz;
-            if (x2 < 0 || y2 < 0 || z2 < 0 || x2 >= ne0 || y2 >= ne1 || z2 >= ne2) continue;
-            bool h2 = is_halo(x2, ne0) || is_halo(y2, ne1) || is_halo(z2, ne2);
-            if (chalo && h2) continue;
-            int c2 = x2 + ne0 * (y2 + ne1 * z2);
-            int b2 = d.cell_start[c2], n2 = d.cell_start[c2 + 1] - b2;
-            if (n2 > 0) segs[ns++] = Seg{b2, n2, 1 | (1 << 2) | (1 << 4)};
-            if (h2) {
-                // images in halo cell (x2,y2,z2) come from the interior cell on the
-                // far side: low halo <- last interior cell shifted by -domain,
-                // high halo <- first interior cell shifted by +domain
-                int ssx = x2 == 0 ? -1 : (x2 == ne0 - 1 ? 1 : 0);
-                int ssy = y2 == 0 ? -1 : (y2 == ne1 - 1 ? 1 : 0);
-                int ssz = z2 == 0 ? -1 : (z2 == ne2 - 1 ? 1 : 0);
-                int xs = x2 == 0 ? ne0 - 2 : (x2 == ne0 - 1 ? 1 : x2);
-                int ys = y2 == 0 ? ne1 - 2 : (y2 == ne1 - 1 ? 1 : y2);
-                int zs = z2 == 0 ? ne2 - 2 : (z2 == ne2 - 1 ? 1 : z2);
-                int cs2 = xs + ne0 * (ys + ne1 * zs);
-                int bs = d.cell_start[cs2], nsrc = d.cell_start[cs2 + 1] - bs;
-                if (nsrc > 0) segs[ns++] = Seg{bs, nsrc, (ssx + 1) | ((ssy + 1) << 2) | ((ssz + 1) << 4)};
-            }
-        }
-        nseg = ns;
-    }
-    __syncthreads();
-    const int ns = nseg;
     const double Lx = d.L[0], Ly = d.L[1], Lz = d.L[2];
     const double rn2 = d.rn2;
     const int maxn = d.maxn;
     const int noshift = 1 | (1 << 2) | (1 << 4);
+    const double csmax = fmax(d.cs[0], fmax(d.cs[1], d.cs[2]));
+    const float cut32 = (float)rn2 + (float)(1e-4 * csmax * csmax) + 1e-6f;
 
-    for (int pass = 0; pass * NB_THREADS < ccount; pass++) {
-        const int mine = pass * NB_THREADS + threadIdx.x;
-        const bool own = mine < ccount;
-        const int i = cstart + (own ? mine : 0);
-        double4 pi = P[i];
-        int cnt = 0;
-        int32_t *out = d.nbr + (size_t)i * maxn;
-        int fill = 0;
-        for (int sgi = 0; sgi < ns; sgi++) {
-            const Seg sg = segs[sgi];
-            const int sxs = (sg.code & 3) - 1, sys = ((sg.code >> 2) & 3) - 1, szs = ((sg.code >> 4) & 3) - 1;
-            int base = 0;
-            while (base < sg.count) {
-                int take = min(sg.count - base, NB_STAGE - fill);
-                for (int t = threadIdx.x; t < take; t += NB_THREADS) {
-                    int j = sg.start + base + t;
-                    double4 pj = P[j];
-                    // image coordinate: one FP64 add per shifted axis, as the halo copy
-                    sx[fill + t] = sxs ? __dadd_rn(pj.x, sxs > 0 ? Lx : -Lx) : pj.x;
-                    sy[fill + t] = sys ? __dadd_rn(pj.y, sys > 0 ? Ly : -Ly) : pj.y;
-                    sz[fill + t] = szs ? __dadd_rn(pj.z, szs > 0 ? Lz : -Lz) : pj.z;
-                    se[fill + t] = j | (sg.code << NB_SHIFT_BITS);
+    __shared__ double s_x[NB_WARPS][NB_STAGE], s_y[NB_WARPS][NB_STAGE], s_z[NB_WARPS][NB_STAGE];
+    __shared__ float s_fx[NB_WARPS][NB_STAGE], s_fy[NB_WARPS][NB_STAGE], s_fz[NB_WARPS][NB_STAGE];
+    __shared__ int32_t s_e[NB_WARPS][NB_STAGE];
+    __shared__ int s_off[NB_WARPS][55];          // candidate offset of segment k (54 segments + total)
+    __shared__ int s_start[NB_WARPS][54], s_code[NB_WARPS][54];
+
+    const int stride = gridDim.x * NB_WARPS;
+    for (int c = blockIdx.x * NB_WARPS + warp; c < d.ncell; c += stride) {
+        const int cstart = d.cell_start[c];
+        const int ccount = d.cell_start[c + 1] - cstart;
+        if (ccount == 0) continue;  // uniform across the warp
+        const int cx = c % ne0, cy = (c / ne0) % ne1, cz = c / (ne0 * ne1);
+        const bool chalo = is_halo(cx, ne0) || is_halo(cy, ne1) || is_halo(cz, ne2);
+        const double refx = (cx - 0.5) * d.cs[0] - d.hd[0];
+        const double refy = (cy - 0.5) * d.cs[1] - d.hd[1];
+        const double refz = (cz - 0.5) * d.cs[2] - d.hd[2];
+
+        // --- segments of neighbour cell q = lane ---
+        int n_real = 0, b_real = 0, n_img = 0, b_img = 0, code_img = noshift;
+        if (lane < 27) {
+            int x2 = cx + lane % 3 - 1, y2 = cy + (lane / 3) % 3 - 1, z2 = cz + lane / 9 - 1;
+            if (x2 >= 0 && y2 >= 0 && z2 >= 0 && x2 < ne0 && y2 < ne1 && z2 < ne2) {
+                bool h2 = is_halo(x2, ne0) || is_halo(y2, ne1) || is_halo(z2, ne2);
+                if (!(chalo && h2)) {
+                    int c2 = x2 + ne0 * (y2 + ne1 * z2);
+                    b_real = d.cell_start[c2];
+                    n_real = d.cell_start[c2 + 1] - b_real;
+                    if (h2) {
+                        // images in a halo cell come from the interior cell on the far
+                        // side: low halo <- last interior cell shifted by -domain, high
+                        // halo <- first interior cell shifted by +domain
+                        int ssx = x2 == 0 ? -1 : (x2 == ne0 - 1 ? 1 : 0);
+                        int ssy = y2 == 0 ? -1 : (y2 == ne1 - 1 ? 1 : 0);
+                        int ssz = z2 == 0 ? -1 : (z2 == ne2 - 1 ? 1 : 0);
+                        int xs = x2 == 0 ? ne0 - 2 : (x2 == ne0 - 1 ? 1 : x2);
+                        int ys = y2 == 0 ? ne1 - 2 : (y2 == ne1 - 1 ? 1 : y2);
+                        int zs = z2 == 0 ? ne2 - 2 : (z2 == ne2 - 1 ? 1 : z2);
+                        int cs2 = xs + ne0 * (ys + ne1 * zs);
+                        b_img = d.cell_start[cs2];
+                        n_img = d.cell_start[cs2 + 1] - b_img;
+                        code_img = (ssx + 1) | ((ssy + 1) << 2) | ((ssz + 1) << 4);
+                    }
                 }
-                fill += take;
-                base += take;
-                if (fill == NB_STAGE) {
-                    __syncthreads();
-                    if (own) {
-                        for (int q = 0; q < fill; q++) {
-                            int e = se[q];
-                            if ((e & NB_INDEX_MASK) == i && (e >> NB_SHIFT_BITS) == noshift) continue;
-                            double dx = __dsub_rn(pi.x, sx[q]);
-                            double dy = __dsub_rn(pi.y, sy[q]);
-                            double dz = __dsub_rn(pi.z, sz[q]);
-                            double r2 = norm2_rn(dx, dy, dz);
-                            if (r2 < rn2) {
-                                if (cnt < maxn) out[cnt] = e;
-                                cnt++;
-                            }
+            }
+        }
+        int tot = n_real + n_img, incl = tot;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const int excl = incl - tot;
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        if (lane < 27) {
+            s_off[warp][2 * lane] = excl;
+            s_off[warp][2 * lane + 1] = excl + n_real;
+            s_start[warp][2 * lane] = b_real;
+            s_start[warp][2 * lane + 1] = b_img;
+            s_code[warp][2 * lane] = noshift;
+            s_code[warp][2 * lane + 1] = code_img;
+        }
+        if (lane == 0) s_off[warp][54] = total;
+        __syncwarp();
+
+        for (int pass = 0; pass * 32 < ccount; pass++) {
+            const int mine = pass * 32 + lane;
+            const bool own = mine < ccount;
+            const int i = cstart + (own ? mine : 0);
+            const double4 pi = P[i];
+            const float xif = (float)(pi.x - refx), yif = (float)(pi.y - refy), zif = (float)(pi.z - refz);
+            int cnt = 0;
+            int32_t *out = d.nbr + (size_t)i * maxn;
+            for (int base = 0; base < total; base += NB_STAGE) {
+                const int take = min(NB_STAGE, total - base);
+                __syncwarp();
+                for (int t = lane; t < take; t += 32) {
+                    const int q = base + t;
+                    int k = 0;  // segment containing q: largest k with s_off[k] <= q
+#pragma unroll
+                    for (int step = 32; step > 0; step >>= 1)
+                        if (k + step < 54 && s_off[warp][k + step] <= q) k += step;
+                    const int j = s_start[warp][k] + (q - s_off[warp][k]);
+                    const int code = s_code[warp][k];
+                    const int sxs = (code & 3) - 1, sys = ((code >> 2) & 3) - 1, szs = ((code >> 4) & 3) - 1;
+                    const double4 pj = ldg_pos(P + j);
+                    const double xj = sxs ? __dadd_rn(pj.x, sxs > 0 ? Lx : -Lx) : pj.x;
+                    const double yj = sys ? __dadd_rn(pj.y, sys > 0 ? Ly : -Ly) : pj.y;
+                    const double zj = szs ? __dadd_rn(pj.z, szs > 0 ? Lz : -Lz) : pj.z;
+                    s_x[warp][t] = xj; s_y[warp][t] = yj; s_z[warp][t] = zj;
+                    s_fx[warp][t] = (float)(xj - refx);
+                    s_fy[warp][t] = (float)(yj - refy);
+                    s_fz[warp][t] = (float)(zj - refz);
+                    s_e[warp][t] = j | (code << NB_SHIFT_BITS);
+                }
+                __syncwarp();
+                if (own) {
+                    for (int q = 0; q < take; q++) {
+                        const float fx = xif - s_fx[warp][q], fy = yif - s_fy[warp][q], fz = zif - s_fz[warp][q];
+                        if (fx * fx + fy * fy + fz * fz > cut32) continue;
+                        const int e = s_e[warp][q];
+                        if ((e & NB_INDEX_MASK) == i && (e >> NB_SHIFT_BITS) == noshift) continue;
+                        const double dx = __dsub_rn(pi.x, s_x[warp][q]);
+                        const double dy = __dsub_rn(pi.y, s_y[warp][q]);
+                        const double dz = __dsub_rn(pi.z, s_z[warp][q]);
+                        if (norm2_rn(dx, dy, dz) < rn2) {
+                            if (cnt < maxn) out[cnt] = e;
+                            cnt++;
                         }
                     }
-                    __syncthreads();
-                    fill = 0;
                 }
             }
-        }
-        __syncthreads();
-        if (own) {
-            for (int q = 0; q < fill; q++) {
-                int e = se[q];
-                if ((e & NB_INDEX_MASK) == i && (e >> NB_SHIFT_BITS) == noshift) continue;
-                double dx = __dsub_rn(pi.x, sx[q]);
-                double dy = __dsub_rn(pi.y, sy[q]);
-                double dz = __dsub_rn(pi.z, sz[q]);
-                double r2 = norm2_rn(dx, dy, dz);
-                if (r2 < rn2) {
-                    if (cnt < maxn) out[cnt] = e;
-                    cnt++;
-                }
+            if (own) {
+                d.nnbr[i] = cnt < maxn ? cnt : maxn;
+                atomicMax(&d.sc->max_nbr, cnt);
+                if (cnt > maxn) raise_status(d, ST_NLIST, iter);
             }
-            d.nnbr[i] = cnt < maxn ? cnt : maxn;
-            atomicMax(&d.sc->max_nbr, cnt);
-            if (cnt > maxn) raise_status(d, ST_NLIST, iter);
         }
-        __syncthreads();
+        __syncwarp();
     }
 }
 
@@ -497,44 +558,54 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force(FmDev d)
     if (active) {
         const double4 pi = P[i];
         const int cnt = d.nnbr[i];
-        const int32_t *__restrict__ L = d.nbr + (size_t)i * d.maxn;
+        const int32_t *__restrict__ L = d.nbr + (size_t)i * d.maxn;  // 16-byte aligned rows (maxn % 8 == 0)
         const double Lx = d.L[0], Ly = d.L[1], Lz = d.L[2];
         const double rc2 = d.rc2;
-        for (int k = lane; k < cnt; k += TPM) {
-            const int e = __ldg(L + k);
-            const double4 pj = ldg_pos(P + (e & NB_INDEX_MASK));
-            const int code = e >> NB_SHIFT_BITS;
-            const int ssx = (code & 3) - 1, ssy = ((code >> 2) & 3) - 1, ssz = ((code >> 4) & 3) - 1;
-            const double xj = ssx ? __dadd_rn(pj.x, ssx > 0 ? Lx : -Lx) : pj.x;
-            const double yj = ssy ? __dadd_rn(pj.y, ssy > 0 ? Ly : -Ly) : pj.y;
-            const double zj = ssz ? __dadd_rn(pj.z, ssz > 0 ? Lz : -Lz) : pj.z;
-            const double dx = __dsub_rn(pi.x, xj);
-            const double dy = __dsub_rn(pi.y, yj);
-            const double dz = __dsub_rn(pi.z, zj);
-            const double r2 = norm2_rn(dx, dy, dz);
-            if (r2 < rc2) {
-                if (PREC == 0) {
-                    // LJ_accijmag = 48 (s^7 - s^4/2), s = 1/r^2 (setup_set_parameters.f90:105-113)
-                    const double s = 1.0 / r2;
-                    const double s2 = s * s, s4 = s2 * s2;
-                    const double acc = 48.0 * (s4 * s2 * s - 0.5 * s4);
-                    fx += acc * dx; fy += acc * dy; fz += acc * dz;
-                    if (REC) {
-                        const double s3 = s2 * s, s6 = s3 * s3;
-                        pe += 4.0 * (s6 - s3) - d.potshift;  // LJ_energy (:126-135)
-                        vir += acc * r2;
-                    }
-                } else {
-                    const float s = 1.0f / (float)r2;
-                    const float s2 = s * s, s4 = s2 * s2;
-                    const float acc = 48.0f * (s4 * s2 * s - 0.5f * s4);
-                    fx += (double)(acc * (float)dx);
-                    fy += (double)(acc * (float)dy);
-                    fz += (double)(acc * (float)dz);
-                    if (REC) {
-                        const float s3 = s2 * s, s6 = s3 * s3;
-                        pe += (double)(4.0f * (s6 - s3)) - d.potshift;
-                        vir += (double)(acc * (float)r2);
+        // each lane takes 4 consecutive entries per iteration (one 16-byte load)
+        // and issues their 4 gathers before any arithmetic
+        for (int k0 = lane * 4; k0 < cnt; k0 += 4 * TPM) {
+            const int4 e4 = __ldg(reinterpret_cast<const int4 *>(L + k0));
+            const int ev[4] = {e4.x, e4.y, e4.z, e4.w};
+            double4 pj[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                if (k0 + q < cnt) pj[q] = ldg_pos(P + (ev[q] & NB_INDEX_MASK));
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                if (k0 + q >= cnt) break;
+                const int code = ev[q] >> NB_SHIFT_BITS;
+                const int ssx = (code & 3) - 1, ssy = ((code >> 2) & 3) - 1, ssz = ((code >> 4) & 3) - 1;
+                const double xj = ssx ? __dadd_rn(pj[q].x, ssx > 0 ? Lx : -Lx) : pj[q].x;
+                const double yj = ssy ? __dadd_rn(pj[q].y, ssy > 0 ? Ly : -Ly) : pj[q].y;
+                const double zj = ssz ? __dadd_rn(pj[q].z, ssz > 0 ? Lz : -Lz) : pj[q].z;
+                const double dx = __dsub_rn(pi.x, xj);
+                const double dy = __dsub_rn(pi.y, yj);
+                const double dz = __dsub_rn(pi.z, zj);
+                const double r2 = norm2_rn(dx, dy, dz);
+                if (r2 < rc2) {
+                    if (PREC == 0) {
+                        // LJ_accijmag = 48 (s^7 - s^4/2), s = 1/r^2 (setup_set_parameters.f90:105-113)
+                        const double s = 1.0 / r2;
+                        const double s2 = s * s, s4 = s2 * s2;
+                        const double acc = 48.0 * (s4 * s2 * s - 0.5 * s4);
+                        fx += acc * dx; fy += acc * dy; fz += acc * dz;
+                        if (REC) {
+                            const double s3 = s2 * s, s6 = s3 * s3;
+                            pe += 4.0 * (s6 - s3) - d.potshift;  // LJ_energy (:126-135)
+                            vir += acc * r2;
+                        }
+                    } else {
+                        const float s = 1.0f / (float)r2;
+                        const float s2 = s * s, s4 = s2 * s2;
+                        const float acc = 48.0f * (s4 * s2 * s - 0.5f * s4);
+                        fx += (double)(acc * (float)dx);
+                        fy += (double)(acc * (float)dy);
+                        fz += (double)(acc * (float)dz);
+                        if (REC) {
+                            const float s3 = s2 * s, s6 = s3 * s3;
+                            pe += (double)(4.0f * (s6 - s3)) - d.potshift;
+                            vir += (double)(acc * (float)r2);
+                        }
                     }
                 }
             }
@@ -886,24 +957,34 @@ void launch_decide(const FmDev &d, int iter, int flip, int crit, int fixed_rebui
 {
     k_decide<<<1, 1, 0, st>>>(d, iter, flip, crit, fixed_rebuild > 0 ? fixed_rebuild : 1, half_min_delta);
 }
+// Gated kernels run grid-stride loops on a bounded grid, so that a launch the
+// device decision turns into a no-op costs a few microseconds at most.
+constexpr int kSMs = 148;
+inline int sgrid(int n, int t, int per_sm) { return std::min(nblk(n, t), kSMs * per_sm); }
+
 void launch_wrap_bin(const FmDev &d, int wrap, int bin, int gated, int iter, cudaStream_t st)
 {
-    k_wrap_bin<<<nblk(d.n, 256), 256, 0, st>>>(d, wrap, bin, gated, iter);
+    k_wrap_bin<<<sgrid(d.n, 256, 8), 256, 0, st>>>(d, wrap, bin, gated, iter);
 }
-void launch_scan_cells(const FmDev &d, int gated, cudaStream_t st) { k_scan_cells<<<1, SCAN_THREADS, 0, st>>>(d, gated); }
+int scan_tiles(int ncell) { return nblk(ncell, SCAN_TILE); }
+void launch_scan_cells(const FmDev &d, int gated, cudaStream_t st)
+{
+    k_scan_tiles<<<scan_tiles(d.ncell), SCAN_THREADS, 0, st>>>(d, gated);
+    k_scan_apply<<<scan_tiles(d.ncell), SCAN_THREADS, 0, st>>>(d, gated);
+}
 void launch_scatter(const FmDev &d, int gated, cudaStream_t st)
 {
-    k_scatter<<<nblk(d.n, 256), 256, 0, st>>>(d, gated);
-    k_sort_cells<<<nblk(d.ncell, 128), 128, 0, st>>>(d, gated);
+    k_scatter<<<sgrid(d.n, 256, 8), 256, 0, st>>>(d, gated);
+    k_sort_cells<<<sgrid(d.ncell, 128, 8), 128, 0, st>>>(d, gated);
 }
 void launch_reorder(const FmDev &d, int gated, double4 *tpos, int32_t *tuidx, cudaStream_t st)
 {
-    k_reorder_gather<<<nblk(d.n, 256), 256, 0, st>>>(d, gated, tpos, tuidx);
-    k_reorder_copy<<<nblk(d.n, 256), 256, 0, st>>>(d, gated, tpos, tuidx);
+    k_reorder_gather<<<sgrid(d.n, 256, 8), 256, 0, st>>>(d, gated, tpos, tuidx);
+    k_reorder_copy<<<sgrid(d.n, 256, 8), 256, 0, st>>>(d, gated, tpos, tuidx);
 }
 void launch_build_nlist(const FmDev &d, int gated, int iter, cudaStream_t st)
 {
-    k_build_nlist<<<d.ncell, NB_THREADS, 0, st>>>(d, gated, iter);
+    k_build_nlist<<<sgrid(d.ncell, NB_WARPS, 8), NB_THREADS, 0, st>>>(d, gated, iter);
 }
 
 int force_blocks(int n, int tpm) { return nblk(n * tpm, FORCE_THREADS); }
