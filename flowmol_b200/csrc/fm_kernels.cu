@@ -360,7 +360,7 @@ __global__ void k_reorder_copy(FmDev d, int gated, const double4 *tpos, const in
 
 constexpr int NB_WARPS = 4;                 // cells processed concurrently per block
 constexpr int NB_THREADS = 32 * NB_WARPS;
-constexpr int NB_STAGE = 128;               // staged candidates per warp
+constexpr int NB_STAGE = 256;               // staged candidates per warp
 
 __device__ __forceinline__ bool is_halo(int x, int ne) { return x == 0 || x == ne - 1; }
 
@@ -378,12 +378,14 @@ __device__ __forceinline__ bool is_halo(int x, int ne) { return x == 0 || x == n
 // for a halo cell, the shifted images of its source); a warp prefix sum lays
 // the candidates out in the reference's visiting order (cell q ascending,
 // real before images, slot ascending).  Candidates are staged in shared
-// memory as FP64 image coordinates (x_src +/- L, one rounding, as the halo
-// copy) and as FP32 offsets from the cell's reference point.  Each lane owns
-// one molecule of the cell: an FP32 distance rejects candidates that are
-// certainly beyond r_n -- the FP32 error of r^2 is below 1e-5 cs^2 for
-// offsets within 1.5 cells, the margin is 1e-4 cs^2 -- and the survivors are
-// decided by the exact FP64 test (dx^2+dy^2)+dz^2 < rneighbr2.
+// memory as FP32 offsets from the cell's reference point, computed from the
+// FP64 image coordinate (x_src +/- L, one rounding, as the halo copy).  Each
+// lane owns one molecule of the cell and walks the staged candidates: the FP32
+// r^2 (error below 1e-5 cs^2 for molecules binned in this build, offsets
+// within 1.5 cells) decides every candidate farther than BAND = 1e-4 cs^2
+// from rneighbr2; a candidate inside the band is re-read in FP64 and decided
+// by the exact test (dx^2+dy^2)+dz^2 < rneighbr2 -- a branch the whole warp
+// skips unless some lane needs it.
 __global__ void __launch_bounds__(NB_THREADS) k_build_nlist(FmDev d, int gated, int iter)
 {
     if (!gate(d, gated)) return;
@@ -395,11 +397,10 @@ __global__ void __launch_bounds__(NB_THREADS) k_build_nlist(FmDev d, int gated, 
     const int maxn = d.maxn;
     const int noshift = 1 | (1 << 2) | (1 << 4);
     const double csmax = fmax(d.cs[0], fmax(d.cs[1], d.cs[2]));
-    const float cut32 = (float)rn2 + (float)(1e-4 * csmax * csmax) + 1e-6f;
+    const float band = (float)(1e-4 * csmax * csmax) + 1e-6f;
+    const float lo32 = (float)rn2 - band, hi32 = (float)rn2 + band;
 
-    __shared__ double s_x[NB_WARPS][NB_STAGE], s_y[NB_WARPS][NB_STAGE], s_z[NB_WARPS][NB_STAGE];
-    __shared__ float s_fx[NB_WARPS][NB_STAGE], s_fy[NB_WARPS][NB_STAGE], s_fz[NB_WARPS][NB_STAGE];
-    __shared__ int32_t s_e[NB_WARPS][NB_STAGE];
+    __shared__ float4 s_f[NB_WARPS][NB_STAGE];   // x, y, z offsets and the entry bits in w
     __shared__ int s_off[NB_WARPS][55];          // candidate offset of segment k (54 segments + total)
     __shared__ int s_start[NB_WARPS][54], s_code[NB_WARPS][54];
 
@@ -465,7 +466,7 @@ __global__ void __launch_bounds__(NB_THREADS) k_build_nlist(FmDev d, int gated, 
             const int mine = pass * 32 + lane;
             const bool own = mine < ccount;
             const int i = cstart + (own ? mine : 0);
-            const double4 pi = P[i];
+            const double4 pi = ldg_pos(P + i);
             const float xif = (float)(pi.x - refx), yif = (float)(pi.y - refy), zif = (float)(pi.z - refz);
             int cnt = 0;
             int32_t *out = d.nbr + (size_t)i * maxn;
@@ -485,26 +486,35 @@ __global__ void __launch_bounds__(NB_THREADS) k_build_nlist(FmDev d, int gated, 
                     const double xj = sxs ? __dadd_rn(pj.x, sxs > 0 ? Lx : -Lx) : pj.x;
                     const double yj = sys ? __dadd_rn(pj.y, sys > 0 ? Ly : -Ly) : pj.y;
                     const double zj = szs ? __dadd_rn(pj.z, szs > 0 ? Lz : -Lz) : pj.z;
-                    s_x[warp][t] = xj; s_y[warp][t] = yj; s_z[warp][t] = zj;
-                    s_fx[warp][t] = (float)(xj - refx);
-                    s_fy[warp][t] = (float)(yj - refy);
-                    s_fz[warp][t] = (float)(zj - refz);
-                    s_e[warp][t] = j | (code << NB_SHIFT_BITS);
+                    s_f[warp][t] = make_float4((float)(xj - refx), (float)(yj - refy), (float)(zj - refz),
+                                               __int_as_float(j | (code << NB_SHIFT_BITS)));
                 }
                 __syncwarp();
-                if (own) {
-                    for (int q = 0; q < take; q++) {
-                        const float fx = xif - s_fx[warp][q], fy = yif - s_fy[warp][q], fz = zif - s_fz[warp][q];
-                        if (fx * fx + fy * fy + fz * fz > cut32) continue;
-                        const int e = s_e[warp][q];
-                        if ((e & NB_INDEX_MASK) == i && (e >> NB_SHIFT_BITS) == noshift) continue;
-                        const double dx = __dsub_rn(pi.x, s_x[warp][q]);
-                        const double dy = __dsub_rn(pi.y, s_y[warp][q]);
-                        const double dz = __dsub_rn(pi.z, s_z[warp][q]);
-                        if (norm2_rn(dx, dy, dz) < rn2) {
-                            if (cnt < maxn) out[cnt] = e;
-                            cnt++;
+                for (int q = 0; q < take; q++) {
+                    const float4 f = s_f[warp][q];  // broadcast
+                    const float fx = xif - f.x, fy = yif - f.y, fz = zif - f.z;
+                    const float r2f = fx * fx + fy * fy + fz * fz;
+                    const int e = __float_as_int(f.w);
+                    const bool self = (e & NB_INDEX_MASK) == i && (e >> NB_SHIFT_BITS) == noshift;
+                    bool hit = own && !self && r2f < lo32;
+                    const bool in_band = own && !self && r2f >= lo32 && r2f <= hi32;
+                    if (__any_sync(0xffffffffu, in_band)) {
+                        if (in_band) {
+                            const int code = e >> NB_SHIFT_BITS;
+                            const int sxs = (code & 3) - 1, sys = ((code >> 2) & 3) - 1, szs = ((code >> 4) & 3) - 1;
+                            const double4 pj = ldg_pos(P + (e & NB_INDEX_MASK));
+                            const double xj = sxs ? __dadd_rn(pj.x, sxs > 0 ? Lx : -Lx) : pj.x;
+                            const double yj = sys ? __dadd_rn(pj.y, sys > 0 ? Ly : -Ly) : pj.y;
+                            const double zj = szs ? __dadd_rn(pj.z, szs > 0 ? Lz : -Lz) : pj.z;
+                            const double dx = __dsub_rn(pi.x, xj);
+                            const double dy = __dsub_rn(pi.y, yj);
+                            const double dz = __dsub_rn(pi.z, zj);
+                            hit = norm2_rn(dx, dy, dz) < rn2;
                         }
+                    }
+                    if (hit) {
+                        if (cnt < maxn) out[cnt] = e;
+                        cnt++;
                     }
                 }
             }
