@@ -63,6 +63,41 @@ class FmMacro(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad_"}
 
 
+class FmEngineParams(C.Structure):
+    _fields_ = [
+        ("max_molecules", C.c_int64), ("max_cells", C.c_int64), ("max_list_entries", C.c_int64),
+        ("max_slots", C.c_int32), ("precision", C.c_int32), ("threads_per_molecule", C.c_int32),
+        ("ticks_per_chunk", C.c_int32), ("keep_states", C.c_int32), ("pad_", C.c_int32),
+        ("delta_t", C.c_double),
+    ]
+
+
+class FmJob(C.Structure):
+    _fields_ = [
+        ("np", C.c_int32), ("tplot", C.c_int32), ("domain", C.c_double * 3), ("density", C.c_double),
+        ("rcutoff", C.c_double), ("delta_rneighbr", C.c_double * 3), ("nsteps", C.c_int32),
+        ("initialstep", C.c_int32), ("integration_algorithm", C.c_int32), ("ensemble", C.c_int32),
+        ("force_list", C.c_int32), ("pressure_outflag", C.c_int32), ("nthermo", C.c_int32),
+        ("rebuild_criteria", C.c_int32), ("fixed_rebuild", C.c_int32), ("nlist_capacity", C.c_int32),
+        ("thermostat_temperature", C.c_double * 2), ("teth_k2", C.c_double), ("teth_k4", C.c_double),
+        ("teth_k6", C.c_double),
+    ]
+
+
+class FmJobResult(C.Structure):
+    _fields_ = [
+        ("job_id", C.c_int64), ("status", C.c_int32), ("nsamples", C.c_int32), ("final_iter", C.c_int32),
+        ("rebuilds", C.c_int32), ("retries", C.c_int32), ("pad_", C.c_int32), ("ptensor", C.c_double * 9),
+        ("last", FmMacro), ("submit_time", C.c_double), ("admit_time", C.c_double), ("finish_time", C.c_double),
+    ]
+
+    def as_dict(self):
+        return dict(job_id=self.job_id, status=self.status, nsamples=self.nsamples, final_iter=self.final_iter,
+                    rebuilds=self.rebuilds, retries=self.retries,
+                    ptensor=np.array(list(self.ptensor)).reshape(3, 3), last=self.last.as_dict(),
+                    submit_time=self.submit_time, admit_time=self.admit_time, finish_time=self.finish_time)
+
+
 class FlowmolError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"FM_ERR_{ERRORS.get(code, code)}: {msg}")
@@ -113,6 +148,16 @@ def lib():
             "fm_pair_digest": [h, P(C.c_uint64), P(C.c_int64)],
             "fm_get_counters": [h, P(C.c_int64), P(C.c_int32), P(C.c_int32)],
             "fm_last_error": [C.c_char_p, C.c_int32],
+            "fm_engine_create": [P(FmEngineParams), P(h)],
+            "fm_engine_destroy": [h],
+            "fm_engine_set_stream": [h, C.c_void_p],
+            "fm_engine_submit": [h, P(FmJob), P(C.c_double), P(C.c_double), P(C.c_int32), P(C.c_double),
+                                 P(C.c_double), P(C.c_int64)],
+            "fm_engine_step_chunk": [h, P(C.c_int32), P(C.c_int32)],
+            "fm_engine_run": [h, C.c_int32],
+            "fm_engine_take_results": [h, P(FmJobResult), C.c_int32, P(C.c_int32)],
+            "fm_engine_job_state": [h, C.c_int64, P(C.c_double), P(C.c_double)],
+            "fm_engine_counters": [h, P(C.c_int64), P(C.c_int64), P(C.c_int32), P(C.c_int64)],
             "fm_force_kernel_timing": [h, C.c_int32],
             "fm_get_force_kernel_time": [h, P(C.c_double), P(C.c_int64)],
             "fm_get_launch_count": [h, P(C.c_int64)],
@@ -357,3 +402,102 @@ class MDSystem:
         rb = C.c_int64(); cap = C.c_int32(); mx = C.c_int32()
         check(lib().fm_get_counters(self.h, C.byref(rb), C.byref(cap), C.byref(mx)))
         return dict(rebuilds=rb.value, nlist_capacity=cap.value, max_neighbours=mx.value)
+
+
+def make_job(np_, domain, rcutoff, nsteps, delta_rneighbr=(0.3, 0.3, 0.3), tplot=100, density=None,
+             initialstep=0, integration_algorithm=1, ensemble=0, force_list=FORCE_LIST_HALF, pressure_outflag=0,
+             nthermo=0, thermostat_temperature=(1.0, 1.0), teth=(0.0, 0.0, 0.0), rebuild_criteria=0,
+             fixed_rebuild=1, nlist_capacity=0) -> FmJob:
+    j = FmJob()
+    j.np = int(np_)
+    j.tplot = int(tplot)
+    for k in range(3):
+        j.domain[k] = float(domain[k])
+        j.delta_rneighbr[k] = float(delta_rneighbr[k])
+    j.density = float(density) if density is not None else np_ / float(np.prod(domain))
+    j.rcutoff = float(rcutoff)
+    j.nsteps = int(nsteps)
+    j.initialstep = int(initialstep)
+    j.integration_algorithm = int(integration_algorithm)
+    j.ensemble = int(ensemble)
+    j.force_list = int(force_list)
+    j.pressure_outflag = int(pressure_outflag)
+    j.nthermo = int(nthermo)
+    j.thermostat_temperature[0] = float(thermostat_temperature[0])
+    j.thermostat_temperature[1] = float(thermostat_temperature[1])
+    j.teth_k2, j.teth_k4, j.teth_k6 = (float(x) for x in teth)
+    j.rebuild_criteria = int(rebuild_criteria)
+    j.fixed_rebuild = int(fixed_rebuild)
+    j.nlist_capacity = int(nlist_capacity)
+    return j
+
+
+class Engine:
+    """Multi-job slot engine (batched replicas, served jobs)."""
+
+    def __init__(self, max_molecules, max_cells, max_list_entries, max_slots, delta_t=0.005, precision=0,
+                 threads_per_molecule=0, ticks_per_chunk=20, keep_states=True):
+        p = FmEngineParams()
+        p.max_molecules = int(max_molecules)
+        p.max_cells = int(max_cells)
+        p.max_list_entries = int(max_list_entries)
+        p.max_slots = int(max_slots)
+        p.precision = int(precision)
+        p.threads_per_molecule = int(threads_per_molecule)
+        p.ticks_per_chunk = int(ticks_per_chunk)
+        p.keep_states = 1 if keep_states else 0
+        p.delta_t = float(delta_t)
+        hp = C.c_void_p()
+        check(lib().fm_engine_create(C.byref(p), C.byref(hp)))
+        self.h = hp
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().fm_engine_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, job: FmJob, r, v, tag=None, rtether=None, slidev=None) -> int:
+        r = np.ascontiguousarray(r, np.float64); v = np.ascontiguousarray(v, np.float64)
+        args = []
+        for x, t in ((tag, np.int32), (rtether, np.float64), (slidev, np.float64)):
+            if x is None:
+                args.append(None)
+            else:
+                x = np.ascontiguousarray(x, t)
+                args.append(x)
+        jid = C.c_int64()
+        check(lib().fm_engine_submit(self.h, C.byref(job), _dp(r), _dp(v),
+                                     None if args[0] is None else args[0].ctypes.data_as(C.POINTER(C.c_int32)),
+                                     None if args[1] is None else _dp(args[1]),
+                                     None if args[2] is None else _dp(args[2]), C.byref(jid)))
+        return jid.value
+
+    def step_chunk(self):
+        res = C.c_int32(); q = C.c_int32()
+        check(lib().fm_engine_step_chunk(self.h, C.byref(res), C.byref(q)))
+        return res.value, q.value
+
+    def run(self, max_chunks=0):
+        check(lib().fm_engine_run(self.h, int(max_chunks)))
+
+    def results(self, cap=100000):
+        arr = (FmJobResult * cap)()
+        n = C.c_int32()
+        check(lib().fm_engine_take_results(self.h, arr, cap, C.byref(n)))
+        return [arr[k].as_dict() for k in range(n.value)]
+
+    def job_state(self, job_id, n):
+        r = np.empty((n, 3)); v = np.empty((n, 3))
+        check(lib().fm_engine_job_state(self.h, int(job_id), _dp(r), _dp(v)))
+        return r, v
+
+    def counters(self):
+        t = C.c_int64(); m = C.c_int64(); tp = C.c_int32(); la = C.c_int64()
+        check(lib().fm_engine_counters(self.h, C.byref(t), C.byref(m), C.byref(tp), C.byref(la)))
+        return dict(ticks=t.value, molecule_steps=m.value, threads_per_molecule=tp.value, launches=la.value)

@@ -13,8 +13,8 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libflowmol_b200.so")
-SOURCES = ["fm_kernels.cu", "fm_api.cu", "fm_noalloc.cu"]
-HEADERS = ["fm_common.cuh"]
+SOURCES = ["fm_kernels.cu", "fm_api.cu", "fm_noalloc.cu", "fm_engine_kernels.cu", "fm_engine.cu"]
+HEADERS = ["fm_common.cuh", "fm_device.cuh", "fm_engine.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -51,6 +51,8 @@ inline double p12(double s) { double t = p6(s); return t * t; }
 
 }  // namespace
 
+void fm::set_last_error(const char *msg) { g_last_error = msg ? msg : ""; }
+
 struct fm_handle {
     fm_params p{};
     FmDev d{};

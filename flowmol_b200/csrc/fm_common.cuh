@@ -91,6 +91,9 @@ constexpr int NB_SHIFT_BITS = 26;
 constexpr int32_t NB_INDEX_MASK = (1 << NB_SHIFT_BITS) - 1;
 constexpr int MAX_MOLECULES = NB_INDEX_MASK;
 
+// Sets the message fm_last_error returns on this thread (fm_api.cu).
+void set_last_error(const char *msg);
+
 // ---- kernel launchers (fm_kernels.cu) -----------------------------------
 // All launchers enqueue on `st` and never synchronise.
 void launch_reset_scalars(const FmDev &d, cudaStream_t st);

@@ -1,0 +1,68 @@
+// fm_device.cuh -- small device helpers shared by the single-system kernels
+// (fm_kernels.cu) and the multi-job slot engine (fm_engine.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace fm {
+
+// |v|^2 in the reference's dot_product order, no contraction.
+__device__ __forceinline__ double norm2_rn(double x, double y, double z)
+{
+    return __dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z));
+}
+
+// Read-only gather of one double4 (32-byte aligned) as a single 256-bit load:
+// one L1 request per partner instead of two.
+__device__ __forceinline__ double4 ldg_pos(const double4 *p)
+{
+    double4 r;
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(r.x), "=d"(r.y), "=d"(r.z), "=d"(r.w) : "l"(p));
+    return r;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ double warp_max(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// icell = ceiling((r + halfdomain)/cellsidelength) + 1 (1-based, halo = 1 and
+// ncells+2); the 0-based extended index is the ceiling itself.  Out-of-grid
+// values are clamped and flagged.
+__device__ __forceinline__ int bin_axis(double x, double hd, double cs, int ne, bool &bad)
+{
+    double q = __ddiv_rn(__dadd_rn(x, hd), cs);
+    if (!(q == q)) { bad = true; return 0; }
+    int c = __double2int_ru(q);  // round toward +inf == ceiling for in-range values
+    if (c < 0 || c > ne - 1) { bad = true; c = c < 0 ? 0 : ne - 1; }
+    return c;
+}
+
+__device__ __forceinline__ bool is_halo(int x, int ne) { return x == 0 || x == ne - 1; }
+
+// Periodic image of a coordinate: one FP64 add of +/-L, as the reference's
+// halo copy r(k,np+m) = r(k,np+m) +/- domain(k).
+__device__ __forceinline__ double image(double x, int s, double L)
+{
+    return s ? __dadd_rn(x, s > 0 ? L : -L) : x;
+}
+
+// Neumaier-compensated accumulation.
+__device__ __forceinline__ void neumaier(double &sum, double &cmp, double x)
+{
+    double t = sum + x;
+    cmp += fabs(sum) >= fabs(x) ? (sum - t) + x : (x - t) + sum;
+    sum = t;
+}
+
+}  // namespace fm

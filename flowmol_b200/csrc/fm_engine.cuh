@@ -1,0 +1,100 @@
+// fm_engine.cuh -- device layout of the multi-job slot engine (batching and
+// serving).  Many independent MD jobs share one arena of molecules, cells and
+// neighbour-list rows; each job owns a slot with its own geometry, iteration
+// counter, step budget, rebuild state and status.  A tick advances every
+// resident job by one time step with a fixed sequence of kernels whose
+// per-job decisions are taken on the device.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fm_common.cuh"
+
+namespace fm {
+
+enum : int { SLOT_EMPTY = 0, SLOT_SETUP = 1, SLOT_RUN = 2, SLOT_DONE = 3, SLOT_FAILED = 4 };
+enum : int { PHASE_IDLE = 0, PHASE_SETUP = 1, PHASE_STEP = 2 };
+enum : int { MODE_LIST = 1, MODE_ALLPAIRS = 2 };
+
+// Molecular tags (modules.f90:79-88).
+enum : int {
+    TAG_FREE = 0, TAG_FIXED = 1, TAG_FIXED_SLIDE = 2, TAG_TETH = 3, TAG_THERMO = 4, TAG_TETH_THERMO = 5,
+    TAG_TETH_SLIDE = 6, TAG_TETH_THERMO_SLIDE = 7
+};
+
+// Per-molecule record terms written on record ticks.
+enum { RT_PE = 0, RT_VIR, RT_MV2, RT_VSUM, RT_PXX, RT_PYY, RT_PZZ, RT_PXY, RT_PXZ, RT_PYZ, RT_N };
+
+struct EngSlot {
+    // ---- static: written by the host at admission ----
+    double L[3], hd[3], cs[3];
+    int ne[3];
+    int ncell, cell_off, cstart_off;  // cells [cell_off, +ncell); starts [cstart_off, +ncell+1)
+    int mol_off, nmol;                // molecules [mol_off, +nmol)
+    int64_t list_off;                 // neighbour rows start here, maxn entries per molecule
+    int maxn;
+    int tplot, integrator, ensemble, mode, pressure, nthermo, crit, fixed_rebuild;
+    int iter0, nsteps;
+    double rc2, rn2, potshift, half_min_delta, volume, density;
+    double therm_T[2];
+    double k2, k4, k6;
+    // ---- dynamic: owned by the device while resident ----
+    int state, phase, iter, pset;
+    int rebuild, wrap, record, last;
+    uint32_t status;
+    int fail_iter;
+    int rebuilds, nsamples;
+    int max_nbr, pad_;
+    unsigned long long vmax2;
+    double rmax, simtime;
+    double zeta[2], ascale[2], bscale[2];
+    double ptensor[9];
+    FmRecord last_rec;
+};
+
+struct EngDev {
+    int nslots;
+    int mol_cap;     // arena molecules
+    int cell_cap;    // arena cells
+    double dt, half_dt, half_dt2;
+    int precision;
+    EngSlot *slots;
+    // molecules (arena order; a job's molecules are contiguous and re-ordered by cell inside it)
+    double4 *pos0, *pos1;
+    double *vx, *vy, *vz, *ax, *ay, *az;
+    int32_t *slot_of;    // slot of a molecule, -1 = free
+    int32_t *uidx;       // index of the molecule in its job's upload order
+    int32_t *tag;
+    double4 *rteth;      // tether anchor (x, y, z, unused)
+    double4 *slidev;     // slide velocity (x, y, z, unused)
+    // reorder scratch
+    double4 *tpos, *trteth, *tslidev;
+    double *tvx, *tvy, *tvz, *tax, *tay, *taz;
+    int32_t *tuidx, *ttag;
+    // cells
+    int32_t *cell_slot;   // slot of an arena cell, -1 = free
+    int32_t *cell_of;     // per molecule
+    int32_t *cell_count;  // per cell
+    int32_t *cell_start;  // per slot: ncell+1 absolute molecule indices
+    int32_t *perm;        // new arena index -> old arena index
+    // neighbour rows
+    int32_t *nbr;
+    int32_t *nnbr;
+    // record terms and thermostat partials
+    double *rterm;        // [mol][RT_N]
+    double *tmv2;         // (v + a dt/2)^2 of thermostatted molecules, else 0
+};
+
+__host__ __device__ inline double4 *eng_pos(const EngDev &d, int pset) { return pset ? d.pos1 : d.pos0; }
+
+// Launchers (fm_engine.cu); `tpm` = lanes per molecule of the force kernel.
+void eng_tick(const EngDev &d, int tpm, cudaStream_t st);
+void eng_force_only(const EngDev &d, int tpm, cudaStream_t st);  // autotuner: forces of running list jobs
+void eng_scatter_job(const EngDev &d, int slot, int mol_off, int n, const double *r3, const double *v3,
+                     const int32_t *tag, const double *rteth3, const double *slidev3, cudaStream_t st);
+void eng_claim_cells(const EngDev &d, int slot, int cell_off, int ncell, cudaStream_t st);
+void eng_gather_job(const EngDev &d, int slot, int mol_off, int n, double *r3, double *v3, cudaStream_t st);
+void eng_release_job(const EngDev &d, int mol_off, int n, int cell_off, int ncell, cudaStream_t st);
+int eng_kernels_per_tick();
+
+}  // namespace fm

@@ -14,6 +14,7 @@
 #include <algorithm>
 
 #include "fm_common.cuh"
+#include "fm_device.cuh"
 
 namespace fm {
 
@@ -27,35 +28,9 @@ __device__ __forceinline__ void raise_status(const FmDev &d, uint32_t bit, int i
     if ((old & ST_FATAL) == 0u) d.sc->fail_iter = iter;
 }
 
-// |v|^2 in the reference's dot_product order, no contraction.
-__device__ __forceinline__ double norm2_rn(double x, double y, double z)
-{
-    return __dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z));
-}
 
-// Read-only gather of one double4 (32-byte aligned) as a single 256-bit load:
-// one L1 request per partner instead of two.
-__device__ __forceinline__ double4 ldg_pos(const double4 *p)
-{
-    double4 r;
-    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(r.x), "=d"(r.y), "=d"(r.z), "=d"(r.w) : "l"(p));
-    return r;
-}
 
-template <typename T>
-__device__ __forceinline__ T warp_sum(T v)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
 
-__device__ __forceinline__ double warp_max(double v)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
-}
 
 // Block max of a non-negative double folded into sc->vmax2 (u64 order of
 // non-negative doubles equals their numeric order).
@@ -175,16 +150,6 @@ __device__ __forceinline__ bool gate(const FmDev &d, int gated)
     return true;
 }
 
-// icell = ceiling((r + halfdomain)/cellsidelength) + 1 (1-based, halo = 1 and
-// ncells+2); the 0-based extended index is the ceiling itself.
-__device__ __forceinline__ int bin_axis(double x, double hd, double cs, int ne, bool &bad)
-{
-    double q = __ddiv_rn(__dadd_rn(x, hd), cs);
-    if (!(q == q)) { bad = true; return 0; }
-    int c = __double2int_ru(q);  // round toward +inf == ceiling for in-range values
-    if (c < 0 || c > ne - 1) { bad = true; c = c < 0 ? 0 : ne - 1; }
-    return c;
-}
 
 __global__ void k_wrap_bin(FmDev d, int wrap, int bin, int gated, int iter)
 {
@@ -362,7 +327,6 @@ constexpr int NB_WARPS = 4;                 // cells processed concurrently per 
 constexpr int NB_THREADS = 32 * NB_WARPS;
 constexpr int NB_STAGE = 256;               // staged candidates per warp
 
-__device__ __forceinline__ bool is_halo(int x, int ne) { return x == 0 || x == ne - 1; }
 
 // Neighbour list build, one warp per extended cell (grid-stride).
 //

@@ -208,6 +208,94 @@ FM_API int fm_pair_digest(fm_handle *h, uint64_t *digest, int64_t *npairs);
 /* Counters: rebuilds done, neighbour capacity in use, largest list seen. */
 FM_API int fm_get_counters(fm_handle *h, int64_t *rebuilds, int32_t *nlist_capacity, int32_t *max_neighbours);
 
+/* ---- multi-job engine: batched replicas and served jobs ---------------- */
+/* No single counterpart in the reference, which runs one system per MPI job:
+ * the engine keeps many independent systems resident on one GPU and advances
+ * all of them one step per tick with the same kernels as above (per-job
+ * geometry, iteration counter, rebuild state and status).  Batching submits
+ * all replicas and runs until drained; serving submits jobs as they arrive
+ * and calls fm_engine_step_chunk in a loop -- jobs are admitted whenever a
+ * slot and enough arena memory (molecules, cells, neighbour rows) are free,
+ * and retired as soon as they finish. */
+typedef struct fm_engine fm_engine;
+
+typedef struct fm_engine_params {
+    int64_t max_molecules;        /* molecule arena: sum of resident job sizes */
+    int64_t max_cells;            /* extended-cell arena */
+    int64_t max_list_entries;     /* neighbour-row arena (entries) */
+    int32_t max_slots;            /* jobs resident at once */
+    int32_t precision;            /* FM_PRECISION_* for every job */
+    int32_t threads_per_molecule; /* 0 = autotuned on the first resident jobs */
+    int32_t ticks_per_chunk;      /* steps per graph launch between admission points */
+    int32_t keep_states;          /* keep final r, v of finished jobs for fm_engine_job_state */
+    int32_t pad_;
+    double delta_t;               /* DELTA_T shared by every job */
+} fm_engine_params;
+
+/* Molecular tags (the reference's modules.f90:79-86). */
+#define FM_TAG_FREE 0
+#define FM_TAG_FIXED 1
+#define FM_TAG_FIXED_SLIDE 2
+#define FM_TAG_TETH 3
+#define FM_TAG_THERMO 4
+#define FM_TAG_TETH_THERMO 5
+#define FM_TAG_TETH_SLIDE 6
+#define FM_TAG_TETH_THERMO_SLIDE 7
+
+typedef struct fm_job {
+    int32_t np;
+    int32_t tplot;
+    double domain[3];
+    double density;
+    double rcutoff;
+    double delta_rneighbr[3];
+    int32_t nsteps;                 /* NSTEPS of this job */
+    int32_t initialstep;
+    int32_t integration_algorithm;  /* 0 leap-frog (tags allowed), 1 velocity Verlet */
+    int32_t ensemble;               /* 0 NVE, 6 tag_move */
+    int32_t force_list;             /* 0 all pairs (any box), 2/3 neighbour list (>= 3 cells) */
+    int32_t pressure_outflag;       /* 1: time-average the virial pressure tensor over record steps */
+    int32_t nthermo;                /* thermostat regions: 0, 1, or 2 split at y = 0 */
+    int32_t rebuild_criteria;       /* 0 vmax, 1 fixed */
+    int32_t fixed_rebuild;
+    int32_t nlist_capacity;         /* neighbour slots per molecule; 0 = automatic */
+    double thermostat_temperature[2];
+    double teth_k2, teth_k4, teth_k6; /* TETHERCOEFFICIENTS */
+} fm_job;
+
+typedef struct fm_job_result {
+    int64_t job_id;
+    int32_t status;          /* FM_OK or the error the job ended with */
+    int32_t nsamples;        /* record steps averaged into ptensor */
+    int32_t final_iter;
+    int32_t rebuilds;
+    int32_t retries;         /* re-admissions after neighbour-list overflow */
+    int32_t pad_;
+    double ptensor[9];       /* time-averaged sum(v v + r f / 2)/V over record steps, row-major */
+    fm_macro last;           /* the last record */
+    double submit_time, admit_time, finish_time;  /* host seconds (steady clock) */
+} fm_job_result;
+
+FM_API int fm_engine_create(const fm_engine_params *p, fm_engine **out);
+FM_API int fm_engine_destroy(fm_engine *e);
+FM_API int fm_engine_set_stream(fm_engine *e, void *cuda_stream);
+/* Queues a job: r, v are (3, np) column-major; tag (np), rtether and slidev
+ * ((3, np)) may be NULL.  The arrays are copied; returns the job id. */
+FM_API int fm_engine_submit(fm_engine *e, const fm_job *job, const double *r, const double *v, const int32_t *tag,
+                            const double *rtether, const double *slidev, int64_t *job_id);
+/* One admission point (retire finished jobs, admit queued ones that fit)
+ * followed by one chunk of ticks; reports how many jobs are resident and
+ * queued afterwards. */
+FM_API int fm_engine_step_chunk(fm_engine *e, int32_t *resident, int32_t *queued);
+/* Chunks until nothing is resident or queued (max_chunks <= 0: no limit). */
+FM_API int fm_engine_run(fm_engine *e, int32_t max_chunks);
+/* Finished jobs' results, oldest first (each returned once). */
+FM_API int fm_engine_take_results(fm_engine *e, fm_job_result *out, int32_t cap, int32_t *n);
+/* Final r, v of a finished job in its upload order (keep_states = 1). */
+FM_API int fm_engine_job_state(fm_engine *e, int64_t job_id, double *r, double *v);
+FM_API int fm_engine_counters(fm_engine *e, int64_t *ticks, int64_t *molecule_steps, int32_t *threads_per_molecule,
+                              int64_t *launches);
+
 /* ---- instrumentation -------------------------------------------------- */
 /* When enabled, every force-kernel launch is bracketed by CUDA events on the
  * handle's stream; fm_get_force_kernel_time returns the summed device time

@@ -73,6 +73,18 @@ typedef struct orc {
     long nn_count, nn_cap;
     /* ---- checkrebuild / record ---- */
     double rmax, simtime;
+    /* tag_move (ensemble 6) data: molecular_properties.f90 */
+    int ensemble;             /* 0 NVE, 6 tag_move */
+    int *tag;                 /* cap */
+    double *rtether, *slidev; /* (3, cap) */
+    double teth_k2, teth_k4, teth_k6;
+    int nthermo;
+    double therm_T[2], zeta[2];
+    /* virial pressure tensor (pressure_outflag 1) */
+    int pressure_outflag;
+    double *rfmol;            /* (9, cap) */
+    double Pxy[9];
+    int nstress;
     double vsum, mv2sum, potenergysum, virial;
     double kinenergy, potenergy, totenergy, temperature, pressure;
     int rebuild_count;
@@ -216,6 +228,10 @@ orc *orc_create(int np, const double domain[3], double rcutoff, const double del
     s->bflag = (int *)xcalloc(4 * cap, sizeof(int));
     s->bond = (int *)xcalloc((size_t)s->max_funcy * (size_t)np, sizeof(int));
     s->bondcount = (int *)xcalloc((size_t)np, sizeof(int));
+    s->tag = (int *)xcalloc(cap, sizeof(int));
+    s->rtether = (double *)xcalloc(3 * cap, sizeof(double));
+    s->slidev = (double *)xcalloc(3 * cap, sizeof(double));
+    s->rfmol = (double *)xcalloc(9 * cap, sizeof(double));
     s->ncell_tot = (s->ncells[0] + 2) * (s->ncells[1] + 2) * (s->ncells[2] + 2);
     s->cellnp = (int *)xcalloc((size_t)s->ncell_tot, sizeof(int));
     s->cellhead = (int *)xcalloc((size_t)s->ncell_tot, sizeof(int));
@@ -241,6 +257,7 @@ void orc_free(orc *s)
     free(s->potenergymol); free(s->potenergymol_POLY); free(s->virialmol); free(s->rdisp);
     free(s->chainID); free(s->subchainID); free(s->funcy); free(s->bflag); free(s->bond);
     free(s->bondcount);
+    free(s->tag); free(s->rtether); free(s->slidev); free(s->rfmol);
     free(s->cellnp); free(s->cellhead); free(s->cn_molno); free(s->cn_next);
     free(s->Nlist); free(s->nhead); free(s->nn_molno); free(s->nn_next);
     free(s);
@@ -746,7 +763,16 @@ static void zero_forces(orc *s)
     memset(s->potenergymol, 0, sizeof(double) * tot);
     memset(s->potenergymol_POLY, 0, sizeof(double) * tot);
     memset(s->virialmol, 0, sizeof(double) * tot);
+    if (s->pressure_outflag) memset(s->rfmol, 0, sizeof(double) * 9 * tot);
     s->virial = 0.0;
+}
+
+/* pressure_tensor_forces (simulation_record.f90:6239-6256). */
+static inline void ptf(orc *s, int molno, const double rij[3], double acc)
+{
+    double *rf = &s->rfmol[9 * (size_t)(molno - 1)];
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) rf[3 * a + b] = rf[3 * a + b] + acc * rij[a] * rij[b];
 }
 
 /* simulation_compute_forces_LJ_neigbr_halfint (:628-726). */
@@ -777,6 +803,10 @@ static void forces_halfint(orc *s)
                     s->potenergymol[j - 1] += e;
                     s->virialmol[i - 1] += acc * r2;
                     s->virialmol[j - 1] += acc * r2;
+                    if (s->pressure_outflag == 1) { /* :698-701 */
+                        ptf(s, i, rij, acc);
+                        if (j <= s->np) ptf(s, j, rij, acc);
+                    }
                 } else if (tev) {
                     s->virialmol[i - 1] += acc * r2;
                     s->virialmol[j - 1] += acc * r2;
@@ -847,6 +877,7 @@ static void forces_AP(orc *s)
                     s->potenergymol[j - 1] += e;
                     s->virialmol[i - 1] += acc * r2;
                     s->virialmol[j - 1] += acc * r2;
+                    if (s->pressure_outflag == 1) { ptf(s, i, rij, acc); ptf(s, j, rij, acc); }
                 } else if (tev) {
                     s->virialmol[i - 1] += acc * r2;
                     s->virialmol[j - 1] += acc * r2;
@@ -991,13 +1022,23 @@ int orc_checkrebuild(orc *s)
 /* periodic wrap on rebuild (messenger.serial.f90:961-1028, in place)        */
 /* ------------------------------------------------------------------------ */
 
+static int is_teth(int t) { return t == 3 || t == 5 || t == 6 || t == 7; }
+
 void orc_sendmols(orc *s)
 {
     for (int n = 0; n < s->np; n++)
         for (int k = 0; k < 3; k++) {
             size_t q = 3 * (size_t)n + k;
-            if (s->r[q] >= s->halfdomain[k]) s->r[q] = s->r[q] - s->domain[k];
-            if (s->r[q] < -s->halfdomain[k]) s->r[q] = s->r[q] + s->domain[k];
+            /* rtether moves with its molecule (messenger.serial.f90:971-1019) */
+            int teth = s->ensemble == 6 && is_teth(s->tag[n]);
+            if (s->r[q] >= s->halfdomain[k]) {
+                s->r[q] = s->r[q] - s->domain[k];
+                if (teth) s->rtether[q] = s->rtether[q] - s->domain[k];
+            }
+            if (s->r[q] < -s->halfdomain[k]) {
+                s->r[q] = s->r[q] + s->domain[k];
+                if (teth) s->rtether[q] = s->rtether[q] + s->domain[k];
+            }
         }
 }
 
@@ -1096,4 +1137,166 @@ void orc_set_monomers(orc *s, const int *chain, const int *subchain, const int *
         s->funcy[n] = funcy[n];
         for (int b = 0; b < 4; b++) s->bflag[4 * (size_t)n + b] = bflag[4 * (size_t)n + b];
     }
+}
+
+/* ------------------------------------------------------------------------ */
+/* leap-frog with tags (simulation_move_particles_lfv.f90:308-514)           */
+/* ------------------------------------------------------------------------ */
+
+void orc_set_tags(orc *s, int ensemble, const int *tag, const double *rtether, const double *slidev, double k2,
+                  double k4, double k6, int nthermo, double T0, double T1)
+{
+    s->ensemble = ensemble;
+    for (int n = 0; n < s->np; n++) {
+        s->tag[n] = tag ? tag[n] : 0;
+        for (int k = 0; k < 3; k++) {
+            s->rtether[3 * (size_t)n + k] = rtether ? rtether[3 * (size_t)n + k] : 0.0;
+            s->slidev[3 * (size_t)n + k] = slidev ? slidev[3 * (size_t)n + k] : 0.0;
+        }
+    }
+    s->teth_k2 = k2; s->teth_k4 = k4; s->teth_k6 = k6;
+    s->nthermo = nthermo;
+    s->therm_T[0] = T0; s->therm_T[1] = T1;
+    s->zeta[0] = s->zeta[1] = 0.0;
+}
+
+void orc_set_pressure(orc *s, int flag) { s->pressure_outflag = flag; }
+
+static int is_thermo(int t) { return t == 4 || t == 5 || t == 7; }
+
+static int therm_region(const orc *s, int n) /* get_therm_region (:286-300) */
+{
+    if (s->nthermo == 2) return s->r[3 * (size_t)n + 1] > 0.0 ? 0 : 1;
+    return 0;
+}
+
+/* tether_force, polynomial form (molecular_properties.f90:833-915). */
+static void tether_force(orc *s, int n)
+{
+    double rio[3];
+    for (int k = 0; k < 3; k++) rio[k] = s->r[3 * (size_t)n + k] - s->rtether[3 * (size_t)n + k];
+    double mag = sqrt(rio[0] * rio[0] + rio[1] * rio[1] + rio[2] * rio[2]);
+    double acct = -2.0 * s->teth_k2 * mag - 4.0 * s->teth_k4 * (mag * mag) - 6.0 * s->teth_k6 * pow(mag, 4.0);
+    for (int k = 0; k < 3; k++) {
+        s->a[3 * (size_t)n + k] = s->a[3 * (size_t)n + k] + acct * rio[k];
+        s->rtether[3 * (size_t)n + k] = s->rtether[3 * (size_t)n + k] + s->slidev[3 * (size_t)n + k] * s->delta_t;
+    }
+}
+
+void orc_move_lfv_tag(orc *s)
+{
+    const double dt = s->delta_t;
+    double ascale[2] = {1.0, 1.0}, bscale[2] = {1.0, 1.0};
+    if (s->nthermo > 0) { /* Nose-Hoover on the thermostatted tags (:325-372) */
+        double mv2sum[2] = {0.0, 0.0}, tnp[2] = {0.0, 0.0};
+        for (int n = 0; n < s->np; n++) {
+            if (!is_thermo(s->tag[n])) continue;
+            double vel[3];
+            for (int k = 0; k < 3; k++) vel[k] = s->v[3 * (size_t)n + k] + 0.5 * s->a[3 * (size_t)n + k] * dt;
+            int tr = therm_region(s, n);
+            double d2 = 0.0;
+            d2 = d2 + vel[0] * vel[0]; d2 = d2 + vel[1] * vel[1]; d2 = d2 + vel[2] * vel[2];
+            mv2sum[tr] = mv2sum[tr] + 1.0 * d2;
+            tnp[tr] = tnp[tr] + 1.0;
+        }
+        for (int r = 0; r < s->nthermo; r++) {
+            double Q = 1.0 * tnp[r] * dt;
+            double dz = tnp[r] > 0.0 ? (mv2sum[r] - (3.0 * tnp[r] + 1) * s->therm_T[r]) / Q : 0.0;
+            s->zeta[r] = s->zeta[r] + dt * dz;
+            bscale[r] = 1.0 / (1.0 + 0.5 * dt * s->zeta[r]);
+            ascale[r] = (1.0 - 0.5 * dt * s->zeta[r]) * bscale[r];
+        }
+    }
+    for (int n = 0; n < s->np; n++) {
+        double *r = &s->r[3 * (size_t)n], *v = &s->v[3 * (size_t)n], *a = &s->a[3 * (size_t)n];
+        const double *sv = &s->slidev[3 * (size_t)n];
+        int t = s->tag[n];
+        int tr;
+        switch (t) {
+        case 0: /* free */
+            for (int k = 0; k < 3; k++) { v[k] = v[k] + dt * a[k]; r[k] = r[k] + dt * v[k]; }
+            break;
+        case 1: break; /* fixed */
+        case 2: for (int k = 0; k < 3; k++) r[k] = r[k] + dt * sv[k]; break;
+        case 3:
+            tether_force(s, n);
+            for (int k = 0; k < 3; k++) { v[k] = v[k] + dt * a[k]; r[k] = r[k] + dt * v[k]; }
+            break;
+        case 4:
+            tr = therm_region(s, n);
+            for (int k = 0; k < 3; k++) { v[k] = v[k] * ascale[tr] + a[k] * dt * bscale[tr]; r[k] = r[k] + v[k] * dt; }
+            break;
+        case 5:
+            tr = therm_region(s, n);
+            tether_force(s, n);
+            for (int k = 0; k < 3; k++) { v[k] = v[k] * ascale[tr] + a[k] * dt * bscale[tr]; r[k] = r[k] + v[k] * dt; }
+            break;
+        case 6:
+            tether_force(s, n);
+            for (int k = 0; k < 3; k++) { v[k] = v[k] + dt * a[k]; r[k] = r[k] + dt * v[k] + dt * sv[k]; }
+            break;
+        case 7:
+            tr = therm_region(s, n);
+            tether_force(s, n);
+            for (int k = 0; k < 3; k++) {
+                v[k] = v[k] * ascale[tr] + a[k] * dt * bscale[tr];
+                r[k] = r[k] + v[k] * dt + sv[k] * dt;
+            }
+            break;
+        default: break;
+        }
+    }
+    s->simtime = s->simtime + dt;
+}
+
+/* cumulative_pressure case 1 (simulation_record.f90:3151-3220). */
+void orc_cumulative_pressure(orc *s)
+{
+    double P[9] = {0};
+    double volume = s->domain[0] * s->domain[1] * s->domain[2];
+    for (int n = 0; n < s->np; n++) {
+        double vel[3];
+        for (int k = 0; k < 3; k++) {
+            vel[k] = s->v[3 * (size_t)n + k];
+            if (s->integration_algorithm == 0) vel[k] = s->v[3 * (size_t)n + k] + 0.5 * s->a[3 * (size_t)n + k] * s->delta_t;
+        }
+        const double *rf = &s->rfmol[9 * (size_t)n];
+        for (int j = 0; j < 3; j++)
+            for (int k = 0; k < 3; k++) P[3 * k + j] += vel[k] * vel[j] + rf[3 * k + j] / 2.0;
+    }
+    for (int q = 0; q < 9; q++) s->Pxy[q] += P[q] / volume;
+    s->nstress += 1;
+}
+
+void orc_pressure_average(orc *s, double out[9], int *nsamples)
+{
+    for (int q = 0; q < 9; q++) out[q] = s->nstress ? s->Pxy[q] / s->nstress : 0.0;
+    *nsamples = s->nstress;
+}
+
+/* md_advance_lfv (md.f90:109-139) for nsteps iterations. */
+int orc_run_lfv(orc *s, int nsteps, double *rec_out, int rec_cap, int *nrec)
+{
+    int rc;
+    *nrec = 0;
+    for (int st = 0; st < nsteps; st++) {
+        s->iter += 1;
+        if ((rc = orc_compute_forces(s))) return rc;
+        if ((s->iter % s->tplot) == 0) {
+            orc_evaluate_macroscopic_properties(s);
+            if (s->pressure_outflag == 1) orc_cumulative_pressure(s);
+            if (rec_out && *nrec < rec_cap) {
+                double *o = &rec_out[10 * (size_t)(*nrec)];
+                o[0] = (double)s->iter;
+                orc_macro(s, o + 1);
+            }
+            (*nrec)++;
+        }
+        if (s->ensemble == 6) orc_move_lfv_tag(s);
+        else orc_move_lfv(s);
+        if (s->force_list != 0 && (rc = orc_updateborders(s, 0))) return rc;
+        int rebuild = orc_checkrebuild(s);
+        if (rebuild && st < nsteps - 1 && (rc = orc_rebuild(s))) return rc;
+    }
+    return ORC_OK;
 }

@@ -80,6 +80,12 @@ def lib():
         L.orc_potshift.restype = C.c_double
         L.orc_potshift.argtypes = [C.c_double]
         L.orc_set_monomers.argtypes = [C.c_void_p, i3, i3, i3, i3]
+        L.orc_set_tags.argtypes = [C.c_void_p, C.c_int, i3, d3, d3, C.c_double, C.c_double, C.c_double, C.c_int,
+                                   C.c_double, C.c_double]
+        L.orc_set_pressure.argtypes = [C.c_void_p, C.c_int]
+        L.orc_run_lfv.restype = C.c_int
+        L.orc_run_lfv.argtypes = [C.c_void_p, C.c_int, d3, C.c_int, i3]
+        L.orc_pressure_average.argtypes = [C.c_void_p, d3, i3]
         _lib = L
     return _lib
 
@@ -241,6 +247,30 @@ class Oracle:
         nrec = C.c_int(0)
         _check(lib().orc_run_vv(self.h, int(nsteps), _dp(out), rec_cap, C.byref(nrec)))
         return out[:min(nrec.value, rec_cap)]
+
+    def set_tags(self, ensemble, tag=None, rtether=None, slidev=None, k=(0.0, 0.0, 0.0), nthermo=0,
+                 therm_T=(0.0, 0.0)):
+        tg = None if tag is None else np.ascontiguousarray(tag, np.int32)
+        rt = None if rtether is None else np.ascontiguousarray(rtether, np.float64)
+        sv = None if slidev is None else np.ascontiguousarray(slidev, np.float64)
+        lib().orc_set_tags(self.h, int(ensemble), None if tg is None else _ip(tg), None if rt is None else _dp(rt),
+                           None if sv is None else _dp(sv), float(k[0]), float(k[1]), float(k[2]), int(nthermo),
+                           float(therm_T[0]), float(therm_T[1]))
+
+    def set_pressure(self, flag=1):
+        lib().orc_set_pressure(self.h, int(flag))
+
+    def run_lfv(self, nsteps, rec_cap=100000):
+        out = np.zeros((rec_cap, 10))
+        nrec = C.c_int(0)
+        _check(lib().orc_run_lfv(self.h, int(nsteps), _dp(out), rec_cap, C.byref(nrec)))
+        return out[:min(nrec.value, rec_cap)]
+
+    def pressure_average(self):
+        out = np.zeros(9)
+        n = C.c_int(0)
+        lib().orc_pressure_average(self.h, _dp(out), C.byref(n))
+        return out.reshape(3, 3), n.value
 
     def pair_list(self):
         """(owner, partner, code) arrays, 1-based glob_no; code 13 = no image."""

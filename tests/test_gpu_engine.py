@@ -1,0 +1,144 @@
+"""The multi-job slot engine (batched replicas, served jobs) on the GPU.
+
+Tolerances: a job run in the engine follows the single-system path and the
+FP64 oracle to 1e-9 in positions after O(100) steps (different kernels sum the
+same pairs, so the trajectories agree to rounding that chaos amplifies
+slowly); a job's results are bit-identical whether it runs alone or among
+other jobs (jobs never share arithmetic)."""
+import numpy as np
+import pytest
+
+import oracle as O
+from flowmol_b200 import api, couette, lattice
+
+pytestmark = pytest.mark.gpu
+
+TPM = 4
+
+
+def engine(max_mol=300000, slots=16, ticks=20, **kw):
+    return api.Engine(max_molecules=max_mol, max_cells=400000, max_list_entries=max_mol * 160,
+                      max_slots=slots, threads_per_molecule=TPM, ticks_per_chunk=ticks, **kw)
+
+
+def lj_replica(nunits, rho, T, seed, jitter=0.03):
+    r, v, dom = lattice.lj_fluid(nunits, rho, T, seed)
+    return lattice.jitter(r, jitter, seed, dom), v, dom
+
+
+def test_batch_replicas_follow_single_system(gpu_lib):
+    reps = [([6, 6, 6], 0.8, 1.0, 11), ([7, 5, 6], 0.6, 1.3, 12), ([8, 8, 8], 0.85, 0.8, 13),
+            ([3, 3, 3], 0.9, 1.0, 14)]  # the last has fewer than 3 cells: all pairs
+    nsteps = 150
+    e = engine()
+    ids = []
+    for nu, rho, T, seed in reps:
+        r, v, dom = lj_replica(nu, rho, T, seed)
+        fl = 0 if min(np.floor(dom / 2.8)) < 3 else 3
+        ids.append((e.submit(api.make_job(len(r), dom, 2.5, nsteps, tplot=50, force_list=fl), r, v), r, v, dom, fl))
+    e.run()
+    res = {x["job_id"]: x for x in e.results()}
+    for jid, r, v, dom, fl in ids:
+        assert res[jid]["status"] == 0
+        assert res[jid]["final_iter"] == nsteps
+        rg, vg = e.job_state(jid, len(r))
+        p = api.make_params(len(r), dom, 2.5, tplot=50, force_list=fl, threads_per_molecule=TPM)
+        s = api.MDSystem(p)
+        s.upload(r, v)
+        s.setup()
+        s.simulation_md(nsteps)
+        rs, vs, _, _ = s.download()
+        np.testing.assert_allclose(rg, rs, rtol=0, atol=1e-9)
+        np.testing.assert_allclose(vg, vs, rtol=0, atol=1e-9)
+        last = s.records()[-1]
+        assert res[jid]["last"]["iter"] == last["iter"] == nsteps
+        assert res[jid]["last"]["totenergy"] == pytest.approx(last["totenergy"], rel=1e-11)
+        s.close()
+
+
+def couette_inputs(n_target, speed, seed):
+    nu = couette.nunits_for(n_target)
+    r, v, tag, rt, sv, dom = couette.couette_job(nu, 0.8, 1.0, speed, seed)
+    job = dict(np_=len(r), domain=dom, rcutoff=couette.WCA_RC, integration_algorithm=0, ensemble=6,
+               pressure_outflag=1, nthermo=2, thermostat_temperature=(1.0, 1.0), teth=(0.0, 5000.0, 5.0e6),
+               tplot=10)
+    return job, r, v, tag, rt, sv, dom
+
+
+def test_couette_job_follows_oracle(gpu_lib):
+    job, r, v, tag, rt, sv, dom = couette_inputs(500, 1.0, 21)
+    nsteps = 200
+    e = engine()
+    jid = e.submit(api.make_job(nsteps=nsteps, **job), r, v, tag, rt, sv)
+    e.run()
+    res = e.results()[0]
+    assert res["status"] == 0 and res["nsamples"] == nsteps // 10
+    rg, vg = e.job_state(jid, len(r))
+    o = O.Oracle(r, v, dom, couette.WCA_RC, tplot=10, integration_algorithm=0)
+    o.set_tags(6, tag, rt, sv, (0.0, 5000.0, 5.0e6), 2, (1.0, 1.0))
+    o.set_pressure(1)
+    o.setup()
+    o.run_lfv(nsteps)
+    P, ns = o.pressure_average()
+    assert ns == res["nsamples"]
+    np.testing.assert_allclose(res["ptensor"], P, rtol=1e-9, atol=1e-11)
+    np.testing.assert_allclose(rg, o.r, rtol=0, atol=1e-9)
+    np.testing.assert_allclose(vg, o.v, rtol=0, atol=1e-8)
+
+
+def test_jobs_alone_equal_jobs_in_the_mix(gpu_lib):
+    """Served jobs give bit-identical results alone and while other jobs come
+    and go (two slots, five jobs: admission and retirement interleave)."""
+    inputs = []
+    for k, (n, speed) in enumerate([(300, 0.5), (700, 2.0), (420, 1.2), (1100, 0.8)]):
+        job, r, v, tag, rt, sv, dom = couette_inputs(n, speed, 30 + k)
+        inputs.append((api.make_job(nsteps=60 + 40 * k, **job), r, v, tag, rt, sv))
+    rl, vl, doml = lj_replica([6, 6, 6], 0.8, 1.1, 41)
+    inputs.append((api.make_job(len(rl), doml, 2.5, 90, tplot=30), rl, vl, None, None, None))
+    alone = []
+    for job, r, v, tag, rt, sv in inputs:
+        e = engine(slots=1)
+        jid = e.submit(job, r, v, tag, rt, sv)
+        e.run()
+        res = e.results()[0]
+        alone.append((res, e.job_state(jid, len(r))))
+        e.close()
+    mix = engine(slots=2)
+    ids = [mix.submit(job, r, v, tag, rt, sv) for job, r, v, tag, rt, sv in inputs]
+    mix.run()
+    res = {x["job_id"]: x for x in mix.results()}
+    for jid, (a_res, (ra, va)), (job, r, *_rest) in zip(ids, alone, inputs):
+        m = res[jid]
+        assert m["status"] == 0 and a_res["status"] == 0
+        assert np.array_equal(m["ptensor"], a_res["ptensor"])
+        assert m["last"] == a_res["last"]
+        rm, vm = mix.job_state(jid, len(r))
+        assert np.array_equal(rm, ra) and np.array_equal(vm, va)
+
+
+def test_list_overflow_is_retried(gpu_lib):
+    r, v, dom = lj_replica([6, 6, 6], 0.8, 1.0, 51)
+    ref = engine()
+    jr = ref.submit(api.make_job(len(r), dom, 2.5, 60, tplot=20), r, v)
+    ref.run()
+    res_ref = ref.results()[0]
+    small = engine()
+    js = small.submit(api.make_job(len(r), dom, 2.5, 60, tplot=20, nlist_capacity=8), r, v)
+    small.run()
+    res = small.results()[0]
+    assert res["status"] == 0 and res["retries"] >= 1
+    assert np.array_equal(ref.job_state(jr, len(r))[0], small.job_state(js, len(r))[0])
+    assert res["last"] == res_ref["last"]
+
+
+def test_failing_job_does_not_disturb_others(gpu_lib):
+    r, v, dom = lj_replica([6, 6, 6], 0.8, 1.0, 61)
+    bad = r.copy()
+    bad[3] = [5.0 * dom[0], 0.0, 0.0]
+    e = engine()
+    jb = e.submit(api.make_job(len(r), dom, 2.5, 40, tplot=20), bad, v)
+    jg = e.submit(api.make_job(len(r), dom, 2.5, 40, tplot=20), r, v)
+    e.run()
+    res = {x["job_id"]: x for x in e.results()}
+    assert res[jb]["status"] == 4  # FM_ERR_ESCAPE
+    assert res[jg]["status"] == 0 and res[jg]["final_iter"] == 40
