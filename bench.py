@@ -190,6 +190,133 @@ def run_e2e(api, torch, r, v, dom, precision, steps, dev):
             "d2h_bytes_per_step": d2h / steps, "steps": steps, "seconds": t1 - t0}
 
 
+def batch_replicas(nrep=256, seed=0x466D6F6C + 4):
+    """The batched-ensemble configuration: replica sizes log-uniform in
+    500-32000 molecules (rounded to 4 n^3 FCC), densities U(0.3, 0.9),
+    temperatures U(0.7, 1.5), rc 2.5; boxes below 3 cells run all pairs."""
+    from flowmol_b200 import lattice
+    rng = np.random.Generator(np.random.Philox(seed))
+    out = []
+    for k in range(nrep):
+        n_target = float(np.exp(rng.uniform(np.log(500.0), np.log(32000.0))))
+        m = max(2, int(round((n_target / 4.0) ** (1.0 / 3.0))))
+        rho = float(rng.uniform(0.3, 0.9))
+        T = float(rng.uniform(0.7, 1.5))
+        r, v, dom = lattice.lj_fluid([m, m, m], rho, T, seed + 1000 + k)
+        fl = 0 if min(np.floor(dom / (RC + SKIN))) < 3 else 3
+        out.append((r, v, dom, rho, fl))
+    return out
+
+
+def run_batched(api, torch, dev, nsteps, nrep=256):
+    """All replicas in one engine (graph-captured ticks) vs the plain
+    single-system form run one replica at a time (bounded to plain_steps
+    per replica; throughput is per-step so the rates compare)."""
+    reps = batch_replicas(nrep)
+    tot = sum(len(x[0]) for x in reps)
+    e = api.Engine(max_molecules=tot + 1024, max_cells=2_000_000, max_list_entries=(tot + 1024) * 160,
+                   max_slots=nrep, precision=api.PRECISION_FP32, ticks_per_chunk=50, keep_states=False)
+    for r, v, dom, rho, fl in reps:
+        e.submit(api.make_job(len(r), dom, RC, nsteps, density=rho, tplot=TPLOT, force_list=fl), r, v)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    e.run()
+    t_batch = time.perf_counter() - t0
+    res = e.results()
+    c = e.counters()
+    bad = [x for x in res if x["status"] != 0]
+    e.close()
+    plain_steps = min(nsteps, 100)
+    t_plain = 0.0
+    for r, v, dom, rho, fl in reps:
+        p = api.make_params(len(r), dom, RC, (SKIN,) * 3, DT, TPLOT, density=rho, force_list=fl,
+                            precision=api.PRECISION_FP32)
+        s = api.MDSystem(p)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        s.upload(r, v)
+        s.setup()
+        s.simulation_md(plain_steps, blocking=True)
+        t_plain += time.perf_counter() - t0
+        s.close()
+    v_batch = tot * nsteps / t_batch
+    v_plain = tot * plain_steps / t_plain
+    return {"value": v_batch, "unit": UNIT, "replicas": nrep, "molecules": tot, "steps_each": nsteps,
+            "seconds": t_batch, "plain_one_at_a_time": v_plain, "plain_steps_each": plain_steps,
+            "ratio_vs_plain": v_batch / v_plain, "failed": len(bad), "threads_per_molecule": c["threads_per_molecule"],
+            "gpu_launches": c["launches"],
+            "workload": "256 periodic LJ replicas, N log-uniform 500-32000 (4 n^3 FCC), rho U(0.3,0.9), "
+                        "T U(0.7,1.5), rc 2.5, skin 0.3, dt 0.005, VV, FP32 forces; boxes < 3 cells: all pairs"}
+
+
+def run_served(api, torch, dev, njobs, seed=0x466D6F6C + 5):
+    """Poisson-arriving Couette jobs through the engine's admission loop.
+    Job sizes log-uniform in 256-65536 molecules, 200-2000 steps, wall speed
+    U(0.5, 2.0); the arrival rate is set from a measured service rate so the
+    GPU stays busy.  Latency = finish time - scheduled arrival time."""
+    from flowmol_b200 import couette
+    rng = np.random.Generator(np.random.Philox(seed))
+
+    def make(k, rng):
+        n_target = float(np.exp(rng.uniform(np.log(256.0), np.log(65536.0))))
+        nu = couette.nunits_for(n_target)
+        steps = int(rng.integers(200, 2001))
+        speed = float(rng.uniform(0.5, 2.0))
+        r, v, tag, rt, sv, dom = couette.couette_job(nu, 0.8, 1.0, speed, seed + 77 + k)
+        job = api.make_job(len(r), dom, couette.WCA_RC, steps, tplot=10, integration_algorithm=0, ensemble=6,
+                           pressure_outflag=1, nthermo=2, thermostat_temperature=(1.0, 1.0),
+                           teth=(0.0, 5000.0, 5.0e6))
+        return (job, r, v, tag, rt, sv)
+
+    def new_engine():
+        cap = 4_000_000
+        return api.Engine(max_molecules=cap, max_cells=4_000_000, max_list_entries=cap * 48, max_slots=512,
+                          precision=api.PRECISION_FP32, ticks_per_chunk=20, keep_states=False)
+
+    # service-rate probe: 48 jobs of the same distribution submitted at once
+    prng = np.random.Generator(np.random.Philox(seed + 1))
+    probe = [make(100000 + k, prng) for k in range(48)]
+    e = new_engine()
+    for j in probe:
+        e.submit(*j)
+    t0 = time.perf_counter()
+    e.run()
+    rate_work = sum(j[0].np * j[0].nsteps for j in probe) / (time.perf_counter() - t0)
+    e.close()
+    jobs = []
+    for k in range(njobs):
+        jobs.append(make(k, rng))
+    work = sum(j[0].np * j[0].nsteps for j in jobs)
+    e = new_engine()
+    arrivals = np.cumsum(rng.exponential(1.0, njobs))
+    mean_work = work / njobs
+    lam = 0.9 * rate_work / mean_work
+    t_arr = arrivals / lam
+    t0 = time.monotonic()
+    nxt = 0
+    done = []
+    while len(done) < njobs:
+        now = time.monotonic() - t0
+        while nxt < njobs and t_arr[nxt] <= now:
+            e.submit(*jobs[nxt])
+            nxt += 1
+        res, q = e.step_chunk()
+        done += e.results()
+        if res == 0 and q == 0 and nxt < njobs:
+            time.sleep(max(0.0, min(0.01, t_arr[nxt] - (time.monotonic() - t0))))
+    t_total = time.monotonic() - t0
+    lat = np.array([d["finish_time"] - (t0 + t_arr[d["job_id"] - 1]) for d in done])
+    bad = [d for d in done if d["status"] != 0]
+    c = e.counters()
+    e.close()
+    return {"value": work / t_total, "unit": UNIT, "jobs": njobs, "molecule_steps": work, "seconds": t_total,
+            "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
+            "arrival_rate_per_s": lam, "probe_service_rate": rate_work, "failed": len(bad), "threads_per_molecule": c["threads_per_molecule"],
+            "workload": "Couette channels (WCA fluid between tethered, thermostatted FCC walls, top wall "
+                        "sliding U(0.5,2.0)), N log-uniform 256-65536, 200-2000 steps, leap-frog + tags, "
+                        "time-averaged virial pressure tensor, FP32 forces"}
+
+
 def cpu_baseline(r, v, dom, nsteps=8):
     """The FP64 oracle (C restatement of the reference's routines, one
     thread) on the same 1M system: setup excluded, nsteps timed."""
@@ -215,6 +342,10 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--batch-replicas", type=int, default=256)
+    ap.add_argument("--batch-steps", type=int, default=2000)
+    ap.add_argument("--serve-jobs", type=int, default=512)
+    ap.add_argument("--no-forms", action="store_true", help="skip the batched and served forms")
     ap.add_argument("--profile-case", choices=["fp32", "fp64"], default=None,
                     help="profiling workload: setup + 10 fused steps of the 1M system, no timing")
     args = ap.parse_args()
@@ -288,6 +419,14 @@ def main():
     if e2e is not None:
         e2e["value"] = world * n * args.steps / max_over_ranks(e2e["seconds"])
     barrier()
+    batched = served = None
+    if not args.no_forms:
+        batched = run_batched(api, torch, dev, args.batch_steps, args.batch_replicas)
+        batched["value"] = world * batched["value"] * batched["seconds"] / max_over_ranks(batched["seconds"])
+        barrier()
+        served = run_served(api, torch, dev, args.serve_jobs)
+        served["value"] = world * served["value"] * served["seconds"] / max_over_ranks(served["seconds"])
+        barrier()
 
     if rank == 0:
         value = world * n * args.steps / (ms32 * 1e-3)
@@ -319,6 +458,8 @@ def main():
                          "traffic": traffic},
             "clocks": f32["clocks"],
             "gpu_launches": f32["launches"],
+            "batched": batched,
+            "served": served,
             "e2e": e2e,
             "cpu_baseline": cpu,
         }

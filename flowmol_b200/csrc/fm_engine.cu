@@ -144,7 +144,7 @@ int dal(T **p, size_t n)
 void free_all(fm_engine *e)
 {
     fm::EngDev &d = e->d;
-    void *ptrs[] = {d.slots, d.pos0, d.pos1, d.vx, d.vy, d.vz, d.ax, d.ay, d.az, d.slot_of, d.uidx, d.tag,
+    void *ptrs[] = {d.slots, d.flags, d.pos0, d.pos1, d.vx, d.vy, d.vz, d.ax, d.ay, d.az, d.slot_of, d.uidx, d.tag,
                     d.rteth, d.slidev, d.tpos, d.trteth, d.tslidev, d.tvx, d.tvy, d.tvz, d.tax, d.tay, d.taz,
                     d.tuidx, d.ttag, d.cell_slot, d.cell_of, d.cell_count, d.cell_start, d.perm, d.nbr, d.nnbr,
                     d.rterm, d.tmv2, e->stage, e->stage_i};
@@ -407,6 +407,21 @@ int autotune(fm_engine *e)
     return FM_OK;
 }
 
+// High-water marks of the molecule and cell arenas over the resident jobs.
+int update_hwm(fm_engine *e)
+{
+    int mh = 0, ch = 0;
+    for (auto &j : e->resident) {
+        if (j.slot < 0) continue;
+        mh = std::max<int>(mh, (int)(j.mol_off + j.p.np));
+        ch = std::max<int>(ch, (int)(j.cell_off + j.ncell));
+    }
+    int hw[2] = {mh, ch};
+    EN_CUDA(cudaMemcpyAsync(&e->d.flags->mol_hwm, hw, sizeof hw, cudaMemcpyHostToDevice, e->st));
+    EN_CUDA(cudaStreamSynchronize(e->st));
+    return FM_OK;
+}
+
 int sync_table(fm_engine *e)
 {
     EN_CUDA(cudaMemcpyAsync(e->table.data(), e->d.slots, sizeof(fm::EngSlot) * e->table.size(),
@@ -448,7 +463,7 @@ extern "C" int fm_engine_create(const fm_engine_params *p, fm_engine **out)
     const size_t M = (size_t)d.mol_cap, Cc = (size_t)d.cell_cap;
     int rc = FM_OK;
 #define EA(ptr, n) if (rc == FM_OK) rc = dal(&(ptr), (size_t)(n));
-    EA(d.slots, d.nslots) EA(d.pos0, M) EA(d.pos1, M)
+    EA(d.slots, d.nslots) EA(d.flags, 1) EA(d.pos0, M) EA(d.pos1, M)
     EA(d.vx, M) EA(d.vy, M) EA(d.vz, M) EA(d.ax, M) EA(d.ay, M) EA(d.az, M)
     EA(d.slot_of, M) EA(d.uidx, M) EA(d.tag, M) EA(d.rteth, M) EA(d.slidev, M)
     EA(d.tpos, M) EA(d.trteth, M) EA(d.tslidev, M)
@@ -463,6 +478,7 @@ extern "C" int fm_engine_create(const fm_engine_params *p, fm_engine **out)
         return rc;
     }
     cudaMemset(d.slots, 0, sizeof(fm::EngSlot) * (size_t)d.nslots);
+    cudaMemset(d.flags, 0, sizeof(fm::EngFlags));
     cudaMemset(d.slot_of, 0xff, sizeof(int32_t) * M);
     cudaMemset(d.cell_slot, 0xff, sizeof(int32_t) * Cc);
     cudaMemset(d.cell_count, 0, sizeof(int32_t) * Cc);
@@ -568,6 +584,7 @@ extern "C" int fm_engine_step_chunk(fm_engine *e, int32_t *resident_out, int32_t
     if (nres == 0 && !e->queue.empty())
         // nothing resident and the head of the queue cannot be admitted: it never will be
         return efail(FM_ERR_ARG, "queued job does not fit the engine's arenas");
+    EN_TRY(update_hwm(e));
     if (nres > 0) {
         if (!e->tuned) EN_TRY(autotune(e));
         if (!e->graph || e->graph_tpm != e->tpm) EN_TRY(capture(e));

@@ -52,8 +52,17 @@ struct EngSlot {
     FmRecord last_rec;
 };
 
+// Per-tick summary written by the decide kernel, and the arena high-water
+// marks written by the host at admission; kernels bound their loops and skip
+// whole stages with them (device memory, so a captured graph sees updates).
+struct EngFlags {
+    int any_rebuild, any_list, any_ap, any_lfv, any_thermo, any_record;
+    int mol_hwm, cell_hwm;
+};
+
 struct EngDev {
     int nslots;
+    EngFlags *flags;
     int mol_cap;     // arena molecules
     int cell_cap;    // arena cells
     double dt, half_dt, half_dt2;

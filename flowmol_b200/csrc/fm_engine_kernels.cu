@@ -68,11 +68,8 @@ __device__ __forceinline__ void fold_vmax2(EngSlot *slots, int k, double m2)
 // decide
 // ---------------------------------------------------------------------------
 
-__global__ void k_e_decide(EngDev d)
+__device__ void decide_slot(const EngDev &d, EngSlot &s)
 {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= d.nslots) return;
-    EngSlot &s = d.slots[k];
     s.phase = PHASE_IDLE;
     if (s.state == SLOT_EMPTY || s.state == SLOT_DONE || s.state == SLOT_FAILED) return;
     if (s.status & ST_FATAL) { s.state = SLOT_FAILED; return; }
@@ -117,6 +114,31 @@ __global__ void k_e_decide(EngDev d)
     if (vv) s.simtime = s.simtime + d.dt;        // simulation_move_particles_vv.f90:191
 }
 
+constexpr int EDEC = 1024;
+__global__ void __launch_bounds__(EDEC) k_e_decide(EngDev d)
+{
+    __shared__ int f[6];
+    if (threadIdx.x < 6) f[threadIdx.x] = 0;
+    __syncthreads();
+    for (int k = threadIdx.x; k < d.nslots; k += EDEC) {
+        EngSlot &s = d.slots[k];
+        decide_slot(d, s);
+        if (slot_active(s)) {
+            if (s.rebuild) atomicOr(&f[0], 1);
+            if (s.mode == MODE_LIST) atomicOr(&f[1], 1);
+            if (s.mode == MODE_ALLPAIRS) atomicOr(&f[2], 1);
+            if (s.integrator == 0) atomicOr(&f[3], 1);
+            if (s.integrator == 0 && s.nthermo > 0) atomicOr(&f[4], 1);
+            if (s.record) atomicOr(&f[5], 1);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        d.flags->any_rebuild = f[0]; d.flags->any_list = f[1]; d.flags->any_ap = f[2];
+        d.flags->any_lfv = f[3]; d.flags->any_thermo = f[4]; d.flags->any_record = f[5];
+    }
+}
+
 // ---------------------------------------------------------------------------
 // rebuild pipeline (gated per slot)
 // ---------------------------------------------------------------------------
@@ -125,7 +147,9 @@ __device__ __forceinline__ bool slot_rebuilding(const EngSlot &s) { return slot_
 
 __global__ void k_e_wrap_bin(EngDev d)
 {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < d.mol_cap; i += gridDim.x * blockDim.x) {
+    if (!d.flags->any_rebuild) return;
+    const int hwm = d.flags->mol_hwm;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < hwm; i += gridDim.x * blockDim.x) {
         const int k = d.slot_of[i];
         if (k < 0) continue;
         EngSlot &s = d.slots[k];
@@ -166,6 +190,7 @@ __global__ void k_e_wrap_bin(EngDev d)
 constexpr int ESCAN = 1024;
 __global__ void __launch_bounds__(ESCAN) k_e_scan(EngDev d)
 {
+    if (!d.flags->any_rebuild) return;
     const EngSlot &s = d.slots[blockIdx.x];
     if (!slot_rebuilding(s) || s.mode != MODE_LIST) return;
     __shared__ int ws[ESCAN / 32];
@@ -208,7 +233,9 @@ __global__ void __launch_bounds__(ESCAN) k_e_scan(EngDev d)
 
 __global__ void k_e_scatter(EngDev d)
 {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < d.mol_cap; i += gridDim.x * blockDim.x) {
+    if (!d.flags->any_rebuild) return;
+    const int hwm = d.flags->mol_hwm;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < hwm; i += gridDim.x * blockDim.x) {
         const int k = d.slot_of[i];
         if (k < 0) continue;
         const EngSlot &s = d.slots[k];
@@ -221,7 +248,9 @@ __global__ void k_e_scatter(EngDev d)
 
 __global__ void k_e_sort(EngDev d)
 {
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.cell_cap; c += gridDim.x * blockDim.x) {
+    if (!d.flags->any_rebuild) return;
+    const int hwm = d.flags->cell_hwm;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < hwm; c += gridDim.x * blockDim.x) {
         const int k = d.cell_slot[c];
         if (k < 0) continue;
         const EngSlot &s = d.slots[k];
@@ -243,7 +272,9 @@ __global__ void k_e_sort(EngDev d)
 
 __global__ void k_e_reorder_gather(EngDev d)
 {
-    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < d.mol_cap; n += gridDim.x * blockDim.x) {
+    if (!d.flags->any_rebuild) return;
+    const int hwm = d.flags->mol_hwm;
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < hwm; n += gridDim.x * blockDim.x) {
         const int k = d.slot_of[n];
         if (k < 0) continue;
         const EngSlot &s = d.slots[k];
@@ -261,7 +292,9 @@ __global__ void k_e_reorder_gather(EngDev d)
 
 __global__ void k_e_reorder_copy(EngDev d)
 {
-    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < d.mol_cap; n += gridDim.x * blockDim.x) {
+    if (!d.flags->any_rebuild) return;
+    const int hwm = d.flags->mol_hwm;
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < hwm; n += gridDim.x * blockDim.x) {
         const int k = d.slot_of[n];
         if (k < 0) continue;
         const EngSlot &s = d.slots[k];
@@ -288,8 +321,10 @@ __global__ void __launch_bounds__(EB_WARPS * 32) k_e_build(EngDev d)
     __shared__ float4 s_f[EB_WARPS][EB_STAGE];
     __shared__ int s_off[EB_WARPS][55];
     __shared__ int s_start[EB_WARPS][54], s_code[EB_WARPS][54];
+    if (!d.flags->any_rebuild) return;
+    const int hwm = d.flags->cell_hwm;
     const int stride = gridDim.x * EB_WARPS;
-    for (int c = blockIdx.x * EB_WARPS + warp; c < d.cell_cap; c += stride) {
+    for (int c = blockIdx.x * EB_WARPS + warp; c < hwm; c += stride) {
         const int k = d.cell_slot[c];
         if (k < 0) continue;
         EngSlot &s = d.slots[k];
@@ -543,9 +578,11 @@ __global__ void __launch_bounds__(EF_THREADS) k_e_force(EngDev d)
 {
     constexpr int PER_BLOCK = EF_THREADS / TPM;
     const int lane = threadIdx.x % TPM;
-    for (int base = blockIdx.x * PER_BLOCK; base < d.mol_cap; base += gridDim.x * PER_BLOCK) {
+    if (!FORCE_ONLY && !d.flags->any_list) return;
+    const int hwm = d.flags->mol_hwm;
+    for (int base = blockIdx.x * PER_BLOCK; base < hwm; base += gridDim.x * PER_BLOCK) {
         const int i = base + threadIdx.x / TPM;
-        int k = i < d.mol_cap ? d.slot_of[i] : -1;
+        int k = i < hwm ? d.slot_of[i] : -1;
         const EngSlot *sp = k >= 0 ? &d.slots[k] : nullptr;
         bool act = k >= 0 && sp->mode == MODE_LIST &&
                    (FORCE_ONLY ? (sp->state == SLOT_RUN) : slot_active(*sp));
@@ -597,9 +634,11 @@ __global__ void __launch_bounds__(EF_THREADS) k_e_force(EngDev d)
 template <int PREC>
 __global__ void k_e_force_ap(EngDev d)
 {
-    for (int base = blockIdx.x * blockDim.x; base < d.mol_cap; base += gridDim.x * blockDim.x) {
+    if (!d.flags->any_ap) return;
+    const int hwm = d.flags->mol_hwm;
+    for (int base = blockIdx.x * blockDim.x; base < hwm; base += gridDim.x * blockDim.x) {
         const int i = base + threadIdx.x;
-        int k = i < d.mol_cap ? d.slot_of[i] : -1;
+        int k = i < hwm ? d.slot_of[i] : -1;
         const EngSlot *sp = k >= 0 ? &d.slots[k] : nullptr;
         const bool act = k >= 0 && sp->mode == MODE_ALLPAIRS && slot_active(*sp);
         if (!act) k = -1;
@@ -658,6 +697,7 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double (&c)[NV])
 // at y = 0): Q = N_thermo dt, dzeta/dt = (sum m v^2 - (3 N_thermo + 1) T)/Q.
 __global__ void __launch_bounds__(ER) k_e_thermo(EngDev d)
 {
+    if (!d.flags->any_thermo) return;
     EngSlot &s = d.slots[blockIdx.x];
     if (!slot_active(s) || s.integrator != 0 || s.nthermo <= 0) return;
     double v[4] = {0, 0, 0, 0}, c[4] = {0, 0, 0, 0};  // mv2 region 0/1, count region 0/1
@@ -683,9 +723,11 @@ __global__ void __launch_bounds__(ER) k_e_thermo(EngDev d)
 
 __global__ void k_e_move_lfv(EngDev d)
 {
-    for (int base = blockIdx.x * blockDim.x; base < d.mol_cap; base += gridDim.x * blockDim.x) {
+    if (!d.flags->any_lfv) return;
+    const int hwm = d.flags->mol_hwm;
+    for (int base = blockIdx.x * blockDim.x; base < hwm; base += gridDim.x * blockDim.x) {
         const int i = base + threadIdx.x;
-        int k = i < d.mol_cap ? d.slot_of[i] : -1;
+        int k = i < hwm ? d.slot_of[i] : -1;
         const EngSlot *sp = k >= 0 ? &d.slots[k] : nullptr;
         const bool act = k >= 0 && sp->integrator == 0 && slot_active(*sp);
         if (!act) k = -1;
@@ -738,6 +780,7 @@ __global__ void k_e_move_lfv(EngDev d)
 
 __global__ void __launch_bounds__(ER) k_e_record(EngDev d)
 {
+    if (!d.flags->any_record) return;
     EngSlot &s = d.slots[blockIdx.x];
     if (!slot_active(s) || !s.record) return;
     double v[RT_N + 1], c[RT_N + 1];
@@ -863,7 +906,7 @@ void eng_tick(const EngDev &d, int tpm, cudaStream_t st)
 {
     const int gm = sgrid(d.mol_cap, 256, 8);
     const int gc = sgrid(d.cell_cap, 256, 8);
-    k_e_decide<<<nblk(d.nslots, 128), 128, 0, st>>>(d);
+    k_e_decide<<<1, EDEC, 0, st>>>(d);
     k_e_wrap_bin<<<gm, 256, 0, st>>>(d);
     k_e_scan<<<d.nslots, ESCAN, 0, st>>>(d);
     k_e_scatter<<<gm, 256, 0, st>>>(d);
