@@ -344,7 +344,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--batch-replicas", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=2000)
-    ap.add_argument("--serve-jobs", type=int, default=512)
+    ap.add_argument("--serve-jobs", type=int, default=4096)
     ap.add_argument("--no-forms", action="store_true", help="skip the batched and served forms")
     ap.add_argument("--profile-case", choices=["fp32", "fp64"], default=None,
                     help="profiling workload: setup + 10 fused steps of the 1M system, no timing")

@@ -48,6 +48,8 @@ class FmParams(C.Structure):
         ("R_0", C.c_double),
         ("nlist_capacity", C.c_int32),
         ("threads_per_molecule", C.c_int32),
+        ("integration_algorithm", C.c_int32),
+        ("pad_", C.c_int32),
     ]
 
 
@@ -98,6 +100,49 @@ class FmJobResult(C.Structure):
                     submit_time=self.submit_time, admit_time=self.admit_time, finish_time=self.finish_time)
 
 
+RESTART_MAXPROC = 4096
+
+
+class FmRestartHeader(C.Structure):
+    _fields_ = [
+        ("globalnp", C.c_int32), ("initialnunits", C.c_int32 * 3), ("nsteps", C.c_int32), ("tplot", C.c_int32),
+        ("seed", C.c_int32 * 2), ("periodic", C.c_int32 * 3), ("potential_flag", C.c_int32),
+        ("rtrue_flag", C.c_int32), ("solvent_flag", C.c_int32), ("nmonomers", C.c_int32), ("npx", C.c_int32),
+        ("npy", C.c_int32), ("npz", C.c_int32), ("nproc", C.c_int32), ("mie_potential", C.c_int32),
+        ("global_numbering", C.c_int32), ("header_pos", C.c_int64), ("globaldomain", C.c_double * 3),
+        ("density", C.c_double), ("rcutoff", C.c_double), ("delta_t", C.c_double), ("elapsedtime", C.c_double),
+        ("simtime", C.c_double), ("k_c", C.c_double), ("R_0", C.c_double), ("eps_pp", C.c_double),
+        ("eps_ps", C.c_double), ("eps_ss", C.c_double), ("delta_rneighbr", C.c_double),
+        ("procnp", C.c_int32 * RESTART_MAXPROC), ("proctethernp", C.c_int32 * RESTART_MAXPROC),
+    ]
+
+
+class FmInput(C.Structure):
+    _fields_ = [
+        ("ensemble", C.c_int32), ("integration_algorithm", C.c_int32), ("force_list", C.c_int32),
+        ("potential_flag", C.c_int32), ("nsteps", C.c_int32), ("tplot", C.c_int32),
+        ("rebuild_criteria", C.c_int32), ("fixed_rebuild", C.c_int32), ("initialnunits", C.c_int32 * 3),
+        ("periodic", C.c_int32 * 3), ("sort_flag", C.c_int32), ("global_numbering", C.c_int32),
+        ("pressure_outflag", C.c_int32), ("sLRC_flag", C.c_int32), ("mie_potential", C.c_int32),
+        ("nmonomers", C.c_int32), ("nthermo", C.c_int32), ("pad_", C.c_int32),
+        ("density", C.c_double), ("rcutoff", C.c_double), ("inputtemperature", C.c_double), ("delta_t", C.c_double),
+        ("delta_rneighbr", C.c_double * 3), ("k_c", C.c_double), ("R_0", C.c_double),
+        ("tethereddisttop", C.c_double * 3), ("tethereddistbottom", C.c_double * 3),
+        ("thermstattop", C.c_double * 3), ("thermstatbottom", C.c_double * 3), ("slidedisttop", C.c_double * 3),
+        ("slidedistbottom", C.c_double * 3), ("fixdisttop", C.c_double * 3), ("fixdistbottom", C.c_double * 3),
+        ("wallslidev", C.c_double * 3), ("teth_k", C.c_double * 3), ("thermostattemperature", C.c_double * 2),
+    ]
+
+    def as_dict(self):
+        out = {}
+        for k, _ in self._fields_:
+            if k == "pad_":
+                continue
+            x = getattr(self, k)
+            out[k] = list(x) if hasattr(x, "__len__") else x
+        return out
+
+
 class FlowmolError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"FM_ERR_{ERRORS.get(code, code)}: {msg}")
@@ -130,6 +175,7 @@ def lib():
             "fm_download_state_device": [h, C.c_void_p, C.c_void_p, C.c_void_p],
             "fm_setup": [h],
             "fm_move_vv": [h, C.c_int32],
+            "fm_move_lfv": [h],
             "fm_update_borders": [h, C.c_int32],
             "fm_check_rebuild": [h, P(C.c_int32)],
             "fm_linklist_deallocateall": [h],
@@ -158,6 +204,12 @@ def lib():
             "fm_engine_take_results": [h, P(FmJobResult), C.c_int32, P(C.c_int32)],
             "fm_engine_job_state": [h, C.c_int64, P(C.c_double), P(C.c_double)],
             "fm_engine_counters": [h, P(C.c_int64), P(C.c_int64), P(C.c_int32), P(C.c_int64)],
+            "fm_read_final_state": [C.c_char_p, P(FmRestartHeader), C.c_int32, P(C.c_double), P(C.c_double),
+                                    P(C.c_int32), P(C.c_double), P(C.c_int32), P(C.c_double), P(C.c_int32),
+                                    P(C.c_double)],
+            "fm_write_final_state": [C.c_char_p, P(FmRestartHeader), P(C.c_double), P(C.c_double), P(C.c_int32),
+                                     P(C.c_double), P(C.c_int32), P(C.c_double), P(C.c_int32), P(C.c_double)],
+            "fm_read_input": [C.c_char_p, P(FmInput)],
             "fm_force_kernel_timing": [h, C.c_int32],
             "fm_get_force_kernel_time": [h, P(C.c_double), P(C.c_int64)],
             "fm_get_launch_count": [h, P(C.c_int64)],
@@ -200,7 +252,7 @@ def _dp(a):
 def make_params(np_, domain, rcutoff, delta_rneighbr=(0.3, 0.3, 0.3), delta_t=0.005, tplot=100,
                 density=None, initialstep=0, simtime=0.0, force_list=FORCE_LIST_HALF, potential_flag=0,
                 rebuild_criteria=0, fixed_rebuild=1, sLRC_flag=0, precision=PRECISION_FP64, k_c=30.0,
-                R_0=1.5, nlist_capacity=0, threads_per_molecule=0) -> FmParams:
+                R_0=1.5, nlist_capacity=0, threads_per_molecule=0, integration_algorithm=1) -> FmParams:
     p = FmParams()
     p.np = int(np_)
     for k in range(3):
@@ -222,6 +274,7 @@ def make_params(np_, domain, rcutoff, delta_rneighbr=(0.3, 0.3, 0.3), delta_t=0.
     p.R_0 = float(R_0)
     p.nlist_capacity = int(nlist_capacity)
     p.threads_per_molecule = int(threads_per_molecule)
+    p.integration_algorithm = int(integration_algorithm)
     return p
 
 
@@ -294,6 +347,23 @@ class MDSystem:
 
     def simulation_move_particles_vv(self, pass_num):
         check(lib().fm_move_vv(self.h, int(pass_num)))
+
+    def simulation_move_particles_lfv(self):
+        check(lib().fm_move_lfv(self.h))
+
+    def md_advance_lfv(self):
+        """One leap-frog iteration, subroutine by subroutine (md.f90:109-139)."""
+        self.iter = self.iter + 1
+        self.simulation_compute_forces()
+        self.simulation_move_particles_lfv()
+        self.messenger_updateborders(0)
+        if self.simulation_checkrebuild():
+            self.linklist_deallocateall()
+            self.sendmols()
+            self.sort_mols()
+            self.assign_to_cell()
+            self.messenger_updateborders(1)
+            self.assign_to_neighbourlist()
 
     def messenger_updateborders(self, rebuild):
         check(lib().fm_update_borders(self.h, int(rebuild)))
@@ -501,3 +571,41 @@ class Engine:
         t = C.c_int64(); m = C.c_int64(); tp = C.c_int32(); la = C.c_int64()
         check(lib().fm_engine_counters(self.h, C.byref(t), C.byref(m), C.byref(tp), C.byref(la)))
         return dict(ticks=t.value, molecule_steps=m.value, threads_per_molecule=tp.value, launches=la.value)
+
+
+def _ip32(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+def _dpn(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def read_final_state(path):
+    """(header, dict of arrays) of a final_state restart file; arrays are
+    (n, 3) for r, v, rtether, rtrue and (n, 8) for monomer."""
+    h = FmRestartHeader()
+    check(lib().fm_read_final_state(os.fsencode(path), C.byref(h), 0, None, None, None, None, None, None, None,
+                                    None))
+    n = h.globalnp
+    r = np.empty((n, 3)); v = np.empty((n, 3)); rt = np.empty((n, 3)); rtrue = np.empty((n, 3))
+    tag = np.empty(n, np.int32); glob = np.empty(n, np.int32); mt = np.empty(n, np.int32)
+    mono = np.empty((n, 8))
+    check(lib().fm_read_final_state(os.fsencode(path), C.byref(h), n, _dpn(r), _dpn(v), _ip32(tag), _dpn(rt),
+                                    _ip32(glob), _dpn(rtrue), _ip32(mt), _dpn(mono)))
+    return h, dict(r=r, v=v, tag=tag, rtether=rt, glob_no=glob, rtrue=rtrue, moltype=mt, monomer=mono)
+
+
+def write_final_state(path, h, r, v, tag=None, rtether=None, glob_no=None, rtrue=None, moltype=None, monomer=None):
+    arr = lambda x, t: None if x is None else np.ascontiguousarray(x, t)  # noqa: E731
+    r = arr(r, np.float64); v = arr(v, np.float64); tag = arr(tag, np.int32); rtether = arr(rtether, np.float64)
+    glob_no = arr(glob_no, np.int32); rtrue = arr(rtrue, np.float64); moltype = arr(moltype, np.int32)
+    monomer = arr(monomer, np.float64)
+    check(lib().fm_write_final_state(os.fsencode(path), C.byref(h), _dpn(r), _dpn(v), _ip32(tag), _dpn(rtether),
+                                     _ip32(glob_no), _dpn(rtrue), _ip32(moltype), _dpn(monomer)))
+
+
+def read_input(path) -> FmInput:
+    x = FmInput()
+    check(lib().fm_read_input(os.fsencode(path), C.byref(x)))
+    return x

@@ -13,7 +13,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libflowmol_b200.so")
-SOURCES = ["fm_kernels.cu", "fm_api.cu", "fm_noalloc.cu", "fm_engine_kernels.cu", "fm_engine.cu"]
+SOURCES = ["fm_kernels.cu", "fm_api.cu", "fm_noalloc.cu", "fm_engine_kernels.cu", "fm_engine.cu", "fm_io.cpp"]
 HEADERS = ["fm_common.cuh", "fm_device.cuh", "fm_engine.cuh"]
 
 NVCC_FLAGS = [
@@ -43,7 +43,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         return LIB
     objs = []
     for src in SOURCES:
-        obj = os.path.join(CSRC, src.replace(".cu", ".o"))
+        obj = os.path.join(CSRC, os.path.splitext(src)[0] + ".o")
         cmd = [_nvcc(), *NVCC_FLAGS, "-I", os.path.join(ROOT, "include"), "-I", CSRC,
                "-DFM_BUILDING_LIBRARY", "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:

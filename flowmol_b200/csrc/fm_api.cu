@@ -200,6 +200,8 @@ extern "C" int fm_create(const fm_params *p, fm_handle **out)
     if (p->potential_flag != 0) return fail(FM_ERR_ARG, "potential_flag 1 (FENE) is served by fm_poly_* handles");
     if (p->rebuild_criteria != 0 && p->rebuild_criteria != 1)
         return fail(FM_ERR_ARG, "rebuild_criteria must be 0 (vmax) or 1 (fixed)");
+    if (p->integration_algorithm != 0 && p->integration_algorithm != 1)
+        return fail(FM_ERR_ARG, "integration_algorithm must be 0 (leap-frog) or 1 (velocity Verlet)");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(FM_ERR_NODEVICE, "no CUDA device");
 
@@ -234,6 +236,7 @@ extern "C" int fm_create(const fm_params *p, fm_handle **out)
                    (4.0 / (9.0 * std::pow(p->rcutoff, 9)) - 2.0 / (3.0 * p3(p->rcutoff)));
     }
     d.tplot = p->tplot;
+    d.integrator = p->integration_algorithm;
     d.precision = p->precision;
     double dmin = std::min(p->delta_rneighbr[0], std::min(p->delta_rneighbr[1], p->delta_rneighbr[2]));
     h->half_min_delta = 0.5 * dmin;
@@ -578,10 +581,45 @@ extern "C" int fm_setup(fm_handle *h)
 
 // Queues iterations [first, first + nsteps) of md_advance_vv, starting at
 // `phase` 0 (move(1)) or 1 (forces) of the first iteration.
+static void queue_rebuild_check(fm_handle *h, int it, int flip)
+{
+    const fm_params &p = h->p;
+    fm::launch_decide(h->d, it, flip, p.rebuild_criteria, p.fixed_rebuild, h->half_min_delta, h->st);
+    h->launches += 1;
+    if (p.force_list != 0) {
+        queue_cells(h, 1, 1);
+        fm::launch_build_nlist(h->d, 1, it, h->st);
+        h->launches += 1;
+    } else {
+        fm::launch_wrap_bin(h->d, 1, 0, 1, it, h->st);
+        h->launches += 1;
+    }
+}
+
+// Leap-frog iterations [first, first + nsteps): forces + record + move fused,
+// then the rebuild check and gated rebuild of the same iteration.
+static int queue_steps_lfv(fm_handle *h, int first, int nsteps, const std::vector<double> &simtime_after,
+                           int range_offset)
+{
+    for (int s = 0; s < nsteps; s++) {
+        const int it = first + s;
+        h->iter = it;
+        const int record = (it % h->p.tplot) == 0;
+        const double t_before = h->simtime;
+        queue_force(h, record, 3);
+        if (record) queue_record(h, it, t_before);
+        h->simtime = simtime_after[(size_t)(range_offset + s)];
+        queue_rebuild_check(h, it, 1);
+    }
+    FM_CUDA(cudaGetLastError());
+    return FM_OK;
+}
+
 static int queue_steps(fm_handle *h, int first, int nsteps, int phase, const std::vector<double> &simtime_after,
                        int range_offset)
 {
     const fm_params &p = h->p;
+    if (p.integration_algorithm == 0) return queue_steps_lfv(h, first, nsteps, simtime_after, range_offset);
     bool fused_move1 = false;  // the previous force kernel already did move(1)
     for (int s = 0; s < nsteps; s++) {
         const int it = first + s;
@@ -630,7 +668,13 @@ static int finish_range(fm_handle *h)
         const int off = f - h->q.first_iter;
         if (off < 0 || off >= h->q.nsteps) return status_error(h, s);
         FM_TRY(grow_nlist(h, s, f));
-        FM_TRY(queue_steps(h, f, h->q.nsteps - off, 1, h->q.simtime_after, off));
+        if (h->p.integration_algorithm == 0) {
+            // the list of iteration f overflowed after its move: go on with f + 1
+            h->simtime = h->q.simtime_after[(size_t)off];
+            FM_TRY(queue_steps(h, f + 1, h->q.nsteps - off - 1, 0, h->q.simtime_after, off + 1));
+        } else {
+            FM_TRY(queue_steps(h, f, h->q.nsteps - off, 1, h->q.simtime_after, off));
+        }
     }
     return fail(FM_ERR_NLIST, "neighbour list kept overflowing");
 }
@@ -694,6 +738,15 @@ extern "C" int fm_move_vv(fm_handle *h, int32_t pass_num)
     } else {
         return fail(FM_ERR_ARG, "pass_num must be 1 or 2");
     }
+    FM_CUDA(cudaGetLastError());
+    return FM_OK;
+}
+
+extern "C" int fm_move_lfv(fm_handle *h)
+{
+    FM_TRY(ready(h, 1));
+    fm::launch_move_lfv(h->d, h->st);
+    h->simtime = h->simtime + h->p.delta_t;
     FM_CUDA(cudaGetLastError());
     return FM_OK;
 }

@@ -56,6 +56,7 @@ struct FmDev {
     double rc2, rn2, dt, potshift, half_dt, half_dt2;
     double density, pot_slrc, p_slrc;
     int tplot;
+    int integrator;        // 0 leap-frog, 1 velocity Verlet
     int maxn;              // neighbour slots per molecule
     int precision;
     // positions (double-buffered: pos[sc->pset] is current)
@@ -100,6 +101,7 @@ void launch_reset_scalars(const FmDev &d, cudaStream_t st);
 void launch_move1(const FmDev &d, cudaStream_t st);          // pass 1 in place + vmax2
 void launch_move2(const FmDev &d, cudaStream_t st);          // pass 2 in place
 void launch_vmax(const FmDev &d, cudaStream_t st);           // vmax2 of current v
+void launch_move_lfv(const FmDev &d, cudaStream_t st);       // leap-frog move in place + vmax2
 void launch_decide(const FmDev &d, int iter, int flip, int rebuild_criteria, int fixed_rebuild,
                    double half_min_delta, cudaStream_t st);
 // Rebuild pipeline; gated = 1 makes each kernel a no-op unless sc->rebuild.
@@ -108,7 +110,8 @@ void launch_scan_cells(const FmDev &d, int gated, cudaStream_t st);
 void launch_scatter(const FmDev &d, int gated, cudaStream_t st);
 void launch_reorder(const FmDev &d, int gated, double4 *tpos, int32_t *tuidx, cudaStream_t st);
 void launch_build_nlist(const FmDev &d, int gated, int iter, cudaStream_t st);
-// Forces: mode 0 forces only, 1 forces + move(2), 2 forces + move(2) + next move(1).
+// Forces: mode 0 forces only, 1 forces + move(2), 2 forces + move(2) + next
+// move(1), 3 forces + leap-frog move.
 void launch_force(const FmDev &d, int record, int mode, int tpm, cudaStream_t st);
 void launch_record(const FmDev &d, int iter, double simtime, cudaStream_t st);
 void launch_all_pairs(const FmDev &d, int record, int mode, cudaStream_t st);

@@ -104,6 +104,28 @@ __global__ void k_move2(FmDev d)
     }
 }
 
+// simulation_move_particles_lfv NVE (simulation_move_particles_lfv.f90:81-92), in place.
+__global__ void k_move_lfv(FmDev d)
+{
+    if (frozen(d)) return;
+    double4 *P = cur_pos(d, d.sc->pset);
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double m2 = 0.0;
+    if (i < d.n) {
+        double4 p = P[i];
+        double vx = __dadd_rn(d.vx[i], __dmul_rn(d.dt, d.ax[i]));
+        double vy = __dadd_rn(d.vy[i], __dmul_rn(d.dt, d.ay[i]));
+        double vz = __dadd_rn(d.vz[i], __dmul_rn(d.dt, d.az[i]));
+        p.x = __dadd_rn(p.x, __dmul_rn(d.dt, vx));
+        p.y = __dadd_rn(p.y, __dmul_rn(d.dt, vy));
+        p.z = __dadd_rn(p.z, __dmul_rn(d.dt, vz));
+        P[i] = p;
+        d.vx[i] = vx; d.vy[i] = vy; d.vz[i] = vz;
+        m2 = norm2_rn(vx, vy, vz);
+    }
+    block_vmax2(d, m2);
+}
+
 __global__ void k_vmax(FmDev d)
 {
     if (frozen(d)) return;
@@ -499,6 +521,71 @@ __global__ void __launch_bounds__(NB_THREADS) k_build_nlist(FmDev d, int gated, 
 
 constexpr int FORCE_THREADS = 256;
 
+// Integrator epilogue of molecule i with its summed LJ force: stores a (and PE
+// and virial on record steps) and, by MODE,
+//   1  move(2)                               (simulation_move_particles_vv.f90:132-135)
+//   2  move(2) + move(1) of the next step    (:64-69), new positions into pset^1
+//   3  leap-frog v += dt a, r += dt v        (simulation_move_particles_lfv.f90:81-92)
+// The record partials use v after move(2) for velocity Verlet and v + a dt/2
+// for leap-frog (simulation_record.f90:1236-1252).  Returns |v|^2 after a
+// position update (modes 2, 3), else 0.
+template <bool REC, int MODE>
+__device__ __forceinline__ double epilogue(const FmDev &d, int pset, int i, double4 p, double fx, double fy,
+                                           double fz, double pe, double vir, double (&part)[RS_N])
+{
+    d.ax[i] = fx; d.ay[i] = fy; d.az[i] = fz;
+    if (REC) { d.pe[i] = pe; d.vir[i] = vir; }
+    double vx = d.vx[i], vy = d.vy[i], vz = d.vz[i];
+    double m2 = 0.0;
+    if (MODE == 3) {
+        if (REC) {
+            const double wx = __dadd_rn(vx, __dmul_rn(__dmul_rn(0.5, fx), d.dt));
+            const double wy = __dadd_rn(vy, __dmul_rn(__dmul_rn(0.5, fy), d.dt));
+            const double wz = __dadd_rn(vz, __dmul_rn(__dmul_rn(0.5, fz), d.dt));
+            part[RS_PE] = pe; part[RS_VIR] = vir; part[RS_PEMAX] = pe;
+            part[RS_MV2] = norm2_rn(wx, wy, wz);
+            part[RS_VSUM] = __dadd_rn(__dadd_rn(wx, wy), wz);
+        }
+        vx = __dadd_rn(vx, __dmul_rn(d.dt, fx));
+        vy = __dadd_rn(vy, __dmul_rn(d.dt, fy));
+        vz = __dadd_rn(vz, __dmul_rn(d.dt, fz));
+        p.x = __dadd_rn(p.x, __dmul_rn(d.dt, vx));
+        p.y = __dadd_rn(p.y, __dmul_rn(d.dt, vy));
+        p.z = __dadd_rn(p.z, __dmul_rn(d.dt, vz));
+        cur_pos(d, pset ^ 1)[i] = p;
+        d.vx[i] = vx; d.vy[i] = vy; d.vz[i] = vz;
+        return norm2_rn(vx, vy, vz);
+    }
+    if (MODE >= 1) {
+        vx = __dadd_rn(vx, __dmul_rn(d.half_dt, fx));
+        vy = __dadd_rn(vy, __dmul_rn(d.half_dt, fy));
+        vz = __dadd_rn(vz, __dmul_rn(d.half_dt, fz));
+    }
+    if (REC) {
+        double wx = vx, wy = vy, wz = vz;
+        if (MODE == 0 && d.integrator == 0) {  // forces only, leap-frog record velocity
+            wx = __dadd_rn(vx, __dmul_rn(__dmul_rn(0.5, fx), d.dt));
+            wy = __dadd_rn(vy, __dmul_rn(__dmul_rn(0.5, fy), d.dt));
+            wz = __dadd_rn(vz, __dmul_rn(__dmul_rn(0.5, fz), d.dt));
+        }
+        part[RS_PE] = pe; part[RS_VIR] = vir; part[RS_PEMAX] = pe;
+        part[RS_MV2] = norm2_rn(wx, wy, wz);
+        part[RS_VSUM] = __dadd_rn(__dadd_rn(wx, wy), wz);
+    }
+    if (MODE == 2) {
+        p.x = __dadd_rn(__dadd_rn(p.x, __dmul_rn(d.dt, vx)), __dmul_rn(d.half_dt2, fx));
+        p.y = __dadd_rn(__dadd_rn(p.y, __dmul_rn(d.dt, vy)), __dmul_rn(d.half_dt2, fy));
+        p.z = __dadd_rn(__dadd_rn(p.z, __dmul_rn(d.dt, vz)), __dmul_rn(d.half_dt2, fz));
+        vx = __dadd_rn(vx, __dmul_rn(d.half_dt, fx));
+        vy = __dadd_rn(vy, __dmul_rn(d.half_dt, fy));
+        vz = __dadd_rn(vz, __dmul_rn(d.half_dt, fz));
+        cur_pos(d, pset ^ 1)[i] = p;
+        m2 = norm2_rn(vx, vy, vz);
+    }
+    if (MODE >= 1) { d.vx[i] = vx; d.vy[i] = vy; d.vz[i] = vz; }
+    return m2;
+}
+
 // Block reduction of the record partials; row blockIdx.x of d.partial.
 __device__ __forceinline__ void block_partials(const FmDev &d, double v[RS_N])
 {
@@ -599,44 +686,10 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force(FmDev d)
     }
     double part[RS_N] = {0.0, 0.0, 0.0, 0.0, 0.0};
     double m2 = 0.0;
-    if (active && lane == 0) {
-        // a(:,i) = sum acc rij / mass, mass = 1 (LJ_mass)
-        d.ax[i] = fx; d.ay[i] = fy; d.az[i] = fz;
-        if (REC) { d.pe[i] = pe; d.vir[i] = vir; }
-        if (MODE >= 1) {
-            double vx = __dadd_rn(d.vx[i], __dmul_rn(d.half_dt, fx));
-            double vy = __dadd_rn(d.vy[i], __dmul_rn(d.half_dt, fy));
-            double vz = __dadd_rn(d.vz[i], __dmul_rn(d.half_dt, fz));
-            if (REC) {
-                part[RS_PE] = pe;
-                part[RS_VIR] = vir;
-                part[RS_MV2] = __dadd_rn(__dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)), __dmul_rn(vz, vz));
-                part[RS_VSUM] = __dadd_rn(__dadd_rn(vx, vy), vz);
-                part[RS_PEMAX] = pe;
-            }
-            if (MODE == 2) {
-                double4 p = P[i];
-                p.x = __dadd_rn(__dadd_rn(p.x, __dmul_rn(d.dt, vx)), __dmul_rn(d.half_dt2, fx));
-                p.y = __dadd_rn(__dadd_rn(p.y, __dmul_rn(d.dt, vy)), __dmul_rn(d.half_dt2, fy));
-                p.z = __dadd_rn(__dadd_rn(p.z, __dmul_rn(d.dt, vz)), __dmul_rn(d.half_dt2, fz));
-                vx = __dadd_rn(vx, __dmul_rn(d.half_dt, fx));
-                vy = __dadd_rn(vy, __dmul_rn(d.half_dt, fy));
-                vz = __dadd_rn(vz, __dmul_rn(d.half_dt, fz));
-                cur_pos(d, pset ^ 1)[i] = p;
-                m2 = norm2_rn(vx, vy, vz);
-            }
-            d.vx[i] = vx; d.vy[i] = vy; d.vz[i] = vz;
-        } else if (REC) {
-            double vx = d.vx[i], vy = d.vy[i], vz = d.vz[i];
-            part[RS_PE] = pe;
-            part[RS_VIR] = vir;
-            part[RS_MV2] = __dadd_rn(__dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)), __dmul_rn(vz, vz));
-            part[RS_VSUM] = __dadd_rn(__dadd_rn(vx, vy), vz);
-            part[RS_PEMAX] = pe;
-        }
-    }
+    // a(:,i) = sum acc rij / mass, mass = 1 (LJ_mass)
+    if (active && lane == 0) m2 = epilogue<REC, MODE>(d, pset, i, P[i], fx, fy, fz, pe, vir, part);
     if (REC) block_partials(d, part);
-    if (MODE == 2) block_vmax2(d, m2);
+    if (MODE >= 2) block_vmax2(d, m2);
 }
 
 // Neumaier-compensated reduction of the per-block partials into one record
@@ -707,6 +760,11 @@ __global__ void __launch_bounds__(MACRO_THREADS) k_macro_partials(FmDev d)
     double part[RS_N] = {0.0, 0.0, 0.0, 0.0, 0.0};
     if (i < d.n) {
         double vx = d.vx[i], vy = d.vy[i], vz = d.vz[i];
+        if (d.integrator == 0) {  // leap-frog records v + a dt/2
+            vx = __dadd_rn(vx, __dmul_rn(__dmul_rn(0.5, d.ax[i]), d.dt));
+            vy = __dadd_rn(vy, __dmul_rn(__dmul_rn(0.5, d.ay[i]), d.dt));
+            vz = __dadd_rn(vz, __dmul_rn(__dmul_rn(0.5, d.az[i]), d.dt));
+        }
         part[RS_PE] = d.pe[i];
         part[RS_VIR] = d.vir[i];
         part[RS_MV2] = norm2_rn(vx, vy, vz);
@@ -792,35 +850,7 @@ __global__ void __launch_bounds__(AP_THREADS) k_all_pairs(FmDev d)
     }
     double part[RS_N] = {0.0, 0.0, 0.0, 0.0, 0.0};
     double m2 = 0.0;
-    if (active) {
-        d.ax[i] = fx; d.ay[i] = fy; d.az[i] = fz;
-        if (REC) { d.pe[i] = pe; d.vir[i] = vir; }
-        double vx = d.vx[i], vy = d.vy[i], vz = d.vz[i];
-        if (MODE >= 1) {
-            vx = __dadd_rn(vx, __dmul_rn(d.half_dt, fx));
-            vy = __dadd_rn(vy, __dmul_rn(d.half_dt, fy));
-            vz = __dadd_rn(vz, __dmul_rn(d.half_dt, fz));
-        }
-        if (REC) {
-            part[RS_PE] = pe;
-            part[RS_VIR] = vir;
-            part[RS_MV2] = norm2_rn(vx, vy, vz);
-            part[RS_VSUM] = __dadd_rn(__dadd_rn(vx, vy), vz);
-            part[RS_PEMAX] = pe;
-        }
-        if (MODE == 2) {
-            double4 p = pi;
-            p.x = __dadd_rn(__dadd_rn(p.x, __dmul_rn(d.dt, vx)), __dmul_rn(d.half_dt2, fx));
-            p.y = __dadd_rn(__dadd_rn(p.y, __dmul_rn(d.dt, vy)), __dmul_rn(d.half_dt2, fy));
-            p.z = __dadd_rn(__dadd_rn(p.z, __dmul_rn(d.dt, vz)), __dmul_rn(d.half_dt2, fz));
-            vx = __dadd_rn(vx, __dmul_rn(d.half_dt, fx));
-            vy = __dadd_rn(vy, __dmul_rn(d.half_dt, fy));
-            vz = __dadd_rn(vz, __dmul_rn(d.half_dt, fz));
-            cur_pos(d, pset ^ 1)[i] = p;
-            m2 = norm2_rn(vx, vy, vz);
-        }
-        if (MODE >= 1) { d.vx[i] = vx; d.vy[i] = vy; d.vz[i] = vz; }
-    }
+    if (active) m2 = epilogue<REC, MODE>(d, pset, i, pi, fx, fy, fz, pe, vir, part);
     if (REC) {
         // AP blocks are AP_THREADS wide; reuse the generic reduction layout
         __shared__ double ws[RS_N][AP_THREADS / 32];
@@ -837,7 +867,7 @@ __global__ void __launch_bounds__(AP_THREADS) k_all_pairs(FmDev d)
             d.partial[(size_t)blockIdx.x * RS_N + k] = acc;
         }
     }
-    if (MODE == 2) block_vmax2(d, m2);
+    if (MODE >= 2) block_vmax2(d, m2);
 }
 
 // ---------------------------------------------------------------------------
@@ -926,6 +956,7 @@ void launch_reset_scalars(const FmDev &d, cudaStream_t st) { k_reset_scalars<<<1
 void launch_move1(const FmDev &d, cudaStream_t st) { k_move1<<<nblk(d.n, 256), 256, 0, st>>>(d); }
 void launch_move2(const FmDev &d, cudaStream_t st) { k_move2<<<nblk(d.n, 256), 256, 0, st>>>(d); }
 void launch_vmax(const FmDev &d, cudaStream_t st) { k_vmax<<<nblk(d.n, 256), 256, 0, st>>>(d); }
+void launch_move_lfv(const FmDev &d, cudaStream_t st) { k_move_lfv<<<nblk(d.n, 256), 256, 0, st>>>(d); }
 void launch_decide(const FmDev &d, int iter, int flip, int crit, int fixed_rebuild, double half_min_delta,
                    cudaStream_t st)
 {
@@ -974,8 +1005,8 @@ static void launch_force_tpm(const FmDev &d, int record, int mode, cudaStream_t 
         else k_force<TPM, R, M, 1><<<g, FORCE_THREADS, 0, st>>>(d);                             \
         return;                                                                                 \
     }
-    FM_FORCE_CASE(0, 0) FM_FORCE_CASE(0, 1) FM_FORCE_CASE(0, 2)
-    FM_FORCE_CASE(1, 0) FM_FORCE_CASE(1, 1) FM_FORCE_CASE(1, 2)
+    FM_FORCE_CASE(0, 0) FM_FORCE_CASE(0, 1) FM_FORCE_CASE(0, 2) FM_FORCE_CASE(0, 3)
+    FM_FORCE_CASE(1, 0) FM_FORCE_CASE(1, 1) FM_FORCE_CASE(1, 2) FM_FORCE_CASE(1, 3)
 #undef FM_FORCE_CASE
 }
 
@@ -999,8 +1030,8 @@ void launch_all_pairs(const FmDev &d, int record, int mode, cudaStream_t st)
         else k_all_pairs<R, M, 1><<<g, AP_THREADS, 0, st>>>(d);                     \
         return;                                                                     \
     }
-    FM_AP_CASE(0, 0) FM_AP_CASE(0, 1) FM_AP_CASE(0, 2)
-    FM_AP_CASE(1, 0) FM_AP_CASE(1, 1) FM_AP_CASE(1, 2)
+    FM_AP_CASE(0, 0) FM_AP_CASE(0, 1) FM_AP_CASE(0, 2) FM_AP_CASE(0, 3)
+    FM_AP_CASE(1, 0) FM_AP_CASE(1, 1) FM_AP_CASE(1, 2) FM_AP_CASE(1, 3)
 #undef FM_AP_CASE
 }
 

@@ -76,6 +76,8 @@ typedef struct fm_params {
     double k_c, R_0;              /* FENE_INFO spring constant and maximum extension */
     int32_t nlist_capacity;       /* neighbours per molecule reserved; 0 = automatic */
     int32_t threads_per_molecule; /* force kernel lanes per molecule; 0 = autotuned */
+    int32_t integration_algorithm; /* INTEGRATION_ALGORITHM: 0 leap-frog (NVE), 1 velocity Verlet */
+    int32_t pad_;
 } fm_params;
 
 /* Macroscopic properties of one record step, the columns of
@@ -144,6 +146,8 @@ FM_API int fm_download_state_device(fm_handle *h, double *d_r, double *d_v, doub
 FM_API int fm_setup(fm_handle *h);
 /* simulation_move_particles_vv(pass_num), NVE (simulation_move_particles_vv.f90:64-69,132-135). */
 FM_API int fm_move_vv(fm_handle *h, int32_t pass_num);
+/* simulation_move_particles_lfv, NVE (simulation_move_particles_lfv.f90:81-92). */
+FM_API int fm_move_lfv(fm_handle *h);
 /* messenger_updateborders(rebuild) (messenger.MPI.f90:594-627).  Periodic
  * images are generated on the fly from their source molecule inside the
  * list-build and force kernels (x_img = x_src +/- domain, the same FP64 add),
@@ -177,8 +181,10 @@ FM_API int fm_set_iter(fm_handle *h, int32_t iter);
 FM_API int fm_get_iter(fm_handle *h, int32_t *iter);
 
 /* ---- the fused step loop -------------------------------------------- */
-/* Runs nsteps iterations of md_advance_vv (md.f90:143-163) on the device:
- * move(1), rebuild check, [wrap, bin, list], forces, move(2), record.  The
+/* Runs nsteps iterations of md_advance_vv (md.f90:143-163) on the device --
+ * move(1), rebuild check, [wrap, bin, list], forces, move(2), record -- or,
+ * with integration_algorithm 0, of md_advance_lfv (md.f90:109-139): forces,
+ * record, move, rebuild check, [wrap, bin, list].  The
  * rebuild decision is taken on the device, so the host never waits inside
  * the loop.  Returns after the work is queued unless blocking != 0; errors
  * detected on the device (escape, list overflow that cannot be resized, PE
@@ -207,6 +213,58 @@ FM_API int fm_get_pair_list(fm_handle *h, int32_t *owner, int32_t *partner, int8
 FM_API int fm_pair_digest(fm_handle *h, uint64_t *digest, int64_t *npairs);
 /* Counters: rebuilds done, neighbour capacity in use, largest list seen. */
 FM_API int fm_get_counters(fm_handle *h, int64_t *rebuilds, int32_t *nlist_capacity, int32_t *max_neighbours);
+
+/* ---- restart files and keyword input (host only, no device needed) ---- */
+#define FM_RESTART_MAXPROC 4096
+
+/* Header of a final_state restart file (parallel_io.MPI2.f90:1650-1700). */
+typedef struct fm_restart_header {
+    int32_t globalnp;
+    int32_t initialnunits[3];
+    int32_t nsteps;              /* Nsteps, or iter when written before the end */
+    int32_t tplot;
+    int32_t seed[2];
+    int32_t periodic[3];
+    int32_t potential_flag, rtrue_flag, solvent_flag, nmonomers;
+    int32_t npx, npy, npz, nproc;
+    int32_t mie_potential, global_numbering;
+    int64_t header_pos;          /* byte offset of the header (read only) */
+    double globaldomain[3];
+    double density, rcutoff, delta_t, elapsedtime, simtime, k_c, R_0, eps_pp, eps_ps, eps_ss;
+    double delta_rneighbr;       /* delta_rneighbr(1) */
+    int32_t procnp[FM_RESTART_MAXPROC];
+    int32_t proctethernp[FM_RESTART_MAXPROC];
+} fm_restart_header;
+
+/* Reads a final_state file (the body layout of parallel_io_final_state,
+ * parallel_io.MPI2.f90:1495-1726; global coordinates).  With r and v NULL
+ * only the header is read.  Arrays hold cap >= globalnp molecules: r, v,
+ * rtether, rtrue are (3, n) column-major, monomer is (8, n); any may be NULL.
+ * glob_no is 1..n when the file has no global numbering; rtether is 0 for
+ * untethered molecules. */
+FM_API int fm_read_final_state(const char *path, fm_restart_header *hdr, int32_t cap, double *r, double *v,
+                               int32_t *tag, double *rtether, int32_t *glob_no, double *rtrue, int32_t *moltype,
+                               double *monomer);
+/* Writes a final_state file byte-compatible with the reference's. */
+FM_API int fm_write_final_state(const char *path, const fm_restart_header *hdr, const double *r, const double *v,
+                                const int32_t *tag, const double *rtether, const int32_t *glob_no,
+                                const double *rtrue, const int32_t *moltype, const double *monomer);
+
+/* Hot-path subset of the keyword input file (setup_read_input.f90, keyword
+ * search of functions_lib.f90:1139-1193). */
+typedef struct fm_input {
+    int32_t ensemble, integration_algorithm, force_list, potential_flag;
+    int32_t nsteps, tplot, rebuild_criteria, fixed_rebuild;
+    int32_t initialnunits[3], periodic[3];
+    int32_t sort_flag, global_numbering, pressure_outflag, sLRC_flag, mie_potential, nmonomers, nthermo, pad_;
+    double density, rcutoff, inputtemperature, delta_t, delta_rneighbr[3], k_c, R_0;
+    double tethereddisttop[3], tethereddistbottom[3], thermstattop[3], thermstatbottom[3];
+    double slidedisttop[3], slidedistbottom[3], fixdisttop[3], fixdistbottom[3], wallslidev[3];
+    double teth_k[3];            /* TETHERCOEFFICIENTS k2, k4, k6 */
+    double thermostattemperature[2];
+} fm_input;
+
+FM_API int fm_read_input(const char *path, fm_input *in);
 
 /* ---- multi-job engine: batched replicas and served jobs ---------------- */
 /* No single counterpart in the reference, which runs one system per MPI job:

@@ -8,8 +8,10 @@ Run in a container that has the reference at REFERENCE_ROOT (default
   * runs/Intrinsic_Interface/initial_state decoded with the reference's own
     reader src/reorder_restart/read_final_state.py.
 Outputs: intrinsic_interface_geometry.json, intrinsic_interface_restart.json
-(header as the reference reader decodes it) and
-intrinsic_interface_state.npz (tag, r, v, glob_no per molecule).
+(header as the reference reader decodes it), intrinsic_interface_state.npz
+(tag, r, v, glob_no per molecule), and verbatim copies of the restart file
+(intrinsic_interface_initial_state.bin) and of two keyword input files
+(default.in, MD_2_phase.in) for the reader tests.
 """
 from __future__ import annotations
 
@@ -65,6 +67,11 @@ def main():
     np.savez_compressed(os.path.join(HERE, "intrinsic_interface_state.npz"), tag=tag, r=r, v=v,
                         glob_no=np.asarray(glob), size=np.array([os.path.getsize(
                             os.path.join(REF, "runs/Intrinsic_Interface/initial_state"))]))
+    import shutil
+    shutil.copyfile(os.path.join(REF, "runs/Intrinsic_Interface/initial_state"),
+                    os.path.join(HERE, "intrinsic_interface_initial_state.bin"))
+    shutil.copyfile(os.path.join(REF, "src/default.in"), os.path.join(HERE, "default.in"))
+    shutil.copyfile(os.path.join(REF, "runs/Intrinsic_Interface/MD_2_phase.in"), os.path.join(HERE, "MD_2_phase.in"))
     print("wrote fixtures for", geom["globalnp"], "molecules")
 
 

@@ -228,3 +228,67 @@ def test_large_system_pair_digest_and_forces(gpu_lib):
     s32.setup()
     _, _, a32, _ = s32.download()
     assert rel_err(a32, o.a, F_FLOOR32).max() <= TOL32
+
+
+def wrap_diff(a, b, dom):
+    d = np.asarray(a) - np.asarray(b)
+    dom = np.asarray(dom)
+    return d - dom * np.round(d / dom)
+
+
+def test_leapfrog_trajectory_follows_oracle(liquid):
+    """md_advance_lfv (forces, record, move, rebuild check) on the device."""
+    r, v, dom = liquid
+    nsteps, tplot = 300, 50
+    o = O.Oracle(r, v, dom, 2.5, tplot=tplot, density=0.8442, integration_algorithm=0)
+    o.setup()
+    recs_o = o.run_lfv(nsteps)
+    s = gpu_system(r, v, dom, 2.5, tplot=tplot, density=0.8442, integration_algorithm=0)
+    s.setup()
+    s.records()
+    s.simulation_md(nsteps)
+    recs = s.records()
+    assert len(recs) == len(recs_o)
+    for row, ro in zip(recs, recs_o):
+        assert row["iter"] == int(ro[0])
+        assert row["kinenergy"] == pytest.approx(ro[4], rel=1e-10)
+        assert row["totenergy"] == pytest.approx(ro[6], rel=1e-10)
+    rg, vg, _, _ = s.download()
+    assert np.abs(wrap_diff(rg, o.r, dom)).max() < 1e-8
+    np.testing.assert_allclose(vg, o.v, rtol=0, atol=1e-8)
+
+
+def test_leapfrog_subroutines_equal_fused_loop(liquid):
+    r, v, dom = liquid
+    a_sys = gpu_system(r, v, dom, 2.5, tplot=40, density=0.8442, integration_algorithm=0)
+    a_sys.setup()
+    for _ in range(60):
+        a_sys.md_advance_lfv()
+    b_sys = gpu_system(r, v, dom, 2.5, tplot=40, density=0.8442, integration_algorithm=0)
+    b_sys.setup()
+    b_sys.simulation_md(60)
+    ra, va, _, _ = a_sys.download()
+    rb, vb, _, _ = b_sys.download()
+    assert np.array_equal(ra, rb) and np.array_equal(va, vb)
+
+
+def test_reference_restart_liquid_vapour_state(gpu_lib):
+    """The reference's runs/Intrinsic_Interface/initial_state (2635 molecules,
+    liquid slab + vapour, rc 2.5), read with the library's final_state
+    reader: pair set bit-exact and FP64 forces within 1e-12 of the oracle."""
+    import os
+    path = os.path.join(os.path.dirname(__file__), "golden", "intrinsic_interface_initial_state.bin")
+    h, a = api.read_final_state(path)
+    dom = list(h.globaldomain)
+    delta = (h.delta_rneighbr,) * 3
+    o = O.Oracle(a["r"], a["v"], dom, h.rcutoff, delta, tplot=1, density=h.density)
+    o.setup()
+    p = api.make_params(h.globalnp, dom, h.rcutoff, delta, h.delta_t, tplot=1, density=h.density)
+    s = api.MDSystem(p)
+    s.upload(a["r"], a["v"], glob_no=a["glob_no"])
+    s.setup()
+    assert np.array_equal(canonical_full(*s.pair_list()), canonical_oracle(*o.pair_list()))
+    _, _, acc, _ = s.download()
+    assert rel_err(acc, o.a, 1.0).max() <= TOL64
+    pe, vir = s.per_molecule()
+    np.testing.assert_allclose(pe, o.potenergymol, rtol=TOL64, atol=TOL64)

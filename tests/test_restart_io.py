@@ -1,0 +1,98 @@
+"""final_state reader/writer and keyword-input reader (host only, no GPU).
+
+Pinned against the reference: the header and molecule arrays must equal what
+the reference's own reader (src/reorder_restart/read_final_state.py) decoded
+from runs/Intrinsic_Interface/initial_state (fixtures in tests/golden, made by
+tests/golden/make_golden.py), and writing what was read must reproduce the
+file byte for byte."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from flowmol_b200 import api
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+FIXTURE = os.path.join(GOLD, "intrinsic_interface_initial_state.bin")
+
+
+def test_reader_matches_reference_reader():
+    h, a = api.read_final_state(FIXTURE)
+    ref = json.load(open(os.path.join(GOLD, "intrinsic_interface_restart.json")))
+    st = np.load(os.path.join(GOLD, "intrinsic_interface_state.npz"))
+    assert h.globalnp == ref["globalnp"] == 2635
+    assert list(h.initialnunits) == [ref["initialunits1"], ref["initialunits2"], ref["initialunits3"]]
+    assert h.nsteps == ref["Nsteps"] and h.tplot == ref["tplot"]
+    assert list(h.seed) == [ref["seed1"], ref["seed2"]]
+    assert list(h.periodic) == [ref["periodic1"], ref["periodic2"], ref["periodic3"]]
+    assert (h.npx, h.npy, h.npz) == (ref["npx"], ref["npy"], ref["npz"])
+    assert [h.procnp[p] for p in range(h.nproc)] == [ref["procnp0"], ref["procnp1"]]
+    assert list(h.globaldomain) == [ref["globaldomain1"], ref["globaldomain2"], ref["globaldomain3"]]
+    for k in ("density", "rcutoff", "delta_t", "elapsedtime", "simtime", "k_c", "R_0", "delta_rneighbr"):
+        assert getattr(h, k) == ref[k], k
+    assert h.header_pos == ref["headerstart"]
+    assert np.array_equal(a["r"], st["r"]) and np.array_equal(a["v"], st["v"])
+    assert np.array_equal(a["tag"], st["tag"].astype(np.int32))
+
+
+def test_round_trip_is_byte_identical(tmp_path):
+    h, a = api.read_final_state(FIXTURE)
+    out = tmp_path / "final_state"
+    api.write_final_state(str(out), h, a["r"], a["v"], a["tag"], a["rtether"], a["glob_no"])
+    assert out.read_bytes() == open(FIXTURE, "rb").read()
+
+
+def test_optional_blocks_round_trip(tmp_path):
+    """rtrue, tethers, Mie types, global numbering and monomer records."""
+    rng = np.random.default_rng(3)
+    n = 50
+    h = api.FmRestartHeader()
+    h.globalnp = n; h.npx = h.npy = h.npz = 1; h.nproc = 1; h.procnp[0] = n
+    h.rtrue_flag = 1; h.mie_potential = 1; h.global_numbering = 1; h.potential_flag = 1; h.nmonomers = 8
+    h.globaldomain[0] = h.globaldomain[1] = h.globaldomain[2] = 10.0
+    tag = rng.integers(0, 8, n).astype(np.int32)
+    a = dict(r=rng.normal(size=(n, 3)), v=rng.normal(size=(n, 3)), tag=tag,
+             rtether=np.where(np.isin(tag, [3, 5, 6, 7])[:, None], rng.normal(size=(n, 3)), 0.0),
+             glob_no=rng.permutation(n).astype(np.int32) + 1, rtrue=rng.normal(size=(n, 3)),
+             moltype=rng.integers(1, 3, n).astype(np.int32), monomer=rng.integers(0, 100, (n, 8)).astype(float))
+    p = tmp_path / "s"
+    api.write_final_state(str(p), h, **a)
+    h2, b = api.read_final_state(str(p))
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+    assert h2.nmonomers == 8 and h2.rtrue_flag == 1
+
+
+def test_truncated_file_is_an_error(tmp_path):
+    data = open(FIXTURE, "rb").read()
+    p = tmp_path / "bad"
+    p.write_bytes(data[:-100])
+    with pytest.raises(api.FlowmolError) as e:
+        api.read_final_state(str(p))
+    assert e.value.code == 10  # FM_ERR_IO
+
+
+def test_input_reader_default_in():
+    x = api.read_input(os.path.join(GOLD, "default.in"))
+    assert x.ensemble == 0 and x.density == 0.8 and x.rcutoff == 1.12246204830937
+    assert list(x.initialnunits) == [8, 8, 8]
+    assert x.nsteps == 1000 and x.tplot == 100 and x.delta_t == 0.005
+    assert list(x.delta_rneighbr) == [0.3, 0.3, 0.3]
+    assert x.force_list == 3 and x.integration_algorithm == 0
+
+
+def test_input_reader_two_phase_run():
+    x = api.read_input(os.path.join(GOLD, "MD_2_phase.in"))
+    assert x.rcutoff == 2.5 and x.delta_t == 0.005 and x.force_list == 1
+    assert list(x.initialnunits) == [76, 8, 8]
+    assert x.inputtemperature == 0.6057
+    assert x.integration_algorithm == 0
+
+
+def test_input_reader_reports_missing_keywords(tmp_path):
+    p = tmp_path / "MD.in"
+    p.write_text("DENSITY\n0.8\n")
+    with pytest.raises(api.FlowmolError) as e:
+        api.read_input(str(p))
+    assert "RCUTOFF" in str(e.value)
