@@ -176,6 +176,8 @@ def lib():
             "fm_setup": [h],
             "fm_move_vv": [h, C.c_int32],
             "fm_move_lfv": [h],
+            "fm_upload_monomers": [h, P(C.c_int32), P(C.c_int32), P(C.c_int32)],
+            "fm_get_bonds": [h, P(C.c_int32), P(C.c_int32), P(C.c_int8), C.c_int64, P(C.c_int64)],
             "fm_update_borders": [h, C.c_int32],
             "fm_check_rebuild": [h, P(C.c_int32)],
             "fm_linklist_deallocateall": [h],
@@ -334,6 +336,21 @@ class MDSystem:
             glob_no = np.ascontiguousarray(glob_no, dtype=np.int32)
             gp = glob_no.ctypes.data_as(C.POINTER(C.c_int32))
         check(lib().fm_upload_state(self.h, self.n, _dp(r), _dp(v), ap, gp))
+
+    def upload_monomers(self, chain, subchain, bflag):
+        c = np.ascontiguousarray(chain, np.int32); sc = np.ascontiguousarray(subchain, np.int32)
+        b = np.ascontiguousarray(bflag, np.int32).reshape(-1, 4)
+        P = C.POINTER(C.c_int32)
+        check(lib().fm_upload_monomers(self.h, c.ctypes.data_as(P), sc.ctypes.data_as(P), b.ctypes.data_as(P)))
+
+    def bonds(self):
+        n = C.c_int64()
+        check(lib().fm_get_bonds(self.h, None, None, None, 0, C.byref(n)))
+        o = np.empty(n.value, np.int32); p = np.empty(n.value, np.int32); c = np.empty(n.value, np.int8)
+        P = C.POINTER(C.c_int32)
+        check(lib().fm_get_bonds(self.h, o.ctypes.data_as(P), p.ctypes.data_as(P),
+                                 c.ctypes.data_as(C.POINTER(C.c_int8)), n.value, C.byref(n)))
+        return o, p, c.astype(np.int32)
 
     def download(self):
         r = np.empty((self.n, 3)); v = np.empty((self.n, 3)); a = np.empty((self.n, 3))

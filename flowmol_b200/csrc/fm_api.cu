@@ -151,7 +151,8 @@ static void release(fm_handle *h)
     FmDev &d = h->d;
     void *ptrs[] = {d.pos0, d.pos1, d.vx, d.vy, d.vz, d.ax, d.ay, d.az, d.slot_of, d.tvx, d.tvy, d.tvz,
                     d.tax, d.tay, d.taz, d.cell_of, d.cell_count, d.cell_start, d.perm, d.tile_sum, d.nbr, d.nnbr,
-                    d.pe, d.vir, d.partial, d.rec, d.sc, h->tpos, h->tuidx, h->glob, h->stage3};
+                    d.pe, d.vir, d.partial, d.rec, d.sc, h->tpos, h->tuidx, h->glob, h->stage3, d.chain,
+                    d.subchain, d.bflag, d.tchain, d.tsubchain, d.tbflag, d.bnd, d.nbond};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     d = FmDev{};
@@ -197,7 +198,10 @@ extern "C" int fm_create(const fm_params *p, fm_handle **out)
         return fail(FM_ERR_ARG, "force_list must be 0, 2 or 3");
     if (p->precision != FM_PRECISION_FP64 && p->precision != FM_PRECISION_FP32)
         return fail(FM_ERR_ARG, "precision must be FM_PRECISION_FP64 or FM_PRECISION_FP32");
-    if (p->potential_flag != 0) return fail(FM_ERR_ARG, "potential_flag 1 (FENE) is served by fm_poly_* handles");
+    if (p->potential_flag != 0 && p->potential_flag != 1) return fail(FM_ERR_ARG, "potential_flag must be 0 or 1");
+    if (p->potential_flag == 1 && p->force_list == 0)
+        return fail(FM_ERR_ARG, "potential flag/force_list incompatible - only LJ available with all pairs");
+    if (p->potential_flag == 1 && !(p->R_0 > 0.0 && p->k_c >= 0.0)) return fail(FM_ERR_ARG, "FENE needs R_0 > 0");
     if (p->rebuild_criteria != 0 && p->rebuild_criteria != 1)
         return fail(FM_ERR_ARG, "rebuild_criteria must be 0 (vmax) or 1 (fixed)");
     if (p->integration_algorithm != 0 && p->integration_algorithm != 1)
@@ -237,6 +241,10 @@ extern "C" int fm_create(const fm_params *p, fm_handle **out)
     }
     d.tplot = p->tplot;
     d.integrator = p->integration_algorithm;
+    d.potential_flag = p->potential_flag;
+    d.k_c = p->k_c;
+    d.R0 = p->R_0;
+    d.R0_2 = p->R_0 * p->R_0;
     d.precision = p->precision;
     double dmin = std::min(p->delta_rneighbr[0], std::min(p->delta_rneighbr[1], p->delta_rneighbr[2]));
     h->half_min_delta = 0.5 * dmin;
@@ -264,6 +272,11 @@ extern "C" int fm_create(const fm_params *p, fm_handle **out)
     FM_ALLOC(d.tile_sum, fm::scan_tiles(d.ncell))
     FM_ALLOC(d.pe, n) FM_ALLOC(d.vir, n)
     FM_ALLOC(h->stage3, 9 * n)
+    if (p->potential_flag == 1) {
+        FM_ALLOC(d.chain, n) FM_ALLOC(d.subchain, n) FM_ALLOC(d.bflag, n)
+        FM_ALLOC(d.tchain, n) FM_ALLOC(d.tsubchain, n) FM_ALLOC(d.tbflag, n)
+        FM_ALLOC(d.bnd, 4 * n) FM_ALLOC(d.nbond, n)
+    }
     int nb = std::max(std::max(fm::force_blocks(d.n, 16), fm::all_pairs_blocks(d.n)), fm::macro_blocks(d.n));
     FM_ALLOC(d.partial, (size_t)nb * fm::RS_N)
     d.rec_cap = 4096;
@@ -282,6 +295,10 @@ extern "C" int fm_create(const fm_params *p, fm_handle **out)
     cudaMemset(d.cell_start, 0, sizeof(int32_t) * (size_t)(d.ncell + 1));
     cudaMemset(d.nnbr, 0, sizeof(int32_t) * n);
     cudaMemset(d.pe, 0, sizeof(double) * n);
+    if (d.nbond) cudaMemset(d.nbond, 0, sizeof(int32_t) * n);
+    if (d.chain) cudaMemset(d.chain, 0, sizeof(int32_t) * n);
+    if (d.subchain) cudaMemset(d.subchain, 0, sizeof(int32_t) * n);
+    if (d.bflag) cudaMemset(d.bflag, 0, sizeof(int4) * n);
     cudaMemset(d.vir, 0, sizeof(double) * n);
     cudaMemset(d.sc, 0, sizeof(fm::FmScalars));
     fm::launch_reset_scalars(d, nullptr);
@@ -363,6 +380,52 @@ extern "C" int fm_upload_state_device(fm_handle *h, int32_t n, const double *d_r
     FM_TRY(set_glob(h, nullptr));
     FM_CUDA(cudaGetLastError());
     h->stage = 1;
+    return FM_OK;
+}
+
+extern "C" int fm_upload_monomers(fm_handle *h, const int32_t *chainID, const int32_t *subchainID,
+                                  const int32_t *bin_bflag)
+{
+    if (!h) return fail(FM_ERR_ARG, "null handle");
+    if (h->p.potential_flag != 1) return fail(FM_ERR_STATE, "monomer data needs potential_flag 1");
+    if (h->stage != 1) return fail(FM_ERR_STATE, "upload monomers after fm_upload_state and before fm_setup");
+    if (!chainID || !subchainID || !bin_bflag) return fail(FM_ERR_ARG, "null array");
+    const size_t n = (size_t)h->d.n;
+    // slots still equal upload indices before the first binning
+    FM_CUDA(cudaMemcpyAsync(h->d.chain, chainID, 4 * n, cudaMemcpyHostToDevice, h->st));
+    FM_CUDA(cudaMemcpyAsync(h->d.subchain, subchainID, 4 * n, cudaMemcpyHostToDevice, h->st));
+    FM_CUDA(cudaMemcpyAsync(h->d.bflag, bin_bflag, 16 * n, cudaMemcpyHostToDevice, h->st));
+    FM_CUDA(cudaStreamSynchronize(h->st));
+    return FM_OK;
+}
+
+static int ready(fm_handle *h, int min_stage);
+
+extern "C" int fm_get_bonds(fm_handle *h, int32_t *owner, int32_t *partner, int8_t *code, int64_t cap, int64_t *n_out)
+{
+    FM_TRY(ready(h, 2));
+    if (!n_out) return fail(FM_ERR_ARG, "null output");
+    if (h->p.potential_flag != 1) { *n_out = 0; return FM_OK; }
+    const size_t n = (size_t)h->d.n;
+    std::vector<int32_t> nb(n), slot(n), bnd(4 * n);
+    FM_CUDA(cudaMemcpyAsync(nb.data(), h->d.nbond, 4 * n, cudaMemcpyDeviceToHost, h->st));
+    FM_CUDA(cudaMemcpyAsync(slot.data(), h->d.slot_of, 4 * n, cudaMemcpyDeviceToHost, h->st));
+    FM_CUDA(cudaMemcpyAsync(bnd.data(), h->d.bnd, 16 * n, cudaMemcpyDeviceToHost, h->st));
+    FM_CUDA(cudaStreamSynchronize(h->st));
+    int64_t k = 0;
+    for (size_t i = 0; i < n; i++)
+        for (int b = 0; b < nb[i]; b++) {
+            int32_t e = bnd[4 * i + (size_t)b];
+            int32_t j = e & fm::NB_INDEX_MASK;
+            int c6 = (int)((uint32_t)e >> fm::NB_SHIFT_BITS);
+            if (k < cap) {
+                if (owner) owner[k] = h->glob_host[(size_t)slot[i]];
+                if (partner) partner[k] = h->glob_host[(size_t)slot[(size_t)j]];
+                if (code) code[k] = (int8_t)((c6 & 3) + 3 * ((c6 >> 2) & 3) + 9 * ((c6 >> 4) & 3));
+            }
+            k++;
+        }
+    *n_out = k;
     return FM_OK;
 }
 

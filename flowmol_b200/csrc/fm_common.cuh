@@ -77,6 +77,15 @@ struct FmDev {
     int32_t *nnbr;
     // per-molecule PE / virial (record steps)
     double *pe, *vir;
+    // FENE polymers (potential_flag 1): monomer data per slot and bonds found
+    // at list build, bnd[i*4 + b] = partner | image code, like nbr entries
+    int potential_flag;
+    double k_c, R0, R0_2;
+    int32_t *chain, *subchain;
+    int4 *bflag;
+    int32_t *tchain, *tsubchain;
+    int4 *tbflag;
+    int32_t *bnd, *nbond;
     // record partials [nblocks][RS_N] and finished rows
     double *partial;
     int nblocks_force;

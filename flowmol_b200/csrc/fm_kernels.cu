@@ -324,6 +324,9 @@ __global__ void k_reorder_gather(FmDev d, int gated, double4 *tpos, int32_t *tui
         d.tvx[s] = d.vx[o]; d.tvy[s] = d.vy[o]; d.tvz[s] = d.vz[o];
         d.tax[s] = d.ax[o]; d.tay[s] = d.ay[o]; d.taz[s] = d.az[o];
         tuidx[s] = d.slot_of[o];
+        if (d.potential_flag == 1) {
+            d.tchain[s] = d.chain[o]; d.tsubchain[s] = d.subchain[o]; d.tbflag[s] = d.bflag[o];
+        }
     }
 }
 
@@ -336,6 +339,9 @@ __global__ void k_reorder_copy(FmDev d, int gated, const double4 *tpos, const in
         d.vx[s] = d.tvx[s]; d.vy[s] = d.tvy[s]; d.vz[s] = d.tvz[s];
         d.ax[s] = d.tax[s]; d.ay[s] = d.tay[s]; d.az[s] = d.taz[s];
         d.slot_of[s] = tuidx[s];
+        if (d.potential_flag == 1) {
+            d.chain[s] = d.tchain[s]; d.subchain[s] = d.tsubchain[s]; d.bflag[s] = d.tbflag[s];
+        }
     }
 }
 
@@ -372,6 +378,13 @@ constexpr int NB_STAGE = 256;               // staged candidates per warp
 // from rneighbr2; a candidate inside the band is re-read in FP64 and decided
 // by the exact test (dx^2+dy^2)+dz^2 < rneighbr2 -- a branch the whole warp
 // skips unless some lane needs it.
+//
+// With FENE polymers (POLY) the same scan discovers bonds the way the
+// reference's check_update_adjacentbeadinfo does (linklist.f90:2542-2584): any
+// candidate of the scanned cells -- at any distance -- with the owner's chain
+// whose subchain bit is set in the owner's bin_bflag words (get_bondflag,
+// modules.f90:602-610, 31 bits per word) is a bond partner.
+template <bool POLY>
 __global__ void __launch_bounds__(NB_THREADS) k_build_nlist(FmDev d, int gated, int iter)
 {
     if (!gate(d, gated)) return;
@@ -387,6 +400,7 @@ __global__ void __launch_bounds__(NB_THREADS) k_build_nlist(FmDev d, int gated, 
     const float lo32 = (float)rn2 - band, hi32 = (float)rn2 + band;
 
     __shared__ float4 s_f[NB_WARPS][NB_STAGE];   // x, y, z offsets and the entry bits in w
+    __shared__ int2 s_cs[POLY ? NB_WARPS : 1][POLY ? NB_STAGE : 1];  // chain, subchain of candidates
     __shared__ int s_off[NB_WARPS][55];          // candidate offset of segment k (54 segments + total)
     __shared__ int s_start[NB_WARPS][54], s_code[NB_WARPS][54];
 
@@ -456,6 +470,9 @@ __global__ void __launch_bounds__(NB_THREADS) k_build_nlist(FmDev d, int gated, 
             const float xif = (float)(pi.x - refx), yif = (float)(pi.y - refy), zif = (float)(pi.z - refz);
             int cnt = 0;
             int32_t *out = d.nbr + (size_t)i * maxn;
+            int chain_i = 0, nb = 0;
+            int4 bf = make_int4(0, 0, 0, 0);
+            if (POLY && own) { chain_i = d.chain[i]; bf = d.bflag[i]; }
             for (int base = 0; base < total; base += NB_STAGE) {
                 const int take = min(NB_STAGE, total - base);
                 __syncwarp();
@@ -474,6 +491,7 @@ __global__ void __launch_bounds__(NB_THREADS) k_build_nlist(FmDev d, int gated, 
                     const double zj = szs ? __dadd_rn(pj.z, szs > 0 ? Lz : -Lz) : pj.z;
                     s_f[warp][t] = make_float4((float)(xj - refx), (float)(yj - refy), (float)(zj - refz),
                                                __int_as_float(j | (code << NB_SHIFT_BITS)));
+                    if (POLY) s_cs[warp][t] = make_int2(d.chain[j], d.subchain[j]);
                 }
                 __syncwarp();
                 for (int q = 0; q < take; q++) {
@@ -482,6 +500,17 @@ __global__ void __launch_bounds__(NB_THREADS) k_build_nlist(FmDev d, int gated, 
                     const float r2f = fx * fx + fy * fy + fz * fz;
                     const int e = __float_as_int(f.w);
                     const bool self = (e & NB_INDEX_MASK) == i && (e >> NB_SHIFT_BITS) == noshift;
+                    if (POLY && own && !self) {
+                        const int2 cs = s_cs[warp][q];
+                        if (cs.x == chain_i) {
+                            const int pos = cs.y - 1, grp = pos / 31, ex = pos % 31;
+                            const int word = grp == 0 ? bf.x : grp == 1 ? bf.y : grp == 2 ? bf.z : bf.w;
+                            if (pos >= 0 && grp < 4 && ((word >> ex) & 1)) {
+                                if (nb < 4) d.bnd[(size_t)i * 4 + nb] = e;
+                                nb++;
+                            }
+                        }
+                    }
                     bool hit = own && !self && r2f < lo32;
                     const bool in_band = own && !self && r2f >= lo32 && r2f <= hi32;
                     if (__any_sync(0xffffffffu, in_band)) {
@@ -508,6 +537,10 @@ __global__ void __launch_bounds__(NB_THREADS) k_build_nlist(FmDev d, int gated, 
                 d.nnbr[i] = cnt < maxn ? cnt : maxn;
                 atomicMax(&d.sc->max_nbr, cnt);
                 if (cnt > maxn) raise_status(d, ST_NLIST, iter);
+                if (POLY) {
+                    d.nbond[i] = nb < 4 ? nb : 4;
+                    if (nb > 4) raise_status(d, ST_BOND, iter);  // too_many_bonds_error
+                }
             }
         }
         __syncwarp();
@@ -584,6 +617,41 @@ __device__ __forceinline__ double epilogue(const FmDev &d, int pset, int i, doub
     }
     if (MODE >= 1) { d.vx[i] = vx; d.vy[i] = vy; d.vz[i] = vz; }
     return m2;
+}
+
+// FENE springs of molecule i (simulation_compute_forces_poly,
+// simulation_compute_forces.f90:731-789): accijmag = -k/(1 - r^2/R0^2)
+// (FENE_accijmag, setup_set_parameters.f90:348-358), energy
+// 0.5 k R0^2 log(1 - r^2/R0^2) (:371-380), in FP64 for every precision form.
+// A bond at or beyond R0 is the reference's polymer_bond_error.
+template <bool REC>
+__device__ __forceinline__ void fene_bonds(const FmDev &d, const double4 *P, int i, double &fx, double &fy,
+                                           double &fz, double &pe, double &vir)
+{
+    const double4 pi = P[i];
+    const int nb = d.nbond[i];
+    for (int b = 0; b < nb; b++) {
+        const int e = d.bnd[(size_t)i * 4 + b];
+        const int code = e >> NB_SHIFT_BITS;
+        const double4 pj = P[e & NB_INDEX_MASK];
+        const double xj = (code & 3) != 1 ? __dadd_rn(pj.x, (code & 3) == 2 ? d.L[0] : -d.L[0]) : pj.x;
+        const double yj = ((code >> 2) & 3) != 1 ? __dadd_rn(pj.y, ((code >> 2) & 3) == 2 ? d.L[1] : -d.L[1]) : pj.y;
+        const double zj = ((code >> 4) & 3) != 1 ? __dadd_rn(pj.z, ((code >> 4) & 3) == 2 ? d.L[2] : -d.L[2]) : pj.z;
+        const double dx = __dsub_rn(pi.x, xj), dy = __dsub_rn(pi.y, yj), dz = __dsub_rn(pi.z, zj);
+        const double r2 = norm2_rn(dx, dy, dz);
+        if (r2 >= d.R0_2) {
+            uint32_t old = atomicOr(&d.sc->status, ST_BOND);
+            if ((old & ST_FATAL) == 0u) d.sc->fail_iter = -2;
+            continue;
+        }
+        const double q = r2 / d.R0_2;
+        const double acc = -d.k_c / (1.0 - q);
+        fx += acc * dx; fy += acc * dy; fz += acc * dz;
+        if (REC) {
+            pe += 0.5 * d.k_c * d.R0 * d.R0 * log(1.0 - q);
+            vir += acc * r2;
+        }
+    }
 }
 
 // Block reduction of the record partials; row blockIdx.x of d.partial.
@@ -686,6 +754,7 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force(FmDev d)
     }
     double part[RS_N] = {0.0, 0.0, 0.0, 0.0, 0.0};
     double m2 = 0.0;
+    if (active && lane == 0 && d.potential_flag == 1) fene_bonds<REC>(d, P, i, fx, fy, fz, pe, vir);
     // a(:,i) = sum acc rij / mass, mass = 1 (LJ_mass)
     if (active && lane == 0) m2 = epilogue<REC, MODE>(d, pset, i, P[i], fx, fy, fz, pe, vir, part);
     if (REC) block_partials(d, part);
@@ -989,7 +1058,8 @@ void launch_reorder(const FmDev &d, int gated, double4 *tpos, int32_t *tuidx, cu
 }
 void launch_build_nlist(const FmDev &d, int gated, int iter, cudaStream_t st)
 {
-    k_build_nlist<<<sgrid(d.ncell, NB_WARPS, 8), NB_THREADS, 0, st>>>(d, gated, iter);
+    if (d.potential_flag == 1) k_build_nlist<true><<<sgrid(d.ncell, NB_WARPS, 8), NB_THREADS, 0, st>>>(d, gated, iter);
+    else k_build_nlist<false><<<sgrid(d.ncell, NB_WARPS, 8), NB_THREADS, 0, st>>>(d, gated, iter);
 }
 
 int force_blocks(int n, int tpm) { return nblk(n * tpm, FORCE_THREADS); }

@@ -132,6 +132,16 @@ FM_API int fm_upload_state(fm_handle *h, int32_t n, const double *r, const doubl
  * the upload is row i here whatever order the device keeps internally.
  * Blocks until the stream has drained. */
 FM_API int fm_download_state(fm_handle *h, double *r, double *v, double *a, int32_t *glob_no);
+/* FENE polymers (potential_flag 1): the reference's monomer record per
+ * molecule in upload order -- chainID, subchainID and the four bin_bflag
+ * words (polymer_info_MD; bin_bflag is (4, n)).  Call after fm_upload_state,
+ * before fm_setup.  Bonds are then found while lists are built, as
+ * check_update_adjacentbeadinfo does (linklist.f90:2542-2584). */
+FM_API int fm_upload_monomers(fm_handle *h, const int32_t *chainID, const int32_t *subchainID,
+                              const int32_t *bin_bflag);
+/* Bonds of the last list build as (owner glob_no, partner glob_no, image
+ * code) triplets, like fm_get_pair_list.  Test hook. */
+FM_API int fm_get_bonds(fm_handle *h, int32_t *owner, int32_t *partner, int8_t *code, int64_t cap, int64_t *n);
 /* Device pointers variant for callers that keep the state on the GPU:
  * d_r/d_v are (3, n) column-major FP64 device arrays, read or written on the
  * handle's stream without host staging. */

@@ -1300,3 +1300,26 @@ int orc_run_lfv(orc *s, int nsteps, double *rec_out, int rec_cap, int *nrec)
     }
     return ORC_OK;
 }
+
+/* Bonds found at the last list build as (owner, partner source, image code)
+ * with glob_no identities; code as in orc_pair_list. */
+long orc_bond_list(orc *s, int *owner, int *partner, int *code, long cap)
+{
+    long n = 0;
+    for (int i = 1; i <= s->np; i++)
+        for (int b = 0; b < s->bondcount[i - 1]; b++) {
+            int j = s->bond[(size_t)(i - 1) * s->max_funcy + b];
+            if (j == 0) continue;
+            if (n < cap) {
+                owner[n] = s->glob_no[i - 1];
+                if (j <= s->np) { partner[n] = s->glob_no[j - 1]; code[n] = 13; }
+                else {
+                    const signed char *sh = &s->halo_shift[3 * (size_t)(j - 1)];
+                    partner[n] = s->glob_no[s->halo_src[j - 1] - 1];
+                    code[n] = (sh[0] + 1) + 3 * (sh[1] + 1) + 9 * (sh[2] + 1);
+                }
+            }
+            n++;
+        }
+    return n;
+}

@@ -86,6 +86,8 @@ def lib():
         L.orc_run_lfv.restype = C.c_int
         L.orc_run_lfv.argtypes = [C.c_void_p, C.c_int, d3, C.c_int, i3]
         L.orc_pressure_average.argtypes = [C.c_void_p, d3, i3]
+        L.orc_bond_list.restype = C.c_long
+        L.orc_bond_list.argtypes = [C.c_void_p, i3, i3, i3, C.c_long]
         _lib = L
     return _lib
 
@@ -271,6 +273,12 @@ class Oracle:
         n = C.c_int(0)
         lib().orc_pressure_average(self.h, _dp(out), C.byref(n))
         return out.reshape(3, 3), n.value
+
+    def bond_list(self):
+        cap = 4 * self.np_ + 16
+        o = np.zeros(cap, np.int32); p = np.zeros(cap, np.int32); c = np.zeros(cap, np.int32)
+        n = lib().orc_bond_list(self.h, _ip(o), _ip(p), _ip(c), cap)
+        return o[:n], p[:n], c[:n]
 
     def pair_list(self):
         """(owner, partner, code) arrays, 1-based glob_no; code 13 = no image."""

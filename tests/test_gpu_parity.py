@@ -292,3 +292,31 @@ def test_reference_restart_liquid_vapour_state(gpu_lib):
     assert rel_err(acc, o.a, 1.0).max() <= TOL64
     pe, vir = s.per_molecule()
     np.testing.assert_allclose(pe, o.potenergymol, rtol=TOL64, atol=TOL64)
+
+
+def test_fene_melt_bonds_forces_trajectory(gpu_lib):
+    """FENE bead-spring melt (512 chains of 8, WCA + FENE k=30, R0=1.5, the
+    rneighbr = R0 override): bonds found at list build equal the reference's
+    check_update_adjacentbeadinfo set, pair set bit-exact, forces 1e-12."""
+    from flowmol_b200 import polymer
+    r, v, ch, sub, fy, bf, dom = polymer.fene_melt(512)
+    o = O.Oracle(r, v, dom, WCA_RC, tplot=20, potential_flag=1, k_c=30.0, R_0=1.5, density=0.85)
+    o.set_monomers(ch, sub, fy, bf)
+    o.setup()
+    s = gpu_system(r, v, dom, WCA_RC, tplot=20, density=0.85, potential_flag=1, k_c=30.0, R_0=1.5)
+    s.upload_monomers(ch, sub, bf)
+    s.setup()
+    key = lambda t: np.sort((t[0].astype(np.int64) << 32) | (t[1].astype(np.int64) << 5) | t[2])  # noqa: E731
+    assert np.array_equal(key(s.bonds()), key(o.bond_list()))
+    assert np.array_equal(canonical_full(*s.pair_list()), canonical_oracle(*o.pair_list()))
+    _, _, a, _ = s.download()
+    assert rel_err(a, o.a, 1.0).max() <= TOL64
+    recs_o = o.run_vv(100)
+    s.records()
+    s.simulation_md(100)
+    recs = s.records()
+    assert [r_["iter"] for r_ in recs] == [int(x) for x in recs_o[:, 0]]
+    for row, ro in zip(recs, recs_o):
+        assert row["potenergy"] == pytest.approx(ro[5], rel=1e-9)
+    rg, _, _, _ = s.download()
+    assert np.abs(wrap_diff(rg, o.r, dom)).max() < 1e-7
