@@ -38,6 +38,40 @@ DENSITY, TEMP, RC, SKIN, DT, TPLOT = 0.8442, 0.722, 2.5, 0.3, 0.005, 100
 SEED = 0x466D6F6C + 1
 
 
+class Ranks:
+    """Rank plumbing of replica runs: a barrier, and the MAX over ranks of a
+    time, so that a whole-job value is the units all ranks processed divided
+    by the slowest rank's time.  `device` None means CPU tensors (gloo)."""
+
+    def __init__(self, dist=None, device=None):
+        self.dist = dist
+        self.device = device
+
+    @property
+    def world(self):
+        return self.dist.get_world_size() if self.dist is not None else 1
+
+    def barrier(self):
+        import torch
+        if self.dist is not None:
+            self.dist.barrier()
+        if self.device is not None:
+            torch.cuda.synchronize(self.device)
+
+    def max(self, x):
+        if self.dist is None:
+            return float(x)
+        import torch
+        t = torch.tensor([float(x)], dtype=torch.float64,
+                         device=f"cuda:{self.device}" if self.device is not None else "cpu")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def whole_job(self, units_per_rank, seconds):
+        """Weak-scaling aggregate: world * units / max-over-ranks seconds."""
+        return self.world * units_per_rank / self.max(seconds)
+
+
 def alg_bytes_per_molecule_step(rn=RC + SKIN, rho=DENSITY):
     """192 B of FP64 r, v, a read and written once, plus 4-byte half-list
     indices: n_h = (2/3) pi r_n^3 rho."""
@@ -125,10 +159,11 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def run_form(api, torch, r, v, dom, precision, steps, warmup, dev, timing_pass=True):
+def run_form(api, torch, r, v, dom, precision, steps, warmup, dev, timing_pass=True, tpm=0):
     """Device-resident throughput of one precision form."""
     stream = torch.cuda.Stream(device=dev)
-    p = api.make_params(len(r), dom, RC, (SKIN,) * 3, DT, TPLOT, density=DENSITY, precision=precision)
+    p = api.make_params(len(r), dom, RC, (SKIN,) * 3, DT, TPLOT, density=DENSITY, precision=precision,
+                        threads_per_molecule=tpm)
     s = api.MDSystem(p, stream=stream)
     s.upload(r, v)
     s.setup()
@@ -158,6 +193,7 @@ def run_form(api, torch, r, v, dom, precision, steps, warmup, dev, timing_pass=T
         out["force_launches"] = nl
     out["records"] = s.records()
     out["capacity"] = s.counters()["nlist_capacity"]
+    out["tpm"] = s.threads_per_molecule
     s.close()
     return out
 
@@ -346,6 +382,8 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=2000)
     ap.add_argument("--serve-jobs", type=int, default=4096)
     ap.add_argument("--no-forms", action="store_true", help="skip the batched and served forms")
+    ap.add_argument("--tpm", type=int, default=0,
+                    help="force-kernel lanes per molecule (0: the autotuner's choice)")
     ap.add_argument("--profile-case", choices=["fp32", "fp64"], default=None,
                     help="profiling workload: setup + 10 fused steps of the 1M system, no timing")
     args = ap.parse_args()
@@ -379,7 +417,8 @@ def main():
     if args.profile_case:
         r, v, dom = make_state()
         prec = api.PRECISION_FP32 if args.profile_case == "fp32" else api.PRECISION_FP64
-        p = api.make_params(len(r), dom, RC, (SKIN,) * 3, DT, TPLOT, density=DENSITY, precision=prec)
+        p = api.make_params(len(r), dom, RC, (SKIN,) * 3, DT, TPLOT, density=DENSITY, precision=prec,
+                            threads_per_molecule=args.tpm)
         s = api.MDSystem(p)
         s.upload(r, v)
         s.setup()
@@ -395,24 +434,15 @@ def main():
                                 device_id=torch.device("cuda", dev))
     r, v, dom = make_state()
     n = len(r)
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize(dev)
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    ranks = Ranks(dist, dev)
+    barrier = ranks.barrier
+    max_over_ranks = ranks.max
 
     barrier()
-    f32 = run_form(api, torch, r, v, dom, api.PRECISION_FP32, args.steps, args.warmup, dev)
+    f32 = run_form(api, torch, r, v, dom, api.PRECISION_FP32, args.steps, args.warmup, dev, tpm=args.tpm)
     ms32 = max_over_ranks(f32["ms"])
     barrier()
-    f64 = run_form(api, torch, r, v, dom, api.PRECISION_FP64, args.steps, args.warmup, dev)
+    f64 = run_form(api, torch, r, v, dom, api.PRECISION_FP64, args.steps, args.warmup, dev, tpm=args.tpm)
     ms64 = max_over_ranks(f64["ms"])
     barrier()
     e2e = None if args.no_e2e else run_e2e(api, torch, r, v, dom, api.PRECISION_FP32, args.steps, dev)
@@ -448,9 +478,9 @@ def main():
                        "rebuilds_in_timed_region": f32["rebuilds"], "parallelism": f"replicas x{world}"},
             "forms": {
                 "fp32_forces": {"value": value, "ms_per_step": ms32 / args.steps,
-                                "force_kernel_ms": f32["force_ms_avg"]},
+                                "force_kernel_ms": f32["force_ms_avg"], "threads_per_molecule": f32["tpm"]},
                 "fp64_plain": {"value": world * n * args.steps / (ms64 * 1e-3), "ms_per_step": ms64 / args.steps,
-                               "force_kernel_ms": f64["force_ms_avg"]},
+                               "force_kernel_ms": f64["force_ms_avg"], "threads_per_molecule": f64["tpm"]},
             },
             "roofline": {"bound": "hbm", "kernel": "k_force (fused forces + move(2) + next move(1))",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

@@ -195,6 +195,7 @@ def lib():
             "fm_get_pair_list": [h, P(C.c_int32), P(C.c_int32), P(C.c_int8), C.c_int64, P(C.c_int64)],
             "fm_pair_digest": [h, P(C.c_uint64), P(C.c_int64)],
             "fm_get_counters": [h, P(C.c_int64), P(C.c_int32), P(C.c_int32)],
+            "fm_get_threads_per_molecule": [h, P(C.c_int32)],
             "fm_last_error": [C.c_char_p, C.c_int32],
             "fm_engine_create": [P(FmEngineParams), P(h)],
             "fm_engine_destroy": [h],
@@ -484,6 +485,12 @@ class MDSystem:
         n = C.c_int64()
         check(lib().fm_get_launch_count(self.h, C.byref(n)))
         return n.value
+
+    @property
+    def threads_per_molecule(self):
+        t = C.c_int32()
+        check(lib().fm_get_threads_per_molecule(self.h, C.byref(t)))
+        return t.value
 
     def counters(self):
         rb = C.c_int64(); cap = C.c_int32(); mx = C.c_int32()

@@ -221,6 +221,8 @@ FM_API int fm_get_pair_list(fm_handle *h, int32_t *owner, int32_t *partner, int8
  * (owner, partner, code) for image pairs); matches the oracle's digest of
  * the reference half list. */
 FM_API int fm_pair_digest(fm_handle *h, uint64_t *digest, int64_t *npairs);
+/* Force-kernel lanes per molecule in use (fixed, or chosen by the autotuner at fm_setup). */
+FM_API int fm_get_threads_per_molecule(fm_handle *h, int32_t *tpm);
 /* Counters: rebuilds done, neighbour capacity in use, largest list seen. */
 FM_API int fm_get_counters(fm_handle *h, int64_t *rebuilds, int32_t *nlist_capacity, int32_t *max_neighbours);
 
