@@ -411,8 +411,9 @@ def main():
     ap.add_argument("--no-forms", action="store_true", help="skip the batched and served forms")
     ap.add_argument("--tpm", type=int, default=0,
                     help="force-kernel lanes per molecule (0: the autotuner's choice)")
-    ap.add_argument("--profile-case", choices=["fp32", "fp64"], default=None,
-                    help="profiling workload: setup + 10 fused steps of the 1M system, no timing")
+    ap.add_argument("--profile-case", choices=["fp32", "fp64", "batched"], default=None,
+                    help="profiling workload, no timing: setup + 10 fused steps of the 1M system "
+                         "(fp32, fp64), or the batched replicas for --batch-steps steps")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -441,6 +442,18 @@ def main():
     fb.build()
     dev = local
     torch.cuda.set_device(dev)
+    if args.profile_case == "batched":
+        reps = batch_replicas(args.batch_replicas)
+        tot = sum(len(x[0]) for x in reps)
+        e = api.Engine(max_molecules=tot + 1024, max_cells=2_000_000, max_list_entries=(tot + 1024) * 160,
+                       max_slots=len(reps), precision=api.PRECISION_FP32, ticks_per_chunk=50, keep_states=False)
+        for r, v, dom, rho, fl in reps:
+            e.submit(api.make_job(len(r), dom, RC, args.batch_steps, density=rho, tplot=TPLOT, force_list=fl), r, v)
+        e.run()
+        bad = [x for x in e.results() if x["status"] != 0]
+        print(json.dumps({"profile_case": "batched", "molecules": tot, "failed": len(bad), **e.counters()}))
+        e.close()
+        return
     if args.profile_case:
         r, v, dom = make_state()
         prec = api.PRECISION_FP32 if args.profile_case == "fp32" else api.PRECISION_FP64

@@ -183,7 +183,7 @@ static int alloc_nlist(fm_handle *h, int maxn)
     if (d.nbr) cudaFree(d.nbr);
     d.nbr = nullptr;
     d.maxn = maxn;
-    FM_TRY(dalloc(&d.nbr, (size_t)d.n * (size_t)maxn));
+    FM_TRY(dalloc(&d.nbr, fm::nb_rows(d.n) * (size_t)maxn));
     return FM_OK;
 }
 
@@ -977,7 +977,7 @@ extern "C" int fm_get_pair_list(fm_handle *h, int32_t *owner, int32_t *partner, 
     if (!n_out) return fail(FM_ERR_ARG, "null output");
     if (h->p.force_list == 0) { *n_out = 0; return FM_OK; }
     const size_t n = (size_t)h->d.n;
-    std::vector<int32_t> nnbr(n), slot(n), nbr(n * (size_t)h->d.maxn);
+    std::vector<int32_t> nnbr(n), slot(n), nbr(fm::nb_rows((int)n) * (size_t)h->d.maxn);
     FM_CUDA(cudaMemcpyAsync(nnbr.data(), h->d.nnbr, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, h->st));
     FM_CUDA(cudaMemcpyAsync(slot.data(), h->d.slot_of, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, h->st));
     FM_CUDA(cudaMemcpyAsync(nbr.data(), h->d.nbr, sizeof(int32_t) * nbr.size(), cudaMemcpyDeviceToHost, h->st));
@@ -985,7 +985,7 @@ extern "C" int fm_get_pair_list(fm_handle *h, int32_t *owner, int32_t *partner, 
     int64_t k = 0;
     for (size_t i = 0; i < n; i++) {
         for (int q = 0; q < nnbr[i]; q++) {
-            int32_t e = nbr[i * (size_t)h->d.maxn + (size_t)q];
+            int32_t e = nbr[fm::nb_row((int)i, h->d.maxn) + fm::nb_col(q)];
             int32_t j = e & fm::NB_INDEX_MASK;
             int c6 = (int)((uint32_t)e >> fm::NB_SHIFT_BITS);
             int sx = (c6 & 3) - 1, sy = ((c6 >> 2) & 3) - 1, sz = ((c6 >> 4) & 3) - 1;

@@ -1,0 +1,314 @@
+// fm_build.cuh -- the neighbour-list build of one cell, shared by the
+// single-system kernel (fm_kernels.cu) and the slot engine
+// (fm_engine_kernels.cu).
+//
+// Pair set of assign_to_neighbourlist_halfint_opt (linklist.f90:660-804,
+// 1118-1180), stored for both partners.  The reference visits every pair of
+// adjacent cells of which at least one is interior exactly once (13 forward
+// shifts from interior cells + 27 sweeps from halo cells); a halo cell holds
+// the images of the interior cell on the far side (plus any real molecule
+// that binned onto it).  Here each molecule of cell c collects, from the 27
+// cells around c that are not both halo with c, every candidate with
+// r^2 < rneighbr^2 -- the same set.
+//
+// Lane q < 27 computes the segments of neighbour cell q (its real members and,
+// for a halo cell, the shifted images of its source); a warp prefix sum lays
+// the candidates out in the reference's visiting order (cell q ascending,
+// real before images, slot ascending).  Candidates are staged in shared
+// memory as FP32 offsets from the cell's reference point, computed from the
+// FP64 image coordinate (x_src +/- L, one rounding, as the halo copy); those
+// farther than rneighbr from the bounding box of the owners being processed
+// are dropped at staging (the order of the rest is kept).  Then each lane
+// takes one staged candidate and the warp loops over the owners, NB_OG at a
+// time: the FP32 r^2 (error below 1e-5 cs^2 for molecules binned in this
+// build, offsets within 1.5 cells) decides every candidate farther than
+// BAND = 1e-4 cs^2 from rneighbr2; a candidate inside the band, or at FP32
+// distance 0 (the owner itself), is re-read in FP64 and decided by the exact
+// test (dx^2+dy^2)+dz^2 < rneighbr2 -- a branch the whole warp skips unless
+// some lane needs it.  An owner's hits among 32 candidates are one ballot,
+// appended to its row in candidate order, so every row lists its partners in
+// the visiting order.
+//
+// With FENE polymers (POLY) the same scan discovers bonds the way the
+// reference's check_update_adjacentbeadinfo does (linklist.f90:2542-2584): any
+// candidate of the scanned cells -- at any distance -- with the owner's chain
+// whose subchain bit is set in the owner's bin_bflag words (get_bondflag,
+// modules.f90:602-610, 31 bits per word) is a bond partner.  Pruning is off
+// then (a stretched bond is still found, and fails at the force).
+#pragma once
+#include "fm_common.cuh"
+#include "fm_device.cuh"
+
+namespace fm {
+
+constexpr int NB_WARPS = 4;                 // cells processed concurrently per block
+constexpr int NB_THREADS = 32 * NB_WARPS;
+constexpr int NB_STAGE = 256;               // staged candidates per warp
+constexpr int NB_OG = 4;                    // owners per step of the candidate loop
+constexpr int NB_NOSHIFT = 1 | (1 << 2) | (1 << 4);
+
+// One periodic system as the build sees it.  Molecule indices in entries,
+// rows and the per-molecule arrays count from the system's first molecule;
+// cell_start holds arena indices, mol_off is subtracted from them.
+struct CellSys {
+    const double4 *P;           // positions of the system's molecules
+    const int32_t *cell_start;  // ncell + 1 starts (arena molecule indices)
+    int mol_off;
+    int ne[3];
+    double cs[3], hd[3], L[3];
+    double rn2;
+    int32_t *nbr;               // rows nb_row(i, maxn) + nb_col(k)
+    int32_t *nnbr;
+    int maxn;
+    int *max_nbr;               // atomicMax of the row lengths
+    // FENE (POLY only)
+    const int32_t *chain, *subchain;
+    const int4 *bflag;
+    int32_t *bnd, *nbond;
+};
+
+// Per-warp shared staging.
+template <bool POLY>
+struct BuildShared {
+    float4 f[NB_STAGE];         // x, y, z offsets and the entry bits in w
+    int2 cs[POLY ? NB_STAGE : 1];  // chain, subchain of candidates
+    int off[55];                // candidate offset of segment k (54 segments + total)
+    int start[54], code[54];
+    float4 own[32];             // owners' offsets, molecule index in w
+    int ochain[POLY ? 32 : 1];
+    int4 obf[POLY ? 32 : 1];
+};
+
+constexpr uint32_t BUILD_OVER_LIST = 1u, BUILD_OVER_BONDS = 2u;
+
+// Exact FP64 decision of a staged candidate (entry e) for owner io: not the
+// owner itself, and (dx^2+dy^2)+dz^2 < rneighbr2 with the image x_src +/- L.
+__device__ __forceinline__ bool exact_pair(const double4 *P, int io, int e, const double (&L)[3], double rn2)
+{
+    const int code = e >> NB_SHIFT_BITS, jj = e & NB_INDEX_MASK;
+    if (jj == io && code == NB_NOSHIFT) return false;
+    const double4 po = ldg_pos(P + io);
+    const double4 pj = ldg_pos(P + jj);
+    const double xj = image(pj.x, (code & 3) - 1, L[0]);
+    const double yj = image(pj.y, ((code >> 2) & 3) - 1, L[1]);
+    const double zj = image(pj.z, ((code >> 4) & 3) - 1, L[2]);
+    return norm2_rn(__dsub_rn(po.x, xj), __dsub_rn(po.y, yj), __dsub_rn(po.z, zj)) < rn2;
+}
+
+// Rows of every molecule of cell c (0-based extended index) of system y, by
+// one warp.  Returns BUILD_OVER_* bits when a row or a bond set overflowed
+// (the counts past the capacity are still reported through max_nbr).
+template <bool POLY>
+__device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY> &sh, int lane)
+{
+    const int ne0 = y.ne[0], ne1 = y.ne[1], ne2 = y.ne[2];
+    const int cstart = y.cell_start[c] - y.mol_off;
+    const int ccount = y.cell_start[c + 1] - y.mol_off - cstart;
+    if (ccount == 0) return 0u;  // uniform across the warp
+    const double4 *P = y.P;
+    const int maxn = y.maxn;
+    const unsigned lt = (1u << lane) - 1u;
+    const double csmax = fmax(y.cs[0], fmax(y.cs[1], y.cs[2]));
+    const float band = (float)(1e-4 * csmax * csmax) + 1e-6f;
+    const float lo32 = (float)y.rn2 - band, hi32 = (float)y.rn2 + band;
+    // candidate pruning radius^2: rneighbr (1 + 5e-5) + 1e-4, far above the
+    // error of the FP32 offsets (~1e-6)
+    const float prune2 = (float)(y.rn2 * 1.0001 + 1e-4);
+    const int cx = c % ne0, cy = (c / ne0) % ne1, cz = c / (ne0 * ne1);
+    const bool chalo = is_halo(cx, ne0) || is_halo(cy, ne1) || is_halo(cz, ne2);
+    const double refx = (cx - 0.5) * y.cs[0] - y.hd[0];
+    const double refy = (cy - 0.5) * y.cs[1] - y.hd[1];
+    const double refz = (cz - 0.5) * y.cs[2] - y.hd[2];
+
+    // --- segments of neighbour cell q = lane ---
+    int n_real = 0, b_real = 0, n_img = 0, b_img = 0, code_img = NB_NOSHIFT;
+    if (lane < 27) {
+        const int x2 = cx + lane % 3 - 1, y2 = cy + (lane / 3) % 3 - 1, z2 = cz + lane / 9 - 1;
+        if (x2 >= 0 && y2 >= 0 && z2 >= 0 && x2 < ne0 && y2 < ne1 && z2 < ne2) {
+            const bool h2 = is_halo(x2, ne0) || is_halo(y2, ne1) || is_halo(z2, ne2);
+            if (!(chalo && h2)) {
+                const int c2 = x2 + ne0 * (y2 + ne1 * z2);
+                b_real = y.cell_start[c2] - y.mol_off;
+                n_real = y.cell_start[c2 + 1] - y.mol_off - b_real;
+                if (h2) {
+                    // images in a halo cell come from the interior cell on the far
+                    // side: low halo <- last interior cell shifted by -domain, high
+                    // halo <- first interior cell shifted by +domain
+                    const int ssx = x2 == 0 ? -1 : (x2 == ne0 - 1 ? 1 : 0);
+                    const int ssy = y2 == 0 ? -1 : (y2 == ne1 - 1 ? 1 : 0);
+                    const int ssz = z2 == 0 ? -1 : (z2 == ne2 - 1 ? 1 : 0);
+                    const int xs = x2 == 0 ? ne0 - 2 : (x2 == ne0 - 1 ? 1 : x2);
+                    const int ys = y2 == 0 ? ne1 - 2 : (y2 == ne1 - 1 ? 1 : y2);
+                    const int zs = z2 == 0 ? ne2 - 2 : (z2 == ne2 - 1 ? 1 : z2);
+                    const int cs2 = xs + ne0 * (ys + ne1 * zs);
+                    b_img = y.cell_start[cs2] - y.mol_off;
+                    n_img = y.cell_start[cs2 + 1] - y.mol_off - b_img;
+                    code_img = (ssx + 1) | ((ssy + 1) << 2) | ((ssz + 1) << 4);
+                }
+            }
+        }
+    }
+    const int tot = n_real + n_img;
+    int incl = tot;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    const int excl = incl - tot;
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    __syncwarp();
+    if (lane < 27) {
+        sh.off[2 * lane] = excl;
+        sh.off[2 * lane + 1] = excl + n_real;
+        sh.start[2 * lane] = b_real;
+        sh.start[2 * lane + 1] = b_img;
+        sh.code[2 * lane] = NB_NOSHIFT;
+        sh.code[2 * lane + 1] = code_img;
+    }
+    if (lane == 0) sh.off[54] = total;
+    __syncwarp();
+
+    uint32_t over = 0u;
+    for (int pass = 0; pass * 32 < ccount; pass++) {
+        const int mine = pass * 32 + lane;
+        const bool own = mine < ccount;
+        const int i = cstart + (own ? mine : 0);
+        const double4 pi = ldg_pos(P + i);
+        const float xif = (float)(pi.x - refx), yif = (float)(pi.y - refy), zif = (float)(pi.z - refz);
+        // bounding box of this pass's owners (lanes without an owner repeat owner 0)
+        const float bx0 = warp_min(xif), bx1 = warp_max(xif);
+        const float by0 = warp_min(yif), by1 = warp_max(yif);
+        const float bz0 = warp_min(zif), bz1 = warp_max(zif);
+        int cnt = 0, nb = 0;  // the owner lane's list and bond counts
+        const int nown = min(32, ccount - pass * 32);
+        __syncwarp();
+        sh.own[lane] = make_float4(xif, yif, zif, __int_as_float(i));
+        if (POLY) {
+            sh.ochain[lane] = own ? y.chain[i] : -1;
+            sh.obf[lane] = own ? y.bflag[i] : make_int4(0, 0, 0, 0);
+        }
+        for (int base = 0; base < total; base += NB_STAGE) {
+            const int take = min(NB_STAGE, total - base);
+            __syncwarp();
+            // stage the window's candidates that can lie within rneighbr of
+            // some owner of this pass, in visiting order (ballot compaction)
+            int kept = 0;
+            for (int t0 = 0; t0 < take; t0 += 32) {
+                const int t = t0 + lane;
+                bool keep = false;
+                float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
+                int j = 0;
+                if (t < take) {
+                    const int q = base + t;
+                    int k = 0;  // segment containing q: largest k with off[k] <= q
+#pragma unroll
+                    for (int step = 32; step > 0; step >>= 1)
+                        if (k + step < 54 && sh.off[k + step] <= q) k += step;
+                    j = sh.start[k] + (q - sh.off[k]);
+                    const int code = sh.code[k];
+                    const double4 pj = ldg_pos(P + j);
+                    const double xj = image(pj.x, (code & 3) - 1, y.L[0]);
+                    const double yj = image(pj.y, ((code >> 2) & 3) - 1, y.L[1]);
+                    const double zj = image(pj.z, ((code >> 4) & 3) - 1, y.L[2]);
+                    f = make_float4((float)(xj - refx), (float)(yj - refy), (float)(zj - refz),
+                                    __int_as_float(j | (code << NB_SHIFT_BITS)));
+                    // squared distance from the owners' box: beyond prune2 no
+                    // owner of this pass can be within rneighbr
+                    const float ex = fmaxf(fmaxf(bx0 - f.x, f.x - bx1), 0.f);
+                    const float ey = fmaxf(fmaxf(by0 - f.y, f.y - by1), 0.f);
+                    const float ez = fmaxf(fmaxf(bz0 - f.z, f.z - bz1), 0.f);
+                    keep = POLY || ex * ex + ey * ey + ez * ez < prune2;
+                }
+                const unsigned m = __ballot_sync(0xffffffffu, keep);
+                if (keep) {
+                    const int pos = kept + __popc(m & lt);
+                    sh.f[pos] = f;
+                    if (POLY) sh.cs[pos] = make_int2(y.chain[j], y.subchain[j]);
+                }
+                kept += __popc(m);
+            }
+            __syncwarp();
+            // lane = candidate, loop over owners
+            for (int t0 = 0; t0 < kept; t0 += 32) {
+                const int cq = t0 + lane;
+                const bool valid = cq < kept;
+                const float4 f = sh.f[valid ? cq : 0];
+                const int e = __float_as_int(f.w);
+                int2 cs = make_int2(-2, 0);
+                if (POLY && valid) cs = sh.cs[cq];
+                // owners in groups of NB_OG: independent chains for the scheduler
+                for (int o0 = 0; o0 < nown; o0 += NB_OG) {
+                    bool hit[NB_OG], exact[NB_OG];
+                    int io[NB_OG];
+                    bool anyx = false;
+#pragma unroll
+                    for (int u = 0; u < NB_OG; u++) {
+                        const float4 ow = sh.own[o0 + u];  // broadcast
+                        io[u] = __float_as_int(ow.w);
+                        const float fx = ow.x - f.x, fy = ow.y - f.y, fz = ow.z - f.z;
+                        const float r2f = fx * fx + fy * fy + fz * fz;
+                        const bool ok = valid && o0 + u < nown;
+                        // r2f is exactly 0 for the owner itself (identical operands);
+                        // 0 and the band around rneighbr2 are decided in FP64
+                        hit[u] = ok && r2f < lo32 && r2f > 0.f;
+                        exact[u] = ok && !hit[u] && r2f <= hi32;
+                        anyx |= exact[u];
+                    }
+                    if (__any_sync(0xffffffffu, anyx)) {
+#pragma unroll
+                        for (int u = 0; u < NB_OG; u++)
+                            if (exact[u]) hit[u] = exact_pair(P, io[u], e, y.L, y.rn2);
+                    }
+                    int add = 0;
+#pragma unroll
+                    for (int u = 0; u < NB_OG; u++) {
+                        const unsigned m = __ballot_sync(0xffffffffu, hit[u]);
+                        const int c0 = __shfl_sync(0xffffffffu, cnt, o0 + u);
+                        if (hit[u]) {
+                            const int k = c0 + __popc(m & lt);
+                            if (k < maxn) y.nbr[nb_row(io[u], maxn) + nb_col(k)] = e;
+                        }
+                        if (lane == o0 + u) add = __popc(m);
+                    }
+                    cnt += add;
+                    if (POLY) {
+                        int addb = 0;
+#pragma unroll
+                        for (int u = 0; u < NB_OG; u++) {
+                            bool bond = false;
+                            if (valid && o0 + u < nown && cs.x == sh.ochain[o0 + u] &&
+                                !((e & NB_INDEX_MASK) == io[u] && (e >> NB_SHIFT_BITS) == NB_NOSHIFT)) {
+                                const int pos = cs.y - 1, grp = pos / 31, ex = pos % 31;
+                                const int4 bf = sh.obf[o0 + u];
+                                const int word = grp == 0 ? bf.x : grp == 1 ? bf.y : grp == 2 ? bf.z : bf.w;
+                                bond = pos >= 0 && grp < 4 && ((word >> ex) & 1);
+                            }
+                            const unsigned mb = __ballot_sync(0xffffffffu, bond);
+                            const int b0 = __shfl_sync(0xffffffffu, nb, o0 + u);
+                            if (bond) {
+                                const int k = b0 + __popc(mb & lt);
+                                if (k < 4) y.bnd[(size_t)io[u] * 4 + k] = e;
+                            }
+                            if (lane == o0 + u) addb = __popc(mb);
+                        }
+                        nb += addb;
+                    }
+                }
+            }
+        }
+        if (own) {
+            y.nnbr[i] = cnt < maxn ? cnt : maxn;
+            atomicMax(y.max_nbr, cnt);
+            if (cnt > maxn) over |= BUILD_OVER_LIST;
+            if (POLY) {
+                y.nbond[i] = nb < 4 ? nb : 4;
+                if (nb > 4) over |= BUILD_OVER_BONDS;  // too_many_bonds_error
+            }
+        }
+    }
+    __syncwarp();
+    return over;
+}
+
+}  // namespace fm

@@ -72,7 +72,8 @@ struct FmDev {
     int32_t *cell_start;   // ncell + 1
     int32_t *perm;         // new slot -> old slot
     int32_t *tile_sum;     // per scan tile (4096 cells)
-    // neighbour list: nbr[i*maxn + k] = j | (sx+1)<<26 | (sy+1)<<28 | (sz+1)<<30
+    // neighbour list: entry k of molecule i, at nb_row(i, maxn) + nb_col(k), is
+    // j | (sx+1)<<26 | (sy+1)<<28 | (sz+1)<<30
     int32_t *nbr;
     int32_t *nnbr;
     // per-molecule PE / virial (record steps)
@@ -100,6 +101,18 @@ __host__ __device__ inline double4 *cur_pos(const FmDev &d, int pset) { return p
 constexpr int NB_SHIFT_BITS = 26;
 constexpr int32_t NB_INDEX_MASK = (1 << NB_SHIFT_BITS) - 1;
 constexpr int MAX_MOLECULES = NB_INDEX_MASK;
+
+// Neighbour list layout: molecules in groups of 32, each molecule's entries
+// in chunks of 4; chunk c of the 32 molecules of a group is one contiguous
+// 512-byte block (molecule i%32 at offset 16 (i%32) bytes), so a warp that
+// reads chunk c of its 32 molecules with 16-byte loads reads one segment.
+// The array holds ceil(n/32)*32 rows of maxn (a multiple of 8) entries.
+__host__ __device__ inline size_t nb_row(int i, int maxn)
+{
+    return (size_t)(i >> 5) * (size_t)maxn * 32u + (size_t)(i & 31) * 4u;
+}
+__host__ __device__ inline size_t nb_col(int k) { return (size_t)(k & ~3) * 32u + (size_t)(k & 3); }
+inline size_t nb_rows(int n) { return ((size_t)n + 31u) / 32u * 32u; }
 
 // Sets the message fm_last_error returns on this thread (fm_api.cu).
 void set_last_error(const char *msg);

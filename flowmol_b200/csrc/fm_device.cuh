@@ -36,6 +36,20 @@ __device__ __forceinline__ double warp_max(double v)
     return v;
 }
 
+__device__ __forceinline__ float warp_min(float v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__device__ __forceinline__ float warp_max(float v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
 // icell = ceiling((r + halfdomain)/cellsidelength) + 1 (1-based, halo = 1 and
 // ncells+2); the 0-based extended index is the ceiling itself.  Out-of-grid
 // values are clamped and flagged.

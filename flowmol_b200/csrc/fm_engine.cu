@@ -218,7 +218,7 @@ Footprint footprint(const fm_job &j, int maxn_override)
     int maxn = maxn_override > 0 ? maxn_override
                                  : (j.nlist_capacity > 0 ? j.nlist_capacity : (int)std::ceil(1.5 * expected) + 24);
     f.maxn = ((std::max(maxn, 8) + 7) / 8) * 8;
-    f.list = (int64_t)j.np * f.maxn;
+    f.list = (int64_t)fm::nb_rows(j.np) * f.maxn;  // rows of 32-molecule groups
     return f;
 }
 
@@ -357,7 +357,7 @@ int retire(fm_engine *e, int slot)
     if (jb.mode == fm::MODE_LIST) {
         e->cell.release(jb.cell_off, jb.ncell);
         e->cstart.release(jb.cstart_off, jb.ncell + 1);
-        e->list.release(jb.list_off, (int64_t)jb.p.np * jb.maxn);
+        e->list.release(jb.list_off, (int64_t)fm::nb_rows(jb.p.np) * jb.maxn);
     }
     fm::EngSlot empty;
     std::memset(&empty, 0, sizeof empty);

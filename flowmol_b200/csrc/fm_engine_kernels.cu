@@ -30,6 +30,7 @@
 
 #include "fm_device.cuh"
 #include "fm_engine.cuh"
+#include "fm_build.cuh"
 
 namespace fm {
 
@@ -309,143 +310,40 @@ __global__ void k_e_reorder_copy(EngDev d)
     }
 }
 
-// Neighbour rows, one warp per arena cell; the same visiting order, FP32 band
-// decision and exact FP64 in-band test as the single-system build
-// (assign_to_neighbourlist_halfint_opt, linklist.f90:660-804, pair set).
-constexpr int EB_WARPS = 4;
-constexpr int EB_STAGE = 256;
-__global__ void __launch_bounds__(EB_WARPS * 32) k_e_build(EngDev d)
+// Neighbour rows, one warp per arena cell: the single-system routine
+// (build_cell, fm_build.cuh: pair set of assign_to_neighbourlist_halfint_opt,
+// linklist.f90:660-804) on the cell's job.
+__global__ void __launch_bounds__(NB_THREADS, 6) k_e_build(EngDev d)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int noshift = 1 | (1 << 2) | (1 << 4);
-    __shared__ float4 s_f[EB_WARPS][EB_STAGE];
-    __shared__ int s_off[EB_WARPS][55];
-    __shared__ int s_start[EB_WARPS][54], s_code[EB_WARPS][54];
+    __shared__ BuildShared<false> sh[NB_WARPS];
+    __shared__ CellSys ys[NB_WARPS];  // the cell's job, read through shared memory
     if (!d.flags->any_rebuild) return;
     const int hwm = d.flags->cell_hwm;
-    const int stride = gridDim.x * EB_WARPS;
-    for (int c = blockIdx.x * EB_WARPS + warp; c < hwm; c += stride) {
+    for (int c = blockIdx.x * NB_WARPS + warp; c < hwm; c += gridDim.x * NB_WARPS) {
         const int k = d.cell_slot[c];
         if (k < 0) continue;
         EngSlot &s = d.slots[k];
         if (!slot_rebuilding(s) || s.mode != MODE_LIST) continue;
-        const int lc = c - s.cell_off;
-        const int cstart = d.cell_start[s.cstart_off + lc];
-        const int ccount = d.cell_start[s.cstart_off + lc + 1] - cstart;
-        if (ccount == 0) continue;
-        const int ne0 = s.ne[0], ne1 = s.ne[1], ne2 = s.ne[2];
-        const int cx = lc % ne0, cy = (lc / ne0) % ne1, cz = lc / (ne0 * ne1);
-        const bool chalo = is_halo(cx, ne0) || is_halo(cy, ne1) || is_halo(cz, ne2);
-        const double refx = (cx - 0.5) * s.cs[0] - s.hd[0];
-        const double refy = (cy - 0.5) * s.cs[1] - s.hd[1];
-        const double refz = (cz - 0.5) * s.cs[2] - s.hd[2];
-        const double csmax = fmax(s.cs[0], fmax(s.cs[1], s.cs[2]));
-        const float band = (float)(1e-4 * csmax * csmax) + 1e-6f;
-        const float lo32 = (float)s.rn2 - band, hi32 = (float)s.rn2 + band;
-        const double4 *P = eng_pos(d, s.pset);
-
-        int n_real = 0, b_real = 0, n_img = 0, b_img = 0, code_img = noshift;
-        if (lane < 27) {
-            int x2 = cx + lane % 3 - 1, y2 = cy + (lane / 3) % 3 - 1, z2 = cz + lane / 9 - 1;
-            if (x2 >= 0 && y2 >= 0 && z2 >= 0 && x2 < ne0 && y2 < ne1 && z2 < ne2) {
-                bool h2 = is_halo(x2, ne0) || is_halo(y2, ne1) || is_halo(z2, ne2);
-                if (!(chalo && h2)) {
-                    int c2 = x2 + ne0 * (y2 + ne1 * z2);
-                    b_real = d.cell_start[s.cstart_off + c2];
-                    n_real = d.cell_start[s.cstart_off + c2 + 1] - b_real;
-                    if (h2) {
-                        int ssx = x2 == 0 ? -1 : (x2 == ne0 - 1 ? 1 : 0);
-                        int ssy = y2 == 0 ? -1 : (y2 == ne1 - 1 ? 1 : 0);
-                        int ssz = z2 == 0 ? -1 : (z2 == ne2 - 1 ? 1 : 0);
-                        int xs = x2 == 0 ? ne0 - 2 : (x2 == ne0 - 1 ? 1 : x2);
-                        int ys = y2 == 0 ? ne1 - 2 : (y2 == ne1 - 1 ? 1 : y2);
-                        int zs = z2 == 0 ? ne2 - 2 : (z2 == ne2 - 1 ? 1 : z2);
-                        int cs2 = xs + ne0 * (ys + ne1 * zs);
-                        b_img = d.cell_start[s.cstart_off + cs2];
-                        n_img = d.cell_start[s.cstart_off + cs2 + 1] - b_img;
-                        code_img = (ssx + 1) | ((ssy + 1) << 2) | ((ssz + 1) << 4);
-                    }
-                }
-            }
-        }
-        int tot = n_real + n_img, incl = tot;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            int t = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += t;
-        }
-        const int excl = incl - tot;
-        const int total = __shfl_sync(0xffffffffu, incl, 31);
-        if (lane < 27) {
-            s_off[warp][2 * lane] = excl;
-            s_off[warp][2 * lane + 1] = excl + n_real;
-            s_start[warp][2 * lane] = b_real;
-            s_start[warp][2 * lane + 1] = b_img;
-            s_code[warp][2 * lane] = noshift;
-            s_code[warp][2 * lane + 1] = code_img;
-        }
-        if (lane == 0) s_off[warp][54] = total;
         __syncwarp();
-
-        for (int pass = 0; pass * 32 < ccount; pass++) {
-            const int mine = pass * 32 + lane;
-            const bool own = mine < ccount;
-            const int i = cstart + (own ? mine : 0);
-            const double4 pi = ldg_pos(P + i);
-            const float xif = (float)(pi.x - refx), yif = (float)(pi.y - refy), zif = (float)(pi.z - refz);
-            int cnt = 0;
-            int32_t *out = d.nbr + s.list_off + (int64_t)(i - s.mol_off) * s.maxn;
-            for (int base = 0; base < total; base += EB_STAGE) {
-                const int take = min(EB_STAGE, total - base);
-                __syncwarp();
-                for (int t = lane; t < take; t += 32) {
-                    const int q = base + t;
-                    int kk = 0;
-#pragma unroll
-                    for (int step = 32; step > 0; step >>= 1)
-                        if (kk + step < 54 && s_off[warp][kk + step] <= q) kk += step;
-                    const int j = s_start[warp][kk] + (q - s_off[warp][kk]);
-                    const int code = s_code[warp][kk];
-                    const double4 pj = ldg_pos(P + j);
-                    const double xj = image(pj.x, (code & 3) - 1, s.L[0]);
-                    const double yj = image(pj.y, ((code >> 2) & 3) - 1, s.L[1]);
-                    const double zj = image(pj.z, ((code >> 4) & 3) - 1, s.L[2]);
-                    // the entry stores the partner's offset inside the job
-                    s_f[warp][t] = make_float4((float)(xj - refx), (float)(yj - refy), (float)(zj - refz),
-                                               __int_as_float((j - s.mol_off) | (code << NB_SHIFT_BITS)));
-                }
-                __syncwarp();
-                for (int q = 0; q < take; q++) {
-                    const float4 f = s_f[warp][q];
-                    const float fx = xif - f.x, fy = yif - f.y, fz = zif - f.z;
-                    const float r2f = fx * fx + fy * fy + fz * fz;
-                    const int e = __float_as_int(f.w);
-                    const bool self = (e & NB_INDEX_MASK) == i - s.mol_off && (e >> NB_SHIFT_BITS) == noshift;
-                    bool hit = own && !self && r2f < lo32;
-                    const bool in_band = own && !self && r2f >= lo32 && r2f <= hi32;
-                    if (__any_sync(0xffffffffu, in_band)) {
-                        if (in_band) {
-                            const int code = e >> NB_SHIFT_BITS;
-                            const double4 pj = ldg_pos(P + s.mol_off + (e & NB_INDEX_MASK));
-                            const double dx = __dsub_rn(pi.x, image(pj.x, (code & 3) - 1, s.L[0]));
-                            const double dy = __dsub_rn(pi.y, image(pj.y, ((code >> 2) & 3) - 1, s.L[1]));
-                            const double dz = __dsub_rn(pi.z, image(pj.z, ((code >> 4) & 3) - 1, s.L[2]));
-                            hit = norm2_rn(dx, dy, dz) < s.rn2;
-                        }
-                    }
-                    if (hit) {
-                        if (cnt < s.maxn) out[cnt] = e;
-                        cnt++;
-                    }
-                }
-            }
-            if (own) {
-                d.nnbr[i] = cnt < s.maxn ? cnt : s.maxn;
-                atomicMax(&s.max_nbr, cnt);
-                if (cnt > s.maxn) slot_fail(&s, ST_NLIST, s.iter);
-            }
+        if (lane == 0) {
+            CellSys &y = ys[warp];
+            y.P = eng_pos(d, s.pset) + s.mol_off;
+            y.cell_start = d.cell_start + s.cstart_off;
+            y.mol_off = s.mol_off;
+            for (int q = 0; q < 3; q++) { y.ne[q] = s.ne[q]; y.cs[q] = s.cs[q]; y.hd[q] = s.hd[q]; y.L[q] = s.L[q]; }
+            y.rn2 = s.rn2;
+            y.nbr = d.nbr + s.list_off;
+            y.nnbr = d.nnbr + s.mol_off;
+            y.maxn = s.maxn;
+            y.max_nbr = &s.max_nbr;
+            y.chain = y.subchain = nullptr;
+            y.bflag = nullptr;
+            y.bnd = y.nbond = nullptr;
         }
         __syncwarp();
+        const uint32_t over = build_cell<false>(ys[warp], c - s.cell_off, sh[warp], lane);
+        if (lane == 0 && (over & BUILD_OVER_LIST)) slot_fail(&s, ST_NLIST, s.iter);
     }
 }
 
@@ -463,7 +361,7 @@ __device__ __forceinline__ void lj_pair(PairAcc &a, double dx, double dy, double
                                         bool rec, bool ptens)
 {
     if (PREC == 0) {
-        const double s = 1.0 / r2, s2 = s * s, s4 = s2 * s2;
+        const double s = __drcp_rn(r2), s2 = s * s, s4 = s2 * s2;  // == 1.0 / r2
         const double acc = 48.0 * (s4 * s2 * s - 0.5 * s4);
         a.fx += acc * dx; a.fy += acc * dy; a.fz += acc * dz;
         if (rec) {
@@ -476,18 +374,17 @@ __device__ __forceinline__ void lj_pair(PairAcc &a, double dx, double dy, double
             }
         }
     } else {
-        const float s = 1.0f / (float)r2, s2 = s * s, s4 = s2 * s2;
-        const float acc = 48.0f * (s4 * s2 * s - 0.5f * s4);
-        const float fdx = (float)dx, fdy = (float)dy, fdz = (float)dz;
-        a.fx += (double)(acc * fdx); a.fy += (double)(acc * fdy); a.fz += (double)(acc * fdz);
+        // FP32 pair magnitude; the FP64 rij scales it (one conversion)
+        const float s = __frcp_rn((float)r2), s2 = s * s, s4 = s2 * s2;
+        const double acc = (double)(48.0f * (s4 * s2 * s - 0.5f * s4));
+        a.fx = fma(acc, dx, a.fx); a.fy = fma(acc, dy, a.fy); a.fz = fma(acc, dz, a.fz);
         if (rec) {
             const float s3 = s2 * s;
             a.pe += (double)(4.0f * (s3 * s3 - s3)) - potshift;
-            a.vir += (double)(acc * (float)r2);
+            a.vir += acc * r2;
             if (ptens) {
-                a.rxx += (double)(acc * fdx * fdx); a.ryy += (double)(acc * fdy * fdy);
-                a.rzz += (double)(acc * fdz * fdz); a.rxy += (double)(acc * fdx * fdy);
-                a.rxz += (double)(acc * fdx * fdz); a.ryz += (double)(acc * fdy * fdz);
+                a.rxx += acc * dx * dx; a.ryy += acc * dy * dy; a.rzz += acc * dz * dz;
+                a.rxy += acc * dx * dy; a.rxz += acc * dx * dz; a.ryz += acc * dy * dz;
             }
         }
     }
@@ -595,10 +492,10 @@ __global__ void __launch_bounds__(EF_THREADS) k_e_force(EngDev d)
             const double4 *P = eng_pos(d, s.pset);
             const double4 pi = P[i];
             const int cnt = d.nnbr[i];
-            const int32_t *L = d.nbr + s.list_off + (int64_t)(i - s.mol_off) * s.maxn;
+            const int32_t *L = d.nbr + s.list_off + nb_row(i - s.mol_off, s.maxn);
             const double4 *Pj = P + s.mol_off;
             for (int k0 = lane * 4; k0 < cnt; k0 += 4 * TPM) {
-                const int4 e4 = __ldg(reinterpret_cast<const int4 *>(L + k0));
+                const int4 e4 = __ldg(reinterpret_cast<const int4 *>(L + (size_t)k0 * 32));
                 const int ev[4] = {e4.x, e4.y, e4.z, e4.w};
                 double4 pj[4];
 #pragma unroll
@@ -630,40 +527,44 @@ __global__ void __launch_bounds__(EF_THREADS) k_e_force(EngDev d)
     }
 }
 
-// All pairs with per-axis minimum image for jobs below 3 cells per axis.
+// All pairs with per-axis minimum image for jobs below 3 cells per axis
+// (simulation_compute_forces_LJ_AP, simulation_compute_forces.f90:280-341).
+// Blocks (slot, EAP_YBLOCKS of them), one warp per molecule: lane l takes
+// partners mol_off + l, + 32, ... and the lanes' sums are combined in a fixed
+// order.
+constexpr int EAP_THREADS = 256;
+constexpr int EAP_YBLOCKS = 16;
 template <int PREC>
-__global__ void k_e_force_ap(EngDev d)
+__global__ void __launch_bounds__(EAP_THREADS) k_e_force_ap(EngDev d)
 {
     if (!d.flags->any_ap) return;
-    const int hwm = d.flags->mol_hwm;
-    for (int base = blockIdx.x * blockDim.x; base < hwm; base += gridDim.x * blockDim.x) {
-        const int i = base + threadIdx.x;
-        int k = i < hwm ? d.slot_of[i] : -1;
-        const EngSlot *sp = k >= 0 ? &d.slots[k] : nullptr;
-        const bool act = k >= 0 && sp->mode == MODE_ALLPAIRS && slot_active(*sp);
-        if (!act) k = -1;
-        double m2 = 0.0;
-        if (act) {
-            const EngSlot &s = *sp;
-            const double4 *P = eng_pos(d, s.pset);
-            const double4 pi = P[i];
-            const bool rec = s.record, ptens = rec && s.pressure;
-            PairAcc a;
-            for (int j = s.mol_off; j < s.mol_off + s.nmol; j++) {
-                if (j == i) continue;
-                const double4 pj = ldg_pos(P + j);
-                double r[3] = {__dsub_rn(pi.x, pj.x), __dsub_rn(pi.y, pj.y), __dsub_rn(pi.z, pj.z)};
-                double r2 = 0.0;
+    const int k = blockIdx.x;
+    const EngSlot &s = d.slots[k];
+    if (s.mode != MODE_ALLPAIRS || !slot_active(s)) return;  // uniform per block
+    const int lane = threadIdx.x & 31;
+    const double4 *P = eng_pos(d, s.pset);
+    const bool rec = s.record, ptens = rec && s.pressure;
+    constexpr int WPB = EAP_THREADS / 32;
+    for (int i = s.mol_off + blockIdx.y * WPB + (threadIdx.x >> 5); i < s.mol_off + s.nmol;
+         i += EAP_YBLOCKS * WPB) {
+        const double4 pi = P[i];
+        PairAcc a;
+        for (int j = s.mol_off + lane; j < s.mol_off + s.nmol; j += 32) {
+            if (j == i) continue;
+            const double4 pj = ldg_pos(P + j);
+            double r[3] = {__dsub_rn(pi.x, pj.x), __dsub_rn(pi.y, pj.y), __dsub_rn(pi.z, pj.z)};
+            double r2 = 0.0;
 #pragma unroll
-                for (int q = 0; q < 3; q++) {
-                    if (fabs(r[q]) > s.hd[q]) r[q] = __dsub_rn(r[q], copysign(s.L[q], r[q]));
-                    r2 = __dadd_rn(r2, __dmul_rn(r[q], r[q]));
-                }
-                if (r2 < s.rc2) lj_pair<PREC>(a, r[0], r[1], r[2], r2, s.potshift, rec, ptens);
+            for (int q = 0; q < 3; q++) {
+                if (fabs(r[q]) > s.hd[q]) r[q] = __dsub_rn(r[q], copysign(s.L[q], r[q]));
+                r2 = __dadd_rn(r2, __dmul_rn(r[q], r[q]));
             }
-            m2 = epilogue(d, s, i, a);
+            if (r2 < s.rc2) lj_pair<PREC>(a, r[0], r[1], r[2], r2, s.potshift, rec, ptens);
         }
-        fold_vmax2(d.slots, k, m2);
+        reduce_lanes(a, 32, rec, ptens);
+        double m2 = 0.0;
+        if (lane == 0) m2 = epilogue(d, s, i, a);
+        fold_vmax2(d.slots, lane == 0 ? k : -1, m2);
     }
 }
 
@@ -913,10 +814,11 @@ void eng_tick(const EngDev &d, int tpm, cudaStream_t st)
     k_e_sort<<<gc, 256, 0, st>>>(d);
     k_e_reorder_gather<<<gm, 256, 0, st>>>(d);
     k_e_reorder_copy<<<gm, 256, 0, st>>>(d);
-    k_e_build<<<sgrid(d.cell_cap, EB_WARPS, 8), EB_WARPS * 32, 0, st>>>(d);
+    k_e_build<<<sgrid(d.cell_cap, NB_WARPS, 6), NB_THREADS, 0, st>>>(d);  // one resident wave
     launch_force_any(d, tpm, false, st);
-    if (d.precision == 0) k_e_force_ap<0><<<gm, 256, 0, st>>>(d);
-    else k_e_force_ap<1><<<gm, 256, 0, st>>>(d);
+    const dim3 gap(d.nslots, EAP_YBLOCKS);
+    if (d.precision == 0) k_e_force_ap<0><<<gap, EAP_THREADS, 0, st>>>(d);
+    else k_e_force_ap<1><<<gap, EAP_THREADS, 0, st>>>(d);
     k_e_thermo<<<d.nslots, ER, 0, st>>>(d);
     k_e_move_lfv<<<gm, 256, 0, st>>>(d);
     k_e_record<<<d.nslots, ER, 0, st>>>(d);

@@ -15,6 +15,7 @@
 
 #include "fm_common.cuh"
 #include "fm_device.cuh"
+#include "fm_build.cuh"
 
 namespace fm {
 
@@ -351,199 +352,32 @@ __global__ void k_reorder_copy(FmDev d, int gated, const double4 *tpos, const in
 //  1118-1180, stored in both directions)
 // ---------------------------------------------------------------------------
 
-constexpr int NB_WARPS = 4;                 // cells processed concurrently per block
-constexpr int NB_THREADS = 32 * NB_WARPS;
-constexpr int NB_STAGE = 256;               // staged candidates per warp
-
-
-// Neighbour list build, one warp per extended cell (grid-stride).
-//
-// The reference visits every pair of adjacent cells of which at least one is
-// interior exactly once (13 forward shifts from interior cells + 27 sweeps
-// from halo cells); a halo cell holds the images of the interior cell on the
-// far side (plus any real molecule that binned onto it).  Here each molecule
-// of cell c collects, from the 27 cells around c that are not both halo with
-// c, every candidate with r^2 < rneighbr^2 -- the same set, stored for both
-// partners.
-//
-// Lane q < 27 computes the segments of neighbour cell q (its real members and,
-// for a halo cell, the shifted images of its source); a warp prefix sum lays
-// the candidates out in the reference's visiting order (cell q ascending,
-// real before images, slot ascending).  Candidates are staged in shared
-// memory as FP32 offsets from the cell's reference point, computed from the
-// FP64 image coordinate (x_src +/- L, one rounding, as the halo copy).  Each
-// lane owns one molecule of the cell and walks the staged candidates: the FP32
-// r^2 (error below 1e-5 cs^2 for molecules binned in this build, offsets
-// within 1.5 cells) decides every candidate farther than BAND = 1e-4 cs^2
-// from rneighbr2; a candidate inside the band is re-read in FP64 and decided
-// by the exact test (dx^2+dy^2)+dz^2 < rneighbr2 -- a branch the whole warp
-// skips unless some lane needs it.
-//
-// With FENE polymers (POLY) the same scan discovers bonds the way the
-// reference's check_update_adjacentbeadinfo does (linklist.f90:2542-2584): any
-// candidate of the scanned cells -- at any distance -- with the owner's chain
-// whose subchain bit is set in the owner's bin_bflag words (get_bondflag,
-// modules.f90:602-610, 31 bits per word) is a bond partner.
+// Neighbour rows of every extended cell, one warp per cell (grid-stride);
+// the per-cell routine and its pair-set argument are in fm_build.cuh.
 template <bool POLY>
-__global__ void __launch_bounds__(NB_THREADS) k_build_nlist(FmDev d, int gated, int iter)
+__global__ void __launch_bounds__(NB_THREADS, 8) k_build_nlist(FmDev d, int gated, int iter)
 {
     if (!gate(d, gated)) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int ne0 = d.ne[0], ne1 = d.ne[1], ne2 = d.ne[2];
-    const double4 *P = cur_pos(d, d.sc->pset);
-    const double Lx = d.L[0], Ly = d.L[1], Lz = d.L[2];
-    const double rn2 = d.rn2;
-    const int maxn = d.maxn;
-    const int noshift = 1 | (1 << 2) | (1 << 4);
-    const double csmax = fmax(d.cs[0], fmax(d.cs[1], d.cs[2]));
-    const float band = (float)(1e-4 * csmax * csmax) + 1e-6f;
-    const float lo32 = (float)rn2 - band, hi32 = (float)rn2 + band;
-
-    __shared__ float4 s_f[NB_WARPS][NB_STAGE];   // x, y, z offsets and the entry bits in w
-    __shared__ int2 s_cs[POLY ? NB_WARPS : 1][POLY ? NB_STAGE : 1];  // chain, subchain of candidates
-    __shared__ int s_off[NB_WARPS][55];          // candidate offset of segment k (54 segments + total)
-    __shared__ int s_start[NB_WARPS][54], s_code[NB_WARPS][54];
-
-    const int stride = gridDim.x * NB_WARPS;
-    for (int c = blockIdx.x * NB_WARPS + warp; c < d.ncell; c += stride) {
-        const int cstart = d.cell_start[c];
-        const int ccount = d.cell_start[c + 1] - cstart;
-        if (ccount == 0) continue;  // uniform across the warp
-        const int cx = c % ne0, cy = (c / ne0) % ne1, cz = c / (ne0 * ne1);
-        const bool chalo = is_halo(cx, ne0) || is_halo(cy, ne1) || is_halo(cz, ne2);
-        const double refx = (cx - 0.5) * d.cs[0] - d.hd[0];
-        const double refy = (cy - 0.5) * d.cs[1] - d.hd[1];
-        const double refz = (cz - 0.5) * d.cs[2] - d.hd[2];
-
-        // --- segments of neighbour cell q = lane ---
-        int n_real = 0, b_real = 0, n_img = 0, b_img = 0, code_img = noshift;
-        if (lane < 27) {
-            int x2 = cx + lane % 3 - 1, y2 = cy + (lane / 3) % 3 - 1, z2 = cz + lane / 9 - 1;
-            if (x2 >= 0 && y2 >= 0 && z2 >= 0 && x2 < ne0 && y2 < ne1 && z2 < ne2) {
-                bool h2 = is_halo(x2, ne0) || is_halo(y2, ne1) || is_halo(z2, ne2);
-                if (!(chalo && h2)) {
-                    int c2 = x2 + ne0 * (y2 + ne1 * z2);
-                    b_real = d.cell_start[c2];
-                    n_real = d.cell_start[c2 + 1] - b_real;
-                    if (h2) {
-                        // images in a halo cell come from the interior cell on the far
-                        // side: low halo <- last interior cell shifted by -domain, high
-                        // halo <- first interior cell shifted by +domain
-                        int ssx = x2 == 0 ? -1 : (x2 == ne0 - 1 ? 1 : 0);
-                        int ssy = y2 == 0 ? -1 : (y2 == ne1 - 1 ? 1 : 0);
-                        int ssz = z2 == 0 ? -1 : (z2 == ne2 - 1 ? 1 : 0);
-                        int xs = x2 == 0 ? ne0 - 2 : (x2 == ne0 - 1 ? 1 : x2);
-                        int ys = y2 == 0 ? ne1 - 2 : (y2 == ne1 - 1 ? 1 : y2);
-                        int zs = z2 == 0 ? ne2 - 2 : (z2 == ne2 - 1 ? 1 : z2);
-                        int cs2 = xs + ne0 * (ys + ne1 * zs);
-                        b_img = d.cell_start[cs2];
-                        n_img = d.cell_start[cs2 + 1] - b_img;
-                        code_img = (ssx + 1) | ((ssy + 1) << 2) | ((ssz + 1) << 4);
-                    }
-                }
-            }
-        }
-        int tot = n_real + n_img, incl = tot;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            int t = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += t;
-        }
-        const int excl = incl - tot;
-        const int total = __shfl_sync(0xffffffffu, incl, 31);
-        if (lane < 27) {
-            s_off[warp][2 * lane] = excl;
-            s_off[warp][2 * lane + 1] = excl + n_real;
-            s_start[warp][2 * lane] = b_real;
-            s_start[warp][2 * lane + 1] = b_img;
-            s_code[warp][2 * lane] = noshift;
-            s_code[warp][2 * lane + 1] = code_img;
-        }
-        if (lane == 0) s_off[warp][54] = total;
-        __syncwarp();
-
-        for (int pass = 0; pass * 32 < ccount; pass++) {
-            const int mine = pass * 32 + lane;
-            const bool own = mine < ccount;
-            const int i = cstart + (own ? mine : 0);
-            const double4 pi = ldg_pos(P + i);
-            const float xif = (float)(pi.x - refx), yif = (float)(pi.y - refy), zif = (float)(pi.z - refz);
-            int cnt = 0;
-            int32_t *out = d.nbr + (size_t)i * maxn;
-            int chain_i = 0, nb = 0;
-            int4 bf = make_int4(0, 0, 0, 0);
-            if (POLY && own) { chain_i = d.chain[i]; bf = d.bflag[i]; }
-            for (int base = 0; base < total; base += NB_STAGE) {
-                const int take = min(NB_STAGE, total - base);
-                __syncwarp();
-                for (int t = lane; t < take; t += 32) {
-                    const int q = base + t;
-                    int k = 0;  // segment containing q: largest k with s_off[k] <= q
-#pragma unroll
-                    for (int step = 32; step > 0; step >>= 1)
-                        if (k + step < 54 && s_off[warp][k + step] <= q) k += step;
-                    const int j = s_start[warp][k] + (q - s_off[warp][k]);
-                    const int code = s_code[warp][k];
-                    const int sxs = (code & 3) - 1, sys = ((code >> 2) & 3) - 1, szs = ((code >> 4) & 3) - 1;
-                    const double4 pj = ldg_pos(P + j);
-                    const double xj = sxs ? __dadd_rn(pj.x, sxs > 0 ? Lx : -Lx) : pj.x;
-                    const double yj = sys ? __dadd_rn(pj.y, sys > 0 ? Ly : -Ly) : pj.y;
-                    const double zj = szs ? __dadd_rn(pj.z, szs > 0 ? Lz : -Lz) : pj.z;
-                    s_f[warp][t] = make_float4((float)(xj - refx), (float)(yj - refy), (float)(zj - refz),
-                                               __int_as_float(j | (code << NB_SHIFT_BITS)));
-                    if (POLY) s_cs[warp][t] = make_int2(d.chain[j], d.subchain[j]);
-                }
-                __syncwarp();
-                for (int q = 0; q < take; q++) {
-                    const float4 f = s_f[warp][q];  // broadcast
-                    const float fx = xif - f.x, fy = yif - f.y, fz = zif - f.z;
-                    const float r2f = fx * fx + fy * fy + fz * fz;
-                    const int e = __float_as_int(f.w);
-                    const bool self = (e & NB_INDEX_MASK) == i && (e >> NB_SHIFT_BITS) == noshift;
-                    if (POLY && own && !self) {
-                        const int2 cs = s_cs[warp][q];
-                        if (cs.x == chain_i) {
-                            const int pos = cs.y - 1, grp = pos / 31, ex = pos % 31;
-                            const int word = grp == 0 ? bf.x : grp == 1 ? bf.y : grp == 2 ? bf.z : bf.w;
-                            if (pos >= 0 && grp < 4 && ((word >> ex) & 1)) {
-                                if (nb < 4) d.bnd[(size_t)i * 4 + nb] = e;
-                                nb++;
-                            }
-                        }
-                    }
-                    bool hit = own && !self && r2f < lo32;
-                    const bool in_band = own && !self && r2f >= lo32 && r2f <= hi32;
-                    if (__any_sync(0xffffffffu, in_band)) {
-                        if (in_band) {
-                            const int code = e >> NB_SHIFT_BITS;
-                            const int sxs = (code & 3) - 1, sys = ((code >> 2) & 3) - 1, szs = ((code >> 4) & 3) - 1;
-                            const double4 pj = ldg_pos(P + (e & NB_INDEX_MASK));
-                            const double xj = sxs ? __dadd_rn(pj.x, sxs > 0 ? Lx : -Lx) : pj.x;
-                            const double yj = sys ? __dadd_rn(pj.y, sys > 0 ? Ly : -Ly) : pj.y;
-                            const double zj = szs ? __dadd_rn(pj.z, szs > 0 ? Lz : -Lz) : pj.z;
-                            const double dx = __dsub_rn(pi.x, xj);
-                            const double dy = __dsub_rn(pi.y, yj);
-                            const double dz = __dsub_rn(pi.z, zj);
-                            hit = norm2_rn(dx, dy, dz) < rn2;
-                        }
-                    }
-                    if (hit) {
-                        if (cnt < maxn) out[cnt] = e;
-                        cnt++;
-                    }
-                }
-            }
-            if (own) {
-                d.nnbr[i] = cnt < maxn ? cnt : maxn;
-                atomicMax(&d.sc->max_nbr, cnt);
-                if (cnt > maxn) raise_status(d, ST_NLIST, iter);
-                if (POLY) {
-                    d.nbond[i] = nb < 4 ? nb : 4;
-                    if (nb > 4) raise_status(d, ST_BOND, iter);  // too_many_bonds_error
-                }
-            }
-        }
-        __syncwarp();
+    __shared__ BuildShared<POLY> sh[NB_WARPS];
+    CellSys y;
+    y.P = cur_pos(d, d.sc->pset);
+    y.cell_start = d.cell_start;
+    y.mol_off = 0;
+    for (int k = 0; k < 3; k++) { y.ne[k] = d.ne[k]; y.cs[k] = d.cs[k]; y.hd[k] = d.hd[k]; y.L[k] = d.L[k]; }
+    y.rn2 = d.rn2;
+    y.nbr = d.nbr;
+    y.nnbr = d.nnbr;
+    y.maxn = d.maxn;
+    y.max_nbr = &d.sc->max_nbr;
+    y.chain = d.chain; y.subchain = d.subchain; y.bflag = d.bflag;
+    y.bnd = d.bnd; y.nbond = d.nbond;
+    uint32_t over = 0u;
+    for (int c = blockIdx.x * NB_WARPS + warp; c < d.ncell; c += gridDim.x * NB_WARPS)
+        over |= build_cell<POLY>(y, c, sh[warp], lane);
+    if (lane == 0) {
+        if (over & BUILD_OVER_LIST) raise_status(d, ST_NLIST, iter);
+        if (over & BUILD_OVER_BONDS) raise_status(d, ST_BOND, iter);
     }
 }
 
@@ -687,13 +521,13 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force(FmDev d)
     if (active) {
         const double4 pi = P[i];
         const int cnt = d.nnbr[i];
-        const int32_t *__restrict__ L = d.nbr + (size_t)i * d.maxn;  // 16-byte aligned rows (maxn % 8 == 0)
+        const int32_t *__restrict__ L = d.nbr + nb_row(i, d.maxn);  // chunk k0/4 at L + 32 k0 (16-byte aligned)
         const double Lx = d.L[0], Ly = d.L[1], Lz = d.L[2];
         const double rc2 = d.rc2;
         // each lane takes 4 consecutive entries per iteration (one 16-byte load)
         // and issues their 4 gathers before any arithmetic
         for (int k0 = lane * 4; k0 < cnt; k0 += 4 * TPM) {
-            const int4 e4 = __ldg(reinterpret_cast<const int4 *>(L + k0));
+            const int4 e4 = __ldg(reinterpret_cast<const int4 *>(L + (size_t)k0 * 32));
             const int ev[4] = {e4.x, e4.y, e4.z, e4.w};
             double4 pj[4];
 #pragma unroll
@@ -714,7 +548,7 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force(FmDev d)
                 if (r2 < rc2) {
                     if (PREC == 0) {
                         // LJ_accijmag = 48 (s^7 - s^4/2), s = 1/r^2 (setup_set_parameters.f90:105-113)
-                        const double s = 1.0 / r2;
+                        const double s = __drcp_rn(r2);  // == 1.0 / r2 (both correctly rounded)
                         const double s2 = s * s, s4 = s2 * s2;
                         const double acc = 48.0 * (s4 * s2 * s - 0.5 * s4);
                         fx += acc * dx; fy += acc * dy; fz += acc * dz;
@@ -724,16 +558,17 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force(FmDev d)
                             vir += acc * r2;
                         }
                     } else {
-                        const float s = 1.0f / (float)r2;
+                        // FP32 pair magnitude; the FP64 rij scales it (one conversion)
+                        const float s = __frcp_rn((float)r2);
                         const float s2 = s * s, s4 = s2 * s2;
-                        const float acc = 48.0f * (s4 * s2 * s - 0.5f * s4);
-                        fx += (double)(acc * (float)dx);
-                        fy += (double)(acc * (float)dy);
-                        fz += (double)(acc * (float)dz);
+                        const double acc = (double)(48.0f * (s4 * s2 * s - 0.5f * s4));
+                        fx = fma(acc, dx, fx);
+                        fy = fma(acc, dy, fy);
+                        fz = fma(acc, dz, fz);
                         if (REC) {
                             const float s3 = s2 * s, s6 = s3 * s3;
                             pe += (double)(4.0f * (s6 - s3)) - d.potshift;
-                            vir += (double)(acc * (float)r2);
+                            vir += acc * r2;
                         }
                     }
                 }
@@ -890,7 +725,7 @@ __global__ void __launch_bounds__(AP_THREADS) k_all_pairs(FmDev d)
                 }
                 if (r2 < d.rc2) {
                     if (PREC == 0) {
-                        const double s = 1.0 / r2;
+                        const double s = __drcp_rn(r2);  // == 1.0 / r2 (both correctly rounded)
                         const double s2 = s * s, s4 = s2 * s2;
                         const double acc = 48.0 * (s4 * s2 * s - 0.5 * s4);
                         fx += acc * r[0]; fy += acc * r[1]; fz += acc * r[2];
@@ -958,9 +793,9 @@ __global__ void k_pair_digest(FmDev d, const int32_t *glob_of_upload)
     long long cnt = 0;
     if (i < d.n) {
         int gi = glob_of_upload[d.slot_of[i]];
-        const int32_t *L = d.nbr + (size_t)i * d.maxn;
+        const int32_t *L = d.nbr + nb_row(i, d.maxn);
         for (int k = 0; k < d.nnbr[i]; k++) {
-            int e = L[k];
+            int e = L[nb_col(k)];
             int j = e & NB_INDEX_MASK;
             int code6 = e >> NB_SHIFT_BITS;
             int sx = (code6 & 3) - 1, sy = ((code6 >> 2) & 3) - 1, sz = ((code6 >> 4) & 3) - 1;
@@ -1056,10 +891,26 @@ void launch_reorder(const FmDev &d, int gated, double4 *tpos, int32_t *tuidx, cu
     k_reorder_gather<<<sgrid(d.n, 256, 8), 256, 0, st>>>(d, gated, tpos, tuidx);
     k_reorder_copy<<<sgrid(d.n, 256, 8), 256, 0, st>>>(d, gated, tpos, tuidx);
 }
+// The list build walks the cells grid-stride with every block resident (one
+// wave: a second partial wave would double the kernel's time).
+template <bool POLY>
+static int build_grid(int ncell)
+{
+    static int resident = 0;
+    if (resident == 0) {
+        int dev = 0, nsm = kSMs, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_build_nlist<POLY>, NB_THREADS, 0);
+        resident = std::max(nsm, 1) * std::max(per_sm, 1);
+    }
+    return std::min(nblk(ncell, NB_WARPS), resident);
+}
+
 void launch_build_nlist(const FmDev &d, int gated, int iter, cudaStream_t st)
 {
-    if (d.potential_flag == 1) k_build_nlist<true><<<sgrid(d.ncell, NB_WARPS, 8), NB_THREADS, 0, st>>>(d, gated, iter);
-    else k_build_nlist<false><<<sgrid(d.ncell, NB_WARPS, 8), NB_THREADS, 0, st>>>(d, gated, iter);
+    if (d.potential_flag == 1) k_build_nlist<true><<<build_grid<true>(d.ncell), NB_THREADS, 0, st>>>(d, gated, iter);
+    else k_build_nlist<false><<<build_grid<false>(d.ncell), NB_THREADS, 0, st>>>(d, gated, iter);
 }
 
 int force_blocks(int n, int tpm) { return nblk(n * tpm, FORCE_THREADS); }
