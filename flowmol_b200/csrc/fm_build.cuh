@@ -26,8 +26,8 @@
 // distance 0 (the owner itself), is re-read in FP64 and decided by the exact
 // test (dx^2+dy^2)+dz^2 < rneighbr2 -- a branch the whole warp skips unless
 // some lane needs it.  An owner's hits among 32 candidates are one ballot,
-// appended to its row in candidate order, so every row lists its partners in
-// the visiting order.
+// kept by the owner's lane, which appends them to its row in candidate order,
+// so every row lists its partners in the visiting order.
 //
 // With FENE polymers (POLY) the same scan discovers bonds the way the
 // reference's check_update_adjacentbeadinfo does (linklist.f90:2542-2584): any
@@ -181,6 +181,7 @@ __device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY> &sh, i
         const float by0 = warp_min(yif), by1 = warp_max(yif);
         const float bz0 = warp_min(zif), bz1 = warp_max(zif);
         int cnt = 0, nb = 0;  // the owner lane's list and bond counts
+        int32_t *const row = y.nbr + nb_row(i, maxn);
         const int nown = min(32, ccount - pass * 32);
         __syncwarp();
         sh.own[lane] = make_float4(xif, yif, zif, __int_as_float(i));
@@ -237,6 +238,7 @@ __device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY> &sh, i
                 const int e = __float_as_int(f.w);
                 int2 cs = make_int2(-2, 0);
                 if (POLY && valid) cs = sh.cs[cq];
+                unsigned mine_hits = 0u;  // this lane's owner: which of the 32 candidates hit
                 // owners in groups of NB_OG: independent chains for the scheduler
                 for (int o0 = 0; o0 < nown; o0 += NB_OG) {
                     bool hit[NB_OG], exact[NB_OG];
@@ -260,18 +262,11 @@ __device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY> &sh, i
                         for (int u = 0; u < NB_OG; u++)
                             if (exact[u]) hit[u] = exact_pair(P, io[u], e, y.L, y.rn2);
                     }
-                    int add = 0;
 #pragma unroll
                     for (int u = 0; u < NB_OG; u++) {
                         const unsigned m = __ballot_sync(0xffffffffu, hit[u]);
-                        const int c0 = __shfl_sync(0xffffffffu, cnt, o0 + u);
-                        if (hit[u]) {
-                            const int k = c0 + __popc(m & lt);
-                            if (k < maxn) y.nbr[nb_row(io[u], maxn) + nb_col(k)] = e;
-                        }
-                        if (lane == o0 + u) add = __popc(m);
+                        if (lane == o0 + u) mine_hits = m;
                     }
-                    cnt += add;
                     if (POLY) {
                         int addb = 0;
 #pragma unroll
@@ -294,6 +289,13 @@ __device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY> &sh, i
                         }
                         nb += addb;
                     }
+                }
+                // the owner lane appends its hits in candidate order
+                while (mine_hits) {
+                    const int b = __ffs(mine_hits) - 1;
+                    mine_hits &= mine_hits - 1u;
+                    if (cnt < maxn) row[nb_col(cnt)] = __float_as_int(sh.f[t0 + b].w);
+                    cnt++;
                 }
             }
         }
