@@ -226,6 +226,66 @@ def run_e2e(api, torch, r, v, dom, precision, steps, dev):
             "d2h_bytes_per_step": d2h / steps, "steps": steps, "seconds": t1 - t0}
 
 
+def run_drift(api, r, v, dom, precision, nsteps=10000, tplot=1000):
+    """NVE energy drift of the 1M fluid over nsteps (records every tplot):
+    relative change of the total energy per molecule from the first record."""
+    p = api.make_params(len(r), dom, RC, (SKIN,) * 3, DT, tplot, density=DENSITY, precision=precision)
+    s = api.MDSystem(p)
+    s.upload(r, v)
+    s.setup()
+    s.simulation_md(nsteps, blocking=True)
+    recs = s.records()
+    s.close()
+    e = np.array([x["totenergy"] for x in recs])
+    return {"steps": nsteps, "records": len(e), "totenergy_first": float(e[0]), "totenergy_last": float(e[-1]),
+            "rel_drift_end": float((e[-1] - e[0]) / abs(e[0])),
+            "rel_drift_max": float(np.abs(e - e[0]).max() / abs(e[0]))}
+
+
+FENE_CHAINS, FENE_BEADS, FENE_DENSITY, FENE_K, FENE_R0 = 32768, 8, 0.85, 30.0, 1.5
+
+
+def run_fene(api, torch, dev, steps, warmup):
+    """The FENE bead-spring melt: 32768 chains of 8 beads (262,144 beads) at
+    density 0.85, WCA + FENE (k 30, R0 1.5, rneighbr = R0), FP32 pair forces
+    with FP64 bonds and integration, timed with CUDA events on the handle's
+    stream; energy drift from the records of the timed steps."""
+    from flowmol_b200 import polymer
+    r, v, ch, sub, _fy, bf, dom = polymer.fene_melt(FENE_CHAINS, FENE_BEADS, FENE_DENSITY)
+    stream = torch.cuda.Stream(device=dev)
+    wca = 2.0 ** (1.0 / 6.0)
+    p = api.make_params(len(r), dom, wca, (SKIN,) * 3, DT, TPLOT, density=FENE_DENSITY,
+                        precision=api.PRECISION_FP32, potential_flag=1, k_c=FENE_K, R_0=FENE_R0)
+    s = api.MDSystem(p, stream=stream)
+    s.upload(r, v)
+    s.upload_monomers(ch, sub, bf)
+    s.setup()
+    nbonds = len(s.bonds()[0])
+    s.simulation_md(warmup, blocking=True)
+    s.records()
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    s.simulation_md(steps, blocking=False)
+    e1.record(stream)
+    e1.synchronize()
+    s.sync()
+    ms = e0.elapsed_time(e1)
+    recs = s.records()
+    rebuilds = s.counters()["rebuilds"]
+    s.close()
+    e = np.array([x["totenergy"] for x in recs])
+    return {"value": len(r) * steps / (ms * 1e-3), "unit": UNIT, "beads": len(r), "steps": steps,
+            "ms_per_step": ms / steps, "bond_entries": nbonds, "rebuilds": rebuilds,
+            "rel_drift_end": float((e[-1] - e[0]) / abs(e[0])) if len(e) > 1 else None,
+            "drift_note": "total energy as the reference reports it: its FENE_energy has the opposite sign "
+                          "of the potential its FENE force derives from, so this sum is not conserved",
+            "workload": f"FENE melt: {FENE_CHAINS} chains x {FENE_BEADS} beads, rho {FENE_DENSITY}, WCA + FENE "
+                        f"k {FENE_K} R0 {FENE_R0} (rneighbr = R0), dt {DT}, VV, FP32 pair forces, FP64 bonds; "
+                        "start: self-avoiding walks on FCC sites"}
+
+
 def batch_replicas(nrep=256, seed=0x466D6F6C + 4):
     """The batched-ensemble configuration: replica sizes log-uniform in
     500-32000 molecules (rounded to 4 n^3 FCC), densities U(0.3, 0.9),
@@ -288,8 +348,10 @@ def run_batched(api, torch, dev, nsteps, nrep=256):
 def run_served(api, torch, dev, njobs, seed=0x466D6F6C + 5):
     """Poisson-arriving Couette jobs through the engine's admission loop.
     Job sizes log-uniform in 256-65536 molecules, 200-2000 steps, wall speed
-    U(0.5, 2.0); the arrival rate is set from a measured service rate so the
-    GPU stays busy.  Latency = finish time - scheduled arrival time."""
+    U(0.5, 2.0); the arrival rate is 0.8 x the service rate measured with 48
+    jobs resident at once, which keeps the GPU busy (served jobs overlap less
+    than the probe's, so they are served more slowly) without an unbounded
+    queue.  Latency = finish time - scheduled arrival time."""
     from flowmol_b200 import couette
     rng = np.random.Generator(np.random.Philox(seed))
 
@@ -326,7 +388,7 @@ def run_served(api, torch, dev, njobs, seed=0x466D6F6C + 5):
     e = new_engine()
     arrivals = np.cumsum(rng.exponential(1.0, njobs))
     mean_work = work / njobs
-    lam = 0.9 * rate_work / mean_work
+    lam = 0.8 * rate_work / mean_work
     t_arr = arrivals / lam
     t0 = time.monotonic()
     nxt = 0
@@ -408,7 +470,10 @@ def main():
     ap.add_argument("--batch-replicas", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=2000)
     ap.add_argument("--serve-jobs", type=int, default=4096)
-    ap.add_argument("--no-forms", action="store_true", help="skip the batched and served forms")
+    ap.add_argument("--no-forms", action="store_true", help="skip the FENE, batched and served forms")
+    ap.add_argument("--fene-steps", type=int, default=5000)
+    ap.add_argument("--drift-steps", type=int, default=10000,
+                    help="NVE drift run of the 1M fluid per precision form (0: skip)")
     ap.add_argument("--tpm", type=int, default=0,
                     help="force-kernel lanes per molecule (0: the autotuner's choice)")
     ap.add_argument("--profile-case", choices=["fp32", "fp64", "batched"], default=None,
@@ -489,8 +554,16 @@ def main():
     if e2e is not None:
         e2e["value"] = world * n * args.steps / max_over_ranks(e2e["seconds"])
     barrier()
-    batched = served = None
+    drift = None
+    if args.drift_steps > 0:
+        drift = {"fp32_forces": run_drift(api, r, v, dom, api.PRECISION_FP32, args.drift_steps),
+                 "fp64_plain": run_drift(api, r, v, dom, api.PRECISION_FP64, args.drift_steps)}
+    barrier()
+    batched = served = fene = None
     if not args.no_forms:
+        fene = run_fene(api, torch, dev, args.fene_steps, args.warmup)
+        fene["value"] = world * fene["value"] * fene["ms_per_step"] / max_over_ranks(fene["ms_per_step"])
+        barrier()
         batched = run_batched(api, torch, dev, args.batch_steps, args.batch_replicas)
         batched["value"] = world * batched["value"] * batched["seconds"] / max_over_ranks(batched["seconds"])
         barrier()
@@ -528,6 +601,8 @@ def main():
                          "traffic": traffic},
             "clocks": f32["clocks"],
             "gpu_launches": f32["launches"],
+            "nve_drift": drift,
+            "fene": fene,
             "batched": batched,
             "served": served,
             "e2e": e2e,

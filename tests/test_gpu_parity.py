@@ -320,3 +320,34 @@ def test_fene_melt_bonds_forces_trajectory(gpu_lib):
         assert row["potenergy"] == pytest.approx(ro[5], rel=1e-9)
     rg, _, _, _ = s.download()
     assert np.abs(wrap_diff(rg, o.r, dom)).max() < 1e-7
+
+
+def test_cfg1_nve_energy_drift_1e4_steps(gpu_lib):
+    """NVE drift over 10^4 steps on the plain configuration (2048 molecules,
+    WCA, dt 0.005): the FP64 and FP32 forms and the FP64 oracle all conserve
+    the total energy per molecule to well below 1e-3 relative, and the GPU
+    forms' records agree with the oracle's (same iterations; total energy to
+    1e-3: the trajectories separate by chaos within a few thousand steps and
+    the energy then fluctuates around the same value with a different phase)."""
+    r, v, dom = cfg1_state()
+    nsteps, tplot = 10000, 1000
+    o = O.Oracle(r, v, dom, WCA_RC, tplot=tplot)
+    o.setup()
+    recs_o = o.run_vv(nsteps)
+    e_o = recs_o[:, 6]
+    drifts = {"oracle": (e_o[-1] - e_o[0]) / abs(e_o[0])}
+    assert np.abs(e_o - e_o[0]).max() / abs(e_o[0]) < 1e-3
+    for prec, name in ((api.PRECISION_FP64, "fp64"), (api.PRECISION_FP32, "fp32")):
+        s = gpu_system(r, v, dom, WCA_RC, precision=prec, tplot=tplot)
+        s.setup()
+        s.records()  # the setup record (iteration 0)
+        s.simulation_md(nsteps)
+        recs = s.records()
+        s.close()
+        assert [x["iter"] for x in recs] == [int(x) for x in recs_o[:, 0]]
+        e = np.array([x["totenergy"] for x in recs])
+        drifts[name] = (e[-1] - e[0]) / abs(e[0])
+        assert np.abs(e - e[0]).max() / abs(e[0]) < 1e-3, (name, e)
+        np.testing.assert_allclose(e, e_o, rtol=1e-3)
+    print("\ncfg1 NVE relative drift over %d steps: " % nsteps +
+          ", ".join("%s %.3e" % (k, x) for k, x in drifts.items()))
