@@ -511,7 +511,8 @@ def main():
         reps = batch_replicas(args.batch_replicas)
         tot = sum(len(x[0]) for x in reps)
         e = api.Engine(max_molecules=tot + 1024, max_cells=2_000_000, max_list_entries=(tot + 1024) * 160,
-                       max_slots=len(reps), precision=api.PRECISION_FP32, ticks_per_chunk=50, keep_states=False)
+                       max_slots=len(reps), precision=api.PRECISION_FP32, ticks_per_chunk=50, keep_states=False,
+                       threads_per_molecule=args.tpm)
         for r, v, dom, rho, fl in reps:
             e.submit(api.make_job(len(r), dom, RC, args.batch_steps, density=rho, tplot=TPLOT, force_list=fl), r, v)
         e.run()

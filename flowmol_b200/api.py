@@ -74,6 +74,15 @@ class FmEngineParams(C.Structure):
     ]
 
 
+class FmMieTables(C.Structure):
+    _fields_ = [("ntypes", C.c_int32), ("pad_", C.c_int32)] + [
+        (k, C.POINTER(C.c_double)) for k in ("mass", "epsilon", "lambdar", "lambdaa", "C", "alpha", "potshift",
+                                             "k_harmonic", "r0")]
+
+
+MIE_TABLE_KEYS = ("epsilon", "lambdar", "lambdaa", "C", "alpha", "potshift", "k_harmonic", "r0")
+
+
 class FmJob(C.Structure):
     _fields_ = [
         ("np", C.c_int32), ("tplot", C.c_int32), ("domain", C.c_double * 3), ("density", C.c_double),
@@ -177,6 +186,7 @@ def lib():
             "fm_move_vv": [h, C.c_int32],
             "fm_move_lfv": [h],
             "fm_upload_monomers": [h, P(C.c_int32), P(C.c_int32), P(C.c_int32)],
+            "fm_set_mie": [h, P(FmMieTables), P(C.c_int32)],
             "fm_get_bonds": [h, P(C.c_int32), P(C.c_int32), P(C.c_int8), C.c_int64, P(C.c_int64)],
             "fm_update_borders": [h, C.c_int32],
             "fm_check_rebuild": [h, P(C.c_int32)],
@@ -343,6 +353,23 @@ class MDSystem:
         b = np.ascontiguousarray(bflag, np.int32).reshape(-1, 4)
         P = C.POINTER(C.c_int32)
         check(lib().fm_upload_monomers(self.h, c.ctypes.data_as(P), sc.ctypes.data_as(P), b.ctypes.data_as(P)))
+
+    def set_mie(self, tables, moltype):
+        """Mie_potential 1 (fm_set_mie): `tables` maps mass (ntypes) and
+        epsilon, lambdar, lambdaa, C, alpha, potshift, k_harmonic, r0
+        (ntypes x ntypes, indexed [i-1, j-1]) -- the reference's lookup
+        arrays; moltype is 1-based in upload order."""
+        nt = len(tables["mass"])
+        self._mie_keep = [np.ascontiguousarray(tables["mass"], np.float64)]
+        t = FmMieTables()
+        t.ntypes = nt
+        t.mass = self._mie_keep[0].ctypes.data_as(C.POINTER(C.c_double))
+        for k in MIE_TABLE_KEYS:
+            a = np.ascontiguousarray(np.asarray(tables[k], np.float64).T).reshape(-1)  # (i,j) at i + nt*j
+            self._mie_keep.append(a)
+            setattr(t, k, a.ctypes.data_as(C.POINTER(C.c_double)))
+        mt = np.ascontiguousarray(moltype, np.int32)
+        check(lib().fm_set_mie(self.h, C.byref(t), mt.ctypes.data_as(C.POINTER(C.c_int32))))
 
     def bonds(self):
         n = C.c_int64()

@@ -152,7 +152,8 @@ static void release(fm_handle *h)
     void *ptrs[] = {d.pos0, d.pos1, d.vx, d.vy, d.vz, d.ax, d.ay, d.az, d.slot_of, d.tvx, d.tvy, d.tvz,
                     d.tax, d.tay, d.taz, d.cell_of, d.cell_count, d.cell_start, d.perm, d.tile_sum, d.nbr, d.nnbr,
                     d.pe, d.vir, d.partial, d.rec, d.sc, h->tpos, h->tuidx, h->glob, h->stage3, d.chain,
-                    d.subchain, d.bflag, d.tchain, d.tsubchain, d.tbflag, d.bnd, d.nbond};
+                    d.subchain, d.bflag, d.tchain, d.tsubchain, d.tbflag, d.bnd, d.nbond,
+                    (void *)d.mie_pair, (void *)d.mie_mass, (void *)d.mie_type_up};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     d = FmDev{};
@@ -400,6 +401,66 @@ extern "C" int fm_upload_monomers(fm_handle *h, const int32_t *chainID, const in
 }
 
 static int ready(fm_handle *h, int min_stage);
+
+extern "C" int fm_set_mie(fm_handle *h, const fm_mie_tables *t, const int32_t *moltype)
+{
+    if (!h || !t || !moltype) return fail(FM_ERR_ARG, "null argument");
+    if (h->stage != 1) return fail(FM_ERR_STATE, "set the Mie tables after fm_upload_state and before fm_setup");
+    const int nt = t->ntypes;
+    if (nt < 1 || nt > FM_MIE_MAXTYPES) return fail(FM_ERR_ARG, "ntypes out of range (1 .. FM_MIE_MAXTYPES)");
+    if (!t->mass || !t->epsilon || !t->lambdar || !t->lambdaa || !t->C || !t->alpha || !t->potshift ||
+        !t->k_harmonic || !t->r0)
+        return fail(FM_ERR_ARG, "null table");
+    for (int a = 0; a < nt; a++)
+        if (!(t->mass[a] > 0.0)) return fail(FM_ERR_ARG, "mass_lookup must be > 0");
+    const size_t n = (size_t)h->d.n;
+    for (size_t u = 0; u < n; u++)
+        if (moltype[u] < 1 || moltype[u] > nt) return fail(FM_ERR_ARG, "moltype out of range (1 .. ntypes)");
+    // the reference's evaluation order, precombined per type pair (Mie_accijmag,
+    // Mie_energy, harmonic_*: setup_set_parameters.f90:149-204, 384-437)
+    std::vector<fm::FmMiePair> pairs((size_t)fm::MIE_MAXT * fm::MIE_MAXT);
+    for (int a = 0; a < nt; a++)
+        for (int b = 0; b < nt; b++) {
+            const size_t q = (size_t)a + (size_t)nt * (size_t)b;
+            fm::FmMiePair &m = pairs[(size_t)a + (size_t)fm::MIE_MAXT * (size_t)b];
+            m.ceps = t->C[q] * t->epsilon[q];
+            m.lr = t->lambdar[q];
+            m.ala = t->alpha[q] * t->lambdaa[q];
+            m.er1 = 0.5 * t->lambdar[q] + 1.0;
+            m.ea1 = 0.5 * t->lambdaa[q] + 1.0;
+            m.er = 0.5 * t->lambdar[q];
+            m.ea = 0.5 * t->lambdaa[q];
+            m.alpha = t->alpha[q];
+            m.shift = t->potshift[q];
+            m.k = t->k_harmonic[q];
+            m.r0 = t->r0[q];
+        }
+    std::vector<double> mass(fm::MIE_MAXT, 1.0);
+    for (int a = 0; a < nt; a++) mass[(size_t)a] = t->mass[a];
+    FmDev &d = h->d;
+    if (!d.mie_pair) {
+        fm::FmMiePair *dp = nullptr;
+        double *dm = nullptr;
+        int32_t *dt = nullptr;
+        FM_CUDA(cudaMalloc(&dp, sizeof(fm::FmMiePair) * pairs.size()));
+        d.mie_pair = dp;
+        FM_CUDA(cudaMalloc(&dm, sizeof(double) * mass.size()));
+        d.mie_mass = dm;
+        FM_CUDA(cudaMalloc(&dt, sizeof(int32_t) * n));
+        d.mie_type_up = dt;
+    }
+    FM_CUDA(cudaMemcpyAsync((void *)d.mie_pair, pairs.data(), sizeof(fm::FmMiePair) * pairs.size(),
+                            cudaMemcpyHostToDevice, h->st));
+    FM_CUDA(cudaMemcpyAsync((void *)d.mie_mass, mass.data(), sizeof(double) * mass.size(), cudaMemcpyHostToDevice,
+                            h->st));
+    FM_CUDA(cudaMemcpyAsync((void *)d.mie_type_up, moltype, sizeof(int32_t) * n, cudaMemcpyHostToDevice, h->st));
+    d.mie = 1;
+    fm::launch_set_types(d, h->st);  // slots still equal upload indices before the first binning
+    FM_CUDA(cudaGetLastError());
+    FM_CUDA(cudaStreamSynchronize(h->st));
+    return FM_OK;
+}
+
 
 extern "C" int fm_get_bonds(fm_handle *h, int32_t *owner, int32_t *partner, int8_t *code, int64_t cap, int64_t *n_out)
 {

@@ -46,6 +46,15 @@ struct FmRecord {
 };
 
 // Everything a kernel needs, passed by value.
+// Mie pair constants for one (type_i, type_j), precombined in the
+// reference's evaluation order: Mie_accijmag = (C eps)(lr s^(lr/2+1) -
+// (alpha la) s^(la/2+1)), Mie_energy = (C eps)(s^(lr/2) - alpha s^(la/2)) -
+// potshift, harmonic bonds -k (r - r0)/r and k/2 (r - r0)^2.
+constexpr int MIE_MAXT = 16;
+struct FmMiePair {
+    double ceps, lr, ala, er1, ea1, er, ea, alpha, shift, k, r0;
+};
+
 struct FmDev {
     // geometry and constants
     int n;                 // real molecules
@@ -87,6 +96,12 @@ struct FmDev {
     int32_t *tchain, *tsubchain;
     int4 *tbflag;
     int32_t *bnd, *nbond;
+    // Mie_potential 1: per-type-pair constants, per-type masses; a molecule's
+    // type (1-based) rides in the w component of its position
+    int mie;
+    const FmMiePair *mie_pair;   // [(ti-1) + MIE_MAXT*(tj-1)]
+    const double *mie_mass;      // [ti-1]
+    const int32_t *mie_type_up;  // moltype by upload index (written into w at upload)
     // record partials [nblocks][RS_N] and finished rows
     double *partial;
     int nblocks_force;
@@ -147,6 +162,7 @@ int scan_tiles(int ncell);
 int all_pairs_blocks(int n);
 // Layout conversion between the reference's (3,n) column-major arrays and
 // the device layout; `order` maps upload index -> slot.
+void launch_set_types(const FmDev &d, cudaStream_t st);
 void launch_scatter_state(const FmDev &d, const double *r3, const double *v3, const double *a3,
                           cudaStream_t st);
 void launch_gather_state(const FmDev &d, double *r3, double *v3, double *a3, int32_t *gid,

@@ -388,6 +388,62 @@ __global__ void __launch_bounds__(NB_THREADS, 6) k_build_nlist(FmDev d, int gate
 
 constexpr int FORCE_THREADS = 256;
 
+// One pair inside the cutoff: acc (the pair force over rij) accumulated as
+// acc * rij, and on record steps the energy and acc * r^2.  PREC bit 0: FP32
+// pair magnitude (FP64 rij scales it); bit 1: Mie_potential 1, constants by
+// the molecules' types (w of the positions): Mie_accijmag and Mie_energy
+// (setup_set_parameters.f90:149-204) with real powers, as s**(lr/2+1).
+// Otherwise LJ_accijmag = 48 (s^7 - s^4/2), s = 1/r^2, and LJ_energy
+// (:105-135).
+template <int PREC, bool REC>
+__device__ __forceinline__ void pair_acc(const FmDev &d, double r2, double dx, double dy, double dz, double wi,
+                                         double wj, double &fx, double &fy, double &fz, double &pe, double &vir)
+{
+    constexpr bool F32 = (PREC & 1) != 0, MIE = (PREC & 2) != 0;
+    if (MIE) {
+        const FmMiePair &m = d.mie_pair[((int)wi - 1) + MIE_MAXT * ((int)wj - 1)];
+        if (!F32) {
+            const double s = __drcp_rn(r2);  // == 1.0 / r2
+            const double acc = m.ceps * (m.lr * pow(s, m.er1) - m.ala * pow(s, m.ea1));
+            fx += acc * dx; fy += acc * dy; fz += acc * dz;
+            if (REC) {
+                pe += m.ceps * (pow(s, m.er) - m.alpha * pow(s, m.ea)) - m.shift;
+                vir += acc * r2;
+            }
+        } else {
+            const float s = __frcp_rn((float)r2);
+            const double acc = (double)((float)m.ceps * ((float)m.lr * powf(s, (float)m.er1) -
+                                                         (float)m.ala * powf(s, (float)m.ea1)));
+            fx = fma(acc, dx, fx); fy = fma(acc, dy, fy); fz = fma(acc, dz, fz);
+            if (REC) {
+                pe += (double)((float)m.ceps * (powf(s, (float)m.er) - (float)m.alpha * powf(s, (float)m.ea))) - m.shift;
+                vir += acc * r2;
+            }
+        }
+    } else if (!F32) {
+        const double s = __drcp_rn(r2);  // == 1.0 / r2 (both correctly rounded)
+        const double s2 = s * s, s4 = s2 * s2;
+        const double acc = 48.0 * (s4 * s2 * s - 0.5 * s4);
+        fx += acc * dx; fy += acc * dy; fz += acc * dz;
+        if (REC) {
+            const double s3 = s2 * s, s6 = s3 * s3;
+            pe += 4.0 * (s6 - s3) - d.potshift;  // LJ_energy (:126-135)
+            vir += acc * r2;
+        }
+    } else {
+        // FP32 pair magnitude; the FP64 rij scales it (one conversion)
+        const float s = __frcp_rn((float)r2);
+        const float s2 = s * s, s4 = s2 * s2;
+        const double acc = (double)(48.0f * (s4 * s2 * s - 0.5f * s4));
+        fx = fma(acc, dx, fx); fy = fma(acc, dy, fy); fz = fma(acc, dz, fz);
+        if (REC) {
+            const float s3 = s2 * s, s6 = s3 * s3;
+            pe += (double)(4.0f * (s6 - s3)) - d.potshift;
+            vir += acc * r2;
+        }
+    }
+}
+
 // Integrator epilogue of molecule i with its summed LJ force: stores a (and PE
 // and virial on record steps) and, by MODE,
 //   1  move(2)                               (simulation_move_particles_vv.f90:132-135)
@@ -396,10 +452,15 @@ constexpr int FORCE_THREADS = 256;
 // The record partials use v after move(2) for velocity Verlet and v + a dt/2
 // for leap-frog (simulation_record.f90:1236-1252).  Returns |v|^2 after a
 // position update (modes 2, 3), else 0.
-template <bool REC, int MODE>
+template <bool REC, int MODE, bool MIE = false>
 __device__ __forceinline__ double epilogue(const FmDev &d, int pset, int i, double4 p, double fx, double fy,
                                            double fz, double pe, double vir, double (&part)[RS_N])
 {
+    double mass = 1.0;  // LJ_mass; Mie_mass = mass_lookup(moltype)
+    if (MIE) {
+        mass = d.mie_mass[(int)p.w - 1];
+        fx = fx / mass; fy = fy / mass; fz = fz / mass;
+    }
     d.ax[i] = fx; d.ay[i] = fy; d.az[i] = fz;
     if (REC) { d.pe[i] = pe; d.vir[i] = vir; }
     double vx = d.vx[i], vy = d.vy[i], vz = d.vz[i];
@@ -410,8 +471,8 @@ __device__ __forceinline__ double epilogue(const FmDev &d, int pset, int i, doub
             const double wy = __dadd_rn(vy, __dmul_rn(__dmul_rn(0.5, fy), d.dt));
             const double wz = __dadd_rn(vz, __dmul_rn(__dmul_rn(0.5, fz), d.dt));
             part[RS_PE] = pe; part[RS_VIR] = vir; part[RS_PEMAX] = pe;
-            part[RS_MV2] = norm2_rn(wx, wy, wz);
-            part[RS_VSUM] = __dadd_rn(__dadd_rn(wx, wy), wz);
+            part[RS_MV2] = MIE ? mass * norm2_rn(wx, wy, wz) : norm2_rn(wx, wy, wz);
+            part[RS_VSUM] = MIE ? mass * __dadd_rn(__dadd_rn(wx, wy), wz) : __dadd_rn(__dadd_rn(wx, wy), wz);
         }
         vx = __dadd_rn(vx, __dmul_rn(d.dt, fx));
         vy = __dadd_rn(vy, __dmul_rn(d.dt, fy));
@@ -436,8 +497,8 @@ __device__ __forceinline__ double epilogue(const FmDev &d, int pset, int i, doub
             wz = __dadd_rn(vz, __dmul_rn(__dmul_rn(0.5, fz), d.dt));
         }
         part[RS_PE] = pe; part[RS_VIR] = vir; part[RS_PEMAX] = pe;
-        part[RS_MV2] = norm2_rn(wx, wy, wz);
-        part[RS_VSUM] = __dadd_rn(__dadd_rn(wx, wy), wz);
+        part[RS_MV2] = MIE ? mass * norm2_rn(wx, wy, wz) : norm2_rn(wx, wy, wz);
+        part[RS_VSUM] = MIE ? mass * __dadd_rn(__dadd_rn(wx, wy), wz) : __dadd_rn(__dadd_rn(wx, wy), wz);
     }
     if (MODE == 2) {
         p.x = __dadd_rn(__dadd_rn(p.x, __dmul_rn(d.dt, vx)), __dmul_rn(d.half_dt2, fx));
@@ -458,7 +519,7 @@ __device__ __forceinline__ double epilogue(const FmDev &d, int pset, int i, doub
 // (FENE_accijmag, setup_set_parameters.f90:348-358), energy
 // 0.5 k R0^2 log(1 - r^2/R0^2) (:371-380), in FP64 for every precision form.
 // A bond at or beyond R0 is the reference's polymer_bond_error.
-template <bool REC>
+template <bool REC, bool MIE>
 __device__ __forceinline__ void fene_bonds(const FmDev &d, const double4 *P, int i, double &fx, double &fy,
                                            double &fz, double &pe, double &vir)
 {
@@ -473,6 +534,19 @@ __device__ __forceinline__ void fene_bonds(const FmDev &d, const double4 *P, int
         const double zj = ((code >> 4) & 3) != 1 ? __dadd_rn(pj.z, ((code >> 4) & 3) == 2 ? d.L[2] : -d.L[2]) : pj.z;
         const double dx = __dsub_rn(pi.x, xj), dy = __dsub_rn(pi.y, yj), dz = __dsub_rn(pi.z, zj);
         const double r2 = norm2_rn(dx, dy, dz);
+        if (MIE) {
+            // harmonic_accijmag / harmonic_energy (setup_set_parameters.f90:384-437):
+            // -k (|r| - r0)/|r| and k/2 (|r| - r0)^2, constants by type pair
+            const FmMiePair &m = d.mie_pair[((int)pi.w - 1) + MIE_MAXT * ((int)pj.w - 1)];
+            const double rm = sqrt(r2), dr = rm - m.r0;
+            const double acc = -m.k * dr / rm;
+            fx += acc * dx; fy += acc * dy; fz += acc * dz;
+            if (REC) {
+                pe += 0.5 * m.k * (dr * dr);
+                vir += acc * r2;
+            }
+            continue;
+        }
         if (r2 >= d.R0_2) {
             uint32_t old = atomicOr(&d.sc->status, ST_BOND);
             if ((old & ST_FATAL) == 0u) d.sc->fail_iter = -2;
@@ -545,33 +619,7 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force(FmDev d)
                 const double dy = __dsub_rn(pi.y, yj);
                 const double dz = __dsub_rn(pi.z, zj);
                 const double r2 = norm2_rn(dx, dy, dz);
-                if (r2 < rc2) {
-                    if (PREC == 0) {
-                        // LJ_accijmag = 48 (s^7 - s^4/2), s = 1/r^2 (setup_set_parameters.f90:105-113)
-                        const double s = __drcp_rn(r2);  // == 1.0 / r2 (both correctly rounded)
-                        const double s2 = s * s, s4 = s2 * s2;
-                        const double acc = 48.0 * (s4 * s2 * s - 0.5 * s4);
-                        fx += acc * dx; fy += acc * dy; fz += acc * dz;
-                        if (REC) {
-                            const double s3 = s2 * s, s6 = s3 * s3;
-                            pe += 4.0 * (s6 - s3) - d.potshift;  // LJ_energy (:126-135)
-                            vir += acc * r2;
-                        }
-                    } else {
-                        // FP32 pair magnitude; the FP64 rij scales it (one conversion)
-                        const float s = __frcp_rn((float)r2);
-                        const float s2 = s * s, s4 = s2 * s2;
-                        const double acc = (double)(48.0f * (s4 * s2 * s - 0.5f * s4));
-                        fx = fma(acc, dx, fx);
-                        fy = fma(acc, dy, fy);
-                        fz = fma(acc, dz, fz);
-                        if (REC) {
-                            const float s3 = s2 * s, s6 = s3 * s3;
-                            pe += (double)(4.0f * (s6 - s3)) - d.potshift;
-                            vir += acc * r2;
-                        }
-                    }
-                }
+                if (r2 < rc2) pair_acc<PREC, REC>(d, r2, dx, dy, dz, pi.w, pj[q].w, fx, fy, fz, pe, vir);
             }
         }
     }
@@ -589,9 +637,9 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force(FmDev d)
     }
     double part[RS_N] = {0.0, 0.0, 0.0, 0.0, 0.0};
     double m2 = 0.0;
-    if (active && lane == 0 && d.potential_flag == 1) fene_bonds<REC>(d, P, i, fx, fy, fz, pe, vir);
-    // a(:,i) = sum acc rij / mass, mass = 1 (LJ_mass)
-    if (active && lane == 0) m2 = epilogue<REC, MODE>(d, pset, i, P[i], fx, fy, fz, pe, vir, part);
+    if (active && lane == 0 && d.potential_flag == 1) fene_bonds<REC, (PREC & 2) != 0>(d, P, i, fx, fy, fz, pe, vir);
+    // a(:,i) = sum acc rij / mass (LJ_mass = 1; Mie_mass by type)
+    if (active && lane == 0) m2 = epilogue<REC, MODE, (PREC & 2) != 0>(d, pset, i, P[i], fx, fy, fz, pe, vir, part);
     if (REC) block_partials(d, part);
     if (MODE >= 2) block_vmax2(d, m2);
 }
@@ -669,10 +717,11 @@ __global__ void __launch_bounds__(MACRO_THREADS) k_macro_partials(FmDev d)
             vy = __dadd_rn(vy, __dmul_rn(__dmul_rn(0.5, d.ay[i]), d.dt));
             vz = __dadd_rn(vz, __dmul_rn(__dmul_rn(0.5, d.az[i]), d.dt));
         }
+        const double mass = d.mie ? d.mie_mass[(int)cur_pos(d, d.sc->pset)[i].w - 1] : 1.0;
         part[RS_PE] = d.pe[i];
         part[RS_VIR] = d.vir[i];
-        part[RS_MV2] = norm2_rn(vx, vy, vz);
-        part[RS_VSUM] = __dadd_rn(__dadd_rn(vx, vy), vz);
+        part[RS_MV2] = mass * norm2_rn(vx, vy, vz);
+        part[RS_VSUM] = mass * __dadd_rn(__dadd_rn(vx, vy), vz);
         part[RS_PEMAX] = d.pe[i];
     }
     __shared__ double ws[RS_N][MACRO_THREADS / 32];
@@ -723,38 +772,14 @@ __global__ void __launch_bounds__(AP_THREADS) k_all_pairs(FmDev d)
                     if (fabs(r[k]) > d.hd[k]) r[k] = __dsub_rn(r[k], copysign(d.L[k], r[k]));
                     r2 = __dadd_rn(r2, __dmul_rn(r[k], r[k]));
                 }
-                if (r2 < d.rc2) {
-                    if (PREC == 0) {
-                        const double s = __drcp_rn(r2);  // == 1.0 / r2 (both correctly rounded)
-                        const double s2 = s * s, s4 = s2 * s2;
-                        const double acc = 48.0 * (s4 * s2 * s - 0.5 * s4);
-                        fx += acc * r[0]; fy += acc * r[1]; fz += acc * r[2];
-                        if (REC) {
-                            const double s3 = s2 * s, s6 = s3 * s3;
-                            pe += 4.0 * (s6 - s3) - d.potshift;
-                            vir += acc * r2;
-                        }
-                    } else {
-                        const float s = 1.0f / (float)r2;
-                        const float s2 = s * s, s4 = s2 * s2;
-                        const float acc = 48.0f * (s4 * s2 * s - 0.5f * s4);
-                        fx += (double)(acc * (float)r[0]);
-                        fy += (double)(acc * (float)r[1]);
-                        fz += (double)(acc * (float)r[2]);
-                        if (REC) {
-                            const float s3 = s2 * s, s6 = s3 * s3;
-                            pe += (double)(4.0f * (s6 - s3)) - d.potshift;
-                            vir += (double)(acc * (float)r2);
-                        }
-                    }
-                }
+                if (r2 < d.rc2) pair_acc<PREC, REC>(d, r2, r[0], r[1], r[2], pi.w, pj.w, fx, fy, fz, pe, vir);
             }
         }
         __syncthreads();
     }
     double part[RS_N] = {0.0, 0.0, 0.0, 0.0, 0.0};
     double m2 = 0.0;
-    if (active) m2 = epilogue<REC, MODE>(d, pset, i, pi, fx, fy, fz, pe, vir, part);
+    if (active) m2 = epilogue<REC, MODE, (PREC & 2) != 0>(d, pset, i, pi, fx, fy, fz, pe, vir, part);
     if (REC) {
         // AP blocks are AP_THREADS wide; reuse the generic reduction layout
         __shared__ double ws[RS_N][AP_THREADS / 32];
@@ -820,13 +845,22 @@ __global__ void k_pair_digest(FmDev d, const int32_t *glob_of_upload)
     }
 }
 
+// Types of an uploaded state (slots still equal upload indices).
+__global__ void k_set_types(FmDev d)
+{
+    int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= d.n) return;
+    cur_pos(d, d.sc->pset)[u].w = (double)d.mie_type_up[u];
+}
+
 // upload order u -> slot u (uploads start in upload order)
 __global__ void k_scatter_state(FmDev d, const double *r3, const double *v3, const double *a3)
 {
     int u = blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= d.n) return;
     double4 *P = cur_pos(d, d.sc->pset);
-    P[u] = make_double4(r3[3 * (size_t)u], r3[3 * (size_t)u + 1], r3[3 * (size_t)u + 2], 0.0);
+    P[u] = make_double4(r3[3 * (size_t)u], r3[3 * (size_t)u + 1], r3[3 * (size_t)u + 2],
+                        d.mie ? (double)d.mie_type_up[u] : 0.0);
     d.vx[u] = v3[3 * (size_t)u]; d.vy[u] = v3[3 * (size_t)u + 1]; d.vz[u] = v3[3 * (size_t)u + 2];
     if (a3) { d.ax[u] = a3[3 * (size_t)u]; d.ay[u] = a3[3 * (size_t)u + 1]; d.az[u] = a3[3 * (size_t)u + 2]; }
     else { d.ax[u] = 0.0; d.ay[u] = 0.0; d.az[u] = 0.0; }
@@ -922,8 +956,12 @@ static void launch_force_tpm(const FmDev &d, int record, int mode, cudaStream_t 
     const int g = force_blocks(d.n, TPM);
 #define FM_FORCE_CASE(R, M)                                                                     \
     if (record == R && mode == M) {                                                             \
-        if (d.precision == 0) k_force<TPM, R, M, 0><<<g, FORCE_THREADS, 0, st>>>(d);            \
-        else k_force<TPM, R, M, 1><<<g, FORCE_THREADS, 0, st>>>(d);                             \
+        switch (d.precision + 2 * d.mie) {                                                      \
+        case 0: k_force<TPM, R, M, 0><<<g, FORCE_THREADS, 0, st>>>(d); break;                   \
+        case 1: k_force<TPM, R, M, 1><<<g, FORCE_THREADS, 0, st>>>(d); break;                   \
+        case 2: k_force<TPM, R, M, 2><<<g, FORCE_THREADS, 0, st>>>(d); break;                   \
+        default: k_force<TPM, R, M, 3><<<g, FORCE_THREADS, 0, st>>>(d); break;                  \
+        }                                                                                       \
         return;                                                                                 \
     }
     FM_FORCE_CASE(0, 0) FM_FORCE_CASE(0, 1) FM_FORCE_CASE(0, 2) FM_FORCE_CASE(0, 3)
@@ -947,8 +985,12 @@ void launch_all_pairs(const FmDev &d, int record, int mode, cudaStream_t st)
     const int g = all_pairs_blocks(d.n);
 #define FM_AP_CASE(R, M)                                                            \
     if (record == R && mode == M) {                                                 \
-        if (d.precision == 0) k_all_pairs<R, M, 0><<<g, AP_THREADS, 0, st>>>(d);    \
-        else k_all_pairs<R, M, 1><<<g, AP_THREADS, 0, st>>>(d);                     \
+        switch (d.precision + 2 * d.mie) {                                          \
+        case 0: k_all_pairs<R, M, 0><<<g, AP_THREADS, 0, st>>>(d); break;           \
+        case 1: k_all_pairs<R, M, 1><<<g, AP_THREADS, 0, st>>>(d); break;           \
+        case 2: k_all_pairs<R, M, 2><<<g, AP_THREADS, 0, st>>>(d); break;           \
+        default: k_all_pairs<R, M, 3><<<g, AP_THREADS, 0, st>>>(d); break;          \
+        }                                                                           \
         return;                                                                     \
     }
     FM_AP_CASE(0, 0) FM_AP_CASE(0, 1) FM_AP_CASE(0, 2) FM_AP_CASE(0, 3)
@@ -971,6 +1013,8 @@ void launch_pair_digest(const FmDev &d, const int32_t *glob_of_upload, cudaStrea
 {
     k_pair_digest<<<nblk(d.n, 256), 256, 0, st>>>(d, glob_of_upload);
 }
+
+void launch_set_types(const FmDev &d, cudaStream_t st) { k_set_types<<<nblk(d.n, 256), 256, 0, st>>>(d); }
 
 void launch_scatter_state(const FmDev &d, const double *r3, const double *v3, const double *a3, cudaStream_t st)
 {

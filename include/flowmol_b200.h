@@ -139,6 +139,27 @@ FM_API int fm_download_state(fm_handle *h, double *r, double *v, double *a, int3
  * check_update_adjacentbeadinfo does (linklist.f90:2542-2584). */
 FM_API int fm_upload_monomers(fm_handle *h, const int32_t *chainID, const int32_t *subchainID,
                               const int32_t *bin_bflag);
+/* Mie_potential 1 (setup_set_parameters.f90:1208-1216): non-bonded pairs
+ * use Mie_accijmag / Mie_energy (:149-204) and bonds harmonic_accijmag /
+ * harmonic_energy (:384-437) with per-type-pair constants, and every
+ * molecule has mass_lookup(moltype) (a = F/m; kinetic sums weighted by m,
+ * simulation_record.f90:1236-1252).  The tables are the reference's own
+ * lookup arrays after setup_mie_potential (:566-1092): ntypes x ntypes,
+ * entry (i,j) at [(i-1) + ntypes*(j-1)], types 1-based; mass has ntypes
+ * entries.  moltype(n) is in upload order.  Call after fm_upload_state (and
+ * fm_upload_monomers), before fm_setup.  No counterpart entry point in the
+ * reference, whose tables are module globals. */
+#define FM_MIE_MAXTYPES 16
+typedef struct fm_mie_tables {
+    int32_t ntypes, pad_;
+    const double *mass;                 /* mass_lookup(ntypes) */
+    const double *epsilon;              /* epsilon_lookup */
+    const double *lambdar, *lambdaa;    /* lambdar_lookup, lambdaa_lookup */
+    const double *C, *alpha;            /* C_lookup, alpha_lookup */
+    const double *potshift;             /* potshift_lookup */
+    const double *k_harmonic, *r0;      /* k_lookup, r0_lookup (bonds) */
+} fm_mie_tables;
+FM_API int fm_set_mie(fm_handle *h, const fm_mie_tables *t, const int32_t *moltype);
 /* Bonds of the last list build as (owner glob_no, partner glob_no, image
  * code) triplets, like fm_get_pair_list.  Test hook. */
 FM_API int fm_get_bonds(fm_handle *h, int32_t *owner, int32_t *partner, int8_t *code, int64_t cap, int64_t *n);

@@ -85,6 +85,12 @@ typedef struct orc {
     double *rfmol;            /* (9, cap) */
     double Pxy[9];
     int nstress;
+    /* Mie_potential 1: moltype (cap, 1-based) and the lookup tables of
+     * setup_mie_potential, (i,j) at [(i-1) + MIET*(j-1)] */
+    int mie;
+    int *moltype;
+    double mie_mass[16], mie_eps[256], mie_lr[256], mie_la[256], mie_C[256], mie_alpha[256], mie_shift[256],
+        mie_k[256], mie_r0[256];
     double vsum, mv2sum, potenergysum, virial;
     double kinenergy, potenergy, totenergy, temperature, pressure;
     int rebuild_count;
@@ -159,6 +165,45 @@ static inline double fene_accijmag(double rij2, double k_c, double R_0)
 static inline double fene_energy(double rij2, double k_c, double R_0)
 {
     return 0.5 * k_c * R_0 * R_0 * log(1.0 - (rij2 / (R_0 * R_0)));
+}
+
+/* Mie_potential 1 (setup_set_parameters.f90:149-204, 384-437): constants by
+ * the types of the two molecules (a halo image has its source's type, as
+ * messenger_updateborders sends it, messenger.MPI.f90:693,764). */
+#define MIET 16
+static inline int type_of(const orc *s, int n) /* 1-based molecule or image */
+{
+    return n <= s->np ? s->moltype[n - 1] : s->moltype[s->halo_src[n - 1] - 1];
+}
+static inline double mass_of(const orc *s, int n) /* LJ_mass / Mie_mass */
+{
+    return s->mie ? s->mie_mass[type_of(s, n) - 1] : 1.0;
+}
+static inline double pair_accijmag(const orc *s, double invrij2, int i, int j)
+{
+    if (!s->mie) return lj_accijmag(invrij2);
+    int q = (type_of(s, i) - 1) + MIET * (type_of(s, j) - 1);
+    double C = s->mie_C[q], eps = s->mie_eps[q], lr = s->mie_lr[q], la = s->mie_la[q], al = s->mie_alpha[q];
+    return C * eps * (lr * pow(invrij2, 0.5 * lr + 1) - al * la * pow(invrij2, 0.5 * la + 1));
+}
+static inline double pair_energy(const orc *s, double invrij2, int i, int j)
+{
+    if (!s->mie) return lj_energy(invrij2, s->potshift);
+    int q = (type_of(s, i) - 1) + MIET * (type_of(s, j) - 1);
+    double C = s->mie_C[q], eps = s->mie_eps[q], lr = s->mie_lr[q], la = s->mie_la[q], al = s->mie_alpha[q];
+    return C * eps * (pow(invrij2, 0.5 * lr) - al * pow(invrij2, 0.5 * la)) - s->mie_shift[q];
+}
+static inline double harmonic_accijmag(const orc *s, double rij2, int i, int j)
+{
+    int q = (type_of(s, i) - 1) + MIET * (type_of(s, j) - 1);
+    double rm = sqrt(rij2);
+    return -s->mie_k[q] * (rm - s->mie_r0[q]) / rm;
+}
+static inline double harmonic_energy(const orc *s, double rij2, int i, int j)
+{
+    int q = (type_of(s, i) - 1) + MIET * (type_of(s, j) - 1);
+    double d = sqrt(rij2) - s->mie_r0[q];
+    return 0.5 * s->mie_k[q] * (d * d);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -257,7 +302,7 @@ void orc_free(orc *s)
     free(s->potenergymol); free(s->potenergymol_POLY); free(s->virialmol); free(s->rdisp);
     free(s->chainID); free(s->subchainID); free(s->funcy); free(s->bflag); free(s->bond);
     free(s->bondcount);
-    free(s->tag); free(s->rtether); free(s->slidev); free(s->rfmol);
+    free(s->tag); free(s->rtether); free(s->slidev); free(s->rfmol); free(s->moltype);
     free(s->cellnp); free(s->cellhead); free(s->cn_molno); free(s->cn_next);
     free(s->Nlist); free(s->nhead); free(s->nn_molno); free(s->nn_next);
     free(s);
@@ -789,16 +834,17 @@ static void forces_halfint(orc *s)
             double r2 = rij2_of(s, i, j, rij);
             if (r2 < s->rcutoff2) {
                 double inv = 1.0 / r2;
-                double acc = lj_accijmag(inv);
+                double acc = pair_accijmag(s, inv, i, j);
+                double mi = mass_of(s, i), mj = mass_of(s, j);
                 double *ai = &s->a[3 * (size_t)(i - 1)], *aj = &s->a[3 * (size_t)(j - 1)];
-                ai[0] = ai[0] + acc * rij[0] / 1.0;
-                ai[1] = ai[1] + acc * rij[1] / 1.0;
-                ai[2] = ai[2] + acc * rij[2] / 1.0;
-                aj[0] = aj[0] - acc * rij[0] / 1.0;
-                aj[1] = aj[1] - acc * rij[1] / 1.0;
-                aj[2] = aj[2] - acc * rij[2] / 1.0;
+                ai[0] = ai[0] + acc * rij[0] / mi;
+                ai[1] = ai[1] + acc * rij[1] / mi;
+                ai[2] = ai[2] + acc * rij[2] / mi;
+                aj[0] = aj[0] - acc * rij[0] / mj;
+                aj[1] = aj[1] - acc * rij[1] / mj;
+                aj[2] = aj[2] - acc * rij[2] / mj;
                 if (rec) {
-                    double e = lj_energy(inv, s->potshift);
+                    double e = pair_energy(s, inv, i, j);
                     s->potenergymol[i - 1] += e;
                     s->potenergymol[j - 1] += e;
                     s->virialmol[i - 1] += acc * r2;
@@ -830,13 +876,14 @@ static void forces_full(orc *s)
             double r2 = rij2_of(s, i, j, rij);
             if (r2 < s->rcutoff2) {
                 double inv = 1.0 / r2;
-                double acc = lj_accijmag(inv);
+                double acc = pair_accijmag(s, inv, i, j);
+                double mi = mass_of(s, i);
                 double *ai = &s->a[3 * (size_t)(i - 1)];
-                ai[0] = ai[0] + acc * rij[0] / 1.0;
-                ai[1] = ai[1] + acc * rij[1] / 1.0;
-                ai[2] = ai[2] + acc * rij[2] / 1.0;
+                ai[0] = ai[0] + acc * rij[0] / mi;
+                ai[1] = ai[1] + acc * rij[1] / mi;
+                ai[2] = ai[2] + acc * rij[2] / mi;
                 if (rec) {
-                    s->potenergymol[i - 1] += lj_energy(inv, s->potshift);
+                    s->potenergymol[i - 1] += pair_energy(s, inv, i, j);
                     s->virialmol[i - 1] += acc * r2;
                 } else if (tev) {
                     s->virialmol[i - 1] += acc * r2;
@@ -865,14 +912,15 @@ static void forces_AP(orc *s)
             }
             if (r2 < s->rcutoff2) {
                 double inv = 1.0 / r2;
-                double acc = lj_accijmag(inv);
+                double acc = pair_accijmag(s, inv, i, j);
+                double mi = mass_of(s, i), mj = mass_of(s, j);
                 double *ai = &s->a[3 * (size_t)(i - 1)], *aj = &s->a[3 * (size_t)(j - 1)];
                 for (int k = 0; k < 3; k++) {
-                    ai[k] = ai[k] + acc * rij[k] / 1.0;
-                    aj[k] = aj[k] - acc * rij[k] / 1.0;
+                    ai[k] = ai[k] + acc * rij[k] / mi;
+                    aj[k] = aj[k] - acc * rij[k] / mj;
                 }
                 if (rec) {
-                    double e = lj_energy(inv, s->potshift);
+                    double e = pair_energy(s, inv, i, j);
                     s->potenergymol[i - 1] += e;
                     s->potenergymol[j - 1] += e;
                     s->virialmol[i - 1] += acc * r2;
@@ -898,14 +946,20 @@ static int forces_poly(orc *s)
             int j = s->bond[(size_t)(i - 1) * s->max_funcy + b];
             if (j == 0) continue;
             double r2 = rij2_of(s, i, j, rij);
-            if (r2 >= s->R_0 * s->R_0) return ORC_ERR_BOND; /* polymer_bond_error */
-            double acc = fene_accijmag(r2, s->k_c, s->R_0);
+            double acc;
+            if (s->mie) {
+                acc = harmonic_accijmag(s, r2, i, j); /* get_poly_accijmag => harmonic (:1215) */
+            } else {
+                if (r2 >= s->R_0 * s->R_0) return ORC_ERR_BOND; /* polymer_bond_error */
+                acc = fene_accijmag(r2, s->k_c, s->R_0);
+            }
+            double mi = mass_of(s, i);
             double *ai = &s->a[3 * (size_t)(i - 1)];
-            ai[0] = ai[0] + acc * rij[0] / 1.0;
-            ai[1] = ai[1] + acc * rij[1] / 1.0;
-            ai[2] = ai[2] + acc * rij[2] / 1.0;
+            ai[0] = ai[0] + acc * rij[0] / mi;
+            ai[1] = ai[1] + acc * rij[1] / mi;
+            ai[2] = ai[2] + acc * rij[2] / mi;
             if (rec) {
-                s->potenergymol_POLY[i - 1] += fene_energy(r2, s->k_c, s->R_0);
+                s->potenergymol_POLY[i - 1] += s->mie ? harmonic_energy(s, r2, i, j) : fene_energy(r2, s->k_c, s->R_0);
                 s->virialmol[i - 1] += acc * r2;
             } else if (tev) {
                 s->virialmol[i - 1] += acc * r2;
@@ -1055,8 +1109,9 @@ void orc_evaluate_macroscopic_properties(orc *s)
             size_t q = 3 * (size_t)n + k;
             double vel = s->v[q];
             if (s->integration_algorithm == 0) vel = s->v[q] + 0.5 * s->a[q] * s->delta_t;
-            vsum = vsum + 1.0 * vel;
-            mv2sum = mv2sum + 1.0 * (vel * vel);
+            double m = mass_of(s, n + 1);
+            vsum = vsum + m * vel;
+            mv2sum = mv2sum + m * (vel * vel);
         }
     for (int n = 0; n < s->np; n++) vir = vir + s->virialmol[n];
     double gnp = (double)s->globalnp;
@@ -1125,6 +1180,30 @@ int orc_run_vv(orc *s, int nsteps, double *rec_out, int rec_cap, int *nrec)
             (*nrec)++;
         }
     }
+    return ORC_OK;
+}
+
+/* Mie_potential 1: the caller's lookup tables (ntypes x ntypes, (i,j) at
+ * [(i-1) + ntypes*(j-1)]) and moltype per molecule. */
+int orc_set_mie(orc *s, int ntypes, const double *mass, const double *eps, const double *lr, const double *la,
+                const double *C, const double *alpha, const double *shift, const double *k, const double *r0,
+                const int *moltype)
+{
+    if (ntypes < 1 || ntypes > MIET) return ORC_ERR_PARAM;
+    if (!s->moltype) s->moltype = (int *)xcalloc((size_t)s->np, sizeof(int));
+    for (int n = 0; n < s->np; n++) {
+        if (moltype[n] < 1 || moltype[n] > ntypes) return ORC_ERR_PARAM;
+        s->moltype[n] = moltype[n];
+    }
+    for (int a = 0; a < ntypes; a++) {
+        s->mie_mass[a] = mass[a];
+        for (int b = 0; b < ntypes; b++) {
+            int q = a + ntypes * b, t = a + MIET * b;
+            s->mie_eps[t] = eps[q]; s->mie_lr[t] = lr[q]; s->mie_la[t] = la[q]; s->mie_C[t] = C[q];
+            s->mie_alpha[t] = alpha[q]; s->mie_shift[t] = shift[q]; s->mie_k[t] = k[q]; s->mie_r0[t] = r0[q];
+        }
+    }
+    s->mie = 1;
     return ORC_OK;
 }
 

@@ -80,6 +80,8 @@ def lib():
         L.orc_potshift.restype = C.c_double
         L.orc_potshift.argtypes = [C.c_double]
         L.orc_set_monomers.argtypes = [C.c_void_p, i3, i3, i3, i3]
+        d8 = C.POINTER(C.c_double)
+        L.orc_set_mie.argtypes = [C.c_void_p, C.c_int] + [d8] * 9 + [i3]
         L.orc_set_tags.argtypes = [C.c_void_p, C.c_int, i3, d3, d3, C.c_double, C.c_double, C.c_double, C.c_int,
                                    C.c_double, C.c_double]
         L.orc_set_pressure.argtypes = [C.c_void_p, C.c_int]
@@ -189,6 +191,17 @@ class Oracle:
         f = np.ascontiguousarray(funcy, np.int32)
         b = np.ascontiguousarray(bflag, np.int32).reshape(-1)
         lib().orc_set_monomers(self.h, _ip(c), _ip(s), _ip(f), _ip(b))
+
+    def set_mie(self, tables, moltype):
+        """Mie_potential 1: `tables` maps mass, epsilon, lambdar, lambdaa, C,
+        alpha, potshift, k_harmonic, r0 to arrays (ntypes, or ntypes x
+        ntypes indexed [i-1, j-1]); moltype is 1-based per molecule."""
+        nt = len(tables["mass"])
+        keep = [np.ascontiguousarray(tables["mass"], np.float64)]
+        for k in ("epsilon", "lambdar", "lambdaa", "C", "alpha", "potshift", "k_harmonic", "r0"):
+            keep.append(np.ascontiguousarray(np.asarray(tables[k], np.float64).T).reshape(-1))  # (i,j) at i + nt*j
+        mt = np.ascontiguousarray(moltype, np.int32)
+        _check(lib().orc_set_mie(self.h, nt, *[_dp(a) for a in keep], _ip(mt)))
 
     @property
     def potenergymol(self):

@@ -80,3 +80,34 @@ def rel_err(x, ref, floor):
     d = np.linalg.norm(np.asarray(x) - np.asarray(ref), axis=-1)
     s = np.maximum(np.linalg.norm(np.asarray(ref), axis=-1), floor)
     return d / s
+
+
+def mie_C(lr, la):
+    """C_lookup (setup_set_parameters.f90:940-942)."""
+    return (lr / (lr - la)) * (lr / la) ** (la / (lr - la))
+
+
+def mie_tables(rc, eps, lr, la, mass, alpha=None, k=None, r0=None):
+    """Symmetric ntypes x ntypes lookup tables as setup_mie_potential leaves
+    them: C from (lr, la), potshift_lookup = the unshifted Mie energy at rc
+    (:944), alpha 1 by default, harmonic bond constants k and r0."""
+    eps = np.asarray(eps, float); lr = np.asarray(lr, float); la = np.asarray(la, float)
+    nt = len(mass)
+    alpha = np.ones((nt, nt)) if alpha is None else np.asarray(alpha, float)
+    C = mie_C(lr, la)
+    s = 1.0 / rc ** 2
+    shift = C * eps * (s ** (0.5 * lr) - alpha * s ** (0.5 * la))
+    return {"mass": np.asarray(mass, float), "epsilon": eps, "lambdar": lr, "lambdaa": la, "C": C,
+            "alpha": alpha, "potshift": shift,
+            "k_harmonic": np.zeros((nt, nt)) if k is None else np.asarray(k, float),
+            "r0": np.zeros((nt, nt)) if r0 is None else np.asarray(r0, float)}
+
+
+def mie_mixture_tables(rc):
+    """Two types: Ar (12-6, eps 1, m 1) and a 15-6 type (eps 0.8, m 1.5);
+    cross lambdas by the reference's rule sqrt((l_ii-3)(l_jj-3))+3 and a
+    geometric-mean epsilon (setup_set_parameters.f90:918-938)."""
+    lr = np.array([[12.0, np.sqrt(9.0 * 12.0) + 3.0], [np.sqrt(9.0 * 12.0) + 3.0, 15.0]])
+    la = np.full((2, 2), 6.0)
+    eps = np.array([[1.0, np.sqrt(0.8)], [np.sqrt(0.8), 0.8]])
+    return mie_tables(rc, eps, lr, la, [1.0, 1.5], k=np.full((2, 2), 295.3322), r0=np.ones((2, 2)))

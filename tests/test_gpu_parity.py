@@ -351,3 +351,71 @@ def test_cfg1_nve_energy_drift_1e4_steps(gpu_lib):
         np.testing.assert_allclose(e, e_o, rtol=1e-3)
     print("\ncfg1 NVE relative drift over %d steps: " % nsteps +
           ", ".join("%s %.3e" % (k, x) for k, x in drifts.items()))
+
+
+def test_mie_mixture_forces_and_trajectory(liquid):
+    """Mie_potential 1, two types with different exponents, epsilons and
+    masses: pair set bit-exact, a = F/m and per-molecule PE to 1e-12 (FP64;
+    the kernels' real powers against the oracle's libm), FP32 within 1e-5,
+    and 100 velocity-Verlet steps that follow the oracle."""
+    from helpers import mie_mixture_tables
+    r, v, dom = liquid
+    mt = (np.arange(len(r)) % 2 + 1).astype(np.int32)
+    tab = mie_mixture_tables(2.5)
+    o = O.Oracle(r, v, dom, 2.5, tplot=20, density=0.8442)
+    o.set_mie(tab, mt)
+    o.setup()
+    s = gpu_system(r, v, dom, 2.5, tplot=20, density=0.8442)
+    s.set_mie(tab, mt)
+    s.setup()
+    assert np.array_equal(canonical_full(*s.pair_list()), canonical_oracle(*o.pair_list()))
+    _, _, a, _ = s.download()
+    assert rel_err(a, o.a, 1.0).max() <= TOL64
+    pe, _ = s.per_molecule()
+    np.testing.assert_allclose(pe, o.potenergymol, rtol=TOL64, atol=TOL64)
+    s32 = gpu_system(r, v, dom, 2.5, tplot=20, density=0.8442, precision=api.PRECISION_FP32)
+    s32.set_mie(tab, mt)
+    s32.setup()
+    _, _, a32, _ = s32.download()
+    assert rel_err(a32, o.a, F_FLOOR32).max() <= TOL32
+    s32.close()
+    recs_o = o.run_vv(100)
+    s.records()
+    s.simulation_md(100)
+    recs = s.records()
+    assert [x["iter"] for x in recs] == [int(x) for x in recs_o[:, 0]]
+    for row, ro in zip(recs, recs_o):
+        assert row["kinenergy"] == pytest.approx(ro[4], rel=1e-9)
+        assert row["totenergy"] == pytest.approx(ro[6], rel=1e-9)
+    rg, _, _, _ = s.download()
+    assert np.abs(wrap_diff(rg, o.r, dom)).max() < 1e-7
+
+
+def test_mie_polymer_harmonic_bonds(gpu_lib):
+    """Mie_potential 1 on a bead-spring melt: bonds become harmonic
+    (k 295.3322, r0 1, setup_set_parameters.f90:873, 1215) -- the same bonds
+    found, forces to 1e-12, records over 100 steps."""
+    from flowmol_b200 import polymer
+    from helpers import mie_tables
+    r, v, ch, sub, fy, bf, dom = polymer.fene_melt(512)
+    tab = mie_tables(WCA_RC, [[1.0]], [[12.0]], [[6.0]], [1.0], k=[[295.3322]], r0=[[1.0]])
+    mt = np.ones(len(r), np.int32)
+    o = O.Oracle(r, v, dom, WCA_RC, tplot=20, potential_flag=1, k_c=30.0, R_0=1.5, density=0.85)
+    o.set_monomers(ch, sub, fy, bf)
+    o.set_mie(tab, mt)
+    o.setup()
+    s = gpu_system(r, v, dom, WCA_RC, tplot=20, density=0.85, potential_flag=1, k_c=30.0, R_0=1.5)
+    s.upload_monomers(ch, sub, bf)
+    s.set_mie(tab, mt)
+    s.setup()
+    key = lambda t: np.sort((t[0].astype(np.int64) << 32) | (t[1].astype(np.int64) << 5) | t[2])  # noqa: E731
+    assert np.array_equal(key(s.bonds()), key(o.bond_list()))
+    _, _, a, _ = s.download()
+    assert rel_err(a, o.a, 1.0).max() <= TOL64
+    recs_o = o.run_vv(100)
+    s.records()
+    s.simulation_md(100)
+    recs = s.records()
+    assert [x["iter"] for x in recs] == [int(x) for x in recs_o[:, 0]]
+    for row, ro in zip(recs, recs_o):
+        assert row["potenergy"] == pytest.approx(ro[5], rel=1e-9)

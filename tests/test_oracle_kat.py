@@ -150,3 +150,35 @@ def test_nve_energy_conservation_cfg1():
     te = recs[:, 6]
     assert abs(te[-1] - 1.5) < 2e-3
     assert o.rebuild_count > 10
+
+
+def test_mie_12_6_argon_reproduces_lj():
+    """Mie_potential 1 with the argon entry (lambda 12-6, eps 1, C = 4, mass 1)
+    is the LJ potential: forces and energies to rounding (real powers against
+    integer powers)."""
+    from helpers import mie_tables
+    r, v, dom, _ = liquid_state([6, 6, 6], 0.8442, 0.722, 2.5, steps=20)
+    lj = O.Oracle(r, v, dom, 2.5, tplot=1, density=0.8442)
+    lj.setup()
+    mie = O.Oracle(r, v, dom, 2.5, tplot=1, density=0.8442)
+    mie.set_mie(mie_tables(2.5, [[1.0]], [[12.0]], [[6.0]], [1.0]), np.ones(len(r), np.int32))
+    mie.setup()
+    np.testing.assert_allclose(mie.a, lj.a, rtol=0, atol=1e-12 * np.abs(lj.a).max())
+    np.testing.assert_allclose(mie.potenergymol, lj.potenergymol, rtol=1e-12, atol=1e-12)
+
+
+def test_mie_mixture_mass_and_records():
+    """Two-type Mie fluid: a = F/m per molecule, and the kinetic record sums
+    are mass-weighted (simulation_record.f90:1236-1252)."""
+    from helpers import mie_mixture_tables
+    r, v, dom, _ = liquid_state([6, 6, 6], 0.8, 1.0, 2.5, steps=10)
+    mt = (np.arange(len(r)) % 2 + 1).astype(np.int32)
+    tab = mie_mixture_tables(2.5)
+    o = O.Oracle(r, v, dom, 2.5, tplot=1, density=0.8)
+    o.set_mie(tab, mt)
+    o.setup()
+    m = tab["mass"][mt - 1]
+    rec = o.macro()
+    assert rec["mv2sum"] == pytest.approx((m[:, None] * v * v).sum(), rel=1e-12)
+    # momentum of the forces: sum m a = 0 (Newton's third law over all pairs)
+    assert np.abs((m[:, None] * o.a).sum(0)).max() < 1e-9 * np.abs(m[:, None] * o.a).max()
