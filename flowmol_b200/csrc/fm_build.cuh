@@ -71,15 +71,48 @@ struct CellSys {
 template <bool POLY>
 struct BuildShared {
     float4 f[NB_STAGE];         // x, y, z offsets and the entry bits in w
+    alignas(16) float ox[32];   // owners' offsets (+1e30 past the last owner),
+    alignas(16) float oy[32];   // read in 8-byte pairs
+    alignas(16) float oz[32];
+    int oi[32];                 // owners' molecule indices
     int2 cs[POLY ? NB_STAGE : 1];  // chain, subchain of candidates
     int off[55];                // candidate offset of segment k (54 segments + total)
     int start[54], code[54];
-    float4 own[32];             // owners' offsets, molecule index in w
     int ochain[POLY ? 32 : 1];
-    int4 obf[POLY ? 32 : 1];
+    alignas(16) int4 obf[POLY ? 32 : 1];
 };
 
 constexpr uint32_t BUILD_OVER_LIST = 1u, BUILD_OVER_BONDS = 2u;
+
+// Packed FP32 pairs (sm_100 f32x2 arithmetic): two owners' distance terms
+// per instruction, each half rounded exactly as the scalar operation.
+__device__ __forceinline__ unsigned long long pack_f32x2(float lo, float hi)
+{
+    return (unsigned long long)__float_as_uint(lo) | ((unsigned long long)__float_as_uint(hi) << 32);
+}
+__device__ __forceinline__ unsigned long long lds_f32x2(const float *p)  // 8-byte aligned
+{
+    return *reinterpret_cast<const unsigned long long *>(p);
+}
+__device__ __forceinline__ unsigned long long sub_f32x2(unsigned long long a, unsigned long long b)
+{
+    unsigned long long d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ unsigned long long mul_f32x2(unsigned long long a, unsigned long long b)
+{
+    unsigned long long d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ unsigned long long fma_f32x2(unsigned long long a, unsigned long long b,
+                                                        unsigned long long c)
+{
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
 
 // Exact FP64 decision of a staged candidate (entry e) for owner io: not the
 // owner itself, and (dx^2+dy^2)+dz^2 < rneighbr2 with the image x_src +/- L.
@@ -184,7 +217,10 @@ __device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY> &sh, i
         int32_t *const row = y.nbr + nb_row(i, maxn);
         const int nown = min(32, ccount - pass * 32);
         __syncwarp();
-        sh.own[lane] = make_float4(xif, yif, zif, __int_as_float(i));
+        sh.ox[lane] = own ? xif : 1e30f;  // far sentinels: r^2 = inf, never a hit
+        sh.oy[lane] = own ? yif : 1e30f;
+        sh.oz[lane] = own ? zif : 1e30f;
+        sh.oi[lane] = i;
         if (POLY) {
             sh.ochain[lane] = own ? y.chain[i] : -1;
             sh.obf[lane] = own ? y.bflag[i] : make_int4(0, 0, 0, 0);
@@ -234,33 +270,41 @@ __device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY> &sh, i
             for (int t0 = 0; t0 < kept; t0 += 32) {
                 const int cq = t0 + lane;
                 const bool valid = cq < kept;
-                const float4 f = sh.f[valid ? cq : 0];
+                // candidate sentinel on the other side: r^2 = inf against every owner
+                const float4 f = valid ? sh.f[cq] : make_float4(-1e30f, -1e30f, -1e30f, 0.f);
                 const int e = __float_as_int(f.w);
+                const unsigned long long fx2 = pack_f32x2(f.x, f.x), fy2 = pack_f32x2(f.y, f.y),
+                                         fz2 = pack_f32x2(f.z, f.z);
                 int2 cs = make_int2(-2, 0);
                 if (POLY && valid) cs = sh.cs[cq];
                 unsigned mine_hits = 0u;  // this lane's owner: which of the 32 candidates hit
-                // owners in groups of NB_OG: independent chains for the scheduler
+                // owners in groups of NB_OG (pairs in packed FP32): independent chains
+                // for the scheduler
                 for (int o0 = 0; o0 < nown; o0 += NB_OG) {
                     bool hit[NB_OG], exact[NB_OG];
-                    int io[NB_OG];
+                    float r2f[NB_OG];
                     bool anyx = false;
 #pragma unroll
+                    for (int h = 0; h < NB_OG; h += 2) {
+                        const unsigned long long dx = sub_f32x2(lds_f32x2(&sh.ox[o0 + h]), fx2);
+                        const unsigned long long dy = sub_f32x2(lds_f32x2(&sh.oy[o0 + h]), fy2);
+                        const unsigned long long dz = sub_f32x2(lds_f32x2(&sh.oz[o0 + h]), fz2);
+                        const unsigned long long t = fma_f32x2(dz, dz, fma_f32x2(dy, dy, mul_f32x2(dx, dx)));
+                        r2f[h] = __uint_as_float((unsigned)t);
+                        r2f[h + 1] = __uint_as_float((unsigned)(t >> 32));
+                    }
+#pragma unroll
                     for (int u = 0; u < NB_OG; u++) {
-                        const float4 ow = sh.own[o0 + u];  // broadcast
-                        io[u] = __float_as_int(ow.w);
-                        const float fx = ow.x - f.x, fy = ow.y - f.y, fz = ow.z - f.z;
-                        const float r2f = fx * fx + fy * fy + fz * fz;
-                        const bool ok = valid && o0 + u < nown;
                         // r2f is exactly 0 for the owner itself (identical operands);
                         // 0 and the band around rneighbr2 are decided in FP64
-                        hit[u] = ok && r2f < lo32 && r2f > 0.f;
-                        exact[u] = ok && !hit[u] && r2f <= hi32;
+                        hit[u] = r2f[u] < lo32 && r2f[u] > 0.f;
+                        exact[u] = !hit[u] && r2f[u] <= hi32;
                         anyx |= exact[u];
                     }
                     if (__any_sync(0xffffffffu, anyx)) {
 #pragma unroll
                         for (int u = 0; u < NB_OG; u++)
-                            if (exact[u]) hit[u] = exact_pair(P, io[u], e, y.L, y.rn2);
+                            if (exact[u]) hit[u] = exact_pair(P, sh.oi[o0 + u], e, y.L, y.rn2);
                     }
 #pragma unroll
                     for (int u = 0; u < NB_OG; u++) {
@@ -273,7 +317,7 @@ __device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY> &sh, i
                         for (int u = 0; u < NB_OG; u++) {
                             bool bond = false;
                             if (valid && o0 + u < nown && cs.x == sh.ochain[o0 + u] &&
-                                !((e & NB_INDEX_MASK) == io[u] && (e >> NB_SHIFT_BITS) == NB_NOSHIFT)) {
+                                !((e & NB_INDEX_MASK) == sh.oi[o0 + u] && (e >> NB_SHIFT_BITS) == NB_NOSHIFT)) {
                                 const int pos = cs.y - 1, grp = pos / 31, ex = pos % 31;
                                 const int4 bf = sh.obf[o0 + u];
                                 const int word = grp == 0 ? bf.x : grp == 1 ? bf.y : grp == 2 ? bf.z : bf.w;
@@ -283,7 +327,7 @@ __device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY> &sh, i
                             const int b0 = __shfl_sync(0xffffffffu, nb, o0 + u);
                             if (bond) {
                                 const int k = b0 + __popc(mb & lt);
-                                if (k < 4) y.bnd[(size_t)io[u] * 4 + k] = e;
+                                if (k < 4) y.bnd[(size_t)sh.oi[o0 + u] * 4 + k] = e;
                             }
                             if (lane == o0 + u) addb = __popc(mb);
                         }
