@@ -470,12 +470,16 @@ __device__ __forceinline__ double epilogue(const EngDev &d, const EngSlot &s, in
 
 constexpr int EF_THREADS = 256;
 
-template <int TPM, int PREC, bool FORCE_ONLY>
-__global__ void __launch_bounds__(EF_THREADS) k_e_force(EngDev d)
+// Two launches per tick: REC false takes the molecules of jobs that do not
+// record this tick (forces only: few registers, full occupancy), REC true the
+// recording ones (PE, virial and the pressure-tensor terms as well).
+template <int TPM, int PREC, bool FORCE_ONLY, bool REC>
+__global__ void __launch_bounds__(EF_THREADS, REC ? 2 : 4) k_e_force(EngDev d)
 {
     constexpr int PER_BLOCK = EF_THREADS / TPM;
     const int lane = threadIdx.x % TPM;
     if (!FORCE_ONLY && !d.flags->any_list) return;
+    if (REC && !d.flags->any_record) return;
     const int hwm = d.flags->mol_hwm;
     for (int base = blockIdx.x * PER_BLOCK; base < hwm; base += gridDim.x * PER_BLOCK) {
         const int i = base + threadIdx.x / TPM;
@@ -483,8 +487,9 @@ __global__ void __launch_bounds__(EF_THREADS) k_e_force(EngDev d)
         const EngSlot *sp = k >= 0 ? &d.slots[k] : nullptr;
         bool act = k >= 0 && sp->mode == MODE_LIST &&
                    (FORCE_ONLY ? (sp->state == SLOT_RUN) : slot_active(*sp));
+        if (!FORCE_ONLY && act && (sp->record != 0) != REC) act = false;
         if (!act) k = -1;
-        const bool rec = act && !FORCE_ONLY && sp->record;
+        const bool rec = REC && act;
         const bool ptens = rec && sp->pressure;
         PairAcc a;
         if (act) {
@@ -780,11 +785,16 @@ void launch_force_t(const EngDev &d, bool force_only, cudaStream_t st)
 {
     const int g = sgrid((long long)d.mol_cap * TPM, EF_THREADS, 8);
     if (force_only) {
-        if (d.precision == 0) k_e_force<TPM, 0, true><<<g, EF_THREADS, 0, st>>>(d);
-        else k_e_force<TPM, 1, true><<<g, EF_THREADS, 0, st>>>(d);
+        if (d.precision == 0) k_e_force<TPM, 0, true, false><<<g, EF_THREADS, 0, st>>>(d);
+        else k_e_force<TPM, 1, true, false><<<g, EF_THREADS, 0, st>>>(d);
     } else {
-        if (d.precision == 0) k_e_force<TPM, 0, false><<<g, EF_THREADS, 0, st>>>(d);
-        else k_e_force<TPM, 1, false><<<g, EF_THREADS, 0, st>>>(d);
+        if (d.precision == 0) {
+            k_e_force<TPM, 0, false, false><<<g, EF_THREADS, 0, st>>>(d);
+            k_e_force<TPM, 0, false, true><<<g, EF_THREADS, 0, st>>>(d);
+        } else {
+            k_e_force<TPM, 1, false, false><<<g, EF_THREADS, 0, st>>>(d);
+            k_e_force<TPM, 1, false, true><<<g, EF_THREADS, 0, st>>>(d);
+        }
     }
 }
 
@@ -801,7 +811,7 @@ void launch_force_any(const EngDev &d, int tpm, bool force_only, cudaStream_t st
 
 }  // namespace
 
-int eng_kernels_per_tick() { return 14; }
+int eng_kernels_per_tick() { return 15; }
 
 void eng_tick(const EngDev &d, int tpm, cudaStream_t st)
 {
