@@ -92,7 +92,14 @@ struct EngDev {
     // record terms and thermostat partials
     double *rterm;        // [mol][RT_N]
     double *tmv2;         // (v + a dt/2)^2 of thermostatted molecules, else 0
+    // per-job reductions split over EY blocks: partial sums [slot][EY][RED_W]
+    // and arrival counters [slot][2] (thermostat, record)
+    double *red_part;
+    int32_t *red_count;
 };
+
+constexpr int EY = 16;      // blocks per job in the thermostat and record reductions
+constexpr int RED_W = 24;   // doubles per partial: (sum, compensation) x up to 11 values, + max
 
 __host__ __device__ inline double4 *eng_pos(const EngDev &d, int pset) { return pset ? d.pos1 : d.pos0; }
 

@@ -534,18 +534,18 @@ __global__ void __launch_bounds__(EF_THREADS, REC ? 2 : 4) k_e_force(EngDev d)
 
 // All pairs with per-axis minimum image for jobs below 3 cells per axis
 // (simulation_compute_forces_LJ_AP, simulation_compute_forces.f90:280-341).
-// Blocks (slot, EAP_YBLOCKS of them), one warp per molecule: lane l takes
-// partners mol_off + l, + 32, ... and the lanes' sums are combined in a fixed
-// order.
+// Blocks (EAP_XBLOCKS x EAP_YBLOCKS; x strides over the slots), one warp per
+// molecule of an all-pairs job: lane l takes partners mol_off + l, + 32, ...
+// and the lanes' sums are combined in a fixed order.
 constexpr int EAP_THREADS = 256;
-constexpr int EAP_YBLOCKS = 16;
+constexpr int EAP_XBLOCKS = 32, EAP_YBLOCKS = 16;
 template <int PREC>
 __global__ void __launch_bounds__(EAP_THREADS) k_e_force_ap(EngDev d)
 {
     if (!d.flags->any_ap) return;
-    const int k = blockIdx.x;
+    for (int k = blockIdx.x; k < d.nslots; k += gridDim.x) {
     const EngSlot &s = d.slots[k];
-    if (s.mode != MODE_ALLPAIRS || !slot_active(s)) return;  // uniform per block
+    if (s.mode != MODE_ALLPAIRS || !slot_active(s)) continue;  // uniform per block
     const int lane = threadIdx.x & 31;
     const double4 *P = eng_pos(d, s.pset);
     const bool rec = s.record, ptens = rec && s.pressure;
@@ -571,6 +571,7 @@ __global__ void __launch_bounds__(EAP_THREADS) k_e_force_ap(EngDev d)
         if (lane == 0) m2 = epilogue(d, s, i, a);
         fold_vmax2(d.slots, lane == 0 ? k : -1, m2);
     }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -579,51 +580,108 @@ __global__ void __launch_bounds__(EAP_THREADS) k_e_force_ap(EngDev d)
 
 constexpr int ER = 256;
 
-// Deterministic block reduction of NV values per thread (fixed order).
+// (s, c) += (s2, c2): Neumaier merge of two compensated partial sums.
+__device__ __forceinline__ void nmerge(double &s, double &c, double s2, double c2)
+{
+    neumaier(s, c, s2);
+    c += c2;
+}
+
+// Compensated sums of NV values over the block, in a fixed tree order (warp
+// xor tree, then the warps in index order); the result is in thread 0.
 template <int NV>
 __device__ __forceinline__ void block_sum(double (&v)[NV], double (&c)[NV])
 {
-    __shared__ double sv[NV][ER], sc[NV][ER];
-    for (int k = 0; k < NV; k++) { sv[k][threadIdx.x] = v[k]; sc[k][threadIdx.x] = c[k]; }
+    __shared__ double sv[NV][ER / 32], sc[NV][ER / 32];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double s2 = __shfl_xor_sync(0xffffffffu, v[k], o), c2 = __shfl_xor_sync(0xffffffffu, c[k], o);
+            nmerge(v[k], c[k], s2, c2);
+        }
+        if (l == 0) { sv[k][w] = v[k]; sc[k][w] = c[k]; }
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
         for (int k = 0; k < NV; k++) {
-            double s = 0.0, cc = 0.0;
-            for (int q = 0; q < ER; q++) {
-                neumaier(s, cc, sv[k][q]);
-                cc += sc[k][q];
-            }
-            v[k] = s + cc;
+            double s = sv[k][0], cc = sc[k][0];
+            for (int q = 1; q < ER / 32; q++) nmerge(s, cc, sv[k][q], sc[k][q]);
+            v[k] = s; c[k] = cc;
         }
     }
     __syncthreads();
 }
 
+// Block y of EY over a job's molecules: [lo, hi) of [mol_off, mol_off + nmol).
+__device__ __forceinline__ void job_chunk(const EngSlot &s, int y, int &lo, int &hi)
+{
+    const int chunk = (s.nmol + EY - 1) / EY;
+    lo = s.mol_off + min(s.nmol, y * chunk);
+    hi = s.mol_off + min(s.nmol, (y + 1) * chunk);
+}
+
+// Publishes block y's NV compensated sums (and a max) for slot k; the last of
+// the EY blocks to arrive merges all partials in y order into (v, c, mx) and
+// returns true (in thread 0 only).  The merge order does not depend on which
+// block arrives last, so the result is deterministic.
+template <int NV>
+__device__ bool job_merge(const EngDev &d, int k, int which, double (&v)[NV], double (&c)[NV], double &mx)
+{
+    __shared__ bool last;
+    double *part = d.red_part + ((size_t)k * EY + blockIdx.y) * RED_W;
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < NV; q++) { part[2 * q] = v[q]; part[2 * q + 1] = c[q]; }
+        part[2 * NV] = mx;
+        __threadfence();
+        const int prev = atomicAdd(&d.red_count[2 * k + which], 1);
+        last = prev == EY - 1;
+    }
+    __syncthreads();
+    if (!last || threadIdx.x != 0) return false;
+    __threadfence();
+    const volatile double *all = d.red_part + (size_t)k * EY * RED_W;
+    for (int q = 0; q < NV; q++) { v[q] = all[2 * q]; c[q] = all[2 * q + 1]; }
+    mx = all[2 * NV];
+    for (int y = 1; y < EY; y++) {
+        const volatile double *py = all + (size_t)y * RED_W;
+        for (int q = 0; q < NV; q++) nmerge(v[q], c[q], py[2 * q], py[2 * q + 1]);
+        mx = fmax(mx, py[2 * NV]);
+    }
+    d.red_count[2 * k + which] = 0;  // ready for the next tick
+    return true;
+}
+
 // Nose-Hoover on thermostatted molecules per region (nthermo = 1, or 2 split
 // at y = 0): Q = N_thermo dt, dzeta/dt = (sum m v^2 - (3 N_thermo + 1) T)/Q.
+// Grid (slot, EY).
 __global__ void __launch_bounds__(ER) k_e_thermo(EngDev d)
 {
     if (!d.flags->any_thermo) return;
-    EngSlot &s = d.slots[blockIdx.x];
+    const int k = blockIdx.x;
+    EngSlot &s = d.slots[k];
     if (!slot_active(s) || s.integrator != 0 || s.nthermo <= 0) return;
     double v[4] = {0, 0, 0, 0}, c[4] = {0, 0, 0, 0};  // mv2 region 0/1, count region 0/1
     const double4 *P = eng_pos(d, s.pset);
-    for (int i = s.mol_off + threadIdx.x; i < s.mol_off + s.nmol; i += ER) {
+    int lo, hi;
+    job_chunk(s, blockIdx.y, lo, hi);
+    for (int i = lo + threadIdx.x; i < hi; i += ER) {
         if (!thermo_tag(d.tag[i])) continue;
         const int tr = (s.nthermo == 2 && !(P[i].y > 0.0)) ? 1 : 0;
         neumaier(v[tr], c[tr], d.tmv2[i]);
         neumaier(v[2 + tr], c[2 + tr], 1.0);
     }
     block_sum<4>(v, c);
-    if (threadIdx.x == 0) {
-        for (int r = 0; r < s.nthermo; r++) {
-            const double np_t = v[2 + r];
-            const double Q = 1.0 * np_t * d.dt;
-            const double dzeta = np_t > 0.0 ? (v[r] - (3.0 * np_t + 1.0) * s.therm_T[r]) / Q : 0.0;
-            s.zeta[r] = s.zeta[r] + d.dt * dzeta;
-            s.bscale[r] = 1.0 / (1.0 + 0.5 * d.dt * s.zeta[r]);
-            s.ascale[r] = (1.0 - 0.5 * d.dt * s.zeta[r]) * s.bscale[r];
-        }
+    double mx = 0.0;
+    if (!job_merge<4>(d, k, 0, v, c, mx)) return;
+    for (int r = 0; r < s.nthermo; r++) {
+        const double np_t = v[2 + r] + c[2 + r];
+        const double Q = 1.0 * np_t * d.dt;
+        const double dzeta = np_t > 0.0 ? ((v[r] + c[r]) - (3.0 * np_t + 1.0) * s.therm_T[r]) / Q : 0.0;
+        s.zeta[r] = s.zeta[r] + d.dt * dzeta;
+        s.bscale[r] = 1.0 / (1.0 + 0.5 * d.dt * s.zeta[r]);
+        s.ascale[r] = (1.0 - 0.5 * d.dt * s.zeta[r]) * s.bscale[r];
     }
 }
 
@@ -684,49 +742,56 @@ __global__ void k_e_move_lfv(EngDev d)
     }
 }
 
+// The record of every recording job (evaluate_macroscopic_properties,
+// simulation_record.f90:1205-1314) and its pressure-tensor sample
+// (cumulative_pressure, :3151-3205).  Grid (slot, EY).
 __global__ void __launch_bounds__(ER) k_e_record(EngDev d)
 {
     if (!d.flags->any_record) return;
-    EngSlot &s = d.slots[blockIdx.x];
+    const int k = blockIdx.x;
+    EngSlot &s = d.slots[k];
     if (!slot_active(s) || !s.record) return;
-    double v[RT_N + 1], c[RT_N + 1];
-    for (int k = 0; k <= RT_N; k++) { v[k] = 0.0; c[k] = 0.0; }
+    double v[RT_N], c[RT_N];
+    for (int q = 0; q < RT_N; q++) { v[q] = 0.0; c[q] = 0.0; }
     double pemax = 0.0;
     const int nterm = s.pressure ? RT_N : RT_VSUM + 1;
-    for (int i = s.mol_off + threadIdx.x; i < s.mol_off + s.nmol; i += ER) {
+    int lo, hi;
+    job_chunk(s, blockIdx.y, lo, hi);
+    for (int i = lo + threadIdx.x; i < hi; i += ER) {
         const double *t = d.rterm + (size_t)i * RT_N;
-        for (int k = 0; k < nterm; k++) neumaier(v[k], c[k], t[k]);
+        for (int q = 0; q < nterm; q++) neumaier(v[q], c[q], t[q]);
         pemax = fmax(pemax, t[RT_PE]);
     }
     __shared__ double smax[ER];
     smax[threadIdx.x] = pemax;
-    block_sum<RT_N + 1>(v, c);
-    if (threadIdx.x == 0) {
+    block_sum<RT_N>(v, c);
+    if (threadIdx.x == 0)
         for (int q = 1; q < ER; q++) pemax = fmax(pemax, smax[q]);
-        const double gnp = (double)s.nmol;
-        FmRecord r;
-        r.iter = s.iter;
-        r.pad_ = 0;
-        r.simtime = s.simtime;
-        r.vsum = v[RT_VSUM];
-        r.mv2sum = v[RT_MV2];
-        r.virial = v[RT_VIR];
-        r.kinenergy = (0.5 * r.mv2sum) / gnp;
-        r.potenergy = (0.5 * v[RT_PE]) / gnp;
-        r.totenergy = r.kinenergy + r.potenergy;
-        r.temperature = r.mv2sum / (3.0 * gnp);
-        r.pressure = (s.density / (gnp * 3.0)) * (r.mv2sum + r.virial / 2.0);
-        s.last_rec = r;
-        if (s.pressure) {
-            const double V = s.volume;
-            s.ptensor[0] += v[RT_PXX] / V; s.ptensor[4] += v[RT_PYY] / V; s.ptensor[8] += v[RT_PZZ] / V;
-            s.ptensor[1] += v[RT_PXY] / V; s.ptensor[3] += v[RT_PXY] / V;
-            s.ptensor[2] += v[RT_PXZ] / V; s.ptensor[6] += v[RT_PXZ] / V;
-            s.ptensor[5] += v[RT_PYZ] / V; s.ptensor[7] += v[RT_PYZ] / V;
-        }
-        s.nsamples += 1;
-        if (pemax > 10000.0) slot_fail(&s, ST_PE, s.iter);
+    if (!job_merge<RT_N>(d, k, 1, v, c, pemax)) return;
+    for (int q = 0; q < RT_N; q++) v[q] = v[q] + c[q];
+    const double gnp = (double)s.nmol;
+    FmRecord r;
+    r.iter = s.iter;
+    r.pad_ = 0;
+    r.simtime = s.simtime;
+    r.vsum = v[RT_VSUM];
+    r.mv2sum = v[RT_MV2];
+    r.virial = v[RT_VIR];
+    r.kinenergy = (0.5 * r.mv2sum) / gnp;
+    r.potenergy = (0.5 * v[RT_PE]) / gnp;
+    r.totenergy = r.kinenergy + r.potenergy;
+    r.temperature = r.mv2sum / (3.0 * gnp);
+    r.pressure = (s.density / (gnp * 3.0)) * (r.mv2sum + r.virial / 2.0);
+    s.last_rec = r;
+    if (s.pressure) {
+        const double V = s.volume;
+        s.ptensor[0] += v[RT_PXX] / V; s.ptensor[4] += v[RT_PYY] / V; s.ptensor[8] += v[RT_PZZ] / V;
+        s.ptensor[1] += v[RT_PXY] / V; s.ptensor[3] += v[RT_PXY] / V;
+        s.ptensor[2] += v[RT_PXZ] / V; s.ptensor[6] += v[RT_PXZ] / V;
+        s.ptensor[5] += v[RT_PYZ] / V; s.ptensor[7] += v[RT_PYZ] / V;
     }
+    s.nsamples += 1;
+    if (pemax > 10000.0) slot_fail(&s, ST_PE, s.iter);
 }
 
 // ---------------------------------------------------------------------------
@@ -826,12 +891,12 @@ void eng_tick(const EngDev &d, int tpm, cudaStream_t st)
     k_e_reorder_copy<<<gm, 256, 0, st>>>(d);
     k_e_build<<<sgrid(d.cell_cap, NB_WARPS, 6), NB_THREADS, 0, st>>>(d);  // one resident wave
     launch_force_any(d, tpm, false, st);
-    const dim3 gap(d.nslots, EAP_YBLOCKS);
+    const dim3 gap(std::min(d.nslots, EAP_XBLOCKS), EAP_YBLOCKS);
     if (d.precision == 0) k_e_force_ap<0><<<gap, EAP_THREADS, 0, st>>>(d);
     else k_e_force_ap<1><<<gap, EAP_THREADS, 0, st>>>(d);
-    k_e_thermo<<<d.nslots, ER, 0, st>>>(d);
+    k_e_thermo<<<dim3(d.nslots, EY), ER, 0, st>>>(d);
     k_e_move_lfv<<<gm, 256, 0, st>>>(d);
-    k_e_record<<<d.nslots, ER, 0, st>>>(d);
+    k_e_record<<<dim3(d.nslots, EY), ER, 0, st>>>(d);
 }
 
 void eng_force_only(const EngDev &d, int tpm, cudaStream_t st) { launch_force_any(d, tpm, true, st); }
