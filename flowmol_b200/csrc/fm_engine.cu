@@ -147,7 +147,8 @@ void free_all(fm_engine *e)
     void *ptrs[] = {d.slots, d.flags, d.pos0, d.pos1, d.vx, d.vy, d.vz, d.ax, d.ay, d.az, d.slot_of, d.uidx, d.tag,
                     d.rteth, d.slidev, d.tpos, d.trteth, d.tslidev, d.tvx, d.tvy, d.tvz, d.tax, d.tay, d.taz,
                     d.tuidx, d.ttag, d.cell_slot, d.cell_of, d.cell_count, d.cell_start, d.perm, d.nbr, d.nnbr,
-                    d.rterm, d.tmv2, d.red_part, d.red_count, e->stage, e->stage_i};
+                    d.rterm, d.tmv2, d.red_part, d.red_count, d.rb_slot, d.rb_mpre, d.rb_cpre, e->stage,
+                    e->stage_i};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     if (e->graph) cudaGraphExecDestroy(e->graph);
@@ -472,6 +473,7 @@ extern "C" int fm_engine_create(const fm_engine_params *p, fm_engine **out)
     EA(d.cell_slot, Cc) EA(d.cell_of, M) EA(d.cell_count, Cc) EA(d.cell_start, Cc + (size_t)d.nslots)
     EA(d.perm, M) EA(d.nbr, p->max_list_entries) EA(d.nnbr, M) EA(d.rterm, M * fm::RT_N) EA(d.tmv2, M)
     EA(d.red_part, (size_t)d.nslots * fm::EY * fm::RED_W) EA(d.red_count, (size_t)d.nslots * 2)
+    EA(d.rb_slot, (size_t)d.nslots + 1) EA(d.rb_mpre, (size_t)d.nslots + 1) EA(d.rb_cpre, (size_t)d.nslots + 1)
 #undef EA
     if (rc != FM_OK) {
         free_all(e);

@@ -58,6 +58,8 @@ struct EngSlot {
 struct EngFlags {
     int any_rebuild, any_list, any_ap, any_lfv, any_thermo, any_record;
     int mol_hwm, cell_hwm;
+    // this tick's rebuilding jobs (slot order): count, their molecules, their cells
+    int rb_n, rb_mtot, rb_ctot, pad_;
 };
 
 struct EngDev {
@@ -96,6 +98,9 @@ struct EngDev {
     // and arrival counters [slot][2] (thermostat, record)
     double *red_part;
     int32_t *red_count;
+    // rebuild work list of the tick: slots, and prefix sums of their molecules
+    // and cells ([rb_n + 1] each), so the rebuild kernels visit only those
+    int32_t *rb_slot, *rb_mpre, *rb_cpre;
 };
 
 constexpr int EY = 16;      // blocks per job in the thermostat and record reductions

@@ -115,6 +115,8 @@ __device__ void decide_slot(const EngDev &d, EngSlot &s)
     if (vv) s.simtime = s.simtime + d.dt;        // simulation_move_particles_vv.f90:191
 }
 
+__device__ __forceinline__ bool slot_rebuilding(const EngSlot &s) { return slot_active(s) && s.rebuild; }
+
 constexpr int EDEC = 1024;
 __global__ void __launch_bounds__(EDEC) k_e_decide(EngDev d)
 {
@@ -138,23 +140,91 @@ __global__ void __launch_bounds__(EDEC) k_e_decide(EngDev d)
         d.flags->any_rebuild = f[0]; d.flags->any_list = f[1]; d.flags->any_ap = f[2];
         d.flags->any_lfv = f[3]; d.flags->any_thermo = f[4]; d.flags->any_record = f[5];
     }
+    // rebuild work list in slot order: a block scan of (flag, molecules, cells)
+    __shared__ int wsum[3][EDEC / 32];
+    __shared__ int carry[3];
+    if (threadIdx.x < 3) carry[threadIdx.x] = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int base = 0; base < d.nslots; base += EDEC) {
+        const int k = base + threadIdx.x;
+        int x[3] = {0, 0, 0};
+        if (k < d.nslots) {
+            const EngSlot &s = d.slots[k];
+            if (slot_rebuilding(s)) {
+                x[0] = 1;
+                x[1] = s.nmol;
+                x[2] = s.mode == MODE_LIST ? s.ncell : 0;
+            }
+        }
+        int incl[3];
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            incl[q] = x[q];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, incl[q], o);
+                if (lane >= o) incl[q] += t;
+            }
+            if (lane == 31) wsum[q][w] = incl[q];
+        }
+        __syncthreads();
+        if (w == 0) {
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                const int v = wsum[q][lane];
+                int vi = v;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(0xffffffffu, vi, o);
+                    if (lane >= o) vi += t;
+                }
+                wsum[q][lane] = vi - v;  // exclusive warp offsets
+            }
+        }
+        __syncthreads();
+        if (x[0]) {
+            const int pos = carry[0] + wsum[0][w] + incl[0] - 1;
+            d.rb_slot[pos] = k;
+            d.rb_mpre[pos] = carry[1] + wsum[1][w] + incl[1] - x[1];
+            d.rb_cpre[pos] = carry[2] + wsum[2][w] + incl[2] - x[2];
+        }
+        __syncthreads();
+        if (threadIdx.x == EDEC - 1)
+            for (int q = 0; q < 3; q++) carry[q] += wsum[q][w] + incl[q];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        d.rb_mpre[carry[0]] = carry[1];
+        d.rb_cpre[carry[0]] = carry[2];
+        d.flags->rb_n = carry[0];
+        d.flags->rb_mtot = carry[1];
+        d.flags->rb_ctot = carry[2];
+    }
+}
+
+// Grid-stride over the tick's rebuild work list: element g of [0, total) is
+// entry r (advanced as g grows) at offset g - pre[r].
+__device__ __forceinline__ int rb_entry(const int32_t *pre, int g, int &r)
+{
+    while (g >= pre[r + 1]) r++;
+    return g - pre[r];
 }
 
 // ---------------------------------------------------------------------------
 // rebuild pipeline (gated per slot)
 // ---------------------------------------------------------------------------
 
-__device__ __forceinline__ bool slot_rebuilding(const EngSlot &s) { return slot_active(s) && s.rebuild; }
 
 __global__ void k_e_wrap_bin(EngDev d)
 {
     if (!d.flags->any_rebuild) return;
-    const int hwm = d.flags->mol_hwm;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < hwm; i += gridDim.x * blockDim.x) {
-        const int k = d.slot_of[i];
-        if (k < 0) continue;
-        EngSlot &s = d.slots[k];
-        if (!slot_rebuilding(s)) continue;
+    const int tot = d.flags->rb_mtot;
+    int r = 0;
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < tot; g += gridDim.x * blockDim.x) {
+        const int off = rb_entry(d.rb_mpre, g, r);
+        EngSlot &s = d.slots[d.rb_slot[r]];
+        const int i = s.mol_off + off;
         double4 *P = eng_pos(d, s.pset);
         double4 p = P[i];
         if (s.wrap) {
@@ -235,12 +305,13 @@ __global__ void __launch_bounds__(ESCAN) k_e_scan(EngDev d)
 __global__ void k_e_scatter(EngDev d)
 {
     if (!d.flags->any_rebuild) return;
-    const int hwm = d.flags->mol_hwm;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < hwm; i += gridDim.x * blockDim.x) {
-        const int k = d.slot_of[i];
-        if (k < 0) continue;
-        const EngSlot &s = d.slots[k];
-        if (!slot_rebuilding(s) || s.mode != MODE_LIST) continue;
+    const int tot = d.flags->rb_mtot;
+    int r = 0;
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < tot; g += gridDim.x * blockDim.x) {
+        const int off = rb_entry(d.rb_mpre, g, r);
+        const EngSlot &s = d.slots[d.rb_slot[r]];
+        if (s.mode != MODE_LIST) continue;
+        const int i = s.mol_off + off;
         const int c = d.cell_of[i];
         const int slot = d.cell_start[s.cstart_off + (c - s.cell_off)] + atomicAdd(&d.cell_count[c], 1);
         d.perm[slot] = i;
@@ -250,13 +321,12 @@ __global__ void k_e_scatter(EngDev d)
 __global__ void k_e_sort(EngDev d)
 {
     if (!d.flags->any_rebuild) return;
-    const int hwm = d.flags->cell_hwm;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < hwm; c += gridDim.x * blockDim.x) {
-        const int k = d.cell_slot[c];
-        if (k < 0) continue;
-        const EngSlot &s = d.slots[k];
-        if (!slot_rebuilding(s) || s.mode != MODE_LIST) continue;
-        const int lc = c - s.cell_off;
+    const int tot = d.flags->rb_ctot;
+    int r = 0;
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < tot; g += gridDim.x * blockDim.x) {
+        const int lc = rb_entry(d.rb_cpre, g, r);
+        const EngSlot &s = d.slots[d.rb_slot[r]];
+        const int c = s.cell_off + lc;
         const int b = d.cell_start[s.cstart_off + lc], e = d.cell_start[s.cstart_off + lc + 1];
         for (int x = b + 1; x < e; x++) {
             int key = d.perm[x];
@@ -274,12 +344,13 @@ __global__ void k_e_sort(EngDev d)
 __global__ void k_e_reorder_gather(EngDev d)
 {
     if (!d.flags->any_rebuild) return;
-    const int hwm = d.flags->mol_hwm;
-    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < hwm; n += gridDim.x * blockDim.x) {
-        const int k = d.slot_of[n];
-        if (k < 0) continue;
-        const EngSlot &s = d.slots[k];
-        if (!slot_rebuilding(s) || s.mode != MODE_LIST) continue;
+    const int tot = d.flags->rb_mtot;
+    int r = 0;
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < tot; g += gridDim.x * blockDim.x) {
+        const int off = rb_entry(d.rb_mpre, g, r);
+        const EngSlot &s = d.slots[d.rb_slot[r]];
+        if (s.mode != MODE_LIST) continue;
+        const int n = s.mol_off + off;
         const int o = d.perm[n];
         d.tpos[n] = eng_pos(d, s.pset)[o];
         d.tvx[n] = d.vx[o]; d.tvy[n] = d.vy[o]; d.tvz[n] = d.vz[o];
@@ -294,12 +365,13 @@ __global__ void k_e_reorder_gather(EngDev d)
 __global__ void k_e_reorder_copy(EngDev d)
 {
     if (!d.flags->any_rebuild) return;
-    const int hwm = d.flags->mol_hwm;
-    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < hwm; n += gridDim.x * blockDim.x) {
-        const int k = d.slot_of[n];
-        if (k < 0) continue;
-        const EngSlot &s = d.slots[k];
-        if (!slot_rebuilding(s) || s.mode != MODE_LIST) continue;
+    const int tot = d.flags->rb_mtot;
+    int r = 0;
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < tot; g += gridDim.x * blockDim.x) {
+        const int off = rb_entry(d.rb_mpre, g, r);
+        const EngSlot &s = d.slots[d.rb_slot[r]];
+        if (s.mode != MODE_LIST) continue;
+        const int n = s.mol_off + off;
         eng_pos(d, s.pset)[n] = d.tpos[n];
         d.vx[n] = d.tvx[n]; d.vy[n] = d.tvy[n]; d.vz[n] = d.tvz[n];
         d.ax[n] = d.tax[n]; d.ay[n] = d.tay[n]; d.az[n] = d.taz[n];
@@ -319,14 +391,13 @@ __global__ void __launch_bounds__(NB_THREADS, 6) k_e_build(EngDev d)
     __shared__ BuildShared<false> sh[NB_WARPS];
     __shared__ CellSys ys[NB_WARPS];  // the cell's job, read through shared memory
     if (!d.flags->any_rebuild) return;
-    const int hwm = d.flags->cell_hwm;
-    for (int c = blockIdx.x * NB_WARPS + warp; c < hwm; c += gridDim.x * NB_WARPS) {
-        const int k = d.cell_slot[c];
-        if (k < 0) continue;
-        EngSlot &s = d.slots[k];
-        if (!slot_rebuilding(s) || s.mode != MODE_LIST) continue;
+    const int tot = d.flags->rb_ctot;
+    int r = 0, r_loaded = -1;
+    for (int g = blockIdx.x * NB_WARPS + warp; g < tot; g += gridDim.x * NB_WARPS) {
+        const int lc = rb_entry(d.rb_cpre, g, r);
+        EngSlot &s = d.slots[d.rb_slot[r]];
         __syncwarp();
-        if (lane == 0) {
+        if (r != r_loaded && lane == 0) {
             CellSys &y = ys[warp];
             y.P = eng_pos(d, s.pset) + s.mol_off;
             y.cell_start = d.cell_start + s.cstart_off;
@@ -342,7 +413,8 @@ __global__ void __launch_bounds__(NB_THREADS, 6) k_e_build(EngDev d)
             y.bnd = y.nbond = nullptr;
         }
         __syncwarp();
-        const uint32_t over = build_cell<false>(ys[warp], c - s.cell_off, sh[warp], lane);
+        r_loaded = r;
+        const uint32_t over = build_cell<false>(ys[warp], lc, sh[warp], lane);
         if (lane == 0 && (over & BUILD_OVER_LIST)) slot_fail(&s, ST_NLIST, s.iter);
     }
 }
