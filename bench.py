@@ -476,9 +476,10 @@ def main():
                     help="NVE drift run of the 1M fluid per precision form (0: skip)")
     ap.add_argument("--tpm", type=int, default=0,
                     help="force-kernel lanes per molecule (0: the autotuner's choice)")
-    ap.add_argument("--profile-case", choices=["fp32", "fp64", "batched"], default=None,
+    ap.add_argument("--profile-case", choices=["fp32", "fp64", "batched", "fene"], default=None,
                     help="profiling workload, no timing: setup + 10 fused steps of the 1M system "
-                         "(fp32, fp64), or the batched replicas for --batch-steps steps")
+                         "(fp32, fp64) or of the FENE melt (fene), or the batched replicas for "
+                         "--batch-steps steps")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -519,6 +520,20 @@ def main():
         bad = [x for x in e.results() if x["status"] != 0]
         print(json.dumps({"profile_case": "batched", "molecules": tot, "failed": len(bad), **e.counters()}))
         e.close()
+        return
+    if args.profile_case == "fene":
+        from flowmol_b200 import polymer
+        r, v, ch, sub, _fy, bf, dom = polymer.fene_melt(FENE_CHAINS, FENE_BEADS, FENE_DENSITY)
+        p = api.make_params(len(r), dom, 2.0 ** (1.0 / 6.0), (SKIN,) * 3, DT, TPLOT, density=FENE_DENSITY,
+                            precision=api.PRECISION_FP32, potential_flag=1, k_c=FENE_K, R_0=FENE_R0,
+                            threads_per_molecule=args.tpm)
+        s = api.MDSystem(p)
+        s.upload(r, v)
+        s.upload_monomers(ch, sub, bf)
+        s.setup()
+        s.simulation_md(10, blocking=True)
+        print(json.dumps({"profile_case": "fene", "beads": len(r), **s.counters()}))
+        s.close()
         return
     if args.profile_case:
         r, v, dom = make_state()

@@ -36,18 +36,22 @@ __device__ __forceinline__ double warp_max(double v)
     return v;
 }
 
+// Float min/max over the warp with one integer reduction each: the bit
+// pattern with the magnitude bits flipped for negatives orders like the
+// float (finite values).
+__device__ __forceinline__ int float_order_key(float v)
+{
+    const int b = __float_as_int(v);
+    return b ^ ((b >> 31) & 0x7fffffff);
+}
+__device__ __forceinline__ float float_from_order_key(int k) { return __int_as_float(k ^ ((k >> 31) & 0x7fffffff)); }
 __device__ __forceinline__ float warp_min(float v)
 {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
+    return float_from_order_key(__reduce_min_sync(0xffffffffu, float_order_key(v)));
 }
-
 __device__ __forceinline__ float warp_max(float v)
 {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
+    return float_from_order_key(__reduce_max_sync(0xffffffffu, float_order_key(v)));
 }
 
 // icell = ceiling((r + halfdomain)/cellsidelength) + 1 (1-based, halo = 1 and
