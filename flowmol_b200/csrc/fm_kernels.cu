@@ -355,7 +355,7 @@ __global__ void k_reorder_copy(FmDev d, int gated, const double4 *tpos, const in
 // Neighbour rows of every extended cell, one warp per cell (grid-stride);
 // the per-cell routine and its pair-set argument are in fm_build.cuh.
 template <bool POLY>
-__global__ void __launch_bounds__(NB_THREADS, 6) k_build_nlist(FmDev d, int gated, int iter)
+__global__ void __launch_bounds__(NB_THREADS, 8) k_build_nlist(FmDev d, int gated, int iter)
 {
     if (!gate(d, gated)) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
