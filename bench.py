@@ -476,10 +476,10 @@ def main():
                     help="NVE drift run of the 1M fluid per precision form (0: skip)")
     ap.add_argument("--tpm", type=int, default=0,
                     help="force-kernel lanes per molecule (0: the autotuner's choice)")
-    ap.add_argument("--profile-case", choices=["fp32", "fp64", "batched", "fene"], default=None,
+    ap.add_argument("--profile-case", choices=["fp32", "fp64", "batched", "fene", "served"], default=None,
                     help="profiling workload, no timing: setup + 10 fused steps of the 1M system "
-                         "(fp32, fp64) or of the FENE melt (fene), or the batched replicas for "
-                         "--batch-steps steps")
+                         "(fp32, fp64) or of the FENE melt (fene), the batched replicas for "
+                         "--batch-steps steps, or --serve-jobs served jobs")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -520,6 +520,10 @@ def main():
         bad = [x for x in e.results() if x["status"] != 0]
         print(json.dumps({"profile_case": "batched", "molecules": tot, "failed": len(bad), **e.counters()}))
         e.close()
+        return
+    if args.profile_case == "served":
+        out = run_served(api, torch, dev, args.serve_jobs)
+        print(json.dumps({"profile_case": "served", "jobs": out["jobs"], "failed": out["failed"]}))
         return
     if args.profile_case == "fene":
         from flowmol_b200 import polymer
