@@ -49,7 +49,7 @@ class FmParams(C.Structure):
         ("nlist_capacity", C.c_int32),
         ("threads_per_molecule", C.c_int32),
         ("integration_algorithm", C.c_int32),
-        ("pad_", C.c_int32),
+        ("list_build", C.c_int32),
     ]
 
 
@@ -80,6 +80,7 @@ class FmMieTables(C.Structure):
                                              "k_harmonic", "r0")]
 
 
+LIST_BUILD_AUTO, LIST_BUILD_CELLS, LIST_BUILD_BLOCKS = 0, 1, 2
 MIE_TABLE_KEYS = ("epsilon", "lambdar", "lambdaa", "C", "alpha", "potshift", "k_harmonic", "r0")
 
 
@@ -265,7 +266,8 @@ def _dp(a):
 def make_params(np_, domain, rcutoff, delta_rneighbr=(0.3, 0.3, 0.3), delta_t=0.005, tplot=100,
                 density=None, initialstep=0, simtime=0.0, force_list=FORCE_LIST_HALF, potential_flag=0,
                 rebuild_criteria=0, fixed_rebuild=1, sLRC_flag=0, precision=PRECISION_FP64, k_c=30.0,
-                R_0=1.5, nlist_capacity=0, threads_per_molecule=0, integration_algorithm=1) -> FmParams:
+                R_0=1.5, nlist_capacity=0, threads_per_molecule=0, integration_algorithm=1,
+                list_build=0) -> FmParams:
     p = FmParams()
     p.np = int(np_)
     for k in range(3):
@@ -288,6 +290,7 @@ def make_params(np_, domain, rcutoff, delta_rneighbr=(0.3, 0.3, 0.3), delta_t=0.
     p.nlist_capacity = int(nlist_capacity)
     p.threads_per_molecule = int(threads_per_molecule)
     p.integration_algorithm = int(integration_algorithm)
+    p.list_build = int(list_build)
     return p
 
 

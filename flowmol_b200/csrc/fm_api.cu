@@ -197,6 +197,9 @@ extern "C" int fm_create(const fm_params *p, fm_handle **out)
     if (!(p->delta_t > 0.0)) return fail(FM_ERR_ARG, "delta_t must be > 0");
     if (p->force_list != 0 && p->force_list != 2 && p->force_list != 3)
         return fail(FM_ERR_ARG, "force_list must be 0, 2 or 3");
+    if (p->list_build != FM_LIST_BUILD_AUTO && p->list_build != FM_LIST_BUILD_CELLS &&
+        p->list_build != FM_LIST_BUILD_BLOCKS)
+        return fail(FM_ERR_ARG, "list_build must be FM_LIST_BUILD_AUTO, _CELLS or _BLOCKS");
     if (p->precision != FM_PRECISION_FP64 && p->precision != FM_PRECISION_FP32)
         return fail(FM_ERR_ARG, "precision must be FM_PRECISION_FP64 or FM_PRECISION_FP32");
     if (p->potential_flag != 0 && p->potential_flag != 1) return fail(FM_ERR_ARG, "potential_flag must be 0 or 1");
@@ -252,6 +255,11 @@ extern "C" int fm_create(const fm_params *p, fm_handle **out)
 
     double rho = (double)p->np / (p->domain[0] * p->domain[1] * p->domain[2]);
     double expected = 4.0 / 3.0 * kPi * std::pow(std::sqrt(rn2), 3) * std::max(rho, 0.25);
+    // sparse cells (a few molecules each) are built 2x2x2 at a time: same rows,
+    // the per-cell latency shared by eight cells
+    const double per_cell = rho * d.cs[0] * d.cs[1] * d.cs[2];
+    d.build_blocks = p->list_build == FM_LIST_BUILD_BLOCKS ? 1
+                     : p->list_build == FM_LIST_BUILD_CELLS ? 0 : (per_cell < 8.0 ? 1 : 0);
     int tpm = pick_tpm(*p, expected);
     if (tpm < 0) { delete h; return fail(FM_ERR_ARG, "threads_per_molecule must be 0, 1, 2, 4, 8 or 16"); }
     h->tpm = tpm;

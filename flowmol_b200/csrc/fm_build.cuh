@@ -357,4 +357,301 @@ __device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY> &sh, i
     return over;
 }
 
+// ---------------------------------------------------------------------------
+// Sparse systems (few molecules per cell, e.g. WCA or FENE at r_n ~ 1.4-1.5):
+// one warp per block of 2x2x2 cells.  The candidates of the union of the
+// owners' neighbourhoods (4x4x4 cells, each real then images, in (z, y, x)
+// cell order) are staged once; each owner accepts only the candidates of its
+// own 27 cells (not both halo), so its row is exactly build_cell's row, in the
+// same order (the owner's cells are a sub-box of the union, visited in the same
+// lexicographic order).
+// ---------------------------------------------------------------------------
+
+constexpr int NB_BSEG = 128;  // 64 union cells x (real, images)
+
+template <bool POLY>
+struct BlockShared {
+    float4 f[NB_STAGE];             // candidate offsets from the block centre, entry bits in w
+    alignas(16) float ox[32];       // owners (+1e30 past the last owner)
+    alignas(16) float oy[32];
+    alignas(16) float oz[32];
+    int oi[32];
+    unsigned oallow[32];            // one-hot bit of the owner's cell in the block, 0 past the last
+    unsigned char allow[NB_STAGE];  // owner cells a staged candidate may pair with
+    int2 cs[POLY ? NB_STAGE : 1];
+    int off[NB_BSEG + 1];
+    int start[NB_BSEG], code[NB_BSEG];
+    unsigned char segallow[NB_BSEG];
+    int opre[9], ostart[8];         // owners by block cell: prefix counts, first molecule
+    int ochain[POLY ? 32 : 1];
+    alignas(16) int4 obf[POLY ? 32 : 1];
+};
+
+template <bool POLY>
+__device__ uint32_t build_block(const CellSys &y, int blk, BlockShared<POLY> &sh, int lane)
+{
+    const int ne0 = y.ne[0], ne1 = y.ne[1], ne2 = y.ne[2];
+    const int nb0 = (ne0 + 1) / 2, nb1 = (ne1 + 1) / 2;
+    const int bx0 = 2 * (blk % nb0), by0 = 2 * ((blk / nb0) % nb1), bz0 = 2 * (blk / (nb0 * nb1));
+    const unsigned lt = (1u << lane) - 1u;
+    const double4 *P = y.P;
+    const int maxn = y.maxn;
+
+    // --- the block's owner cells (lanes 0..7: a + 2b + 4c) ---
+    int ocount = 0, ostart = 0;
+    bool ohalo = false;
+    if (lane < 8) {
+        const int x = bx0 + (lane & 1), yy = by0 + ((lane >> 1) & 1), z = bz0 + (lane >> 2);
+        if (x < ne0 && yy < ne1 && z < ne2) {
+            const int c = x + ne0 * (yy + ne1 * z);
+            ostart = y.cell_start[c] - y.mol_off;
+            ocount = y.cell_start[c + 1] - y.mol_off - ostart;
+            ohalo = is_halo(x, ne0) || is_halo(yy, ne1) || is_halo(z, ne2);
+        }
+    }
+    int oincl = ocount;
+#pragma unroll
+    for (int o = 1; o < 8; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, oincl, o);
+        if (lane >= o) oincl += t;
+    }
+    const int nowners = __shfl_sync(0xffffffffu, oincl, 7);
+    if (nowners == 0) return 0u;  // uniform across the warp
+    const unsigned ohalo_bits = __ballot_sync(0xffffffffu, lane < 8 && ohalo) & 0xffu;
+    __syncwarp();
+    if (lane < 8) { sh.opre[lane + 1] = oincl; sh.ostart[lane] = ostart; }
+    if (lane == 0) sh.opre[0] = 0;
+
+    const double csmax = fmax(y.cs[0], fmax(y.cs[1], y.cs[2]));
+    const float band = (float)(1e-4 * csmax * csmax) + 1e-6f;
+    const float lo32 = (float)y.rn2 - band, hi32 = (float)y.rn2 + band;
+    const float prune2 = (float)(y.rn2 * 1.0001 + 1e-4);
+    const double refx = bx0 * y.cs[0] - y.hd[0];  // centre of the 2x2x2 block
+    const double refy = by0 * y.cs[1] - y.hd[1];
+    const double refz = bz0 * y.cs[2] - y.hd[2];
+
+    // --- segments of the union cells u = lane and u = lane + 32 ---
+    int seg_n[4], seg_b[4], seg_code[4];
+    unsigned seg_allow[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int u = lane + 32 * h;
+        const int ux = u & 3, uy = (u >> 2) & 3, uz = u >> 4;
+        const int x2 = bx0 - 1 + ux, y2 = by0 - 1 + uy, z2 = bz0 - 1 + uz;
+        seg_n[2 * h] = seg_n[2 * h + 1] = 0;
+        seg_b[2 * h] = seg_b[2 * h + 1] = 0;
+        seg_code[2 * h] = seg_code[2 * h + 1] = NB_NOSHIFT;
+        seg_allow[h] = 0u;
+        if (x2 >= 0 && y2 >= 0 && z2 >= 0 && x2 < ne0 && y2 < ne1 && z2 < ne2) {
+            const bool h2 = is_halo(x2, ne0) || is_halo(y2, ne1) || is_halo(z2, ne2);
+            // owner cells (a, b, c) whose 27 neighbours include u, not both halo
+            unsigned al = 0u;
+#pragma unroll
+            for (int oc = 0; oc < 8; oc++) {
+                const int a = oc & 1, b = (oc >> 1) & 1, cc = oc >> 2;
+                const bool adj = ux >= a && ux <= a + 2 && uy >= b && uy <= b + 2 && uz >= cc && uz <= cc + 2;
+                if (adj && !(h2 && ((ohalo_bits >> oc) & 1u))) al |= 1u << oc;
+            }
+            seg_allow[h] = al;
+            if (al) {
+                const int c2 = x2 + ne0 * (y2 + ne1 * z2);
+                seg_b[2 * h] = y.cell_start[c2] - y.mol_off;
+                seg_n[2 * h] = y.cell_start[c2 + 1] - y.mol_off - seg_b[2 * h];
+                if (h2) {
+                    // images of the interior cell on the far side, as in build_cell
+                    const int ssx = x2 == 0 ? -1 : (x2 == ne0 - 1 ? 1 : 0);
+                    const int ssy = y2 == 0 ? -1 : (y2 == ne1 - 1 ? 1 : 0);
+                    const int ssz = z2 == 0 ? -1 : (z2 == ne2 - 1 ? 1 : 0);
+                    const int xs = x2 == 0 ? ne0 - 2 : (x2 == ne0 - 1 ? 1 : x2);
+                    const int ys = y2 == 0 ? ne1 - 2 : (y2 == ne1 - 1 ? 1 : y2);
+                    const int zs = z2 == 0 ? ne2 - 2 : (z2 == ne2 - 1 ? 1 : z2);
+                    const int cs2 = xs + ne0 * (ys + ne1 * zs);
+                    seg_b[2 * h + 1] = y.cell_start[cs2] - y.mol_off;
+                    seg_n[2 * h + 1] = y.cell_start[cs2 + 1] - y.mol_off - seg_b[2 * h + 1];
+                    seg_code[2 * h + 1] = (ssx + 1) | ((ssy + 1) << 2) | ((ssz + 1) << 4);
+                }
+            }
+        }
+    }
+    // prefix over the 128 segments in union-cell order: cells 0..31, then 32..63
+    int carry = 0;
+    __syncwarp();
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int tot = seg_n[2 * h] + seg_n[2 * h + 1];
+        int incl = tot;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const int excl = carry + incl - tot;
+        const int u = lane + 32 * h;
+        sh.off[2 * u] = excl;
+        sh.off[2 * u + 1] = excl + seg_n[2 * h];
+        sh.start[2 * u] = seg_b[2 * h];
+        sh.start[2 * u + 1] = seg_b[2 * h + 1];
+        sh.code[2 * u] = seg_code[2 * h];
+        sh.code[2 * u + 1] = seg_code[2 * h + 1];
+        sh.segallow[2 * u] = (unsigned char)seg_allow[h];
+        sh.segallow[2 * u + 1] = (unsigned char)seg_allow[h];
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    const int total = carry;
+    if (lane == 0) sh.off[NB_BSEG] = total;
+    __syncwarp();
+
+    uint32_t over = 0u;
+    for (int pass = 0; pass * 32 < nowners; pass++) {
+        const int k = pass * 32 + lane;
+        const bool own = k < nowners;
+        const int kk = own ? k : 0;  // lanes without an owner read owner 0
+        int oc = 0;                  // the owner's block cell: the last oc with opre[oc] <= kk
+#pragma unroll
+        for (int q = 1; q < 8; q++) oc += kk >= sh.opre[q] ? 1 : 0;
+        const int i = sh.ostart[oc] + (kk - sh.opre[oc]);
+        const double4 pi = ldg_pos(P + i);
+        const float xif = (float)(pi.x - refx), yif = (float)(pi.y - refy), zif = (float)(pi.z - refz);
+        const float bx_lo = warp_min(own ? xif : 3e38f), bx_hi = warp_max(own ? xif : -3e38f);
+        const float by_lo = warp_min(own ? yif : 3e38f), by_hi = warp_max(own ? yif : -3e38f);
+        const float bz_lo = warp_min(own ? zif : 3e38f), bz_hi = warp_max(own ? zif : -3e38f);
+        int cnt = 0, nb = 0;
+        int32_t *const row = y.nbr + nb_row(i, maxn);
+        const int nown = min(32, nowners - pass * 32);
+        __syncwarp();
+        sh.ox[lane] = own ? xif : 1e30f;
+        sh.oy[lane] = own ? yif : 1e30f;
+        sh.oz[lane] = own ? zif : 1e30f;
+        sh.oi[lane] = i;
+        sh.oallow[lane] = own ? 1u << oc : 0u;
+        if (POLY) {
+            sh.ochain[lane] = own ? y.chain[i] : -1;
+            sh.obf[lane] = own ? y.bflag[i] : make_int4(0, 0, 0, 0);
+        }
+        for (int base = 0; base < total; base += NB_STAGE) {
+            const int take = min(NB_STAGE, total - base);
+            __syncwarp();
+            int kept = 0;
+            for (int t0 = 0; t0 < take; t0 += 32) {
+                const int t = t0 + lane;
+                bool keep = false;
+                float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
+                unsigned al = 0u;
+                int j = 0;
+                if (t < take) {
+                    const int q = base + t;
+                    int kk = 0;  // segment containing q: largest kk with off[kk] <= q
+#pragma unroll
+                    for (int step = 64; step > 0; step >>= 1)
+                        if (kk + step < NB_BSEG && sh.off[kk + step] <= q) kk += step;
+                    j = sh.start[kk] + (q - sh.off[kk]);
+                    const int code = sh.code[kk];
+                    al = sh.segallow[kk];
+                    const double4 pj = ldg_pos(P + j);
+                    const double xj = image(pj.x, (code & 3) - 1, y.L[0]);
+                    const double yj = image(pj.y, ((code >> 2) & 3) - 1, y.L[1]);
+                    const double zj = image(pj.z, ((code >> 4) & 3) - 1, y.L[2]);
+                    f = make_float4((float)(xj - refx), (float)(yj - refy), (float)(zj - refz),
+                                    __int_as_float(j | (code << NB_SHIFT_BITS)));
+                    const float ex = fmaxf(fmaxf(bx_lo - f.x, f.x - bx_hi), 0.f);
+                    const float ey = fmaxf(fmaxf(by_lo - f.y, f.y - by_hi), 0.f);
+                    const float ez = fmaxf(fmaxf(bz_lo - f.z, f.z - bz_hi), 0.f);
+                    keep = POLY || ex * ex + ey * ey + ez * ez < prune2;
+                }
+                const unsigned m = __ballot_sync(0xffffffffu, keep);
+                if (keep) {
+                    const int pos = kept + __popc(m & lt);
+                    sh.f[pos] = f;
+                    sh.allow[pos] = (unsigned char)al;
+                    if (POLY) sh.cs[pos] = make_int2(y.chain[j], y.subchain[j]);
+                }
+                kept += __popc(m);
+            }
+            __syncwarp();
+            for (int t0 = 0; t0 < kept; t0 += 32) {
+                const int cq = t0 + lane;
+                const bool valid = cq < kept;
+                const float4 f = valid ? sh.f[cq] : make_float4(-1e30f, -1e30f, -1e30f, 0.f);
+                const unsigned callow = valid ? sh.allow[cq] : 0u;
+                const int e = __float_as_int(f.w);
+                const unsigned long long fx2 = pack_f32x2(f.x, f.x), fy2 = pack_f32x2(f.y, f.y),
+                                         fz2 = pack_f32x2(f.z, f.z);
+                int2 cs = make_int2(-2, 0);
+                if (POLY && valid) cs = sh.cs[cq];
+                unsigned mine_hits = 0u;
+                for (int o0 = 0; o0 < nown; o0 += NB_OG) {
+                    bool hit[NB_OG], exact[NB_OG];
+                    float r2f[NB_OG];
+                    bool anyx = false;
+#pragma unroll
+                    for (int h = 0; h < NB_OG; h += 2) {
+                        const unsigned long long dx = sub_f32x2(lds_f32x2(&sh.ox[o0 + h]), fx2);
+                        const unsigned long long dy = sub_f32x2(lds_f32x2(&sh.oy[o0 + h]), fy2);
+                        const unsigned long long dz = sub_f32x2(lds_f32x2(&sh.oz[o0 + h]), fz2);
+                        const unsigned long long t = fma_f32x2(dz, dz, fma_f32x2(dy, dy, mul_f32x2(dx, dx)));
+                        r2f[h] = __uint_as_float((unsigned)t);
+                        r2f[h + 1] = __uint_as_float((unsigned)(t >> 32));
+                    }
+#pragma unroll
+                    for (int u = 0; u < NB_OG; u++) {
+                        const bool ok = (callow & sh.oallow[o0 + u]) != 0u;
+                        hit[u] = ok && r2f[u] < lo32 && r2f[u] > 0.f;
+                        exact[u] = ok && !hit[u] && r2f[u] <= hi32;
+                        anyx |= exact[u];
+                    }
+                    if (__any_sync(0xffffffffu, anyx)) {
+#pragma unroll
+                        for (int u = 0; u < NB_OG; u++)
+                            if (exact[u]) hit[u] = exact_pair(P, sh.oi[o0 + u], e, y.L, y.rn2);
+                    }
+#pragma unroll
+                    for (int u = 0; u < NB_OG; u++) {
+                        const unsigned m = __ballot_sync(0xffffffffu, hit[u]);
+                        if (lane == o0 + u) mine_hits = m;
+                    }
+                    if (POLY) {
+                        int addb = 0;
+#pragma unroll
+                        for (int u = 0; u < NB_OG; u++) {
+                            bool bond = false;
+                            if ((callow & sh.oallow[o0 + u]) != 0u && cs.x == sh.ochain[o0 + u] &&
+                                !((e & NB_INDEX_MASK) == sh.oi[o0 + u] && (e >> NB_SHIFT_BITS) == NB_NOSHIFT)) {
+                                const int pos = cs.y - 1, grp = pos / 31, ex = pos % 31;
+                                const int4 bf = sh.obf[o0 + u];
+                                const int word = grp == 0 ? bf.x : grp == 1 ? bf.y : grp == 2 ? bf.z : bf.w;
+                                bond = pos >= 0 && grp < 4 && ((word >> ex) & 1);
+                            }
+                            const unsigned mb = __ballot_sync(0xffffffffu, bond);
+                            const int b0 = __shfl_sync(0xffffffffu, nb, o0 + u);
+                            if (bond) {
+                                const int kb = b0 + __popc(mb & lt);
+                                if (kb < 4) y.bnd[(size_t)sh.oi[o0 + u] * 4 + kb] = e;
+                            }
+                            if (lane == o0 + u) addb = __popc(mb);
+                        }
+                        nb += addb;
+                    }
+                }
+                while (mine_hits) {
+                    const int b = __ffs(mine_hits) - 1;
+                    mine_hits &= mine_hits - 1u;
+                    if (cnt < maxn) row[nb_col(cnt)] = __float_as_int(sh.f[t0 + b].w);
+                    cnt++;
+                }
+            }
+        }
+        if (own) {
+            y.nnbr[i] = cnt < maxn ? cnt : maxn;
+            atomicMax(y.max_nbr, cnt);
+            if (cnt > maxn) over |= BUILD_OVER_LIST;
+            if (POLY) {
+                y.nbond[i] = nb < 4 ? nb : 4;
+                if (nb > 4) over |= BUILD_OVER_BONDS;
+            }
+        }
+    }
+    __syncwarp();
+    return over;
+}
+
 }  // namespace fm

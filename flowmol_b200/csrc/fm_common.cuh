@@ -98,6 +98,7 @@ struct FmDev {
     int32_t *bnd, *nbond;
     // Mie_potential 1: per-type-pair constants, per-type masses; a molecule's
     // type (1-based) rides in the w component of its position
+    int build_blocks;            // list build: one warp per 2x2x2 cells (sparse systems)
     int mie;
     const FmMiePair *mie_pair;   // [(ti-1) + MIE_MAXT*(tj-1)]
     const double *mie_mass;      // [ti-1]

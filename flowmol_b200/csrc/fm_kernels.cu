@@ -12,6 +12,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <type_traits>
 
 #include "fm_common.cuh"
 #include "fm_device.cuh"
@@ -352,14 +353,16 @@ __global__ void k_reorder_copy(FmDev d, int gated, const double4 *tpos, const in
 //  1118-1180, stored in both directions)
 // ---------------------------------------------------------------------------
 
-// Neighbour rows of every extended cell, one warp per cell (grid-stride);
-// the per-cell routine and its pair-set argument are in fm_build.cuh.
-template <bool POLY>
+// Neighbour rows of every extended cell, one warp per cell or, for sparse
+// systems (BLOCKS), per block of 2x2x2 cells (grid-stride); the routines and
+// their pair-set argument are in fm_build.cuh.  Both give the same rows.
+template <bool POLY, bool BLOCKS>
 __global__ void __launch_bounds__(NB_THREADS, 8) k_build_nlist(FmDev d, int gated, int iter)
 {
     if (!gate(d, gated)) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    __shared__ BuildShared<POLY> sh[NB_WARPS];
+    using Shared = typename std::conditional<BLOCKS, BlockShared<POLY>, BuildShared<POLY>>::type;
+    __shared__ Shared sh[NB_WARPS];
     CellSys y;
     y.P = cur_pos(d, d.sc->pset);
     y.cell_start = d.cell_start;
@@ -373,8 +376,14 @@ __global__ void __launch_bounds__(NB_THREADS, 8) k_build_nlist(FmDev d, int gate
     y.chain = d.chain; y.subchain = d.subchain; y.bflag = d.bflag;
     y.bnd = d.bnd; y.nbond = d.nbond;
     uint32_t over = 0u;
-    for (int c = blockIdx.x * NB_WARPS + warp; c < d.ncell; c += gridDim.x * NB_WARPS)
-        over |= build_cell<POLY>(y, c, sh[warp], lane);
+    if constexpr (BLOCKS) {
+        const int nblk = ((d.ne[0] + 1) / 2) * ((d.ne[1] + 1) / 2) * ((d.ne[2] + 1) / 2);
+        for (int b = blockIdx.x * NB_WARPS + warp; b < nblk; b += gridDim.x * NB_WARPS)
+            over |= build_block<POLY>(y, b, sh[warp], lane);
+    } else {
+        for (int c = blockIdx.x * NB_WARPS + warp; c < d.ncell; c += gridDim.x * NB_WARPS)
+            over |= build_cell<POLY>(y, c, sh[warp], lane);
+    }
     if (lane == 0) {
         if (over & BUILD_OVER_LIST) raise_status(d, ST_NLIST, iter);
         if (over & BUILD_OVER_BONDS) raise_status(d, ST_BOND, iter);
@@ -927,24 +936,30 @@ void launch_reorder(const FmDev &d, int gated, double4 *tpos, int32_t *tuidx, cu
 }
 // The list build walks the cells grid-stride with every block resident (one
 // wave: a second partial wave would double the kernel's time).
-template <bool POLY>
-static int build_grid(int ncell)
+template <bool POLY, bool BLOCKS>
+static int build_grid(int nwork)
 {
     static int resident = 0;
     if (resident == 0) {
         int dev = 0, nsm = kSMs, per_sm = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_build_nlist<POLY>, NB_THREADS, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_build_nlist<POLY, BLOCKS>, NB_THREADS, 0);
         resident = std::max(nsm, 1) * std::max(per_sm, 1);
     }
-    return std::min(nblk(ncell, NB_WARPS), resident);
+    return std::min(nblk(nwork, NB_WARPS), resident);
 }
 
 void launch_build_nlist(const FmDev &d, int gated, int iter, cudaStream_t st)
 {
-    if (d.potential_flag == 1) k_build_nlist<true><<<build_grid<true>(d.ncell), NB_THREADS, 0, st>>>(d, gated, iter);
-    else k_build_nlist<false><<<build_grid<false>(d.ncell), NB_THREADS, 0, st>>>(d, gated, iter);
+    const int nb = ((d.ne[0] + 1) / 2) * ((d.ne[1] + 1) / 2) * ((d.ne[2] + 1) / 2);
+    if (d.potential_flag == 1) {
+        if (d.build_blocks) k_build_nlist<true, true><<<build_grid<true, true>(nb), NB_THREADS, 0, st>>>(d, gated, iter);
+        else k_build_nlist<true, false><<<build_grid<true, false>(d.ncell), NB_THREADS, 0, st>>>(d, gated, iter);
+    } else {
+        if (d.build_blocks) k_build_nlist<false, true><<<build_grid<false, true>(nb), NB_THREADS, 0, st>>>(d, gated, iter);
+        else k_build_nlist<false, false><<<build_grid<false, false>(d.ncell), NB_THREADS, 0, st>>>(d, gated, iter);
+    }
 }
 
 int force_blocks(int n, int tpm) { return nblk(n * tpm, FORCE_THREADS); }

@@ -77,8 +77,13 @@ typedef struct fm_params {
     int32_t nlist_capacity;       /* neighbours per molecule reserved; 0 = automatic */
     int32_t threads_per_molecule; /* force kernel lanes per molecule; 0 = autotuned */
     int32_t integration_algorithm; /* INTEGRATION_ALGORITHM: 0 leap-frog (NVE), 1 velocity Verlet */
-    int32_t pad_;
+    int32_t list_build;           /* FM_LIST_BUILD_*: one warp per cell or per 2x2x2 cells (same rows) */
 } fm_params;
+
+/* List build granularity: automatic (2x2x2 blocks below 8 molecules per
+ * cell), one warp per cell, one warp per block of 2x2x2 cells.  The rows are
+ * identical; only the speed differs. */
+enum { FM_LIST_BUILD_AUTO = 0, FM_LIST_BUILD_CELLS = 1, FM_LIST_BUILD_BLOCKS = 2 };
 
 /* Macroscopic properties of one record step, the columns of
  * results/macroscopic_properties (parallel_io.MPI2.f90:4589-4646) plus the

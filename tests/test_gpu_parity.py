@@ -419,3 +419,54 @@ def test_mie_polymer_harmonic_bonds(gpu_lib):
     assert [x["iter"] for x in recs] == [int(x) for x in recs_o[:, 0]]
     for row, ro in zip(recs, recs_o):
         assert row["potenergy"] == pytest.approx(ro[5], rel=1e-9)
+
+
+@pytest.mark.parametrize("case", ["wca", "lj", "fene", "faces"])
+def test_list_build_cells_equals_blocks(gpu_lib, case):
+    """The per-cell and the 2x2x2-block list builds give identical rows (same
+    partners in the same order), equal to the oracle's pair set; odd cell
+    counts (partial blocks), box faces and polymers included."""
+    from flowmol_b200 import polymer
+    kw = {}
+    mono = None
+    if case == "wca":
+        r, v, dom = lattice.lj_fluid([7, 7, 7], 0.8, 1.0, 71)
+        r = lattice.jitter(r, 0.05, 71, dom)
+        rc, rho = WCA_RC, 0.8
+    elif case == "lj":
+        r, v, dom = lattice.lj_fluid([7, 6, 8], 0.8442, 0.722, 72)
+        r = lattice.jitter(r, 0.05, 72, dom)
+        rc, rho = 2.5, 0.8442
+    elif case == "faces":
+        r, v, dom = lattice.lj_fluid([7, 7, 7], 0.8, 1.0, 73)
+        r = r - r.min(axis=0) - 0.5 * np.asarray(dom)  # molecules exactly on the -L/2 faces
+        rc, rho = WCA_RC, 0.8
+    else:
+        r, v, ch, sub, fy, bf, dom = polymer.fene_melt(300)
+        rc, rho = WCA_RC, 0.85
+        kw = dict(potential_flag=1, k_c=30.0, R_0=1.5)
+        mono = (ch, sub, bf, fy)
+    rows = {}
+    for mode in (api.LIST_BUILD_CELLS, api.LIST_BUILD_BLOCKS):
+        s = gpu_system(r, v, dom, rc, density=rho, list_build=mode, **kw)
+        if mono is not None:
+            s.upload_monomers(*mono[:3])
+        s.setup()
+        rows[mode] = s.pair_list()
+        if mono is not None:
+            rows[(mode, "bonds")] = s.bonds()
+        _, _, a, _ = s.download()
+        rows[(mode, "a")] = a
+        s.close()
+    c, b = rows[api.LIST_BUILD_CELLS], rows[api.LIST_BUILD_BLOCKS]
+    for x, y in zip(c, b):
+        assert np.array_equal(x, y)  # same rows, same order
+    assert np.array_equal(rows[(api.LIST_BUILD_CELLS, "a")], rows[(api.LIST_BUILD_BLOCKS, "a")])
+    if mono is not None:
+        for x, y in zip(rows[(api.LIST_BUILD_CELLS, "bonds")], rows[(api.LIST_BUILD_BLOCKS, "bonds")]):
+            assert np.array_equal(x, y)
+    o = O.Oracle(r, v, dom, rc, density=rho, **kw)
+    if mono is not None:
+        o.set_monomers(mono[0], mono[1], mono[3], mono[2])
+    o.setup()
+    assert np.array_equal(canonical_full(*b), canonical_oracle(*o.pair_list()))
