@@ -147,7 +147,7 @@ void free_all(fm_engine *e)
     void *ptrs[] = {d.slots, d.flags, d.pos0, d.pos1, d.vx, d.vy, d.vz, d.ax, d.ay, d.az, d.slot_of, d.uidx, d.tag,
                     d.rteth, d.slidev, d.tpos, d.trteth, d.tslidev, d.tvx, d.tvy, d.tvz, d.tax, d.tay, d.taz,
                     d.tuidx, d.ttag, d.cell_slot, d.cell_of, d.cell_count, d.cell_start, d.perm, d.nbr, d.nnbr,
-                    d.rterm, d.tmv2, d.red_part, d.red_count, d.rb_slot, d.rb_mpre, d.rb_cpre, e->stage,
+                    d.rterm, d.tmv2, d.red_part, d.red_count, d.rb_slot, d.rb_mpre, d.rb_cpre, d.rb_upre, e->stage,
                     e->stage_i};
     for (void *q : ptrs)
         if (q) cudaFree(q);
@@ -264,6 +264,10 @@ int admit(fm_engine *e, Job &jb, int slot)
     s.nmol = j.np;
     s.list_off = jb.list_off;
     s.maxn = jb.maxn;
+    // sparse cells (a few molecules each) are built 2x2x2 at a time (same rows)
+    s.build_blocks = f.mode == fm::MODE_LIST && (double)j.np / (j.domain[0] * j.domain[1] * j.domain[2]) *
+                                                        s.cs[0] * s.cs[1] * s.cs[2] < 8.0
+                         ? 1 : 0;
     s.tplot = std::max(1, j.tplot);
     s.integrator = j.integration_algorithm == 0 ? 0 : 1;
     s.ensemble = j.ensemble;
@@ -474,6 +478,7 @@ extern "C" int fm_engine_create(const fm_engine_params *p, fm_engine **out)
     EA(d.perm, M) EA(d.nbr, p->max_list_entries) EA(d.nnbr, M) EA(d.rterm, M * fm::RT_N) EA(d.tmv2, M)
     EA(d.red_part, (size_t)d.nslots * fm::EY * fm::RED_W) EA(d.red_count, (size_t)d.nslots * 2)
     EA(d.rb_slot, (size_t)d.nslots + 1) EA(d.rb_mpre, (size_t)d.nslots + 1) EA(d.rb_cpre, (size_t)d.nslots + 1)
+    EA(d.rb_upre, (size_t)d.nslots + 1)
 #undef EA
     if (rc != FM_OK) {
         free_all(e);

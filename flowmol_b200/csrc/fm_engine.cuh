@@ -33,6 +33,7 @@ struct EngSlot {
     int mol_off, nmol;                // molecules [mol_off, +nmol)
     int64_t list_off;                 // neighbour rows start here, maxn entries per molecule
     int maxn;
+    int build_blocks;                 // list build by 2x2x2 cells (sparse jobs), else by cell
     int tplot, integrator, ensemble, mode, pressure, nthermo, crit, fixed_rebuild;
     int iter0, nsteps;
     double rc2, rn2, potshift, half_min_delta, volume, density;
@@ -58,8 +59,9 @@ struct EngSlot {
 struct EngFlags {
     int any_rebuild, any_list, any_ap, any_lfv, any_thermo, any_record;
     int mol_hwm, cell_hwm;
-    // this tick's rebuilding jobs (slot order): count, their molecules, their cells
-    int rb_n, rb_mtot, rb_ctot, pad_;
+    // this tick's rebuilding jobs (slot order): count, their molecules, their
+    // cells, their list-build units (cells or 2x2x2 blocks)
+    int rb_n, rb_mtot, rb_ctot, rb_utot;
 };
 
 struct EngDev {
@@ -100,7 +102,7 @@ struct EngDev {
     int32_t *red_count;
     // rebuild work list of the tick: slots, and prefix sums of their molecules
     // and cells ([rb_n + 1] each), so the rebuild kernels visit only those
-    int32_t *rb_slot, *rb_mpre, *rb_cpre;
+    int32_t *rb_slot, *rb_mpre, *rb_cpre, *rb_upre;
 };
 
 constexpr int EY = 16;      // blocks per job in the thermostat and record reductions

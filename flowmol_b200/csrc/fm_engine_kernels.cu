@@ -141,25 +141,28 @@ __global__ void __launch_bounds__(EDEC) k_e_decide(EngDev d)
         d.flags->any_lfv = f[3]; d.flags->any_thermo = f[4]; d.flags->any_record = f[5];
     }
     // rebuild work list in slot order: a block scan of (flag, molecules, cells)
-    __shared__ int wsum[3][EDEC / 32];
-    __shared__ int carry[3];
-    if (threadIdx.x < 3) carry[threadIdx.x] = 0;
+    __shared__ int wsum[4][EDEC / 32];
+    __shared__ int carry[4];
+    if (threadIdx.x < 4) carry[threadIdx.x] = 0;
     __syncthreads();
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int base = 0; base < d.nslots; base += EDEC) {
         const int k = base + threadIdx.x;
-        int x[3] = {0, 0, 0};
+        int x[4] = {0, 0, 0, 0};
         if (k < d.nslots) {
             const EngSlot &s = d.slots[k];
             if (slot_rebuilding(s)) {
                 x[0] = 1;
                 x[1] = s.nmol;
                 x[2] = s.mode == MODE_LIST ? s.ncell : 0;
+                x[3] = s.mode != MODE_LIST ? 0
+                       : s.build_blocks ? ((s.ne[0] + 1) / 2) * ((s.ne[1] + 1) / 2) * ((s.ne[2] + 1) / 2)
+                                        : s.ncell;
             }
         }
-        int incl[3];
+        int incl[4];
 #pragma unroll
-        for (int q = 0; q < 3; q++) {
+        for (int q = 0; q < 4; q++) {
             incl[q] = x[q];
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -171,7 +174,7 @@ __global__ void __launch_bounds__(EDEC) k_e_decide(EngDev d)
         __syncthreads();
         if (w == 0) {
 #pragma unroll
-            for (int q = 0; q < 3; q++) {
+            for (int q = 0; q < 4; q++) {
                 const int v = wsum[q][lane];
                 int vi = v;
 #pragma unroll
@@ -188,18 +191,21 @@ __global__ void __launch_bounds__(EDEC) k_e_decide(EngDev d)
             d.rb_slot[pos] = k;
             d.rb_mpre[pos] = carry[1] + wsum[1][w] + incl[1] - x[1];
             d.rb_cpre[pos] = carry[2] + wsum[2][w] + incl[2] - x[2];
+            d.rb_upre[pos] = carry[3] + wsum[3][w] + incl[3] - x[3];
         }
         __syncthreads();
         if (threadIdx.x == EDEC - 1)
-            for (int q = 0; q < 3; q++) carry[q] += wsum[q][w] + incl[q];
+            for (int q = 0; q < 4; q++) carry[q] += wsum[q][w] + incl[q];
         __syncthreads();
     }
     if (threadIdx.x == 0) {
         d.rb_mpre[carry[0]] = carry[1];
         d.rb_cpre[carry[0]] = carry[2];
+        d.rb_upre[carry[0]] = carry[3];
         d.flags->rb_n = carry[0];
         d.flags->rb_mtot = carry[1];
         d.flags->rb_ctot = carry[2];
+        d.flags->rb_utot = carry[3];
     }
 }
 
@@ -382,19 +388,24 @@ __global__ void k_e_reorder_copy(EngDev d)
     }
 }
 
-// Neighbour rows, one warp per arena cell: the single-system routine
-// (build_cell, fm_build.cuh: pair set of assign_to_neighbourlist_halfint_opt,
-// linklist.f90:660-804) on the cell's job.
+// Neighbour rows of the tick's rebuilding jobs, one warp per work unit (a
+// cell, or a block of 2x2x2 cells for sparse jobs): the single-system
+// routines (build_cell / build_block, fm_build.cuh: pair set of
+// assign_to_neighbourlist_halfint_opt, linklist.f90:660-804) on the unit's job.
 __global__ void __launch_bounds__(NB_THREADS, 6) k_e_build(EngDev d)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    __shared__ BuildShared<false> sh[NB_WARPS];
-    __shared__ CellSys ys[NB_WARPS];  // the cell's job, read through shared memory
+    union WarpShared {
+        BuildShared<false> cell;
+        BlockShared<false> block;
+    };
+    __shared__ WarpShared sh[NB_WARPS];
+    __shared__ CellSys ys[NB_WARPS];  // the unit's job, read through shared memory
     if (!d.flags->any_rebuild) return;
-    const int tot = d.flags->rb_ctot;
+    const int tot = d.flags->rb_utot;
     int r = 0, r_loaded = -1;
     for (int g = blockIdx.x * NB_WARPS + warp; g < tot; g += gridDim.x * NB_WARPS) {
-        const int lc = rb_entry(d.rb_cpre, g, r);
+        const int unit = rb_entry(d.rb_upre, g, r);
         EngSlot &s = d.slots[d.rb_slot[r]];
         __syncwarp();
         if (r != r_loaded && lane == 0) {
@@ -414,7 +425,9 @@ __global__ void __launch_bounds__(NB_THREADS, 6) k_e_build(EngDev d)
         }
         __syncwarp();
         r_loaded = r;
-        const uint32_t over = build_cell<false>(ys[warp], lc, sh[warp], lane);
+        // a cell or, for sparse jobs, a block of 2x2x2 cells: the same rows
+        const uint32_t over = s.build_blocks ? build_block<false>(ys[warp], unit, sh[warp].block, lane)
+                                             : build_cell<false>(ys[warp], unit, sh[warp].cell, lane);
         if (lane == 0 && (over & BUILD_OVER_LIST)) slot_fail(&s, ST_NLIST, s.iter);
     }
 }
