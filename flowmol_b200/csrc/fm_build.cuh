@@ -22,12 +22,12 @@
 // takes one staged candidate and the warp loops over the owners, NB_OG at a
 // time: the FP32 r^2 (error below 1e-5 cs^2 for molecules binned in this
 // build, offsets within 1.5 cells) decides every candidate farther than
-// BAND = 1e-4 cs^2 from rneighbr2; a candidate inside the band, or at FP32
-// distance 0 (the owner itself), is re-read in FP64 and decided by the exact
-// test (dx^2+dy^2)+dz^2 < rneighbr2 -- a branch the whole warp skips unless
-// some lane needs it.  An owner's hits among 32 candidates are one ballot,
-// kept by the owner's lane, which appends them to its row in candidate order,
-// so every row lists its partners in the visiting order.
+// BAND = 1e-4 cs^2 from rneighbr2; a candidate inside the band is re-read in
+// FP64 and decided by the exact test (dx^2+dy^2)+dz^2 < rneighbr2 -- a branch
+// the whole warp skips unless some lane needs it.  An owner's hits among 32
+// candidates are one ballot; the owner's lane appends them to its row in
+// candidate order (all but its own entry, at distance 0), so every row lists
+// its partners in the visiting order.
 //
 // With FENE polymers (POLY) the same scan discovers bonds the way the
 // reference's check_update_adjacentbeadinfo does (linklist.f90:2542-2584): any
@@ -80,6 +80,7 @@ struct BuildShared {
     int start[54], code[54];
     int ochain[POLY ? 32 : 1];
     alignas(16) int4 obf[POLY ? 32 : 1];
+    unsigned hits[POLY ? 1 : 32];  // per owner: which of the 32 candidates hit (polymers: registers)
 };
 
 constexpr uint32_t BUILD_OVER_LIST = 1u, BUILD_OVER_BONDS = 2u;
@@ -215,6 +216,7 @@ __device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY> &sh, i
         const float bz0 = warp_min(zif), bz1 = warp_max(zif);
         int cnt = 0, nb = 0;  // the owner lane's list and bond counts
         int32_t *const row = y.nbr + nb_row(i, maxn);
+        const int self_e = i | (NB_NOSHIFT << NB_SHIFT_BITS);  // the owner's own entry
         const int nown = min(32, ccount - pass * 32);
         __syncwarp();
         sh.ox[lane] = own ? xif : 1e30f;  // far sentinels: r^2 = inf, never a hit
@@ -277,7 +279,7 @@ __device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY> &sh, i
                                          fz2 = pack_f32x2(f.z, f.z);
                 int2 cs = make_int2(-2, 0);
                 if (POLY && valid) cs = sh.cs[cq];
-                unsigned mine_hits = 0u;  // this lane's owner: which of the 32 candidates hit
+                unsigned mine_reg = 0u;  // polymers: the owner lane keeps its ballot in a register
                 // owners in groups of NB_OG (pairs in packed FP32): independent chains
                 // for the scheduler
                 for (int o0 = 0; o0 < nown; o0 += NB_OG) {
@@ -295,9 +297,9 @@ __device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY> &sh, i
                     }
 #pragma unroll
                     for (int u = 0; u < NB_OG; u++) {
-                        // r2f is exactly 0 for the owner itself (identical operands);
-                        // 0 and the band around rneighbr2 are decided in FP64
-                        hit[u] = r2f[u] < lo32 && r2f[u] > 0.f;
+                        // the band around rneighbr2 is decided in FP64; the owner
+                        // itself (r2f exactly 0) is a hit here, dropped at the append
+                        hit[u] = r2f[u] < lo32 && (!POLY || r2f[u] > 0.f);
                         exact[u] = !hit[u] && r2f[u] <= hi32;
                         anyx |= exact[u];
                     }
@@ -309,7 +311,11 @@ __device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY> &sh, i
 #pragma unroll
                     for (int u = 0; u < NB_OG; u++) {
                         const unsigned m = __ballot_sync(0xffffffffu, hit[u]);
-                        if (lane == o0 + u) mine_hits = m;
+                        if (POLY) {
+                            if (lane == o0 + u) mine_reg = m;
+                        } else if (lane == 0) {
+                            sh.hits[o0 + u] = m;
+                        }
                     }
                     if (POLY) {
                         int addb = 0;
@@ -334,13 +340,19 @@ __device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY> &sh, i
                         nb += addb;
                     }
                 }
-                // the owner lane appends its hits in candidate order
+                // the owner lane appends its hits in candidate order, all but itself
+                if (!POLY) __syncwarp();
+                unsigned mine_hits = POLY ? mine_reg : (lane < nown ? sh.hits[lane] : 0u);
                 while (mine_hits) {
                     const int b = __ffs(mine_hits) - 1;
                     mine_hits &= mine_hits - 1u;
-                    if (cnt < maxn) row[nb_col(cnt)] = __float_as_int(sh.f[t0 + b].w);
-                    cnt++;
+                    const int ent = __float_as_int(sh.f[t0 + b].w);
+                    if (POLY || ent != self_e) {
+                        if (cnt < maxn) row[nb_col(cnt)] = ent;
+                        cnt++;
+                    }
                 }
+                if (!POLY) __syncwarp();
             }
         }
         if (own) {
@@ -385,6 +397,7 @@ struct BlockShared {
     int opre[9], ostart[8];         // owners by block cell: prefix counts, first molecule
     int ochain[POLY ? 32 : 1];
     alignas(16) int4 obf[POLY ? 32 : 1];
+    unsigned hits[POLY ? 1 : 32];   // per owner: which of the 32 candidates hit (polymers: registers)
 };
 
 template <bool POLY>
@@ -517,6 +530,7 @@ __device__ uint32_t build_block(const CellSys &y, int blk, BlockShared<POLY> &sh
         const float bz_lo = warp_min(own ? zif : 3e38f), bz_hi = warp_max(own ? zif : -3e38f);
         int cnt = 0, nb = 0;
         int32_t *const row = y.nbr + nb_row(i, maxn);
+        const int self_e = i | (NB_NOSHIFT << NB_SHIFT_BITS);  // the owner's own entry
         const int nown = min(32, nowners - pass * 32);
         __syncwarp();
         sh.ox[lane] = own ? xif : 1e30f;
@@ -578,7 +592,7 @@ __device__ uint32_t build_block(const CellSys &y, int blk, BlockShared<POLY> &sh
                                          fz2 = pack_f32x2(f.z, f.z);
                 int2 cs = make_int2(-2, 0);
                 if (POLY && valid) cs = sh.cs[cq];
-                unsigned mine_hits = 0u;
+                unsigned mine_reg = 0u;  // polymers: the owner lane keeps its ballot in a register
                 for (int o0 = 0; o0 < nown; o0 += NB_OG) {
                     bool hit[NB_OG], exact[NB_OG];
                     float r2f[NB_OG];
@@ -595,7 +609,8 @@ __device__ uint32_t build_block(const CellSys &y, int blk, BlockShared<POLY> &sh
 #pragma unroll
                     for (int u = 0; u < NB_OG; u++) {
                         const bool ok = (callow & sh.oallow[o0 + u]) != 0u;
-                        hit[u] = ok && r2f[u] < lo32 && r2f[u] > 0.f;
+                        // the owner itself: dropped at the append (polymers: decided in FP64)
+                        hit[u] = ok && r2f[u] < lo32 && (!POLY || r2f[u] > 0.f);
                         exact[u] = ok && !hit[u] && r2f[u] <= hi32;
                         anyx |= exact[u];
                     }
@@ -607,7 +622,11 @@ __device__ uint32_t build_block(const CellSys &y, int blk, BlockShared<POLY> &sh
 #pragma unroll
                     for (int u = 0; u < NB_OG; u++) {
                         const unsigned m = __ballot_sync(0xffffffffu, hit[u]);
-                        if (lane == o0 + u) mine_hits = m;
+                        if (POLY) {
+                            if (lane == o0 + u) mine_reg = m;
+                        } else if (lane == 0) {
+                            sh.hits[o0 + u] = m;
+                        }
                     }
                     if (POLY) {
                         int addb = 0;
@@ -632,12 +651,18 @@ __device__ uint32_t build_block(const CellSys &y, int blk, BlockShared<POLY> &sh
                         nb += addb;
                     }
                 }
+                if (!POLY) __syncwarp();
+                unsigned mine_hits = POLY ? mine_reg : (lane < nown ? sh.hits[lane] : 0u);
                 while (mine_hits) {
                     const int b = __ffs(mine_hits) - 1;
                     mine_hits &= mine_hits - 1u;
-                    if (cnt < maxn) row[nb_col(cnt)] = __float_as_int(sh.f[t0 + b].w);
-                    cnt++;
+                    const int ent = __float_as_int(sh.f[t0 + b].w);
+                    if (POLY || ent != self_e) {
+                        if (cnt < maxn) row[nb_col(cnt)] = ent;
+                        cnt++;
+                    }
                 }
+                if (!POLY) __syncwarp();
             }
         }
         if (own) {
