@@ -32,7 +32,7 @@ struct FmScalars {
     uint64_t digest;          // pair-set digest (test hook)
     int64_t digest_n;
     int32_t nrec_pending;     // record rows written since the host last read
-    int32_t pad_;
+    int32_t build_next;       // list build: next work unit to hand out (zeroed before each build)
 };
 
 // Partial sums of one record step, one row per force-kernel block.

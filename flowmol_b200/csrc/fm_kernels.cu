@@ -376,13 +376,19 @@ __global__ void __launch_bounds__(NB_THREADS, 8) k_build_nlist(FmDev d, int gate
     y.chain = d.chain; y.subchain = d.subchain; y.bflag = d.bflag;
     y.bnd = d.bnd; y.nbond = d.nbond;
     uint32_t over = 0u;
-    if constexpr (BLOCKS) {
-        const int nblk = ((d.ne[0] + 1) / 2) * ((d.ne[1] + 1) / 2) * ((d.ne[2] + 1) / 2);
-        for (int b = blockIdx.x * NB_WARPS + warp; b < nblk; b += gridDim.x * NB_WARPS)
-            over |= build_block<POLY>(y, b, sh[warp], lane);
-    } else {
-        for (int c = blockIdx.x * NB_WARPS + warp; c < d.ncell; c += gridDim.x * NB_WARPS)
-            over |= build_cell<POLY>(y, c, sh[warp], lane);
+    const int nwork = BLOCKS ? ((d.ne[0] + 1) / 2) * ((d.ne[1] + 1) / 2) * ((d.ne[2] + 1) / 2) : d.ncell;
+    // work units handed out NB_CHUNK at a time, so warps that meet empty or
+    // halo cells take more: no tail of a few warps with dense cells left
+    for (;;) {
+        int u0 = 0;
+        if (lane == 0) u0 = atomicAdd(&d.sc->build_next, NB_CHUNK);
+        u0 = __shfl_sync(0xffffffffu, u0, 0);
+        if (u0 >= nwork) break;
+        const int u1 = min(u0 + NB_CHUNK, nwork);
+        for (int u = u0; u < u1; u++) {
+            if constexpr (BLOCKS) over |= build_block<POLY>(y, u, sh[warp], lane);
+            else over |= build_cell<POLY>(y, u, sh[warp], lane);
+        }
     }
     if (lane == 0) {
         if (over & BUILD_OVER_LIST) raise_status(d, ST_NLIST, iter);
@@ -952,6 +958,7 @@ static int build_grid(int nwork)
 
 void launch_build_nlist(const FmDev &d, int gated, int iter, cudaStream_t st)
 {
+    cudaMemsetAsync(&d.sc->build_next, 0, sizeof(int32_t), st);
     const int nb = ((d.ne[0] + 1) / 2) * ((d.ne[1] + 1) / 2) * ((d.ne[2] + 1) / 2);
     if (d.potential_flag == 1) {
         if (d.build_blocks) k_build_nlist<true, true><<<build_grid<true, true>(nb), NB_THREADS, 0, st>>>(d, gated, iter);
