@@ -45,7 +45,7 @@ constexpr int NB_WARPS = 4;                 // cells processed concurrently per 
 constexpr int NB_THREADS = 32 * NB_WARPS;
 constexpr int NB_STAGE = 256;               // staged candidates per warp
 constexpr int NB_OG = 4;                    // owners per step of the candidate loop
-constexpr int NB_CHUNK = 2;                 // work units a warp takes per fetch
+constexpr int NB_CHUNK = 2;                 // work units a warp takes per fetch (one system)
 constexpr int NB_NOSHIFT = 1 | (1 << 2) | (1 << 4);
 
 // One periodic system as the build sees it.  Molecule indices in entries,

@@ -62,7 +62,6 @@ struct EngFlags {
     // this tick's rebuilding jobs (slot order): count, their molecules, their
     // cells, their list-build units (cells or 2x2x2 blocks)
     int rb_n, rb_mtot, rb_ctot, rb_utot;
-    int build_next, pad_;   // list build: next work unit to hand out (zeroed by the decide kernel)
 };
 
 struct EngDev {

@@ -206,7 +206,6 @@ __global__ void __launch_bounds__(EDEC) k_e_decide(EngDev d)
         d.flags->rb_mtot = carry[1];
         d.flags->rb_ctot = carry[2];
         d.flags->rb_utot = carry[3];
-        d.flags->build_next = 0;
     }
 }
 
@@ -404,18 +403,9 @@ __global__ void __launch_bounds__(NB_THREADS, 6) k_e_build(EngDev d)
     __shared__ CellSys ys[NB_WARPS];  // the unit's job, read through shared memory
     if (!d.flags->any_rebuild) return;
     const int tot = d.flags->rb_utot;
-    int r = 0, r_loaded = -1, g = 0, g1 = 0;
-    for (;;) {
-        // units handed out NB_CHUNK at a time (increasing per warp, as rb_entry needs)
-        if (g >= g1) {
-            int u0 = 0;
-            if (lane == 0) u0 = atomicAdd(&d.flags->build_next, NB_CHUNK);
-            g = __shfl_sync(0xffffffffu, u0, 0);
-            g1 = min(g + NB_CHUNK, tot);
-            if (g >= tot) break;
-        }
+    int r = 0, r_loaded = -1;
+    for (int g = blockIdx.x * NB_WARPS + warp; g < tot; g += gridDim.x * NB_WARPS) {
         const int unit = rb_entry(d.rb_upre, g, r);
-        g++;
         EngSlot &s = d.slots[d.rb_slot[r]];
         __syncwarp();
         if (r != r_loaded && lane == 0) {
