@@ -295,22 +295,40 @@ __global__ void k_scatter(FmDev d, int gated)
 }
 
 // Atomics make the in-cell order arbitrary; sorting each cell by old slot
-// makes the whole rebuild deterministic.
-__global__ void k_sort_cells(FmDev d, int gated)
+// makes the whole rebuild deterministic.  One warp per cell: up to 32 members
+// by a bitonic sort in registers, larger cells by lane 0 (insertion sort).
+constexpr int SORT_WARPS = 8;
+__global__ void __launch_bounds__(32 * SORT_WARPS) k_sort_cells(FmDev d, int gated)
 {
     if (!gate(d, gated)) return;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.ncell; c += gridDim.x * blockDim.x) {
-        int b = d.cell_start[c], e = d.cell_start[c + 1];
-        for (int x = b + 1; x < e; x++) {
-            int key = d.perm[x];
-            int y = x - 1;
-            while (y >= b && d.perm[y] > key) {
-                d.perm[y + 1] = d.perm[y];
-                y--;
+    const int lane = threadIdx.x & 31;
+    for (int c = blockIdx.x * SORT_WARPS + (threadIdx.x >> 5); c < d.ncell; c += gridDim.x * SORT_WARPS) {
+        const int b = d.cell_start[c], e = d.cell_start[c + 1];
+        const int m = e - b;  // uniform across the warp
+        if (m <= 32) {
+            int key = lane < m ? d.perm[b + lane] : 0x7fffffff;
+#pragma unroll
+            for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+                for (int j = k >> 1; j > 0; j >>= 1) {
+                    const int other = __shfl_xor_sync(0xffffffffu, key, j);
+                    const bool keep_min = ((lane & j) == 0) == ((lane & k) == 0);
+                    key = keep_min ? min(key, other) : max(key, other);
+                }
             }
-            d.perm[y + 1] = key;
+            if (lane < m) d.perm[b + lane] = key;
+        } else if (lane == 0) {
+            for (int x = b + 1; x < e; x++) {
+                const int key = d.perm[x];
+                int y = x - 1;
+                while (y >= b && d.perm[y] > key) {
+                    d.perm[y + 1] = d.perm[y];
+                    y--;
+                }
+                d.perm[y + 1] = key;
+            }
         }
-        d.cell_count[c] = 0;  // leave counts zeroed for the next histogram
+        if (lane == 0) d.cell_count[c] = 0;  // leave counts zeroed for the next histogram
     }
 }
 
@@ -933,7 +951,7 @@ void launch_scan_cells(const FmDev &d, int gated, cudaStream_t st)
 void launch_scatter(const FmDev &d, int gated, cudaStream_t st)
 {
     k_scatter<<<sgrid(d.n, 256, 8), 256, 0, st>>>(d, gated);
-    k_sort_cells<<<sgrid(d.ncell, 128, 8), 128, 0, st>>>(d, gated);
+    k_sort_cells<<<sgrid(d.ncell, SORT_WARPS, 8), 32 * SORT_WARPS, 0, st>>>(d, gated);
 }
 void launch_reorder(const FmDev &d, int gated, double4 *tpos, int32_t *tuidx, cudaStream_t st)
 {
