@@ -161,6 +161,24 @@ def test_nlist_overflow_is_resized_and_resumed(liquid):
     assert np.array_equal(r1, r2) and np.array_equal(v1, v2)
 
 
+def test_nlist_overflow_resumed_with_block_builds(gpu_lib):
+    """The same resize-and-resume when the rows are built by 2x2x2-cell
+    blocks (a sparse WCA fluid with too small a row capacity)."""
+    r, v, dom = lattice.lj_fluid([7, 7, 7], 0.8, 1.0, 81)
+    r = lattice.jitter(r, 0.05, 81, dom)
+    ref = gpu_system(r, v, dom, WCA_RC, tplot=25, density=0.8, list_build=api.LIST_BUILD_BLOCKS)
+    ref.setup()
+    ref.simulation_md(80)
+    small = gpu_system(r, v, dom, WCA_RC, tplot=25, density=0.8, list_build=api.LIST_BUILD_BLOCKS,
+                       nlist_capacity=8)
+    small.setup()
+    small.simulation_md(80)
+    assert small.counters()["nlist_capacity"] > 8
+    r1, v1, _, _ = ref.download()
+    r2, v2, _, _ = small.download()
+    assert np.array_equal(r1, r2) and np.array_equal(v1, v2)
+
+
 def test_escaped_molecule_is_an_error_code(gpu_lib):
     r, v, dom = cfg1_state()
     r = r.copy()
