@@ -124,6 +124,8 @@ struct fm_engine {
     bool tuned = false;
     cudaGraphExec_t graph = nullptr;
     int graph_tpm = -1;
+    fm::TickExtent graph_x{0, 0, 0};  // launch extents the graph was captured with
+    fm::TickExtent need_x{0, 0, 0};   // extents the resident jobs call for
     double *stage = nullptr;  // device staging for uploads/downloads
     size_t stage_cap = 0;     // doubles
     int32_t *stage_i = nullptr;
@@ -177,14 +179,25 @@ int capture(fm_engine *e)
     if (e->graph) { cudaGraphExecDestroy(e->graph); e->graph = nullptr; }
     cudaGraph_t g;
     EN_CUDA(cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
-    for (int t = 0; t < e->p.ticks_per_chunk; t++) fm::eng_tick(e->d, e->tpm, e->st);
+    for (int t = 0; t < e->p.ticks_per_chunk; t++) fm::eng_tick(e->d, e->tpm, e->need_x, e->st);
     cudaError_t err = cudaStreamEndCapture(e->st, &g);
     if (err != cudaSuccess) return efail(FM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(err));
     err = cudaGraphInstantiate(&e->graph, g, 0);
     cudaGraphDestroy(g);
     if (err != cudaSuccess) return efail(FM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(err));
     e->graph_tpm = e->tpm;
+    e->graph_x = e->need_x;
     return FM_OK;
+}
+
+// A captured tick serves the resident jobs while its slot grid covers every
+// resident slot and none of its grids is more than 4x the load's extent (a
+// power-of-two bucket each), so the graph is recaptured only when the load
+// grows past a bucket or falls well below it.
+bool extent_ok(const fm::TickExtent &g, const fm::TickExtent &n)
+{
+    auto near = [](int have, int want) { return have >= want && have <= 4 * want; };
+    return near(g.slots, n.slots) && near(g.mols, n.mols) && near(g.cells, n.cells);
 }
 
 double pshift(double rc)
@@ -394,9 +407,9 @@ int autotune(fm_engine *e)
     float best = 1e30f;
     int best_t = 4;
     for (int t : cands) {
-        fm::eng_force_only(e->d, t, e->st);
+        fm::eng_force_only(e->d, t, e->need_x.mols, e->st);
         cudaEventRecord(a, e->st);
-        for (int r = 0; r < 3; r++) fm::eng_force_only(e->d, t, e->st);
+        for (int r = 0; r < 3; r++) fm::eng_force_only(e->d, t, e->need_x.mols, e->st);
         cudaEventRecord(b, e->st);
         cudaEventSynchronize(b);
         float ms = 0.f;
@@ -412,15 +425,26 @@ int autotune(fm_engine *e)
     return FM_OK;
 }
 
-// High-water marks of the molecule and cell arenas over the resident jobs.
+int bucket(int n, int lo, int cap)
+{
+    int b = lo;
+    while (b < n && b < cap) b *= 2;
+    return std::min(b, cap);
+}
+
+// High-water marks of the molecule and cell arenas over the resident jobs, and
+// the launch extents they call for.
 int update_hwm(fm_engine *e)
 {
-    int mh = 0, ch = 0;
-    for (auto &j : e->resident) {
+    int mh = 0, ch = 0, top = 0;
+    for (size_t k = 0; k < e->resident.size(); k++) {
+        const Job &j = e->resident[k];
         if (j.slot < 0) continue;
         mh = std::max<int>(mh, (int)(j.mol_off + j.p.np));
         ch = std::max<int>(ch, (int)(j.cell_off + j.ncell));
+        top = (int)k + 1;
     }
+    e->need_x = {bucket(top, 8, e->d.nslots), bucket(mh, 4096, e->d.mol_cap), bucket(ch, 4096, e->d.cell_cap)};
     int hw[2] = {mh, ch};
     EN_CUDA(cudaMemcpyAsync(&e->d.flags->mol_hwm, hw, sizeof hw, cudaMemcpyHostToDevice, e->st));
     EN_CUDA(cudaStreamSynchronize(e->st));
@@ -596,7 +620,7 @@ extern "C" int fm_engine_step_chunk(fm_engine *e, int32_t *resident_out, int32_t
     EN_TRY(update_hwm(e));
     if (nres > 0) {
         if (!e->tuned) EN_TRY(autotune(e));
-        if (!e->graph || e->graph_tpm != e->tpm) EN_TRY(capture(e));
+        if (!e->graph || e->graph_tpm != e->tpm || !extent_ok(e->graph_x, e->need_x)) EN_TRY(capture(e));
         EN_CUDA(cudaGraphLaunch(e->graph, e->st));
         e->ticks += e->p.ticks_per_chunk;
         e->launches += (int64_t)fm::eng_kernels_per_tick() * e->p.ticks_per_chunk;

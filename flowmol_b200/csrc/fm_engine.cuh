@@ -110,9 +110,17 @@ constexpr int RED_W = 24;   // doubles per partial: (sum, compensation) x up to 
 
 __host__ __device__ inline double4 *eng_pos(const EngDev &d, int pset) { return pset ? d.pos1 : d.pos0; }
 
+// Launch extents of a captured tick: the slot-indexed grids (one block row per
+// slot) cover slots [0, slots), which must include every resident slot; the
+// molecule and cell grids are grid-stride loops, so `mols` and `cells` only
+// size them to the resident load (an empty block still costs launch time).
+struct TickExtent {
+    int slots, mols, cells;
+};
+
 // Launchers (fm_engine.cu); `tpm` = lanes per molecule of the force kernel.
-void eng_tick(const EngDev &d, int tpm, cudaStream_t st);
-void eng_force_only(const EngDev &d, int tpm, cudaStream_t st);  // autotuner: forces of running list jobs
+void eng_tick(const EngDev &d, int tpm, const TickExtent &x, cudaStream_t st);
+void eng_force_only(const EngDev &d, int tpm, int mols, cudaStream_t st);  // autotuner: forces of running list jobs
 void eng_scatter_job(const EngDev &d, int slot, int mol_off, int n, const double *r3, const double *v3,
                      const int32_t *tag, const double *rteth3, const double *slidev3, cudaStream_t st);
 void eng_claim_cells(const EngDev &d, int slot, int cell_off, int ncell, cudaStream_t st);

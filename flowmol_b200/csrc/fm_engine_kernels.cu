@@ -931,9 +931,9 @@ __global__ void k_e_release(EngDev d, int mol_off, int n, int cell_off, int ncel
 }
 
 template <int TPM>
-void launch_force_t(const EngDev &d, bool force_only, cudaStream_t st)
+void launch_force_t(const EngDev &d, int mols, bool force_only, cudaStream_t st)
 {
-    const int g = sgrid((long long)d.mol_cap * TPM, EF_THREADS, 8);
+    const int g = sgrid((long long)mols * TPM, EF_THREADS, 8);
     if (force_only) {
         if (d.precision == 0) k_e_force<TPM, 0, true, false><<<g, EF_THREADS, 0, st>>>(d);
         else k_e_force<TPM, 1, true, false><<<g, EF_THREADS, 0, st>>>(d);
@@ -948,14 +948,14 @@ void launch_force_t(const EngDev &d, bool force_only, cudaStream_t st)
     }
 }
 
-void launch_force_any(const EngDev &d, int tpm, bool force_only, cudaStream_t st)
+void launch_force_any(const EngDev &d, int tpm, int mols, bool force_only, cudaStream_t st)
 {
     switch (tpm) {
-    case 1: launch_force_t<1>(d, force_only, st); break;
-    case 2: launch_force_t<2>(d, force_only, st); break;
-    case 4: launch_force_t<4>(d, force_only, st); break;
-    case 16: launch_force_t<16>(d, force_only, st); break;
-    default: launch_force_t<8>(d, force_only, st); break;
+    case 1: launch_force_t<1>(d, mols, force_only, st); break;
+    case 2: launch_force_t<2>(d, mols, force_only, st); break;
+    case 4: launch_force_t<4>(d, mols, force_only, st); break;
+    case 16: launch_force_t<16>(d, mols, force_only, st); break;
+    default: launch_force_t<8>(d, mols, force_only, st); break;
     }
 }
 
@@ -963,28 +963,33 @@ void launch_force_any(const EngDev &d, int tpm, bool force_only, cudaStream_t st
 
 int eng_kernels_per_tick() { return 15; }
 
-void eng_tick(const EngDev &d, int tpm, cudaStream_t st)
+void eng_tick(const EngDev &d, int tpm, const TickExtent &x, cudaStream_t st)
 {
-    const int gm = sgrid(d.mol_cap, 256, 8);
-    const int gc = sgrid(d.cell_cap, 256, 8);
+    const int slots = std::min(x.slots, d.nslots);
+    const int gm = sgrid(std::min(x.mols, d.mol_cap), 256, 8);
+    const int gc = sgrid(std::min(x.cells, d.cell_cap), 256, 8);
     k_e_decide<<<1, EDEC, 0, st>>>(d);
     k_e_wrap_bin<<<gm, 256, 0, st>>>(d);
-    k_e_scan<<<d.nslots, ESCAN, 0, st>>>(d);
+    k_e_scan<<<slots, ESCAN, 0, st>>>(d);
     k_e_scatter<<<gm, 256, 0, st>>>(d);
     k_e_sort<<<gc, 256, 0, st>>>(d);
     k_e_reorder_gather<<<gm, 256, 0, st>>>(d);
     k_e_reorder_copy<<<gm, 256, 0, st>>>(d);
-    k_e_build<<<sgrid(d.cell_cap, NB_WARPS, 6), NB_THREADS, 0, st>>>(d);  // one resident wave
-    launch_force_any(d, tpm, false, st);
-    const dim3 gap(std::min(d.nslots, EAP_XBLOCKS), EAP_YBLOCKS);
+    // at most one resident wave
+    k_e_build<<<sgrid(std::min(x.cells, d.cell_cap), NB_WARPS, 6), NB_THREADS, 0, st>>>(d);
+    launch_force_any(d, tpm, std::min(x.mols, d.mol_cap), false, st);
+    const dim3 gap(std::min(slots, EAP_XBLOCKS), EAP_YBLOCKS);
     if (d.precision == 0) k_e_force_ap<0><<<gap, EAP_THREADS, 0, st>>>(d);
     else k_e_force_ap<1><<<gap, EAP_THREADS, 0, st>>>(d);
-    k_e_thermo<<<dim3(d.nslots, EY), ER, 0, st>>>(d);
+    k_e_thermo<<<dim3(slots, EY), ER, 0, st>>>(d);
     k_e_move_lfv<<<gm, 256, 0, st>>>(d);
-    k_e_record<<<dim3(d.nslots, EY), ER, 0, st>>>(d);
+    k_e_record<<<dim3(slots, EY), ER, 0, st>>>(d);
 }
 
-void eng_force_only(const EngDev &d, int tpm, cudaStream_t st) { launch_force_any(d, tpm, true, st); }
+void eng_force_only(const EngDev &d, int tpm, int mols, cudaStream_t st)
+{
+    launch_force_any(d, tpm, std::min(mols, d.mol_cap), true, st);
+}
 
 void eng_scatter_job(const EngDev &d, int slot, int mol_off, int n, const double *r3, const double *v3,
                      const int32_t *tag, const double *rteth3, const double *slidev3, cudaStream_t st)
