@@ -50,6 +50,10 @@ class FmParams(C.Structure):
         ("threads_per_molecule", C.c_int32),
         ("integration_algorithm", C.c_int32),
         ("list_build", C.c_int32),
+        ("solvent_flag", C.c_int32),
+        ("eps_pp", C.c_double),
+        ("eps_ps", C.c_double),
+        ("eps_ss", C.c_double),
     ]
 
 
@@ -134,13 +138,14 @@ class FmInput(C.Structure):
         ("rebuild_criteria", C.c_int32), ("fixed_rebuild", C.c_int32), ("initialnunits", C.c_int32 * 3),
         ("periodic", C.c_int32 * 3), ("sort_flag", C.c_int32), ("global_numbering", C.c_int32),
         ("pressure_outflag", C.c_int32), ("sLRC_flag", C.c_int32), ("mie_potential", C.c_int32),
-        ("nmonomers", C.c_int32), ("nthermo", C.c_int32), ("pad_", C.c_int32),
+        ("nmonomers", C.c_int32), ("nthermo", C.c_int32), ("solvent_flag", C.c_int32),
         ("density", C.c_double), ("rcutoff", C.c_double), ("inputtemperature", C.c_double), ("delta_t", C.c_double),
         ("delta_rneighbr", C.c_double * 3), ("k_c", C.c_double), ("R_0", C.c_double),
         ("tethereddisttop", C.c_double * 3), ("tethereddistbottom", C.c_double * 3),
         ("thermstattop", C.c_double * 3), ("thermstatbottom", C.c_double * 3), ("slidedisttop", C.c_double * 3),
         ("slidedistbottom", C.c_double * 3), ("fixdisttop", C.c_double * 3), ("fixdistbottom", C.c_double * 3),
         ("wallslidev", C.c_double * 3), ("teth_k", C.c_double * 3), ("thermostattemperature", C.c_double * 2),
+        ("targetconc", C.c_double), ("eps_pp", C.c_double), ("eps_ps", C.c_double), ("eps_ss", C.c_double),
     ]
 
     def as_dict(self):
@@ -267,7 +272,9 @@ def make_params(np_, domain, rcutoff, delta_rneighbr=(0.3, 0.3, 0.3), delta_t=0.
                 density=None, initialstep=0, simtime=0.0, force_list=FORCE_LIST_HALF, potential_flag=0,
                 rebuild_criteria=0, fixed_rebuild=1, sLRC_flag=0, precision=PRECISION_FP64, k_c=30.0,
                 R_0=1.5, nlist_capacity=0, threads_per_molecule=0, integration_algorithm=1,
-                list_build=0) -> FmParams:
+                list_build=0, solvent_flag=0, eps=(1.0, 1.0, 1.0)) -> FmParams:
+    """`eps` = (eps_pp, eps_ps, eps_ss), the SOLVENT_INFO well depths used with
+    solvent_flag 1."""
     p = FmParams()
     p.np = int(np_)
     for k in range(3):
@@ -291,6 +298,8 @@ def make_params(np_, domain, rcutoff, delta_rneighbr=(0.3, 0.3, 0.3), delta_t=0.
     p.threads_per_molecule = int(threads_per_molecule)
     p.integration_algorithm = int(integration_algorithm)
     p.list_build = int(list_build)
+    p.solvent_flag = int(solvent_flag)
+    p.eps_pp, p.eps_ps, p.eps_ss = (float(x) for x in eps)
     return p
 
 

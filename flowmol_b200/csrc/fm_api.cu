@@ -90,6 +90,15 @@ struct fm_handle {
 // geometry (setup_set_parameters.f90)
 // ---------------------------------------------------------------------------
 
+// rcutoff after set_parameters_cells: with the Soddemann solvent a rneighbr
+// below sod_cut raises it to sod_cut (:1871-1876), which the cells, potshift
+// (:1222) and the long-range corrections (:1226-1238) then use.
+static double effective_rcutoff(const fm_params *p)
+{
+    const double rneighbr = p->rcutoff + (p->delta_rneighbr[0] + p->delta_rneighbr[1] + p->delta_rneighbr[2]) / 3.0;
+    return p->potential_flag == 1 && p->solvent_flag == 1 && rneighbr < fm::SOD_CUT ? fm::SOD_CUT : p->rcutoff;
+}
+
 static int derive(const fm_params *p, int32_t nc[3], double cs[3], double *rn2, double *rc2, double *ps)
 {
     if (!p) return fail(FM_ERR_ARG, "null params");
@@ -99,11 +108,13 @@ static int derive(const fm_params *p, int32_t nc[3], double cs[3], double *rn2, 
     // rneighbr = rcutoff + mean(delta) (set_parameters_cells :1858-1859)
     double rneighbr = p->rcutoff + (p->delta_rneighbr[0] + p->delta_rneighbr[1] + p->delta_rneighbr[2]) / 3.0;
     double rneighbr2 = rneighbr * rneighbr;
-    if (p->potential_flag == 1 && rneighbr < p->R_0) rneighbr2 = p->R_0 * p->R_0;  // :1865-1869
-    for (int k = 0; k < 3; k++) nc[k] = (int32_t)std::floor(p->domain[k] / (p->rcutoff + p->delta_rneighbr[k]));
+    if (p->potential_flag == 1 && p->solvent_flag == 0 && rneighbr < p->R_0)
+        rneighbr2 = p->R_0 * p->R_0;  // :1865-1869
+    const double rcutoff = effective_rcutoff(p);  // rneighbr2 stays with the Soddemann raise
+    for (int k = 0; k < 3; k++) nc[k] = (int32_t)std::floor(p->domain[k] / (rcutoff + p->delta_rneighbr[k]));
     *rn2 = rneighbr2;
-    *rc2 = p->rcutoff * p->rcutoff;
-    *ps = 4.0 * (1.0 / p12(p->rcutoff) - 1.0 / p6(p->rcutoff));  // :1222
+    *rc2 = rcutoff * rcutoff;
+    *ps = 4.0 * (1.0 / p12(rcutoff) - 1.0 / p6(rcutoff));  // :1222
     bool few = nc[0] < 3 || nc[1] < 3 || nc[2] < 3;
     for (int k = 0; k < 3; k++) cs[k] = nc[k] > 0 ? p->domain[k] / (double)nc[k] : p->domain[k];
     if (few) return fail(FM_ERR_FEWCELLS, "domain should have at least 3 cells in x, y and z");
@@ -206,6 +217,9 @@ extern "C" int fm_create(const fm_params *p, fm_handle **out)
     if (p->potential_flag == 1 && p->force_list == 0)
         return fail(FM_ERR_ARG, "potential flag/force_list incompatible - only LJ available with all pairs");
     if (p->potential_flag == 1 && !(p->R_0 > 0.0 && p->k_c >= 0.0)) return fail(FM_ERR_ARG, "FENE needs R_0 > 0");
+    if (p->solvent_flag != 0 && p->solvent_flag != 1) return fail(FM_ERR_ARG, "solvent_flag must be 0 or 1");
+    if (p->solvent_flag == 1 && (p->potential_flag != 1 || p->force_list != 3))
+        return fail(FM_ERR_ARG, "the Soddemann solvent (solvent_flag 1) needs potential_flag 1 and force_list 3");
     if (p->rebuild_criteria != 0 && p->rebuild_criteria != 1)
         return fail(FM_ERR_ARG, "rebuild_criteria must be 0 (vmax) or 1 (fixed)");
     if (p->integration_algorithm != 0 && p->integration_algorithm != 1)
@@ -239,13 +253,15 @@ extern "C" int fm_create(const fm_params *p, fm_handle **out)
     d.potshift = ps;
     d.density = p->density > 0.0 ? p->density : (double)p->np / (p->domain[0] * p->domain[1] * p->domain[2]);
     if (p->sLRC_flag) {  // setup_set_parameters.f90:1226-1238
-        d.pot_slrc = 8.0 * kPi * d.density * (1.0 / (9.0 * std::pow(p->rcutoff, 9)) - 1.0 / (3.0 * p3(p->rcutoff)));
-        d.p_slrc = 8.0 * kPi * std::pow(d.density, 2.0) *
-                   (4.0 / (9.0 * std::pow(p->rcutoff, 9)) - 2.0 / (3.0 * p3(p->rcutoff)));
+        const double rc = effective_rcutoff(p);
+        d.pot_slrc = 8.0 * kPi * d.density * (1.0 / (9.0 * std::pow(rc, 9)) - 1.0 / (3.0 * p3(rc)));
+        d.p_slrc = 8.0 * kPi * std::pow(d.density, 2.0) * (4.0 / (9.0 * std::pow(rc, 9)) - 2.0 / (3.0 * p3(rc)));
     }
     d.tplot = p->tplot;
     d.integrator = p->integration_algorithm;
     d.potential_flag = p->potential_flag;
+    d.solvent = p->potential_flag == 1 && p->solvent_flag == 1 ? 1 : 0;
+    d.sod_eps[0] = p->eps_ss; d.sod_eps[1] = p->eps_ps; d.sod_eps[2] = p->eps_pp;
     d.k_c = p->k_c;
     d.R0 = p->R_0;
     d.R0_2 = p->R_0 * p->R_0;
@@ -404,6 +420,8 @@ extern "C" int fm_upload_monomers(fm_handle *h, const int32_t *chainID, const in
     FM_CUDA(cudaMemcpyAsync(h->d.chain, chainID, 4 * n, cudaMemcpyHostToDevice, h->st));
     FM_CUDA(cudaMemcpyAsync(h->d.subchain, subchainID, 4 * n, cudaMemcpyHostToDevice, h->st));
     FM_CUDA(cudaMemcpyAsync(h->d.bflag, bin_bflag, 16 * n, cudaMemcpyHostToDevice, h->st));
+    if (h->d.solvent) fm::launch_set_bead_flags(h->d, h->st);
+    FM_CUDA(cudaGetLastError());
     FM_CUDA(cudaStreamSynchronize(h->st));
     return FM_OK;
 }
@@ -414,6 +432,7 @@ extern "C" int fm_set_mie(fm_handle *h, const fm_mie_tables *t, const int32_t *m
 {
     if (!h || !t || !moltype) return fail(FM_ERR_ARG, "null argument");
     if (h->stage != 1) return fail(FM_ERR_STATE, "set the Mie tables after fm_upload_state and before fm_setup");
+    if (h->d.solvent) return fail(FM_ERR_ARG, "the Mie potential is not combined with the Soddemann solvent here");
     const int nt = t->ntypes;
     if (nt < 1 || nt > FM_MIE_MAXTYPES) return fail(FM_ERR_ARG, "ntypes out of range (1 .. FM_MIE_MAXTYPES)");
     if (!t->mass || !t->epsilon || !t->lambdar || !t->lambdaa || !t->C || !t->alpha || !t->potshift ||

@@ -51,6 +51,14 @@ struct FmRecord {
 // (alpha la) s^(la/2+1)), Mie_energy = (C eps)(s^(lr/2) - alpha s^(la/2)) -
 // potshift, harmonic bonds -k (r - r0)/r and k/2 (r - r0)^2.
 constexpr int MIE_MAXT = 16;
+
+// Soddemann solvent (polymer_info_MD, modules.f90:456-462).  sod_a, sod_b and
+// wca_cut2 are written there as default-real literals, so the FP64 parameters
+// hold their single-precision roundings: these are those values, exactly.
+constexpr double SOD_CUT = 1.5, SOD_CUT2 = 2.25;
+constexpr double SOD_A = 0x1.96274p+1;         // 3.1730728678 as REAL(4) = 3.1730728149414062
+constexpr double SOD_B = -0x1.b6639ap-1;       // -0.85622864544 as REAL(4) = -0.8562286496162415
+constexpr double SOD_WCA_CUT2 = 0x1.428a3p+0;  // 1.25992104989487 as REAL(4) = 1.2599210739135742
 struct FmMiePair {
     double ceps, lr, ala, er1, ea1, er, ea, alpha, shift, k, r0;
 };
@@ -99,6 +107,10 @@ struct FmDev {
     // Mie_potential 1: per-type-pair constants, per-type masses; a molecule's
     // type (1-based) rides in the w component of its position
     int build_blocks;            // list build: one warp per 2x2x2 cells (sparse systems)
+    // solvent_flag 1: Soddemann well depth by chain beads in the pair (eps_ss,
+    // eps_ps, eps_pp); a molecule's bead flag (chainID != 0) rides in w
+    int solvent;
+    double sod_eps[3];
     int mie;
     const FmMiePair *mie_pair;   // [(ti-1) + MIE_MAXT*(tj-1)]
     const double *mie_mass;      // [ti-1]
@@ -164,6 +176,7 @@ int all_pairs_blocks(int n);
 // Layout conversion between the reference's (3,n) column-major arrays and
 // the device layout; `order` maps upload index -> slot.
 void launch_set_types(const FmDev &d, cudaStream_t st);
+void launch_set_bead_flags(const FmDev &d, cudaStream_t st);
 void launch_scatter_state(const FmDev &d, const double *r3, const double *v3, const double *a3,
                           cudaStream_t st);
 void launch_gather_state(const FmDev &d, double *r3, double *v3, double *a3, int32_t *gid,

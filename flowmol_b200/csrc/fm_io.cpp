@@ -343,17 +343,50 @@ extern "C" int fm_read_input(const char *path, fm_input *in)
         int32_t mie[1];
         if (opt_i("MIE_POTENTIAL", mie, 1)) in->mie_potential = mie[0];
     }
-    {  // DENSE_FENE: nmonomers, k_c, r_0, density, initialnunits(3) (setup_read_input.f90:229-254)
+    // INITIAL_CONFIG_FLAG 1 names a special case whose own block follows
+    // (setup_read_input.f90:188-199); the polymer ones set potential_flag 1 and
+    // the WCA cutoff (:232, 256)
+    std::string special;
+    {
+        long at = deck.find("INITIAL_CONFIG_FLAG");
+        int32_t icf = 0;
+        if (at >= 0 && deck.values(at, 2, vals) && to_int(vals[0], icf) && icf == 1) special = vals[1];
+    }
+    if (special == "dense_fene") {  // DENSE_FENE: nmonomers, k_c, r_0, density, initialnunits(3) (:229-254)
         long at = deck.find("DENSE_FENE");
-        if (at >= 0 && deck.values(at, 7, vals)) {
-            double dd;
-            in->potential_flag = 1;
-            to_int(vals[0], in->nmonomers);
-            if (to_double(vals[1], dd)) in->k_c = dd;
-            if (to_double(vals[2], dd)) in->R_0 = dd;
-            if (to_double(vals[3], dd)) in->density = dd;
-            for (int k = 0; k < 3; k++) to_int(vals[(size_t)(4 + k)], in->initialnunits[k]);
-            in->rcutoff = std::pow(2.0, 1.0 / 6.0);  // :232
+        if (at < 0 || !deck.values(at, 7, vals)) return iofail(FM_ERR_IO, "dense_fene needs the DENSE_FENE block");
+        double dd;
+        in->potential_flag = 1;
+        to_int(vals[0], in->nmonomers);
+        if (to_double(vals[1], dd)) in->k_c = dd;
+        if (to_double(vals[2], dd)) in->R_0 = dd;
+        if (to_double(vals[3], dd)) in->density = dd;
+        for (int k = 0; k < 3; k++) to_int(vals[(size_t)(4 + k)], in->initialnunits[k]);
+        in->rcutoff = std::pow(2.0, 1.0 / 6.0);
+    }
+    if (special == "fene_solution" || special == "single_fene") {
+        // FENE_SOLUTION: nmonomers, k_c, r_0, density, targetconc (:253-273)
+        long at = deck.find("FENE_SOLUTION");
+        if (at < 0 || !deck.values(at, 5, vals))
+            return iofail(FM_ERR_IO, special + " needs the FENE_SOLUTION block");
+        double dd;
+        in->potential_flag = 1;
+        to_int(vals[0], in->nmonomers);
+        if (to_double(vals[1], dd)) in->k_c = dd;
+        if (to_double(vals[2], dd)) in->R_0 = dd;
+        if (to_double(vals[3], dd)) in->density = dd;
+        if (to_double(vals[4], dd)) in->targetconc = dd;
+        in->rcutoff = std::pow(2.0, 1.0 / 6.0);
+        // SOLVENT_INFO: flag, then eps_pp, eps_ps, eps_ss when it is 1 (:275-296)
+        at = deck.find("SOLVENT_INFO");
+        if (at < 0 || !deck.values(at, 1, vals) || !to_int(vals[0], in->solvent_flag))
+            return iofail(FM_ERR_IO, special + " needs the SOLVENT_INFO block");
+        if (in->solvent_flag == 1) {
+            if (!deck.values(at, 4, vals) || !to_double(vals[1], in->eps_pp) || !to_double(vals[2], in->eps_ps) ||
+                !to_double(vals[3], in->eps_ss))
+                return iofail(FM_ERR_IO, "SOLVENT_INFO 1 needs eps_pp, eps_ps and eps_ss");
+        } else if (in->solvent_flag != 0) {
+            return iofail(FM_ERR_IO, "Unrecognised solvent flag!");  // :293
         }
     }
     opt_d("TETHEREDDISTTOP", in->tethereddisttop, 3);

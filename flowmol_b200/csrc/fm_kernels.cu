@@ -432,7 +432,57 @@ template <int PREC, bool REC>
 __device__ __forceinline__ void pair_acc(const FmDev &d, double r2, double dx, double dy, double dz, double wi,
                                          double wj, double &fx, double &fy, double &fz, double &pe, double &vir)
 {
-    constexpr bool F32 = (PREC & 1) != 0, MIE = (PREC & 2) != 0;
+    constexpr bool F32 = (PREC & 1) != 0, MIE = (PREC & 2) != 0, SOD = (PREC & 4) != 0;
+    if (SOD) {
+        // simulation_compute_forces_Soddemann_neigbr_halfint (:793-888): WCA
+        // inside wca_cut2, the cosine well eps a s^2 sin(a s + b) beyond it
+        // (the reference's expression, s = 1/r^2); no potshift
+        const double eps = d.sod_eps[(int)wi + (int)wj];
+        const bool wca = r2 < SOD_WCA_CUT2;
+        if (!F32) {
+            const double s = __drcp_rn(r2);
+            const double s2 = s * s;
+            double acc;
+            if (wca) {
+                const double s4 = s2 * s2;
+                acc = 48.0 * (s4 * s2 * s - 0.5 * s4);  // get_accijmag = LJ_accijmag
+            } else {
+                acc = (eps * SOD_A * s2) * sin(s * SOD_A + SOD_B);
+            }
+            fx += acc * dx; fy += acc * dy; fz += acc * dz;
+            if (REC) {
+                if (wca) {
+                    const double s3 = s2 * s, s6 = s3 * s3;
+                    pe += 4.0 * (s6 - s3 + 0.25) - eps;
+                } else {
+                    pe += 0.5 * eps * (cos(SOD_A * r2 + SOD_B) - 1.0);
+                }
+                vir += acc * r2;
+            }
+        } else {
+            const float s = __frcp_rn((float)r2);
+            const float s2 = s * s;
+            float accf;
+            if (wca) {
+                const float s4 = s2 * s2;
+                accf = 48.0f * (s4 * s2 * s - 0.5f * s4);
+            } else {
+                accf = ((float)eps * (float)SOD_A * s2) * sinf(s * (float)SOD_A + (float)SOD_B);
+            }
+            const double acc = (double)accf;
+            fx = fma(acc, dx, fx); fy = fma(acc, dy, fy); fz = fma(acc, dz, fz);
+            if (REC) {
+                if (wca) {
+                    const float s3 = s2 * s, s6 = s3 * s3;
+                    pe += (double)(4.0f * (s6 - s3 + 0.25f)) - eps;
+                } else {
+                    pe += (double)(0.5f * (float)eps * (cosf((float)SOD_A * (float)r2 + (float)SOD_B) - 1.0f));
+                }
+                vir += acc * r2;
+            }
+        }
+        return;
+    }
     if (MIE) {
         const FmMiePair &m = d.mie_pair[((int)wi - 1) + MIE_MAXT * ((int)wj - 1)];
         if (!F32) {
@@ -886,6 +936,15 @@ __global__ void k_set_types(FmDev d)
     cur_pos(d, d.sc->pset)[u].w = (double)d.mie_type_up[u];
 }
 
+// solvent_flag 1: w = 1 for a chain bead, 0 for a solvent molecule (chainID
+// 0); the chain ids are still in upload order = slot order here
+__global__ void k_set_bead_flags(FmDev d)
+{
+    int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= d.n) return;
+    cur_pos(d, d.sc->pset)[u].w = d.chain[u] != 0 ? 1.0 : 0.0;
+}
+
 // upload order u -> slot u (uploads start in upload order)
 __global__ void k_scatter_state(FmDev d, const double *r3, const double *v3, const double *a3)
 {
@@ -996,11 +1055,13 @@ static void launch_force_tpm(const FmDev &d, int record, int mode, cudaStream_t 
     const int g = force_blocks(d.n, TPM);
 #define FM_FORCE_CASE(R, M)                                                                     \
     if (record == R && mode == M) {                                                             \
-        switch (d.precision + 2 * d.mie) {                                                      \
+        switch (d.precision + 2 * d.mie + 4 * d.solvent) {                                      \
         case 0: k_force<TPM, R, M, 0><<<g, FORCE_THREADS, 0, st>>>(d); break;                   \
         case 1: k_force<TPM, R, M, 1><<<g, FORCE_THREADS, 0, st>>>(d); break;                   \
         case 2: k_force<TPM, R, M, 2><<<g, FORCE_THREADS, 0, st>>>(d); break;                   \
-        default: k_force<TPM, R, M, 3><<<g, FORCE_THREADS, 0, st>>>(d); break;                  \
+        case 3: k_force<TPM, R, M, 3><<<g, FORCE_THREADS, 0, st>>>(d); break;                   \
+        case 4: k_force<TPM, R, M, 4><<<g, FORCE_THREADS, 0, st>>>(d); break;                   \
+        default: k_force<TPM, R, M, 5><<<g, FORCE_THREADS, 0, st>>>(d); break;                  \
         }                                                                                       \
         return;                                                                                 \
     }
@@ -1055,6 +1116,11 @@ void launch_pair_digest(const FmDev &d, const int32_t *glob_of_upload, cudaStrea
 }
 
 void launch_set_types(const FmDev &d, cudaStream_t st) { k_set_types<<<nblk(d.n, 256), 256, 0, st>>>(d); }
+
+void launch_set_bead_flags(const FmDev &d, cudaStream_t st)
+{
+    k_set_bead_flags<<<nblk(d.n, 256), 256, 0, st>>>(d);
+}
 
 void launch_scatter_state(const FmDev &d, const double *r3, const double *v3, const double *a3, cudaStream_t st)
 {

@@ -86,3 +86,30 @@ def fene_melt(nchains, nmonomers=8, density=0.85, temperature=1.0, fill=0.9, see
         partners = [p for p in (s - 1, s + 1) if 1 <= p <= nmonomers]
         bf[sub == s] = bflag_words(partners)
     return r, v, chain_id, sub, funcy, bf, np.array([L, L, L])
+
+
+def mark_solvent(chain, subchain, funcy, bflag, chain_ids):
+    """Turns whole chains into solvent molecules as mark_chain_as_solvent does
+    (modules.f90:681-707): chainID 0, subchainID 1, funcy 0, no bond flags.
+    Returns new arrays."""
+    chain, subchain, funcy, bflag = (np.array(x, copy=True) for x in (chain, subchain, funcy, bflag))
+    sel = np.isin(chain, np.asarray(chain_ids))
+    chain[sel] = 0
+    subchain[sel] = 1
+    funcy[sel] = 0
+    bflag[sel] = 0
+    return chain, subchain, funcy, bflag
+
+
+def fene_solution(nchains, nmonomers=8, density=0.85, targetconc=0.5, temperature=1.0,
+                  seed=lattice.SEED_BASE + 3):
+    """A bead-spring melt whose chains are turned into solvent (seeded choice)
+    until the chain-bead fraction is `targetconc`, the end state of the
+    reference's fene_solution start (setup_initialise_microstate.f90:459-486).
+    (r, v, chain, subchain, funcy, bflag(n,4), domain)."""
+    r, v, ch, sub, fy, bf, dom = fene_melt(nchains, nmonomers, density, temperature, seed=seed)
+    rng = np.random.Generator(np.random.Philox(int(seed) ^ 0x5D))
+    keep = int(round(targetconc * nchains))
+    drop = rng.permutation(np.arange(1, nchains + 1))[:nchains - keep]
+    ch, sub, fy, bf = mark_solvent(ch, sub, fy, bf, drop)
+    return r, v, ch, sub, fy, bf, dom

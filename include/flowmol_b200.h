@@ -78,6 +78,10 @@ typedef struct fm_params {
     int32_t threads_per_molecule; /* force kernel lanes per molecule; 0 = autotuned */
     int32_t integration_algorithm; /* INTEGRATION_ALGORITHM: 0 leap-frog (NVE), 1 velocity Verlet */
     int32_t list_build;           /* FM_LIST_BUILD_*: one warp per cell or per 2x2x2 cells (same rows) */
+    int32_t solvent_flag;         /* SOLVENT_INFO with potential_flag 1: 0 all beads alike (WCA + bonds),
+                                     1 Soddemann solvent of variable quality (force_list 3 only) */
+    double eps_pp, eps_ps, eps_ss; /* SOLVENT_INFO well depths: polymer-polymer, polymer-solvent,
+                                      solvent-solvent (solvent_flag 1) */
 } fm_params;
 
 /* List build granularity: automatic (2x2x2 blocks below 8 molecules per
@@ -107,7 +111,9 @@ typedef struct fm_handle fm_handle;
 /* Geometry the reference derives from the parameters (no device needed):
  * ncells = floor(domain/(rcutoff+delta)), cellsidelength = domain/ncells,
  * rneighbr2 = (rcutoff + mean(delta))^2 with the FENE R_0 override, and
- * potshift = 4(rc^-12 - rc^-6).  Replaces set_parameters_cells
+ * potshift = 4(rc^-12 - rc^-6).  With solvent_flag 1 a rneighbr below the
+ * Soddemann range 1.5 raises rcutoff (and so the cells) to 1.5 and leaves
+ * rneighbr2 as it is (:1871-1876).  Replaces set_parameters_cells
  * (setup_set_parameters.f90:1848-1903) and the potshift line (:1222).
  * Returns FM_ERR_FEWCELLS where the reference aborts. */
 FM_API int fm_derive_geometry(const fm_params *p, int32_t ncells[3], double cellsidelength[3],
@@ -141,7 +147,12 @@ FM_API int fm_download_state(fm_handle *h, double *r, double *v, double *a, int3
  * molecule in upload order -- chainID, subchainID and the four bin_bflag
  * words (polymer_info_MD; bin_bflag is (4, n)).  Call after fm_upload_state,
  * before fm_setup.  Bonds are then found while lists are built, as
- * check_update_adjacentbeadinfo does (linklist.f90:2542-2584). */
+ * check_update_adjacentbeadinfo does (linklist.f90:2542-2584).  With
+ * solvent_flag 1, chainID 0 marks a solvent molecule (mark_chain_as_solvent,
+ * modules.f90:681-707) and a pair's Soddemann well depth is eps_ss, eps_ps or
+ * eps_pp by how many of the two are chain beads
+ * (simulation_compute_forces_Soddemann_neigbr_halfint,
+ * simulation_compute_forces.f90:793-888). */
 FM_API int fm_upload_monomers(fm_handle *h, const int32_t *chainID, const int32_t *subchainID,
                               const int32_t *bin_bflag);
 /* Mie_potential 1 (setup_set_parameters.f90:1208-1216): non-bonded pairs
@@ -294,12 +305,15 @@ typedef struct fm_input {
     int32_t ensemble, integration_algorithm, force_list, potential_flag;
     int32_t nsteps, tplot, rebuild_criteria, fixed_rebuild;
     int32_t initialnunits[3], periodic[3];
-    int32_t sort_flag, global_numbering, pressure_outflag, sLRC_flag, mie_potential, nmonomers, nthermo, pad_;
+    int32_t sort_flag, global_numbering, pressure_outflag, sLRC_flag, mie_potential, nmonomers, nthermo;
+    int32_t solvent_flag;        /* SOLVENT_INFO [1] */
     double density, rcutoff, inputtemperature, delta_t, delta_rneighbr[3], k_c, R_0;
     double tethereddisttop[3], tethereddistbottom[3], thermstattop[3], thermstatbottom[3];
     double slidedisttop[3], slidedistbottom[3], fixdisttop[3], fixdistbottom[3], wallslidev[3];
     double teth_k[3];            /* TETHERCOEFFICIENTS k2, k4, k6 */
     double thermostattemperature[2];
+    double targetconc;           /* FENE_SOLUTION [5] */
+    double eps_pp, eps_ps, eps_ss; /* SOLVENT_INFO [2-4] when solvent_flag is 1 */
 } fm_input;
 
 FM_API int fm_read_input(const char *path, fm_input *in);

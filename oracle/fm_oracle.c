@@ -49,6 +49,8 @@ typedef struct orc {
     int integration_algorithm; /* 0 leap-frog, 1 velocity Verlet */
     int potential_flag;    /* 0 LJ, 1 FENE polymer */
     double k_c, R_0;
+    int solvent_flag;      /* 1: Soddemann solvent (chainID 0 = solvent molecule) */
+    double sod_eps[3];     /* well depth by chain beads in the pair: eps_ss, eps_ps, eps_pp */
     int max_funcy;
     /* ---- state (arrays_MD) ---- */
     double *r, *v, *a;        /* (3, cap) */
@@ -114,18 +116,32 @@ void orc_global_domain(const int nunits[3], double density, double domain_out[3]
     *volume_out = vol;
 }
 
-/* set_parameters_cells (setup_set_parameters.f90:1848-1903).  Returns
- * ORC_ERR_FEWCELLS where the reference aborts (fewer than 3 cells). */
-int orc_set_parameters_cells(const double domain[3], double rcutoff, const double delta[3],
-                             int potential_flag, double R_0, int ncells_out[3],
+/* Soddemann solvent constants (polymer_info_MD, modules.f90:456-462).  sod_a,
+ * sod_b and wca_cut2 are default-real literals in the reference, so their
+ * FP64 values are the single-precision roundings: (double)(float)literal. */
+#define SOD_CUT 1.5
+#define SOD_CUT2 2.25
+static double sod_a(void) { return (double)3.1730728678f; }
+static double sod_b(void) { return (double)-0.85622864544f; }
+static double wca_cut2(void) { return (double)1.25992104989487f; }
+
+/* set_parameters_cells (setup_set_parameters.f90:1848-1903).  solvent_flag
+ * 1 (Soddemann) raises rcutoff to sod_cut when rneighbr is below it and
+ * leaves rneighbr2 (1871-1876); *rcutoff_io is rcutoff in and after.
+ * Returns ORC_ERR_FEWCELLS where the reference aborts (fewer than 3 cells). */
+int orc_set_parameters_cells(const double domain[3], double *rcutoff_io, const double delta[3],
+                             int potential_flag, int solvent_flag, double R_0, int ncells_out[3],
                              double cellside_out[3], double *rneighbr2_out)
 {
+    double rcutoff = *rcutoff_io;
     double rneighbr = rcutoff + (delta[0] + delta[1] + delta[2]) / 3.0;
     double rneighbr2 = rneighbr * rneighbr;
-    if (potential_flag == 1 && rneighbr < R_0) { /* FENE override, 1865-1869 */
+    if (potential_flag == 1 && solvent_flag == 0 && rneighbr < R_0) { /* FENE override, 1865-1869 */
         rneighbr = R_0;
         rneighbr2 = R_0 * R_0;
     }
+    if (potential_flag == 1 && solvent_flag == 1 && rneighbr < SOD_CUT) rcutoff = SOD_CUT;
+    *rcutoff_io = rcutoff;
     for (int k = 0; k < 3; k++) ncells_out[k] = (int)floor(domain[k] / (rcutoff + delta[k]));
     *rneighbr2_out = rneighbr2;
     if (ncells_out[0] < 3 || ncells_out[1] < 3 || ncells_out[2] < 3) return ORC_ERR_FEWCELLS;
@@ -251,7 +267,8 @@ orc *orc_create(int np, const double domain[3], double rcutoff, const double del
         s->pressure_sLRC = 8.0 * pi * (density * density) *
                            (4.0 / (9.0 * pow(rcutoff, 9)) - 2.0 / (3.0 * p3(rcutoff)));
     }
-    int rc = orc_set_parameters_cells(s->domain, rcutoff, delta, potential_flag, R_0,
+    double rc_cells = rcutoff;
+    int rc = orc_set_parameters_cells(s->domain, &rc_cells, delta, potential_flag, 0, R_0,
                                       s->ncells, s->cellsidelength, &s->rneighbr2);
     if (rc != ORC_OK && force_list != 0) { *err = rc; orc_free(s); return NULL; }
     if (rc != ORC_OK) { s->ncells[0] = s->ncells[1] = s->ncells[2] = 1; }
@@ -306,6 +323,43 @@ void orc_free(orc *s)
     free(s->cellnp); free(s->cellhead); free(s->cn_molno); free(s->cn_next);
     free(s->Nlist); free(s->nhead); free(s->nn_molno); free(s->nn_next);
     free(s);
+}
+
+/* SOLVENT_INFO (setup_read_input.f90:275-296): solvent_flag and the well
+ * depths, then the geometry again as set_parameters_cells derives it with the
+ * flag (setup_set_parameters.f90:1848-1903); potshift and the long-range
+ * corrections follow the raised rcutoff (:1222-1238).  Call before setup. */
+int orc_set_solvent(orc *s, int solvent_flag, double eps_pp, double eps_ps, double eps_ss)
+{
+    if (solvent_flag != 0 && solvent_flag != 1) return ORC_ERR_PARAM;
+    if (solvent_flag == 1 && (s->potential_flag != 1 || s->force_list != 3)) return ORC_ERR_PARAM;
+    s->solvent_flag = solvent_flag;
+    s->sod_eps[0] = eps_ss; s->sod_eps[1] = eps_ps; s->sod_eps[2] = eps_pp;
+    double rc = s->rcutoff;
+    int ncells[3];
+    double cs[3], rn2;
+    int rc_err = orc_set_parameters_cells(s->domain, &rc, s->delta_rneighbr, s->potential_flag, solvent_flag,
+                                          s->R_0, ncells, cs, &rn2);
+    if (rc_err) return rc_err;
+    s->rcutoff = rc;
+    s->rcutoff2 = rc * rc;
+    s->rneighbr2 = rn2;
+    s->potshift = orc_potshift(rc);
+    if (s->potential_sLRC != 0.0 || s->pressure_sLRC != 0.0) {
+        const double pi = 3.14159265358979323846;
+        s->potential_sLRC = 8.0 * pi * s->density * (1.0 / (9.0 * pow(rc, 9)) - 1.0 / (3.0 * p3(rc)));
+        s->pressure_sLRC = 8.0 * pi * (s->density * s->density) * (4.0 / (9.0 * pow(rc, 9)) - 2.0 / (3.0 * p3(rc)));
+    }
+    for (int k = 0; k < 3; k++) { s->ncells[k] = ncells[k]; s->cellsidelength[k] = cs[k]; }
+    int nt = (ncells[0] + 2) * (ncells[1] + 2) * (ncells[2] + 2);
+    if (nt != s->ncell_tot) {
+        int *np_ = (int *)xcalloc((size_t)nt, sizeof(int)), *hd = (int *)xcalloc((size_t)nt, sizeof(int));
+        if (!np_ || !hd) { free(np_); free(hd); return ORC_ERR_ALLOC; }
+        free(s->cellnp); free(s->cellhead);
+        s->cellnp = np_; s->cellhead = hd;
+        s->ncell_tot = nt;
+    }
+    return ORC_OK;
 }
 
 /* Accessors used by the ctypes wrapper. */
@@ -862,6 +916,52 @@ static void forces_halfint(orc *s)
     }
 }
 
+/* simulation_compute_forces_Soddemann_neigbr_halfint (:793-888): half list;
+ * WCA (get_accijmag, LJ) below wca_cut2 and the reference's cosine-well
+ * expression out to sod_cut2, the well depth by how many of the pair are
+ * chain beads (chainID != 0; an image has its source's).  The minimum-image
+ * line (:821) leaves rij as it is for every listed pair (|rij| < L/2, as
+ * there are at least 3 cells of rcutoff + delta per axis), so it is not
+ * repeated.  Accelerations are not divided by a mass (:852-860); no
+ * pressure-tensor term is recorded (the routine calls none). */
+static void forces_soddemann(orc *s)
+{
+    const int rec = (s->iter % s->tplot) == 0;
+    const int tev = (s->iter % s->teval) == 0;
+    const double A = sod_a(), B = sod_b(), W2 = wca_cut2();
+    double rij[3];
+    for (int i = 1; i <= s->np; i++) {
+        int node = s->nhead[i - 1];
+        for (int q = 0; q < s->Nlist[i - 1]; q++) {
+            int j = s->nn_molno[node - 1];
+            node = s->nn_next[node - 1];
+            double r2 = rij2_of(s, i, j, rij);
+            if (!(r2 < SOD_CUT2)) continue;
+            const int ptot = (s->chainID[i - 1] != 0) + (s->chainID[j - 1] != 0);
+            const double eps = s->sod_eps[ptot];
+            const double inv = 1.0 / r2;
+            double acc;
+            if (r2 < W2) acc = lj_accijmag(inv);
+            else acc = (eps * A * (inv * inv)) * sin(inv * A + B);
+            double *ai = &s->a[3 * (size_t)(i - 1)], *aj = &s->a[3 * (size_t)(j - 1)];
+            for (int k = 0; k < 3; k++) {
+                ai[k] = ai[k] + acc * rij[k];
+                aj[k] = aj[k] - acc * rij[k];
+            }
+            if (rec) {
+                double e = r2 < W2 ? 4.0 * (p6(inv) - p3(inv) + 0.25) - eps : 0.5 * eps * (cos(A * r2 + B) - 1.0);
+                s->potenergymol[i - 1] += e;
+                s->potenergymol[j - 1] += e;
+                s->virialmol[i - 1] += acc * r2;
+                s->virialmol[j - 1] += acc * r2;
+            } else if (tev) {
+                s->virialmol[i - 1] += acc * r2;
+                s->virialmol[j - 1] += acc * r2;
+            }
+        }
+    }
+}
+
 /* simulation_compute_forces_LJ_neigbr (:551-623): full list, i side only. */
 static void forces_full(orc *s)
 {
@@ -976,7 +1076,10 @@ int orc_compute_forces(orc *s)
     switch (s->force_list) {
     case 0: forces_AP(s); break;
     case 2: forces_full(s); break;
-    case 3: forces_halfint(s); break;
+    case 3:
+        if (s->potential_flag == 1 && s->solvent_flag == 1) forces_soddemann(s); /* :264-267 */
+        else forces_halfint(s);
+        break;
     default: return ORC_ERR_PARAM;
     }
     if (s->potential_flag == 1) {

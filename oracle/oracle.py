@@ -72,7 +72,9 @@ def lib():
         L.orc_run_vv.argtypes = [C.c_void_p, C.c_int, d3, C.c_int, i3]
         L.orc_global_domain.argtypes = [i3, C.c_double, d3, d3, d3]
         L.orc_set_parameters_cells.restype = C.c_int
-        L.orc_set_parameters_cells.argtypes = [d3, C.c_double, d3, C.c_int, C.c_double, i3, d3, d3]
+        L.orc_set_parameters_cells.argtypes = [d3, d3, d3, C.c_int, C.c_int, C.c_double, i3, d3, d3]
+        L.orc_set_solvent.restype = C.c_int
+        L.orc_set_solvent.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double]
         L.orc_lj_accijmag.restype = C.c_double
         L.orc_lj_accijmag.argtypes = [C.c_double]
         L.orc_lj_energy.restype = C.c_double
@@ -118,12 +120,13 @@ def global_domain(nunits, density):
     return dom, unit, float(vol[0])
 
 
-def cells(domain, rcutoff, delta, potential_flag=0, R_0=1.5):
+def cells(domain, rcutoff, delta, potential_flag=0, R_0=1.5, solvent_flag=0):
     d = np.ascontiguousarray(domain, dtype=np.float64)
     dl = np.ascontiguousarray(delta, dtype=np.float64)
     nc = np.zeros(3, np.int32); cs = np.zeros(3); rn2 = np.zeros(1)
-    rc = lib().orc_set_parameters_cells(_dp(d), float(rcutoff), _dp(dl), int(potential_flag), float(R_0),
-                                        _ip(nc), _dp(cs), _dp(rn2))
+    rcio = np.array([float(rcutoff)])
+    rc = lib().orc_set_parameters_cells(_dp(d), _dp(rcio), _dp(dl), int(potential_flag), int(solvent_flag),
+                                        float(R_0), _ip(nc), _dp(cs), _dp(rn2))
     return rc, nc, cs, float(rn2[0])
 
 
@@ -191,6 +194,11 @@ class Oracle:
         f = np.ascontiguousarray(funcy, np.int32)
         b = np.ascontiguousarray(bflag, np.int32).reshape(-1)
         lib().orc_set_monomers(self.h, _ip(c), _ip(s), _ip(f), _ip(b))
+
+    def set_solvent(self, solvent_flag, eps_pp=1.0, eps_ps=1.0, eps_ss=1.0):
+        """SOLVENT_INFO: 1 = Soddemann solvent of variable quality (chainID 0
+        marks a solvent molecule); re-derives the cells.  Before setup()."""
+        _check(lib().orc_set_solvent(self.h, int(solvent_flag), float(eps_pp), float(eps_ps), float(eps_ss)))
 
     def set_mie(self, tables, moltype):
         """Mie_potential 1: `tables` maps mass, epsilon, lambdar, lambdaa, C,

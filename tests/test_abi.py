@@ -3,6 +3,7 @@ include/flowmol_b200.h; host-only calls work without a GPU."""
 import ctypes as C
 import os
 import re
+import subprocess
 
 import pytest
 
@@ -20,11 +21,40 @@ def test_library_exports_header_symbols():
     assert declared == exported
 
 
-def test_struct_layouts_match_header():
-    # fm_params / fm_macro as ctypes must match the C layout the library uses
-    assert C.sizeof(api.FmMacro) == 4 + 4 + 8 * 9
+ABI_STRUCTS = {
+    "fm_params": api.FmParams, "fm_macro": api.FmMacro, "fm_engine_params": api.FmEngineParams,
+    "fm_mie_tables": api.FmMieTables, "fm_job": api.FmJob, "fm_job_result": api.FmJobResult,
+    "fm_restart_header": api.FmRestartHeader, "fm_input": api.FmInput,
+}
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """Every ctypes mirror has the C struct's size and, field by field, the
+    offsets and sizes gcc gives the header's declarations."""
     p = api.make_params(10, [10.0, 10.0, 10.0], 2.5)
     assert p.np == 10 and p.tplot == 100
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "flowmol_b200.h"', "int main(void) {"]
+    for cname, ct in ABI_STRUCTS.items():
+        lines.append(f'printf("{cname} . %zu 0\\n", sizeof({cname}));')
+        for fname, _ in ct._fields_:
+            lines.append(f'printf("{cname} {fname} %zu %zu\\n", sizeof((({cname} *)0)->{fname}), '
+                         f"offsetof({cname}, {fname}));")
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {}
+    for ln in out:
+        if ln.strip():
+            cname, fname, size, off = ln.split()
+            got[(cname, fname)] = (int(size), int(off))
+    for cname, ct in ABI_STRUCTS.items():
+        assert got[(cname, ".")][0] == C.sizeof(ct), cname
+        for fname, _ in ct._fields_:
+            f = getattr(ct, fname)
+            assert got[(cname, fname)] == (f.size, f.offset), (cname, fname)
 
 
 def test_errors_are_codes_not_aborts():

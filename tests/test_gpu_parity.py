@@ -439,6 +439,48 @@ def test_mie_polymer_harmonic_bonds(gpu_lib):
         assert row["potenergy"] == pytest.approx(ro[5], rel=1e-9)
 
 
+@pytest.mark.parametrize("prec", [api.PRECISION_FP64, api.PRECISION_FP32])
+def test_soddemann_polymer_solution(gpu_lib, prec):
+    """SOLVENT_INFO 1: 8-bead FENE chains in as many solvent molecules
+    (chainID 0), WCA + the Soddemann well (eps_pp 1.5, eps_ps 1.0, eps_ss 0.5)
+    + FENE bonds.  The Soddemann geometry (cells of rcutoff 1.5 + skin, list
+    range rneighbr 1.42246), bonds and pair set bit-exact; forces to 1e-12
+    (FP64) or 1e-5 (FP32 pair magnitudes); per-molecule PE; 100 steps."""
+    from flowmol_b200 import polymer
+    r, v, ch, sub, fy, bf, dom = polymer.fene_solution(192, targetconc=0.5)
+    r = lattice.jitter(r, 0.08, 92, dom)  # off the lattice: pairs in the cosine well from the start
+    eps = (1.5, 1.0, 0.5)
+    o = O.Oracle(r, v, dom, WCA_RC, tplot=20, potential_flag=1, k_c=30.0, R_0=1.5, density=0.85)
+    o.set_monomers(ch, sub, fy, bf)
+    o.set_solvent(1, *eps)
+    o.setup()
+    s = gpu_system(r, v, dom, WCA_RC, precision=prec, tplot=20, density=0.85, potential_flag=1, k_c=30.0,
+                   R_0=1.5, solvent_flag=1, eps=eps)
+    s.upload_monomers(ch, sub, bf)
+    s.setup()
+    key = lambda t: np.sort((t[0].astype(np.int64) << 32) | (t[1].astype(np.int64) << 5) | t[2])  # noqa: E731
+    assert np.array_equal(key(s.bonds()), key(o.bond_list()))
+    assert np.array_equal(canonical_full(*s.pair_list()), canonical_oracle(*o.pair_list()))
+    _, _, a, _ = s.download()
+    pe, _ = s.per_molecule()
+    if prec == api.PRECISION_FP32:
+        assert rel_err(a, o.a, F_FLOOR32).max() <= TOL32
+        s.close()
+        return
+    assert rel_err(a, o.a, 1.0).max() <= TOL64
+    np.testing.assert_allclose(pe, o.potenergymol, rtol=TOL64, atol=TOL64)
+    recs_o = o.run_vv(100)
+    s.records()
+    s.simulation_md(100)
+    recs = s.records()
+    assert [x["iter"] for x in recs] == [int(x) for x in recs_o[:, 0]]
+    for row, ro in zip(recs, recs_o):
+        assert row["potenergy"] == pytest.approx(ro[5], rel=1e-9)
+    rg, _, _, _ = s.download()
+    assert np.abs(wrap_diff(rg, o.r, dom)).max() < 1e-7
+    s.close()
+
+
 @pytest.mark.parametrize("case", ["wca", "lj", "fene", "faces"])
 def test_list_build_cells_equals_blocks(gpu_lib, case):
     """The per-cell and the 2x2x2-block list builds give identical rows (same

@@ -182,3 +182,94 @@ def test_mie_mixture_mass_and_records():
     assert rec["mv2sum"] == pytest.approx((m[:, None] * v * v).sum(), rel=1e-12)
     # momentum of the forces: sum m a = 0 (Newton's third law over all pairs)
     assert np.abs((m[:, None] * o.a).sum(0)).max() < 1e-9 * np.abs(m[:, None] * o.a).max()
+
+
+SOD_A = float(np.float32(3.1730728678))       # default-real literals of modules.f90:458-462
+SOD_B = float(np.float32(-0.85622864544))
+WCA_CUT2_SOD = float(np.float32(1.25992104989487))
+
+
+def soddemann_pair(dist, beads, eps=(1.7, 1.3, 0.6), L=8.0):
+    """Two molecules at `dist` on x; `beads` = how many of them are chain
+    beads (chainID 1, a one-bead chain without bonds; the rest solvent)."""
+    r = np.array([[-dist / 2, 0.1, 0.2], [dist / 2, 0.1, 0.2]])
+    o = O.Oracle(r, np.zeros((2, 3)), [L, L, L], WCA_RC, tplot=1, potential_flag=1, k_c=30.0, R_0=1.5)
+    chain = np.array([1 if k < beads else 0 for k in range(2)], np.int32)
+    o.set_monomers(chain, np.ones(2, np.int32), np.zeros(2, np.int32), np.zeros((2, 4), np.int32))
+    o.set_solvent(1, *eps)
+    o.setup()
+    return o
+
+
+def test_soddemann_geometry():
+    """SOLVENT_INFO 1 with the WCA cutoff: rneighbr = 1.42246 < sod_cut, so
+    rcutoff becomes 1.5 (cells of 1.5 + skin) and rneighbr2 stays -- no R_0
+    override (setup_set_parameters.f90:1863-1876); the library's geometry
+    says the same."""
+    from flowmol_b200 import api
+    dom = [8.4453, 9.0, 11.0]
+    o = O.Oracle(np.zeros((1, 3)), np.zeros((1, 3)), dom, WCA_RC, potential_flag=1, k_c=30.0, R_0=1.5)
+    g0 = o.geometry()
+    assert g0["rneighbr2"] == 1.5 * 1.5  # solvent_flag 0: the FENE override
+    o.set_solvent(1, 1.0, 1.0, 1.0)
+    g = o.geometry()
+    rn = WCA_RC + (0.3 + 0.3 + 0.3) / 3.0
+    assert g["rcutoff2"] == 2.25 and g["rneighbr2"] == rn * rn
+    assert list(g["ncells"]) == [int(np.floor(x / 1.8)) for x in dom]
+    p = api.make_params(1, dom, WCA_RC, potential_flag=1, k_c=30.0, R_0=1.5, solvent_flag=1)
+    rc, lg = api.derive_geometry(p)
+    assert rc == 0
+    assert lg["ncells"] == list(g["ncells"]) and lg["rneighbr2"] == g["rneighbr2"]
+    assert lg["rcutoff2"] == g["rcutoff2"] and lg["cellside"] == list(g["cellside"])
+    assert lg["potshift"] == g["potshift"]
+
+
+@pytest.mark.parametrize("dist", [1.05, 1.3, 1.41])
+@pytest.mark.parametrize("beads", [0, 1, 2])
+def test_soddemann_two_body_analytic(dist, beads):
+    """simulation_compute_forces_Soddemann_neigbr_halfint (:793-888): WCA
+    below wca_cut2 (the REAL(4) rounding of 2^(1/3)), the reference's cosine
+    expression eps a s^2 sin(a s + b) (s = 1/r^2) out to 1.5, well depth by
+    the number of chain beads; PE per molecule as written there."""
+    eps = (1.7, 1.3, 0.6)  # eps_pp, eps_ps, eps_ss
+    e = {2: eps[0], 1: eps[1], 0: eps[2]}[beads]
+    o = soddemann_pair(dist, beads, eps)
+    r2 = (-dist / 2 - dist / 2) ** 2
+    s = 1.0 / r2
+    if r2 < WCA_CUT2_SOD:
+        acc = 48.0 * ((s * s) * (s * s) * (s * s) * s - 0.5 * ((s * s) * (s * s)))
+        pe = 4.0 * ((s * s * s) * (s * s * s) - s * s * s + 0.25) - e
+    else:
+        acc = (e * SOD_A * (s * s)) * np.sin(s * SOD_A + SOD_B)
+        pe = 0.5 * e * (np.cos(SOD_A * r2 + SOD_B) - 1.0)
+    a = o.a
+    assert a[0, 0] == pytest.approx(acc * -dist, rel=1e-14) and a[1, 0] == pytest.approx(acc * dist, rel=1e-14)
+    assert np.all(a[:, 1:] == 0.0)
+    np.testing.assert_allclose(o.potenergymol, [pe, pe], rtol=1e-13)
+
+
+def test_soddemann_pairs_beyond_rneighbr_are_not_seen():
+    """A pair inside sod_cut but beyond rneighbr (1.42246) is not in the list
+    the forces walk: no force, as in the reference, where rneighbr2 keeps its
+    WCA-based value."""
+    for dist in (1.45, 1.49):
+        assert np.all(soddemann_pair(dist, 2).a == 0.0)
+
+
+def test_soddemann_solution_wells_act():
+    """On a polymer solution the cosine well changes the forces (pairs beyond
+    wca_cut2 exist for every bead count) and vanishes with zero well depths,
+    leaving WCA + FENE with the Soddemann list geometry."""
+    from flowmol_b200 import polymer
+    r, v, ch, sub, fy, bf, dom = polymer.fene_solution(48, targetconc=0.5)
+    r = lattice.jitter(r, 0.08, 91, dom)  # off the lattice: pairs between the shells
+    out = {}
+    for eps in ((1.5, 1.0, 0.5), (0.0, 0.0, 0.0)):
+        o = O.Oracle(r, v, dom, WCA_RC, tplot=1, potential_flag=1, k_c=30.0, R_0=1.5, density=0.85)
+        o.set_monomers(ch, sub, fy, bf)
+        o.set_solvent(1, *eps)
+        o.setup()
+        out[eps] = (o.a, o.potenergymol)
+    a1, pe1 = out[(1.5, 1.0, 0.5)]
+    a0, pe0 = out[(0.0, 0.0, 0.0)]
+    assert np.abs(a1 - a0).max() > 1e-3 and np.all(pe1 <= pe0 + 1e-12)

@@ -96,3 +96,26 @@ def test_input_reader_reports_missing_keywords(tmp_path):
     with pytest.raises(api.FlowmolError) as e:
         api.read_input(str(p))
     assert "RCUTOFF" in str(e.value)
+
+
+def test_input_reader_fene_solution_with_soddemann_solvent(tmp_path):
+    """INITIAL_CONFIG_FLAG 1 fene_solution: the FENE_SOLUTION block sets
+    potential_flag 1, the WCA cutoff and targetconc, and SOLVENT_INFO 1 its
+    three well depths (setup_read_input.f90:188-199, 253-296).  With flag 0
+    the same blocks are present in default.in but not read."""
+    base = open(os.path.join(GOLD, "default.in")).read()
+    x0 = api.read_input(os.path.join(GOLD, "default.in"))
+    assert x0.potential_flag == 0 and x0.solvent_flag == 0 and x0.targetconc == 0.0
+    assert "INITIAL_CONFIG_FLAG\n0\nspecial_case_name" in base and "SOLVENT_INFO\n0\n0.0\n0.0\n0.0" in base
+    deck = base.replace("INITIAL_CONFIG_FLAG\n0\nspecial_case_name", "INITIAL_CONFIG_FLAG\n1\nfene_solution")
+    deck = deck.replace("SOLVENT_INFO\n0\n0.0\n0.0\n0.0", "SOLVENT_INFO\n1\n1.5\n1.0d0\n0.5")
+    p = tmp_path / "MD.in"
+    p.write_text(deck)
+    x = api.read_input(str(p))
+    assert x.potential_flag == 1 and x.rcutoff == 2.0 ** (1.0 / 6.0)
+    assert x.nmonomers == 8 and x.k_c == 30.0 and x.R_0 == 1.5 and x.density == 0.5 and x.targetconc == 0.2
+    assert x.solvent_flag == 1 and (x.eps_pp, x.eps_ps, x.eps_ss) == (1.5, 1.0, 0.5)
+    p.write_text(deck.replace("SOLVENT_INFO\n1\n1.5", "SOLVENT_INFO\n3\n1.5"))
+    with pytest.raises(api.FlowmolError) as e:
+        api.read_input(str(p))
+    assert "solvent flag" in str(e.value)
