@@ -164,7 +164,7 @@ static void release(fm_handle *h)
                     d.tax, d.tay, d.taz, d.cell_of, d.cell_count, d.cell_start, d.perm, d.tile_sum, d.nbr, d.nnbr,
                     d.pe, d.vir, d.partial, d.rec, d.sc, h->tpos, h->tuidx, h->glob, h->stage3, d.chain,
                     d.subchain, d.bflag, d.tchain, d.tsubchain, d.tbflag, d.bnd, d.nbond,
-                    (void *)d.mie_pair, (void *)d.mie_mass, (void *)d.mie_type_up};
+                    (void *)d.mie_pair, (void *)d.mie_mass, (void *)d.mie_type_up, d.rdx, d.rdy, d.rdz};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     d = FmDev{};
@@ -220,8 +220,8 @@ extern "C" int fm_create(const fm_params *p, fm_handle **out)
     if (p->solvent_flag != 0 && p->solvent_flag != 1) return fail(FM_ERR_ARG, "solvent_flag must be 0 or 1");
     if (p->solvent_flag == 1 && (p->potential_flag != 1 || p->force_list != 3))
         return fail(FM_ERR_ARG, "the Soddemann solvent (solvent_flag 1) needs potential_flag 1 and force_list 3");
-    if (p->rebuild_criteria != 0 && p->rebuild_criteria != 1)
-        return fail(FM_ERR_ARG, "rebuild_criteria must be 0 (vmax) or 1 (fixed)");
+    if (p->rebuild_criteria < 0 || p->rebuild_criteria > 2)
+        return fail(FM_ERR_ARG, "rebuild_criteria must be 0 (vmax), 1 (fixed) or 2 (displacement)");
     if (p->integration_algorithm != 0 && p->integration_algorithm != 1)
         return fail(FM_ERR_ARG, "integration_algorithm must be 0 (leap-frog) or 1 (velocity Verlet)");
     int ndev = 0;
@@ -297,6 +297,7 @@ extern "C" int fm_create(const fm_params *p, fm_handle **out)
     FM_ALLOC(d.tile_sum, fm::scan_tiles(d.ncell))
     FM_ALLOC(d.pe, n) FM_ALLOC(d.vir, n)
     FM_ALLOC(h->stage3, 9 * n)
+    if (p->rebuild_criteria == 2) { FM_ALLOC(d.rdx, n) FM_ALLOC(d.rdy, n) FM_ALLOC(d.rdz, n) }
     if (p->potential_flag == 1) {
         FM_ALLOC(d.chain, n) FM_ALLOC(d.subchain, n) FM_ALLOC(d.bflag, n)
         FM_ALLOC(d.tchain, n) FM_ALLOC(d.tsubchain, n) FM_ALLOC(d.tbflag, n)
@@ -738,11 +739,18 @@ extern "C" int fm_setup(fm_handle *h)
 
 // Queues iterations [first, first + nsteps) of md_advance_vv, starting at
 // `phase` 0 (move(1)) or 1 (forces) of the first iteration.
+static void queue_decide(fm_handle *h, int it, int flip)
+{
+    const fm_params &p = h->p;
+    if (p.rebuild_criteria == 2) { fm::launch_disp(h->d, h->st); h->launches += 1; }
+    fm::launch_decide(h->d, it, flip, p.rebuild_criteria, p.fixed_rebuild, h->half_min_delta, h->st);
+    h->launches += 1;
+}
+
 static void queue_rebuild_check(fm_handle *h, int it, int flip)
 {
     const fm_params &p = h->p;
-    fm::launch_decide(h->d, it, flip, p.rebuild_criteria, p.fixed_rebuild, h->half_min_delta, h->st);
-    h->launches += 1;
+    queue_decide(h, it, flip);
     if (p.force_list != 0) {
         queue_cells(h, 1, 1);
         fm::launch_build_nlist(h->d, 1, it, h->st);
@@ -783,9 +791,7 @@ static int queue_steps(fm_handle *h, int first, int nsteps, int phase, const std
         h->iter = it;
         if (!(s == 0 && phase == 1)) {
             if (!fused_move1) { fm::launch_move1(h->d, h->st); h->launches += 1; }
-            fm::launch_decide(h->d, it, fused_move1 ? 1 : 0, p.rebuild_criteria, p.fixed_rebuild,
-                              h->half_min_delta, h->st);
-            h->launches += 1;
+            queue_decide(h, it, fused_move1 ? 1 : 0);
             if (p.force_list != 0) {
                 queue_cells(h, 1, 1);
                 fm::launch_build_nlist(h->d, 1, it, h->st);
@@ -922,7 +928,7 @@ extern "C" int fm_check_rebuild(fm_handle *h, int32_t *rebuild)
     if (!rebuild) return fail(FM_ERR_ARG, "null output");
     FM_CUDA(cudaMemsetAsync(&h->d.sc->vmax2, 0, sizeof(unsigned long long), h->st));
     fm::launch_vmax(h->d, h->st);
-    fm::launch_decide(h->d, h->iter, 0, h->p.rebuild_criteria, h->p.fixed_rebuild, h->half_min_delta, h->st);
+    queue_decide(h, h->iter, 0);
     FM_CUDA(cudaGetLastError());
     fm::FmScalars s;
     FM_TRY(read_scalars(h, &s));

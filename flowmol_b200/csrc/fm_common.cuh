@@ -33,6 +33,8 @@ struct FmScalars {
     int64_t digest_n;
     int32_t nrec_pending;     // record rows written since the host last read
     int32_t build_next;       // list build: next work unit to hand out (zeroed before each build)
+    int32_t disp_reset;       // rebuild criterion 2: the last decision rebuilt, so rdisp restarts at 0
+    unsigned long long dmax;  // rebuild criterion 2: bits of max |rdisp component| this step
 };
 
 // Partial sums of one record step, one row per force-kernel block.
@@ -107,6 +109,10 @@ struct FmDev {
     // Mie_potential 1: per-type-pair constants, per-type masses; a molecule's
     // type (1-based) rides in the w component of its position
     int build_blocks;            // list build: one warp per 2x2x2 cells (sparse systems)
+    // rebuild criterion 2: displacement since the last rebuild, per molecule
+    // (simulation_checkrebuild.f90:111-121); molecules move slots only at rebuilds,
+    // which restart it, so it needs no reordering
+    double *rdx, *rdy, *rdz;
     // solvent_flag 1: Soddemann well depth by chain beads in the pair (eps_ss,
     // eps_ps, eps_pp); a molecule's bead flag (chainID != 0) rides in w
     int solvent;
@@ -152,6 +158,7 @@ void launch_move1(const FmDev &d, cudaStream_t st);          // pass 1 in place 
 void launch_move2(const FmDev &d, cudaStream_t st);          // pass 2 in place
 void launch_vmax(const FmDev &d, cudaStream_t st);           // vmax2 of current v
 void launch_move_lfv(const FmDev &d, cudaStream_t st);       // leap-frog move in place + vmax2
+void launch_disp(const FmDev &d, cudaStream_t st);            // criterion 2: rdisp += v dt, max component
 void launch_decide(const FmDev &d, int iter, int flip, int rebuild_criteria, int fixed_rebuild,
                    double half_min_delta, cudaStream_t st);
 // Rebuild pipeline; gated = 1 makes each kernel a no-op unless sc->rebuild.

@@ -574,6 +574,8 @@ extern "C" int fm_engine_submit(fm_engine *e, const fm_job *job, const double *r
         if (!(job->domain[k] > 0.0)) return efail(FM_ERR_ARG, "domain must be > 0");
     if (job->integration_algorithm != 0 && job->integration_algorithm != 1)
         return efail(FM_ERR_ARG, "integration_algorithm must be 0 or 1");
+    if (job->rebuild_criteria != 0 && job->rebuild_criteria != 1)
+        return efail(FM_ERR_ARG, "engine jobs take rebuild_criteria 0 (vmax) or 1 (fixed)");
     if (job->integration_algorithm == 1 && job->ensemble == 6)
         return efail(FM_ERR_ARG, "tag mode for velocity-Verlet not implemented (simulation_move_particles_vv.f90:119-120)");
     Footprint f = footprint(*job, 0);

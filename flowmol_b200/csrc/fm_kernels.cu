@@ -69,6 +69,8 @@ __global__ void k_reset_scalars(FmDev d)
     s->digest = 0ull;
     s->digest_n = 0;
     s->nrec_pending = 0;
+    s->disp_reset = 1;  // rdisp is allocated as zeros at the first check
+    s->dmax = 0ull;
 }
 
 // r = (r + dt v) + (0.5 dt^2) a ; v = v + (0.5 dt) a   -- pass 1, in place.
@@ -137,8 +139,38 @@ __global__ void k_vmax(FmDev d)
     block_vmax2(d, m2);
 }
 
+// Rebuild criterion 2 (simulation_checkrebuild.f90:106-121): rdisp += v dt
+// for every molecule (v as the check sees it), and the largest |component|
+// into sc->dmax.  After a rebuild the reference deallocates rdisp (:150-152),
+// so the next check starts it from zero.
+__global__ void k_disp(FmDev d)
+{
+    if (frozen(d)) return;
+    const bool restart = d.sc->disp_reset != 0;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double m = 0.0;
+    if (i < d.n) {
+        const double x = __dadd_rn(restart ? 0.0 : d.rdx[i], __dmul_rn(d.vx[i], d.dt));
+        const double y = __dadd_rn(restart ? 0.0 : d.rdy[i], __dmul_rn(d.vy[i], d.dt));
+        const double z = __dadd_rn(restart ? 0.0 : d.rdz[i], __dmul_rn(d.vz[i], d.dt));
+        d.rdx[i] = x; d.rdy[i] = y; d.rdz[i] = z;
+        m = fmax(fabs(x), fmax(fabs(y), fabs(z)));
+    }
+    m = warp_max(m);
+    __shared__ double wmax[32];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) wmax[w] = m;
+    __syncthreads();
+    if (w == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        double v = l < nw ? wmax[l] : 0.0;
+        v = warp_max(v);
+        if (l == 0 && v > 0.0) atomicMax(&d.sc->dmax, (unsigned long long)__double_as_longlong(v));
+    }
+}
+
 // ---------------------------------------------------------------------------
-// rebuild decision (simulation_checkrebuild.f90:34, 83-99, 101-103, 148-155)
+// rebuild decision (simulation_checkrebuild.f90:34, 83-99, 101-103, 106-121, 148-155)
 // ---------------------------------------------------------------------------
 
 __global__ void k_decide(FmDev d, int iter, int flip, int crit, int fixed_rebuild, double half_min_delta)
@@ -153,6 +185,11 @@ __global__ void k_decide(FmDev d, int iter, int flip, int crit, int fixed_rebuil
         if (s->rmax > half_min_delta) rebuild = 1;
     } else if (crit == 1) {
         if ((iter % fixed_rebuild) == 0) rebuild = 1;
+    } else if (crit == 2) {
+        // any(abs(rdisp(:,n)) > 0.5 minval(delta_rneighbr))
+        if (__longlong_as_double((long long)s->dmax) > half_min_delta) rebuild = 1;
+        s->dmax = 0ull;
+        s->disp_reset = rebuild;
     }
     s->vmax2 = 0ull;
     if (rebuild) {
@@ -987,6 +1024,8 @@ void launch_move1(const FmDev &d, cudaStream_t st) { k_move1<<<nblk(d.n, 256), 2
 void launch_move2(const FmDev &d, cudaStream_t st) { k_move2<<<nblk(d.n, 256), 256, 0, st>>>(d); }
 void launch_vmax(const FmDev &d, cudaStream_t st) { k_vmax<<<nblk(d.n, 256), 256, 0, st>>>(d); }
 void launch_move_lfv(const FmDev &d, cudaStream_t st) { k_move_lfv<<<nblk(d.n, 256), 256, 0, st>>>(d); }
+void launch_disp(const FmDev &d, cudaStream_t st) { k_disp<<<nblk(d.n, 256), 256, 0, st>>>(d); }
+
 void launch_decide(const FmDev &d, int iter, int flip, int crit, int fixed_rebuild, double half_min_delta,
                    cudaStream_t st)
 {

@@ -69,7 +69,7 @@ typedef struct fm_params {
     double simtime;               /* simulated time of the uploaded state */
     int32_t force_list;           /* FORCE_LIST: 0, 2 or 3 */
     int32_t potential_flag;       /* POTENTIAL_FLAG: 0 LJ, 1 FENE polymer */
-    int32_t rebuild_criteria;     /* REBUILD_CRITERIA: 0 vmax (Rapaport), 1 fixed */
+    int32_t rebuild_criteria;     /* REBUILD_CRITERIA: 0 vmax (Rapaport), 1 fixed, 2 exact displacement */
     int32_t fixed_rebuild;        /* FIXED_REBUILD period when rebuild_criteria = 1 */
     int32_t sLRC_flag;            /* SLRC_FLAG: long-range corrections on PE and P */
     int32_t precision;            /* FM_PRECISION_* */

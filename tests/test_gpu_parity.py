@@ -481,6 +481,27 @@ def test_soddemann_polymer_solution(gpu_lib, prec):
     s.close()
 
 
+@pytest.mark.parametrize("crit,fixed", [(0, 1), (1, 7), (2, 1)])
+def test_rebuild_criteria_schedule(liquid, crit, fixed):
+    """REBUILD_CRITERIA 0 (Rapaport vmax), 1 (every FIXED_REBUILD steps) and 2
+    (exact per-molecule displacement, simulation_checkrebuild.f90:83-121):
+    the device decides the same rebuilds as the oracle over 300 steps (plus the
+    record-forced ones, :34) and the trajectories agree."""
+    r, v, dom = liquid
+    o = O.Oracle(r, v, dom, 2.5, tplot=50, density=0.8442, rebuild_criteria=crit, fixed_rebuild=fixed)
+    o.setup()
+    o.run_vv(300)
+    s = gpu_system(r, v, dom, 2.5, tplot=50, density=0.8442, rebuild_criteria=crit, fixed_rebuild=fixed)
+    s.setup()
+    s.simulation_md(300)
+    assert s.counters()["rebuilds"] == o.rebuild_count
+    if crit == 1:
+        assert o.rebuild_count == len([i for i in range(1, 301) if i % fixed == 0 or (i + 1) % 50 == 0])
+    rg, _, _, _ = s.download()
+    assert np.abs(wrap_diff(rg, o.r, dom)).max() < 1e-7
+    s.close()
+
+
 @pytest.mark.parametrize("case", ["wca", "lj", "fene", "faces"])
 def test_list_build_cells_equals_blocks(gpu_lib, case):
     """The per-cell and the 2x2x2-block list builds give identical rows (same
