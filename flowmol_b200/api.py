@@ -211,6 +211,8 @@ def lib():
             "fm_get_pair_list": [h, P(C.c_int32), P(C.c_int32), P(C.c_int8), C.c_int64, P(C.c_int64)],
             "fm_pair_digest": [h, P(C.c_uint64), P(C.c_int64)],
             "fm_get_counters": [h, P(C.c_int64), P(C.c_int32), P(C.c_int32)],
+            "fm_set_pressure_outflag": [h, C.c_int32],
+            "fm_get_pressure_tensor": [h, P(C.c_double), P(C.c_int32), C.c_int32],
             "fm_get_threads_per_molecule": [h, P(C.c_int32)],
             "fm_last_error": [C.c_char_p, C.c_int32],
             "fm_engine_create": [P(FmEngineParams), P(h)],
@@ -535,6 +537,16 @@ class MDSystem:
         rb = C.c_int64(); cap = C.c_int32(); mx = C.c_int32()
         check(lib().fm_get_counters(self.h, C.byref(rb), C.byref(cap), C.byref(mx)))
         return dict(rebuilds=rb.value, nlist_capacity=cap.value, max_neighbours=mx.value)
+
+    def set_pressure_outflag(self, flag=1):
+        check(lib().fm_set_pressure_outflag(self.h, int(flag)))
+
+    def pressure_tensor(self, reset=False):
+        """(3x3 mean virial pressure tensor over the record steps sampled, samples)."""
+        out = (C.c_double * 9)()
+        n = C.c_int32()
+        check(lib().fm_get_pressure_tensor(self.h, out, C.byref(n), int(bool(reset))))
+        return np.array(list(out)).reshape(3, 3), n.value
 
 
 def make_job(np_, domain, rcutoff, nsteps, delta_rneighbr=(0.3, 0.3, 0.3), tplot=100, density=None,

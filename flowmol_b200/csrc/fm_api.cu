@@ -164,7 +164,7 @@ static void release(fm_handle *h)
                     d.tax, d.tay, d.taz, d.cell_of, d.cell_count, d.cell_start, d.perm, d.tile_sum, d.nbr, d.nnbr,
                     d.pe, d.vir, d.partial, d.rec, d.sc, h->tpos, h->tuidx, h->glob, h->stage3, d.chain,
                     d.subchain, d.bflag, d.tchain, d.tsubchain, d.tbflag, d.bnd, d.nbond,
-                    (void *)d.mie_pair, (void *)d.mie_mass, (void *)d.mie_type_up, d.rdx, d.rdy, d.rdz};
+                    (void *)d.mie_pair, (void *)d.mie_mass, (void *)d.mie_type_up, d.rdx, d.rdy, d.rdz, d.rf6};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     d = FmDev{};
@@ -643,9 +643,12 @@ static void queue_force(fm_handle *h, int record, int mode)
     h->launches += 1;
 }
 
-static void queue_record(fm_handle *h, int iter, double simtime)
+// `pressure_sample`: simulation_record's pressure_averaging (:1189) runs with
+// the record of a step; the setup record (setup_initial_record.f90:89) has none.
+static void queue_record(fm_handle *h, int iter, double simtime, bool pressure_sample = true)
 {
     FmDev d = h->d;
+    if (!pressure_sample) d.pressure = 0;
     d.nblocks_force = h->p.force_list == 0 ? fm::all_pairs_blocks(d.n) : fm::force_blocks(d.n, h->tpm);
     fm::launch_record(d, iter, simtime, h->st);
     h->launches += 1;
@@ -727,7 +730,7 @@ extern "C" int fm_setup(fm_handle *h)
     FM_TRY(autotune_tpm(h));
     const int record = (h->iter % h->p.tplot) == 0;
     queue_force(h, record, 0);
-    if (record) queue_record(h, h->iter, h->simtime);
+    if (record) queue_record(h, h->iter, h->simtime, false);
     FM_CUDA(cudaGetLastError());
     FM_TRY(read_scalars(h, &s));
     FM_TRY(status_error(h, s));
@@ -1125,6 +1128,44 @@ extern "C" int fm_get_counters(fm_handle *h, int64_t *rebuilds, int32_t *cap, in
     if (rebuilds) *rebuilds = s.rebuilds;
     if (cap) *cap = h->d.maxn;
     if (max_nbr) *max_nbr = s.max_nbr;
+    return FM_OK;
+}
+
+extern "C" int fm_set_pressure_outflag(fm_handle *h, int32_t flag)
+{
+    FM_TRY(ready(h, 1));
+    if (flag != 0 && flag != 1)
+        return fail(FM_ERR_ARG, "pressure_outflag must be 0 or 1 (the volume-averaged forms are not built)");
+    FmDev &d = h->d;
+    if (flag == 1 && !d.rf6) {
+        double *p = nullptr;
+        FM_CUDA(cudaMalloc(&p, sizeof(double) * 6 * (size_t)d.n));
+        d.rf6 = p;
+        FM_CUDA(cudaMemsetAsync(d.rf6, 0, sizeof(double) * 6 * (size_t)d.n, h->st));
+    }
+    d.pressure = flag;
+    FM_CUDA(cudaMemsetAsync(d.sc->pacc, 0, sizeof(d.sc->pacc), h->st));
+    FM_CUDA(cudaMemsetAsync(&d.sc->pcount, 0, sizeof(int32_t), h->st));
+    FM_CUDA(cudaStreamSynchronize(h->st));
+    return FM_OK;
+}
+
+extern "C" int fm_get_pressure_tensor(fm_handle *h, double P[9], int32_t *nsamples, int32_t reset)
+{
+    FM_TRY(ready(h, 1));
+    if (!P) return fail(FM_ERR_ARG, "null output");
+    fm::FmScalars s;
+    FM_TRY(read_scalars(h, &s));
+    const int n = s.pcount;
+    const double *a = s.pacc;  // xx yy zz xy xz yz
+    const double m[9] = {a[0], a[3], a[4], a[3], a[1], a[5], a[4], a[5], a[2]};
+    for (int q = 0; q < 9; q++) P[q] = n > 0 ? m[q] / (double)n : 0.0;
+    if (nsamples) *nsamples = n;
+    if (reset) {
+        FM_CUDA(cudaMemsetAsync(h->d.sc->pacc, 0, sizeof(s.pacc), h->st));
+        FM_CUDA(cudaMemsetAsync(&h->d.sc->pcount, 0, sizeof(int32_t), h->st));
+        FM_CUDA(cudaStreamSynchronize(h->st));
+    }
     return FM_OK;
 }
 

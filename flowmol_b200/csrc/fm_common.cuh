@@ -35,10 +35,14 @@ struct FmScalars {
     int32_t build_next;       // list build: next work unit to hand out (zeroed before each build)
     int32_t disp_reset;       // rebuild criterion 2: the last decision rebuilt, so rdisp restarts at 0
     unsigned long long dmax;  // rebuild criterion 2: bits of max |rdisp component| this step
+    double pacc[6];           // pressure_outflag 1: sum over samples of P (xx yy zz xy xz yz)
+    int32_t pcount;           // samples in pacc
 };
 
 // Partial sums of one record step, one row per force-kernel block.
-enum { RS_PE = 0, RS_VIR, RS_MV2, RS_VSUM, RS_PEMAX, RS_N };
+// With pressure_outflag 1 the six distinct components of v v + rf/2 follow
+// (cumulative_pressure case 1, simulation_record.f90:3151-3220).
+enum { RS_PE = 0, RS_VIR, RS_MV2, RS_VSUM, RS_PEMAX, RS_PXX, RS_PYY, RS_PZZ, RS_PXY, RS_PXZ, RS_PYZ, RS_N };
 
 // Record row layout in device memory (matches fm_macro on the host).
 struct FmRecord {
@@ -109,6 +113,10 @@ struct FmDev {
     // Mie_potential 1: per-type-pair constants, per-type masses; a molecule's
     // type (1-based) rides in the w component of its position
     int build_blocks;            // list build: one warp per 2x2x2 cells (sparse systems)
+    // pressure_outflag 1: rf (xx yy zz xy xz yz) per molecule of the last
+    // record step (pressure_tensor_forces, simulation_record.f90:6239-6256)
+    int pressure;
+    double *rf6;
     // rebuild criterion 2: displacement since the last rebuild, per molecule
     // (simulation_checkrebuild.f90:111-121); molecules move slots only at rebuilds,
     // which restart it, so it needs no reordering

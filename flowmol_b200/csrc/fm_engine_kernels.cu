@@ -633,7 +633,9 @@ __global__ void __launch_bounds__(EAP_THREADS) k_e_force_ap(EngDev d)
     if (s.mode != MODE_ALLPAIRS || !slot_active(s)) continue;  // uniform per block
     const int lane = threadIdx.x & 31;
     const double4 *P = eng_pos(d, s.pset);
-    const bool rec = s.record, ptens = rec && s.pressure;
+    // simulation_compute_forces_LJ_AP (:280-341) calls no pressure_tensor_forces:
+    // an all-pairs job's pressure tensor has the kinetic part only
+    const bool rec = s.record, ptens = false;
     constexpr int WPB = EAP_THREADS / 32;
     for (int i = s.mol_off + blockIdx.y * WPB + (threadIdx.x >> 5); i < s.mol_off + s.nmol;
          i += EAP_YBLOCKS * WPB) {

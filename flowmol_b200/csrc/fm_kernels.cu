@@ -71,6 +71,8 @@ __global__ void k_reset_scalars(FmDev d)
     s->nrec_pending = 0;
     s->disp_reset = 1;  // rdisp is allocated as zeros at the first check
     s->dmax = 0ull;
+    for (int q = 0; q < 6; q++) s->pacc[q] = 0.0;
+    s->pcount = 0;
 }
 
 // r = (r + dt v) + (0.5 dt^2) a ; v = v + (0.5 dt) a   -- pass 1, in place.
@@ -466,8 +468,8 @@ constexpr int FORCE_THREADS = 256;
 // Otherwise LJ_accijmag = 48 (s^7 - s^4/2), s = 1/r^2, and LJ_energy
 // (:105-135).
 template <int PREC, bool REC>
-__device__ __forceinline__ void pair_acc(const FmDev &d, double r2, double dx, double dy, double dz, double wi,
-                                         double wj, double &fx, double &fy, double &fz, double &pe, double &vir)
+__device__ __forceinline__ double pair_acc(const FmDev &d, double r2, double dx, double dy, double dz, double wi,
+                                           double wj, double &fx, double &fy, double &fz, double &pe, double &vir)
 {
     constexpr bool F32 = (PREC & 1) != 0, MIE = (PREC & 2) != 0, SOD = (PREC & 4) != 0;
     if (SOD) {
@@ -518,7 +520,7 @@ __device__ __forceinline__ void pair_acc(const FmDev &d, double r2, double dx, d
                 vir += acc * r2;
             }
         }
-        return;
+        return 0.0;  // the Soddemann routine records no pressure-tensor term
     }
     if (MIE) {
         const FmMiePair &m = d.mie_pair[((int)wi - 1) + MIE_MAXT * ((int)wj - 1)];
@@ -530,6 +532,7 @@ __device__ __forceinline__ void pair_acc(const FmDev &d, double r2, double dx, d
                 pe += m.ceps * (pow(s, m.er) - m.alpha * pow(s, m.ea)) - m.shift;
                 vir += acc * r2;
             }
+            return acc;
         } else {
             const float s = __frcp_rn((float)r2);
             const double acc = (double)((float)m.ceps * ((float)m.lr * powf(s, (float)m.er1) -
@@ -539,6 +542,7 @@ __device__ __forceinline__ void pair_acc(const FmDev &d, double r2, double dx, d
                 pe += (double)((float)m.ceps * (powf(s, (float)m.er) - (float)m.alpha * powf(s, (float)m.ea))) - m.shift;
                 vir += acc * r2;
             }
+            return acc;
         }
     } else if (!F32) {
         const double s = __drcp_rn(r2);  // == 1.0 / r2 (both correctly rounded)
@@ -550,6 +554,7 @@ __device__ __forceinline__ void pair_acc(const FmDev &d, double r2, double dx, d
             pe += 4.0 * (s6 - s3) - d.potshift;  // LJ_energy (:126-135)
             vir += acc * r2;
         }
+        return acc;
     } else {
         // FP32 pair magnitude; the FP64 rij scales it (one conversion)
         const float s = __frcp_rn((float)r2);
@@ -561,7 +566,27 @@ __device__ __forceinline__ void pair_acc(const FmDev &d, double r2, double dx, d
             pe += (double)(4.0f * (s6 - s3)) - d.potshift;
             vir += acc * r2;
         }
+        return acc;
     }
+}
+
+// pressure_tensor_forces (simulation_record.f90:6239-6256): rf += acc rij rij,
+// the six distinct components xx yy zz xy xz yz.
+__device__ __forceinline__ void add_rf(double (&rf)[6], double acc, double dx, double dy, double dz)
+{
+    const double ax = acc * dx, ay = acc * dy, az = acc * dz;
+    rf[0] += ax * dx; rf[1] += ay * dy; rf[2] += az * dz;
+    rf[3] += ax * dy; rf[4] += ax * dz; rf[5] += ay * dz;
+}
+
+// Record-step pressure terms of one molecule: v v + rf/2 (cumulative_pressure
+// case 1, simulation_record.f90:3170-3199; no mass factor there).
+__device__ __forceinline__ void pressure_part(double (&part)[RS_N], double wx, double wy, double wz,
+                                              const double (&rf)[6])
+{
+    part[RS_PXX] = wx * wx + rf[0] / 2.0; part[RS_PYY] = wy * wy + rf[1] / 2.0;
+    part[RS_PZZ] = wz * wz + rf[2] / 2.0; part[RS_PXY] = wx * wy + rf[3] / 2.0;
+    part[RS_PXZ] = wx * wz + rf[4] / 2.0; part[RS_PYZ] = wy * wz + rf[5] / 2.0;
 }
 
 // Integrator epilogue of molecule i with its summed LJ force: stores a (and PE
@@ -574,8 +599,14 @@ __device__ __forceinline__ void pair_acc(const FmDev &d, double r2, double dx, d
 // position update (modes 2, 3), else 0.
 template <bool REC, int MODE, bool MIE = false>
 __device__ __forceinline__ double epilogue(const FmDev &d, int pset, int i, double4 p, double fx, double fy,
-                                           double fz, double pe, double vir, double (&part)[RS_N])
+                                           double fz, double pe, double vir, double (&part)[RS_N],
+                                           const double (&rf)[6])
 {
+    if (REC && d.pressure) {  // kept for a record taken after the move (fm_evaluate_macroscopic_properties)
+        double *q = d.rf6 + 6 * (size_t)i;
+#pragma unroll
+        for (int k = 0; k < 6; k++) q[k] = rf[k];
+    }
     double mass = 1.0;  // LJ_mass; Mie_mass = mass_lookup(moltype)
     if (MIE) {
         mass = d.mie_mass[(int)p.w - 1];
@@ -593,6 +624,7 @@ __device__ __forceinline__ double epilogue(const FmDev &d, int pset, int i, doub
             part[RS_PE] = pe; part[RS_VIR] = vir; part[RS_PEMAX] = pe;
             part[RS_MV2] = MIE ? mass * norm2_rn(wx, wy, wz) : norm2_rn(wx, wy, wz);
             part[RS_VSUM] = MIE ? mass * __dadd_rn(__dadd_rn(wx, wy), wz) : __dadd_rn(__dadd_rn(wx, wy), wz);
+            if (d.pressure) pressure_part(part, wx, wy, wz, rf);
         }
         vx = __dadd_rn(vx, __dmul_rn(d.dt, fx));
         vy = __dadd_rn(vy, __dmul_rn(d.dt, fy));
@@ -619,6 +651,7 @@ __device__ __forceinline__ double epilogue(const FmDev &d, int pset, int i, doub
         part[RS_PE] = pe; part[RS_VIR] = vir; part[RS_PEMAX] = pe;
         part[RS_MV2] = MIE ? mass * norm2_rn(wx, wy, wz) : norm2_rn(wx, wy, wz);
         part[RS_VSUM] = MIE ? mass * __dadd_rn(__dadd_rn(wx, wy), wz) : __dadd_rn(__dadd_rn(wx, wy), wz);
+        if (d.pressure) pressure_part(part, wx, wy, wz, rf);
     }
     if (MODE == 2) {
         p.x = __dadd_rn(__dadd_rn(p.x, __dmul_rn(d.dt, vx)), __dmul_rn(d.half_dt2, fx));
@@ -641,7 +674,7 @@ __device__ __forceinline__ double epilogue(const FmDev &d, int pset, int i, doub
 // A bond at or beyond R0 is the reference's polymer_bond_error.
 template <bool REC, bool MIE>
 __device__ __forceinline__ void fene_bonds(const FmDev &d, const double4 *P, int i, double &fx, double &fy,
-                                           double &fz, double &pe, double &vir)
+                                           double &fz, double &pe, double &vir, double (&rf)[6])
 {
     const double4 pi = P[i];
     const int nb = d.nbond[i];
@@ -664,6 +697,7 @@ __device__ __forceinline__ void fene_bonds(const FmDev &d, const double4 *P, int
             if (REC) {
                 pe += 0.5 * m.k * (dr * dr);
                 vir += acc * r2;
+                if (d.pressure) add_rf(rf, acc, dx, dy, dz);  // :768-770
             }
             continue;
         }
@@ -678,6 +712,7 @@ __device__ __forceinline__ void fene_bonds(const FmDev &d, const double4 *P, int
         if (REC) {
             pe += 0.5 * d.k_c * d.R0 * d.R0 * log(1.0 - q);
             vir += acc * r2;
+            if (d.pressure) add_rf(rf, acc, dx, dy, dz);  // :768-770
         }
     }
 }
@@ -712,6 +747,7 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force(FmDev d)
     const int lane = gt % TPM;
     const bool active = i < d.n;
     double fx = 0.0, fy = 0.0, fz = 0.0, pe = 0.0, vir = 0.0;
+    double rf[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     if (active) {
         const double4 pi = P[i];
         const int cnt = d.nnbr[i];
@@ -739,7 +775,11 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force(FmDev d)
                 const double dy = __dsub_rn(pi.y, yj);
                 const double dz = __dsub_rn(pi.z, zj);
                 const double r2 = norm2_rn(dx, dy, dz);
-                if (r2 < rc2) pair_acc<PREC, REC>(d, r2, dx, dy, dz, pi.w, pj[q].w, fx, fy, fz, pe, vir);
+                if (r2 < rc2) {
+                    const double acc = pair_acc<PREC, REC>(d, r2, dx, dy, dz, pi.w, pj[q].w, fx, fy, fz, pe, vir);
+                    // every partner of i in the full list: the half list's i and j sides
+                    if (REC && d.pressure) add_rf(rf, acc, dx, dy, dz);
+                }
             }
         }
     }
@@ -752,14 +792,20 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force(FmDev d)
             if (REC) {
                 pe += __shfl_xor_sync(0xffffffffu, pe, o);
                 vir += __shfl_xor_sync(0xffffffffu, vir, o);
+                if (d.pressure) {
+#pragma unroll
+                    for (int k = 0; k < 6; k++) rf[k] += __shfl_xor_sync(0xffffffffu, rf[k], o);
+                }
             }
         }
     }
-    double part[RS_N] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    double part[RS_N] = {};
     double m2 = 0.0;
-    if (active && lane == 0 && d.potential_flag == 1) fene_bonds<REC, (PREC & 2) != 0>(d, P, i, fx, fy, fz, pe, vir);
+    if (active && lane == 0 && d.potential_flag == 1)
+        fene_bonds<REC, (PREC & 2) != 0>(d, P, i, fx, fy, fz, pe, vir, rf);
     // a(:,i) = sum acc rij / mass (LJ_mass = 1; Mie_mass by type)
-    if (active && lane == 0) m2 = epilogue<REC, MODE, (PREC & 2) != 0>(d, pset, i, P[i], fx, fy, fz, pe, vir, part);
+    if (active && lane == 0)
+        m2 = epilogue<REC, MODE, (PREC & 2) != 0>(d, pset, i, P[i], fx, fy, fz, pe, vir, part, rf);
     if (REC) block_partials(d, part);
     if (MODE >= 2) block_vmax2(d, m2);
 }
@@ -818,6 +864,11 @@ __global__ void __launch_bounds__(REC_THREADS) k_record(FmDev d, int iter, doubl
         int slot = d.sc->nrec_pending % d.rec_cap;
         d.rec[slot] = r;
         d.sc->nrec_pending += 1;
+        if (d.pressure) {  // Pxy = Pxy + Pxytemp / volume (simulation_record.f90:3213-3217)
+            const double volume = d.L[0] * d.L[1] * d.L[2];
+            for (int q = 0; q < 6; q++) d.sc->pacc[q] += tot[RS_PXX + q] / volume;
+            d.sc->pcount += 1;
+        }
         if (tot[RS_PEMAX] > 10000.0) raise_status(d, ST_PE, iter);
     }
 }
@@ -829,7 +880,7 @@ __global__ void __launch_bounds__(MACRO_THREADS) k_macro_partials(FmDev d)
 {
     if (frozen(d)) return;
     int i = blockIdx.x * MACRO_THREADS + threadIdx.x;
-    double part[RS_N] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    double part[RS_N] = {};
     if (i < d.n) {
         double vx = d.vx[i], vy = d.vy[i], vz = d.vz[i];
         if (d.integrator == 0) {  // leap-frog records v + a dt/2
@@ -843,6 +894,11 @@ __global__ void __launch_bounds__(MACRO_THREADS) k_macro_partials(FmDev d)
         part[RS_MV2] = mass * norm2_rn(vx, vy, vz);
         part[RS_VSUM] = mass * __dadd_rn(__dadd_rn(vx, vy), vz);
         part[RS_PEMAX] = d.pe[i];
+        if (d.pressure) {
+            const double *q = d.rf6 + 6 * (size_t)i;
+            const double rf[6] = {q[0], q[1], q[2], q[3], q[4], q[5]};
+            pressure_part(part, vx, vy, vz, rf);
+        }
     }
     __shared__ double ws[RS_N][MACRO_THREADS / 32];
     int w = threadIdx.x >> 5, l = threadIdx.x & 31;
@@ -897,9 +953,10 @@ __global__ void __launch_bounds__(AP_THREADS) k_all_pairs(FmDev d)
         }
         __syncthreads();
     }
-    double part[RS_N] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    double part[RS_N] = {};
     double m2 = 0.0;
-    if (active) m2 = epilogue<REC, MODE, (PREC & 2) != 0>(d, pset, i, pi, fx, fy, fz, pe, vir, part);
+    const double rf[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // simulation_compute_forces_LJ_AP records no rf
+    if (active) m2 = epilogue<REC, MODE, (PREC & 2) != 0>(d, pset, i, pi, fx, fy, fz, pe, vir, part, rf);
     if (REC) {
         // AP blocks are AP_THREADS wide; reuse the generic reduction layout
         __shared__ double ws[RS_N][AP_THREADS / 32];

@@ -412,6 +412,19 @@ FM_API int fm_engine_counters(fm_engine *e, int64_t *ticks, int64_t *molecule_st
  * (ms) and the number of launches since it was last read. */
 FM_API int fm_force_kernel_timing(fm_handle *h, int32_t enable);
 FM_API int fm_get_force_kernel_time(fm_handle *h, double *ms, int64_t *launches);
+/* PRESSURE_OUTFLAG 1, the full-domain virial stress (pressure_averaging and
+ * cumulative_pressure case 1, simulation_record.f90:3103-3220).  On every
+ * record step P = sum_i (v_i v_i + rf_i / 2) / volume is added to a running
+ * sum, with rf_i = sum of accijmag rij rij over i's pair and bond terms
+ * (pressure_tensor_forces, :6239-6256: the LJ/Mie half- and full-list pairs
+ * and the FENE/harmonic bonds; the all-pairs and Soddemann routines add none,
+ * as in the reference) and v the record velocity (leap-frog: v + a dt/2).
+ * Setting the flag clears the sum.  fm_get_pressure_tensor gives the mean of
+ * the samples (row-major 3x3) and their count, and clears the sum when
+ * `reset` is non-zero -- Pxy / Nstress_ave when read every Nstress_ave
+ * samples. */
+FM_API int fm_set_pressure_outflag(fm_handle *h, int32_t flag);
+FM_API int fm_get_pressure_tensor(fm_handle *h, double P[9], int32_t *nsamples, int32_t reset);
 /* Kernels this handle has launched since creation. */
 FM_API int fm_get_launch_count(fm_handle *h, int64_t *launches);
 

@@ -985,6 +985,7 @@ static void forces_full(orc *s)
                 if (rec) {
                     s->potenergymol[i - 1] += pair_energy(s, inv, i, j);
                     s->virialmol[i - 1] += acc * r2;
+                    if (s->pressure_outflag == 1) ptf(s, i, rij, acc); /* :603 */
                 } else if (tev) {
                     s->virialmol[i - 1] += acc * r2;
                 }
@@ -994,7 +995,7 @@ static void forces_full(orc *s)
 }
 
 /* simulation_compute_forces_LJ_AP (:280-341): all pairs, per-axis minimum
- * image. */
+ * image.  The routine records no pressure-tensor term. */
 static void forces_AP(orc *s)
 {
     const int rec = (s->iter % s->tplot) == 0;
@@ -1025,7 +1026,6 @@ static void forces_AP(orc *s)
                     s->potenergymol[j - 1] += e;
                     s->virialmol[i - 1] += acc * r2;
                     s->virialmol[j - 1] += acc * r2;
-                    if (s->pressure_outflag == 1) { ptf(s, i, rij, acc); ptf(s, j, rij, acc); }
                 } else if (tev) {
                     s->virialmol[i - 1] += acc * r2;
                     s->virialmol[j - 1] += acc * r2;
@@ -1059,6 +1059,7 @@ static int forces_poly(orc *s)
             ai[1] = ai[1] + acc * rij[1] / mi;
             ai[2] = ai[2] + acc * rij[2] / mi;
             if (rec) {
+                if (s->pressure_outflag == 1) ptf(s, i, rij, acc); /* :768-770 */
                 s->potenergymol_POLY[i - 1] += s->mie ? harmonic_energy(s, r2, i, j) : fene_energy(r2, s->k_c, s->R_0);
                 s->virialmol[i - 1] += acc * r2;
             } else if (tev) {
@@ -1258,6 +1259,8 @@ int orc_rebuild(orc *s)
     return orc_assign_to_neighbourlist(s);
 }
 
+void orc_cumulative_pressure(orc *s);
+
 /* md_advance_vv (md.f90:143-163) for nsteps iterations; the record callback
  * is replaced by storing the macroscopic properties of every tplot step into
  * rec_out (9 doubles per record, see orc_macro) when non-null. */
@@ -1275,6 +1278,7 @@ int orc_run_vv(orc *s, int nsteps, double *rec_out, int rec_cap, int *nrec)
         orc_move_vv(s, 2);
         if ((s->iter % s->tplot) == 0) {
             orc_evaluate_macroscopic_properties(s);
+            if (s->pressure_outflag == 1) orc_cumulative_pressure(s);
             if (rec_out && *nrec < rec_cap) {
                 double *o = &rec_out[10 * (size_t)(*nrec)];
                 o[0] = (double)s->iter;

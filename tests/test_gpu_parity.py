@@ -502,6 +502,56 @@ def test_rebuild_criteria_schedule(liquid, crit, fixed):
     s.close()
 
 
+@pytest.mark.parametrize("case", ["half", "full", "lfv", "fene", "allpairs"])
+def test_pressure_tensor_single_system(liquid, case):
+    """PRESSURE_OUTFLAG 1 on the single-system path: the time-averaged virial
+    pressure tensor sum_i (v v + rf/2)/V over the record steps (cumulative_
+    pressure, simulation_record.f90:3151-3220) equals the oracle's for the
+    half and full lists, leap-frog, FENE bonds (rf from the bond loop too)
+    and all pairs (kinetic part only: LJ_AP records no rf); none at setup."""
+    from flowmol_b200 import polymer
+    kw, okw, mono = {}, {}, None
+    rc, rho = 2.5, 0.8442
+    if case == "fene":
+        r, v, ch, sub, fy, bf, dom = polymer.fene_melt(256)
+        rc, rho = WCA_RC, 0.85
+        kw = okw = dict(potential_flag=1, k_c=30.0, R_0=1.5)
+        mono = (ch, sub, fy, bf)
+    elif case == "allpairs":
+        r, v, dom = lattice.lj_fluid([3, 3, 3], 0.8, 1.0, 17)
+        kw = okw = dict(force_list=0)
+        rho = 0.8
+    else:
+        r, v, dom = liquid
+        if case == "full":
+            kw = okw = dict(force_list=2)
+        if case == "lfv":
+            kw = okw = dict(integration_algorithm=0)
+    o = O.Oracle(r, v, dom, rc, tplot=10, density=rho, **okw)
+    if mono is not None:
+        o.set_monomers(*mono)
+    o.set_pressure(1)
+    o.setup()
+    if case == "lfv":
+        o.run_lfv(100)
+    else:
+        o.run_vv(100)
+    po, no = o.pressure_average()
+    s = gpu_system(r, v, dom, rc, tplot=10, density=rho, **kw)
+    if mono is not None:
+        s.upload_monomers(mono[0], mono[1], mono[3])
+    s.set_pressure_outflag(1)
+    s.setup()
+    s.simulation_md(100)
+    pg, ng = s.pressure_tensor()
+    assert ng == no == 10
+    np.testing.assert_allclose(pg, po, rtol=1e-9, atol=1e-9 * np.abs(po).max())
+    assert np.allclose(pg, pg.T, rtol=1e-12, atol=1e-12 * np.abs(pg).max())
+    pr, nr = s.pressure_tensor(reset=True)
+    assert nr == 10 and s.pressure_tensor()[1] == 0
+    s.close()
+
+
 @pytest.mark.parametrize("case", ["wca", "lj", "fene", "faces"])
 def test_list_build_cells_equals_blocks(gpu_lib, case):
     """The per-cell and the 2x2x2-block list builds give identical rows (same

@@ -273,3 +273,27 @@ def test_soddemann_solution_wells_act():
     a1, pe1 = out[(1.5, 1.0, 0.5)]
     a0, pe0 = out[(0.0, 0.0, 0.0)]
     assert np.abs(a1 - a0).max() > 1e-3 and np.all(pe1 <= pe0 + 1e-12)
+
+
+def test_pressure_tensor_sampling_follows_the_reference_routines():
+    """pressure_averaging samples on the record steps of a run, not at setup
+    (setup_initial_record.f90:89 calls evaluate_macroscopic_properties only);
+    the all-pairs routine adds no rf (kinetic part only), the half list adds
+    acc rij rij on both sides."""
+    r, v, dom = lattice.lj_fluid([3, 3, 3], 0.8, 1.0, 17)
+    o = O.Oracle(r, v, dom, 2.5, tplot=5, force_list=0)
+    o.set_pressure(1)
+    o.setup()
+    assert o.pressure_average()[1] == 0
+    o.run_vv(20)
+    p, n = o.pressure_average()
+    assert n == 4
+    # kinetic only: with zero velocities the all-pairs tensor would vanish
+    o0 = O.Oracle(r, np.zeros_like(v), dom, 2.5, tplot=1, force_list=0)
+    o0.set_pressure(1)
+    o0.setup()
+    o0.run_vv(1)
+    p0, _ = o0.pressure_average()
+    vnew = o0.v
+    kin = np.einsum("ni,nj->ij", vnew, vnew) / np.prod(dom)
+    np.testing.assert_allclose(p0, kin, rtol=1e-12, atol=1e-15)
