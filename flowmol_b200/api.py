@@ -198,6 +198,7 @@ def lib():
             "fm_check_rebuild": [h, P(C.c_int32)],
             "fm_linklist_deallocateall": [h],
             "fm_sendmols": [h],
+            "fm_sort_mols": [h],
             "fm_assign_to_cell": [h],
             "fm_assign_to_neighbourlist": [h],
             "fm_compute_forces": [h],
@@ -439,8 +440,9 @@ class MDSystem:
         check(lib().fm_sendmols(self.h))
 
     def sort_mols(self):
-        """SORT_FLAG 0: molecules keep their identity (the device re-orders by
-        cell internally, invisibly)."""
+        """The device keeps molecules in cell order internally; transfers use
+        upload order, so the reference's Hilbert re-order is invisible."""
+        check(lib().fm_sort_mols(self.h))
 
     def assign_to_cell(self):
         check(lib().fm_assign_to_cell(self.h))

@@ -940,6 +940,8 @@ extern "C" int fm_check_rebuild(fm_handle *h, int32_t *rebuild)
     return FM_OK;
 }
 
+extern "C" int fm_sort_mols(fm_handle *h) { return ready(h, 1); }
+
 extern "C" int fm_sendmols(fm_handle *h)
 {
     FM_TRY(ready(h, 1));

@@ -209,6 +209,12 @@ FM_API int fm_linklist_deallocateall(fm_handle *h);
 /* sendmols, single-rank form: periodic wrap r >= L/2 -> r-L, r < -L/2 -> r+L
  * (messenger.serial.f90:961-1028; messenger.MPI.f90:1383-1424). */
 FM_API int fm_sendmols(fm_handle *h);
+/* sort_mols (linklist.f90:2744-2869): the reference re-orders r and v along a
+ * Hilbert curve every sort_freq rebuilds for cache locality.  The device keeps
+ * its molecules in cell order at every rebuild anyway, and state transfers use
+ * upload order, so the order is invisible to the caller and this call only
+ * validates the handle. */
+FM_API int fm_sort_mols(fm_handle *h);
 /* assign_to_cell (linklist.f90:2645-2679) as a counting sort: histogram,
  * exclusive scan, scatter.  Molecules are also re-ordered by cell on the
  * device (invisible through fm_download_state). */
