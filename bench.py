@@ -504,6 +504,9 @@ def main():
         n = NUNITS[0] * NUNITS[1] * NUNITS[2] * 4
         line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "impl": "reference",
                 "n_gpus": args.gpus, "steps": steps, "warmup": 0,
+                # the CPU sample is bounded (2-16 velocity-Verlet steps of the full
+                # 1M system on every core) so that the arm ends within minutes
+                "steps_requested": args.steps, "warmup_requested": args.warmup,
                 "ms_per_step": 1e3 * n / cb["value"], "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": {"workload": workload_name(), "molecules": n, "form": "oracle FP64 CPU restatement"},
