@@ -552,6 +552,59 @@ def test_pressure_tensor_single_system(liquid, case):
     s.close()
 
 
+@pytest.mark.parametrize("prec", [api.PRECISION_FP64, api.PRECISION_FP32])
+def test_dense_cells_beyond_one_warp(gpu_lib, prec):
+    """Cells holding more than 32 molecules (rho 1.05, skin 0.8: cell side
+    3.3, ~38 per cell): the build's second owner pass, the per-cell sort's
+    one-lane path for large cells and the list's wide rows, against the
+    oracle -- pair set bit-exact, forces to 1e-12 (FP64) or 1e-5 (FP32), and
+    60 steps with rebuilds."""
+    r, v, dom = lattice.lj_fluid([8, 8, 8], 1.05, 1.2, 93)
+    r = lattice.jitter(r, 0.04, 93, dom)
+    skin = (0.8, 0.8, 0.8)
+    o = O.Oracle(r, v, dom, 2.5, skin, tplot=20, density=1.05)
+    o.setup()
+    g = o.geometry()
+    per_cell = len(r) / np.prod(g["ncells"])
+    assert per_cell > 32, per_cell
+    s = gpu_system(r, v, dom, 2.5, precision=prec, tplot=20, density=1.05, delta_rneighbr=skin)
+    s.setup()
+    assert np.array_equal(canonical_full(*s.pair_list()), canonical_oracle(*o.pair_list()))
+    _, _, a, _ = s.download()
+    if prec == api.PRECISION_FP32:
+        assert rel_err(a, o.a, F_FLOOR32).max() <= TOL32
+        s.close()
+        return
+    assert rel_err(a, o.a, 1.0).max() <= TOL64
+    o.run_vv(60)
+    s.simulation_md(60)
+    assert s.counters()["rebuilds"] == o.rebuild_count > 0
+    rg, _, _, _ = s.download()
+    assert np.abs(wrap_diff(rg, o.r, dom)).max() < 1e-7
+    s.close()
+
+
+def test_two_molecules_in_the_cell_path(gpu_lib):
+    """The smallest list-path system: two molecules in a box of 3x3x3 cells
+    (all other cells empty), one pair inside r_c: the force is the two-body
+    LJ force, equal and opposite, and 30 steps follow the oracle."""
+    L = 8.5
+    r = np.array([[-0.6, 0.1, 0.2], [0.55, 0.1, 0.25]])
+    v = np.array([[0.3, -0.1, 0.05], [-0.3, 0.1, -0.05]])
+    o = O.Oracle(r, v, [L, L, L], 2.5, tplot=10)
+    o.setup()
+    s = gpu_system(r, v, [L, L, L], 2.5, tplot=10)
+    s.setup()
+    _, _, a, _ = s.download()
+    assert rel_err(a, o.a, 1.0).max() <= TOL64
+    assert np.abs(a[0] + a[1]).max() <= 1e-12 * np.abs(a).max()
+    o.run_vv(30)
+    s.simulation_md(30)
+    rg, vg, _, _ = s.download()
+    assert np.abs(wrap_diff(rg, o.r, [L, L, L])).max() < 1e-10
+    s.close()
+
+
 @pytest.mark.parametrize("case", ["wca", "lj", "fene", "faces"])
 def test_list_build_cells_equals_blocks(gpu_lib, case):
     """The per-cell and the 2x2x2-block list builds give identical rows (same
