@@ -12,6 +12,18 @@ __device__ __forceinline__ double norm2_rn(double x, double y, double z)
     return __dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z));
 }
 
+// Neighbour-list entries are read once per step and never again before the
+// next step: keep them out of L1, so that the partner positions they point at
+// stay cached there.
+__device__ __forceinline__ int4 ld_stream_int4(const int4 *p)
+{
+    int4 r;
+    asm("ld.global.nc.L1::no_allocate.v4.s32 {%0, %1, %2, %3}, [%4];"
+        : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+        : "l"(p));
+    return r;
+}
+
 // Read-only gather of one double4 (32-byte aligned) as a single 256-bit load:
 // one L1 request per partner instead of two.
 __device__ __forceinline__ double4 ldg_pos(const double4 *p)

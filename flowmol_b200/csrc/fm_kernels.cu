@@ -757,7 +757,7 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force(FmDev d)
         // each lane takes 4 consecutive entries per iteration (one 16-byte load)
         // and issues their 4 gathers before any arithmetic
         for (int k0 = lane * 4; k0 < cnt; k0 += 4 * TPM) {
-            const int4 e4 = __ldg(reinterpret_cast<const int4 *>(L + (size_t)k0 * 32));
+            const int4 e4 = ld_stream_int4(reinterpret_cast<const int4 *>(L + (size_t)k0 * 32));
             const int ev[4] = {e4.x, e4.y, e4.z, e4.w};
             double4 pj[4];
 #pragma unroll
