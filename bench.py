@@ -23,6 +23,7 @@ import json
 import os
 import statistics
 import subprocess
+import tempfile
 import sys
 import time
 
@@ -116,7 +117,9 @@ class Clocks:
     def __init__(self, device):
         self.device = device
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+        # raw samples; the JSON line carries their summary
+        out_dir = os.environ.get("FM_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(out_dir, f"clocks_bench_{os.getpid()}.csv")
 
     def __enter__(self):
         try:

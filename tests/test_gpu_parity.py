@@ -1,6 +1,6 @@
 """Parity of the CUDA path (through the C ABI) with the FP64 CPU oracle.
 
-Tolerances:
+Tolerances (the stated contract of the path):
   * pair sets: bit-exact (FP64 distance test, no FMA, same image roundings);
   * FP64 forces: |F_gpu - F_ref| <= 1e-12 * max(|F_ref|, 1), per molecule;
   * FP32 pair forces: |F_gpu - F_ref| <= 1e-5 * max(|F_ref|, F_FLOOR32), per
