@@ -12,6 +12,16 @@ __device__ __forceinline__ double norm2_rn(double x, double y, double z)
     return __dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z));
 }
 
+// Programmatic dependent launch (kernels started with pdl_launch): wait for
+// the predecessor grid to complete and its memory to be visible before
+// touching anything, then let the successor grid begin launching.  Both are
+// no-ops for a kernel launched without the attribute.
+__device__ __forceinline__ void pdl_enter()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Neighbour-list entries are read once per step and never again before the
 // next step: keep them out of L1, so that the partner positions they point at
 // stay cached there.

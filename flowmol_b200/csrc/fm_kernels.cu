@@ -78,6 +78,7 @@ __global__ void k_reset_scalars(FmDev d)
 // r = (r + dt v) + (0.5 dt^2) a ; v = v + (0.5 dt) a   -- pass 1, in place.
 __global__ void k_move1(FmDev d)
 {
+    pdl_enter();
     if (frozen(d)) return;
     double4 *P = cur_pos(d, d.sc->pset);
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -101,6 +102,7 @@ __global__ void k_move1(FmDev d)
 
 __global__ void k_move2(FmDev d)
 {
+    pdl_enter();
     if (frozen(d)) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < d.n) {
@@ -113,6 +115,7 @@ __global__ void k_move2(FmDev d)
 // simulation_move_particles_lfv NVE (simulation_move_particles_lfv.f90:81-92), in place.
 __global__ void k_move_lfv(FmDev d)
 {
+    pdl_enter();
     if (frozen(d)) return;
     double4 *P = cur_pos(d, d.sc->pset);
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -134,6 +137,7 @@ __global__ void k_move_lfv(FmDev d)
 
 __global__ void k_vmax(FmDev d)
 {
+    pdl_enter();
     if (frozen(d)) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double m2 = 0.0;
@@ -147,6 +151,7 @@ __global__ void k_vmax(FmDev d)
 // so the next check starts it from zero.
 __global__ void k_disp(FmDev d)
 {
+    pdl_enter();
     if (frozen(d)) return;
     const bool restart = d.sc->disp_reset != 0;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -177,6 +182,7 @@ __global__ void k_disp(FmDev d)
 
 __global__ void k_decide(FmDev d, int iter, int flip, int crit, int fixed_rebuild, double half_min_delta)
 {
+    pdl_enter();
     FmScalars *s = d.sc;
     if (s->status & ST_FATAL) return;
     if (flip) s->pset ^= 1;
@@ -216,6 +222,7 @@ __device__ __forceinline__ bool gate(const FmDev &d, int gated)
 
 __global__ void k_wrap_bin(FmDev d, int wrap, int bin, int gated, int iter)
 {
+    pdl_enter();
     if (!gate(d, gated)) return;
     double4 *P = cur_pos(d, d.sc->pset);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < d.n; i += gridDim.x * blockDim.x) {
@@ -282,6 +289,7 @@ __device__ __forceinline__ int block_excl_scan(int v, int *total)
 
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan_tiles(FmDev d, int gated)
 {
+    pdl_enter();
     if (!gate(d, gated)) return;
     __shared__ int tot;
     const int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_PER;
@@ -295,6 +303,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_tiles(FmDev d, int gated)
 
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(FmDev d, int gated)
 {
+    pdl_enter();
     if (!gate(d, gated)) return;
     __shared__ int tot, prefix;
     if (threadIdx.x < 32) {
@@ -325,6 +334,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(FmDev d, int gated)
 
 __global__ void k_scatter(FmDev d, int gated)
 {
+    pdl_enter();
     if (!gate(d, gated)) return;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < d.n; i += gridDim.x * blockDim.x) {
         int c = d.cell_of[i];
@@ -339,6 +349,7 @@ __global__ void k_scatter(FmDev d, int gated)
 constexpr int SORT_WARPS = 8;
 __global__ void __launch_bounds__(32 * SORT_WARPS) k_sort_cells(FmDev d, int gated)
 {
+    pdl_enter();
     if (!gate(d, gated)) return;
     const int lane = threadIdx.x & 31;
     for (int c = blockIdx.x * SORT_WARPS + (threadIdx.x >> 5); c < d.ncell; c += gridDim.x * SORT_WARPS) {
@@ -375,6 +386,7 @@ __global__ void __launch_bounds__(32 * SORT_WARPS) k_sort_cells(FmDev d, int gat
 // its address (the step loop never needs to know whether a rebuild ran).
 __global__ void k_reorder_gather(FmDev d, int gated, double4 *tpos, int32_t *tuidx)
 {
+    pdl_enter();
     if (!gate(d, gated)) return;
     const double4 *P = cur_pos(d, d.sc->pset);
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < d.n; s += gridDim.x * blockDim.x) {
@@ -391,6 +403,7 @@ __global__ void k_reorder_gather(FmDev d, int gated, double4 *tpos, int32_t *tui
 
 __global__ void k_reorder_copy(FmDev d, int gated, const double4 *tpos, const int32_t *tuidx)
 {
+    pdl_enter();
     if (!gate(d, gated)) return;
     double4 *P = cur_pos(d, d.sc->pset);
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < d.n; s += gridDim.x * blockDim.x) {
@@ -416,6 +429,7 @@ __global__ void k_reorder_copy(FmDev d, int gated, const double4 *tpos, const in
 template <bool POLY, bool BLOCKS>
 __global__ void __launch_bounds__(NB_THREADS, 8) k_build_nlist(FmDev d, int gated, int iter)
 {
+    pdl_enter();
     if (!gate(d, gated)) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     using Shared = typename std::conditional<BLOCKS, BlockShared<POLY>, BuildShared<POLY>>::type;
@@ -739,6 +753,7 @@ __device__ __forceinline__ void block_partials(const FmDev &d, double v[RS_N])
 template <int TPM, bool REC, int MODE, int PREC>
 __global__ void __launch_bounds__(FORCE_THREADS) k_force(FmDev d)
 {
+    pdl_enter();
     if (frozen(d)) return;
     const int pset = d.sc->pset;
     const double4 *__restrict__ P = cur_pos(d, pset);
@@ -815,6 +830,7 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force(FmDev d)
 constexpr int REC_THREADS = 256;
 __global__ void __launch_bounds__(REC_THREADS) k_record(FmDev d, int iter, double simtime)
 {
+    pdl_enter();
     if (frozen(d)) return;
     __shared__ double ssum[RS_N][REC_THREADS], scmp[RS_N][REC_THREADS];
     double sum[RS_N], cmp[RS_N];
@@ -878,6 +894,7 @@ __global__ void __launch_bounds__(REC_THREADS) k_record(FmDev d, int iter, doubl
 constexpr int MACRO_THREADS = 256;
 __global__ void __launch_bounds__(MACRO_THREADS) k_macro_partials(FmDev d)
 {
+    pdl_enter();
     if (frozen(d)) return;
     int i = blockIdx.x * MACRO_THREADS + threadIdx.x;
     double part[RS_N] = {};
@@ -924,6 +941,7 @@ constexpr int AP_THREADS = 128;
 template <bool REC, int MODE, int PREC>
 __global__ void __launch_bounds__(AP_THREADS) k_all_pairs(FmDev d)
 {
+    pdl_enter();
     if (frozen(d)) return;
     const int pset = d.sc->pset;
     const double4 *P = cur_pos(d, pset);
@@ -1076,17 +1094,37 @@ inline int nblk(int n, int t) { return (n + t - 1) / t; }
 // launchers
 // ---------------------------------------------------------------------------
 
+// Launches k with programmatic stream serialization: the next kernel of the
+// step may be launched while k's last blocks run, and waits in pdl_enter for
+// k to complete before it reads anything (so the chain of small, often gated
+// kernels of a step does not pay a full launch gap each).
+template <typename... P, typename... A>
+void pdl_launch(void (*k)(P...), dim3 grid, dim3 block, cudaStream_t st, A... args)
+{
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t c = {};
+    c.gridDim = grid;
+    c.blockDim = block;
+    c.dynamicSmemBytes = 0;
+    c.stream = st;
+    c.attrs = at;
+    c.numAttrs = 1;
+    cudaLaunchKernelEx(&c, k, args...);
+}
+
 void launch_reset_scalars(const FmDev &d, cudaStream_t st) { k_reset_scalars<<<1, 1, 0, st>>>(d); }
-void launch_move1(const FmDev &d, cudaStream_t st) { k_move1<<<nblk(d.n, 256), 256, 0, st>>>(d); }
-void launch_move2(const FmDev &d, cudaStream_t st) { k_move2<<<nblk(d.n, 256), 256, 0, st>>>(d); }
-void launch_vmax(const FmDev &d, cudaStream_t st) { k_vmax<<<nblk(d.n, 256), 256, 0, st>>>(d); }
-void launch_move_lfv(const FmDev &d, cudaStream_t st) { k_move_lfv<<<nblk(d.n, 256), 256, 0, st>>>(d); }
-void launch_disp(const FmDev &d, cudaStream_t st) { k_disp<<<nblk(d.n, 256), 256, 0, st>>>(d); }
+void launch_move1(const FmDev &d, cudaStream_t st) { pdl_launch(k_move1, nblk(d.n, 256), 256, st, d); }
+void launch_move2(const FmDev &d, cudaStream_t st) { pdl_launch(k_move2, nblk(d.n, 256), 256, st, d); }
+void launch_vmax(const FmDev &d, cudaStream_t st) { pdl_launch(k_vmax, nblk(d.n, 256), 256, st, d); }
+void launch_move_lfv(const FmDev &d, cudaStream_t st) { pdl_launch(k_move_lfv, nblk(d.n, 256), 256, st, d); }
+void launch_disp(const FmDev &d, cudaStream_t st) { pdl_launch(k_disp, nblk(d.n, 256), 256, st, d); }
 
 void launch_decide(const FmDev &d, int iter, int flip, int crit, int fixed_rebuild, double half_min_delta,
                    cudaStream_t st)
 {
-    k_decide<<<1, 1, 0, st>>>(d, iter, flip, crit, fixed_rebuild > 0 ? fixed_rebuild : 1, half_min_delta);
+    pdl_launch(k_decide, 1, 1, st, d, iter, flip, crit, fixed_rebuild > 0 ? fixed_rebuild : 1, half_min_delta);
 }
 // Gated kernels run grid-stride loops on a bounded grid, so that a launch the
 // device decision turns into a no-op costs a few microseconds at most.
@@ -1095,23 +1133,23 @@ inline int sgrid(int n, int t, int per_sm) { return std::min(nblk(n, t), kSMs * 
 
 void launch_wrap_bin(const FmDev &d, int wrap, int bin, int gated, int iter, cudaStream_t st)
 {
-    k_wrap_bin<<<sgrid(d.n, 256, 8), 256, 0, st>>>(d, wrap, bin, gated, iter);
+    pdl_launch(k_wrap_bin, sgrid(d.n, 256, 8), 256, st, d, wrap, bin, gated, iter);
 }
 int scan_tiles(int ncell) { return nblk(ncell, SCAN_TILE); }
 void launch_scan_cells(const FmDev &d, int gated, cudaStream_t st)
 {
-    k_scan_tiles<<<scan_tiles(d.ncell), SCAN_THREADS, 0, st>>>(d, gated);
-    k_scan_apply<<<scan_tiles(d.ncell), SCAN_THREADS, 0, st>>>(d, gated);
+    pdl_launch(k_scan_tiles, scan_tiles(d.ncell), SCAN_THREADS, st, d, gated);
+    pdl_launch(k_scan_apply, scan_tiles(d.ncell), SCAN_THREADS, st, d, gated);
 }
 void launch_scatter(const FmDev &d, int gated, cudaStream_t st)
 {
-    k_scatter<<<sgrid(d.n, 256, 8), 256, 0, st>>>(d, gated);
-    k_sort_cells<<<sgrid(d.ncell, SORT_WARPS, 8), 32 * SORT_WARPS, 0, st>>>(d, gated);
+    pdl_launch(k_scatter, sgrid(d.n, 256, 8), 256, st, d, gated);
+    pdl_launch(k_sort_cells, sgrid(d.ncell, SORT_WARPS, 8), 32 * SORT_WARPS, st, d, gated);
 }
 void launch_reorder(const FmDev &d, int gated, double4 *tpos, int32_t *tuidx, cudaStream_t st)
 {
-    k_reorder_gather<<<sgrid(d.n, 256, 8), 256, 0, st>>>(d, gated, tpos, tuidx);
-    k_reorder_copy<<<sgrid(d.n, 256, 8), 256, 0, st>>>(d, gated, tpos, tuidx);
+    pdl_launch(k_reorder_gather, sgrid(d.n, 256, 8), 256, st, d, gated, tpos, tuidx);
+    pdl_launch(k_reorder_copy, sgrid(d.n, 256, 8), 256, st, d, gated, tpos, tuidx);
 }
 // The list build walks the cells grid-stride with every block resident (one
 // wave: a second partial wave would double the kernel's time).
@@ -1134,11 +1172,11 @@ void launch_build_nlist(const FmDev &d, int gated, int iter, cudaStream_t st)
     cudaMemsetAsync(&d.sc->build_next, 0, sizeof(int32_t), st);
     const int nb = ((d.ne[0] + 1) / 2) * ((d.ne[1] + 1) / 2) * ((d.ne[2] + 1) / 2);
     if (d.potential_flag == 1) {
-        if (d.build_blocks) k_build_nlist<true, true><<<build_grid<true, true>(nb), NB_THREADS, 0, st>>>(d, gated, iter);
-        else k_build_nlist<true, false><<<build_grid<true, false>(d.ncell), NB_THREADS, 0, st>>>(d, gated, iter);
+        if (d.build_blocks) pdl_launch(k_build_nlist<true, true>, build_grid<true, true>(nb), NB_THREADS, st, d, gated, iter);
+        else pdl_launch(k_build_nlist<true, false>, build_grid<true, false>(d.ncell), NB_THREADS, st, d, gated, iter);
     } else {
-        if (d.build_blocks) k_build_nlist<false, true><<<build_grid<false, true>(nb), NB_THREADS, 0, st>>>(d, gated, iter);
-        else k_build_nlist<false, false><<<build_grid<false, false>(d.ncell), NB_THREADS, 0, st>>>(d, gated, iter);
+        if (d.build_blocks) pdl_launch(k_build_nlist<false, true>, build_grid<false, true>(nb), NB_THREADS, st, d, gated, iter);
+        else pdl_launch(k_build_nlist<false, false>, build_grid<false, false>(d.ncell), NB_THREADS, st, d, gated, iter);
     }
 }
 
@@ -1152,12 +1190,12 @@ static void launch_force_tpm(const FmDev &d, int record, int mode, cudaStream_t 
 #define FM_FORCE_CASE(R, M)                                                                     \
     if (record == R && mode == M) {                                                             \
         switch (d.precision + 2 * d.mie + 4 * d.solvent) {                                      \
-        case 0: k_force<TPM, R, M, 0><<<g, FORCE_THREADS, 0, st>>>(d); break;                   \
-        case 1: k_force<TPM, R, M, 1><<<g, FORCE_THREADS, 0, st>>>(d); break;                   \
-        case 2: k_force<TPM, R, M, 2><<<g, FORCE_THREADS, 0, st>>>(d); break;                   \
-        case 3: k_force<TPM, R, M, 3><<<g, FORCE_THREADS, 0, st>>>(d); break;                   \
-        case 4: k_force<TPM, R, M, 4><<<g, FORCE_THREADS, 0, st>>>(d); break;                   \
-        default: k_force<TPM, R, M, 5><<<g, FORCE_THREADS, 0, st>>>(d); break;                  \
+        case 0: pdl_launch(k_force<TPM, R, M, 0>, g, FORCE_THREADS, st, d); break;                   \
+        case 1: pdl_launch(k_force<TPM, R, M, 1>, g, FORCE_THREADS, st, d); break;                   \
+        case 2: pdl_launch(k_force<TPM, R, M, 2>, g, FORCE_THREADS, st, d); break;                   \
+        case 3: pdl_launch(k_force<TPM, R, M, 3>, g, FORCE_THREADS, st, d); break;                   \
+        case 4: pdl_launch(k_force<TPM, R, M, 4>, g, FORCE_THREADS, st, d); break;                   \
+        default: pdl_launch(k_force<TPM, R, M, 5>, g, FORCE_THREADS, st, d); break;                  \
         }                                                                                       \
         return;                                                                                 \
     }
@@ -1183,10 +1221,10 @@ void launch_all_pairs(const FmDev &d, int record, int mode, cudaStream_t st)
 #define FM_AP_CASE(R, M)                                                            \
     if (record == R && mode == M) {                                                 \
         switch (d.precision + 2 * d.mie) {                                          \
-        case 0: k_all_pairs<R, M, 0><<<g, AP_THREADS, 0, st>>>(d); break;           \
-        case 1: k_all_pairs<R, M, 1><<<g, AP_THREADS, 0, st>>>(d); break;           \
-        case 2: k_all_pairs<R, M, 2><<<g, AP_THREADS, 0, st>>>(d); break;           \
-        default: k_all_pairs<R, M, 3><<<g, AP_THREADS, 0, st>>>(d); break;          \
+        case 0: pdl_launch(k_all_pairs<R, M, 0>, g, AP_THREADS, st, d); break;           \
+        case 1: pdl_launch(k_all_pairs<R, M, 1>, g, AP_THREADS, st, d); break;           \
+        case 2: pdl_launch(k_all_pairs<R, M, 2>, g, AP_THREADS, st, d); break;           \
+        default: pdl_launch(k_all_pairs<R, M, 3>, g, AP_THREADS, st, d); break;          \
         }                                                                           \
         return;                                                                     \
     }
@@ -1198,12 +1236,12 @@ void launch_all_pairs(const FmDev &d, int record, int mode, cudaStream_t st)
 int macro_blocks(int n) { return nblk(n, MACRO_THREADS); }
 void launch_macro_partials(const FmDev &d, cudaStream_t st)
 {
-    k_macro_partials<<<macro_blocks(d.n), MACRO_THREADS, 0, st>>>(d);
+    pdl_launch(k_macro_partials, macro_blocks(d.n), MACRO_THREADS, st, d);
 }
 
 void launch_record(const FmDev &d, int iter, double simtime, cudaStream_t st)
 {
-    k_record<<<1, REC_THREADS, 0, st>>>(d, iter, simtime);
+    pdl_launch(k_record, 1, REC_THREADS, st, d, iter, simtime);
 }
 
 void launch_pair_digest(const FmDev &d, const int32_t *glob_of_upload, cudaStream_t st)
