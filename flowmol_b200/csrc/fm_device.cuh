@@ -22,6 +22,26 @@ __device__ __forceinline__ void pdl_enter()
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
+// Launches k with programmatic stream serialization: the next kernel of the
+// step may be launched while k's last blocks run, and waits in pdl_enter for
+// k to complete before it reads anything (so the chain of small, often gated
+// kernels of a step does not pay a full launch gap each).
+template <typename... P, typename... A>
+void pdl_launch(void (*k)(P...), dim3 grid, dim3 block, cudaStream_t st, A... args)
+{
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t c = {};
+    c.gridDim = grid;
+    c.blockDim = block;
+    c.dynamicSmemBytes = 0;
+    c.stream = st;
+    c.attrs = at;
+    c.numAttrs = 1;
+    cudaLaunchKernelEx(&c, k, args...);
+}
+
 // Neighbour-list entries are read once per step and never again before the
 // next step: keep them out of L1, so that the partner positions they point at
 // stay cached there.

@@ -1094,25 +1094,6 @@ inline int nblk(int n, int t) { return (n + t - 1) / t; }
 // launchers
 // ---------------------------------------------------------------------------
 
-// Launches k with programmatic stream serialization: the next kernel of the
-// step may be launched while k's last blocks run, and waits in pdl_enter for
-// k to complete before it reads anything (so the chain of small, often gated
-// kernels of a step does not pay a full launch gap each).
-template <typename... P, typename... A>
-void pdl_launch(void (*k)(P...), dim3 grid, dim3 block, cudaStream_t st, A... args)
-{
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[0].val.programmaticStreamSerializationAllowed = 1;
-    cudaLaunchConfig_t c = {};
-    c.gridDim = grid;
-    c.blockDim = block;
-    c.dynamicSmemBytes = 0;
-    c.stream = st;
-    c.attrs = at;
-    c.numAttrs = 1;
-    cudaLaunchKernelEx(&c, k, args...);
-}
 
 void launch_reset_scalars(const FmDev &d, cudaStream_t st) { k_reset_scalars<<<1, 1, 0, st>>>(d); }
 void launch_move1(const FmDev &d, cudaStream_t st) { pdl_launch(k_move1, nblk(d.n, 256), 256, st, d); }
