@@ -119,3 +119,22 @@ def test_input_reader_fene_solution_with_soddemann_solvent(tmp_path):
     with pytest.raises(api.FlowmolError) as e:
         api.read_input(str(p))
     assert "solvent flag" in str(e.value)
+
+
+def test_input_reader_dense_fene_special_case(tmp_path):
+    """INITIAL_CONFIG_FLAG 1 dense_fene reads the DENSE_FENE block (nmonomers,
+    k_c, r_0, density, initialnunits) and sets potential_flag 1 with the WCA
+    cutoff (setup_read_input.f90:229-254); a missing block is an error, not a
+    silent LJ run."""
+    base = open(os.path.join(GOLD, "default.in")).read()
+    deck = base.replace("INITIAL_CONFIG_FLAG\n0\nspecial_case_name", "INITIAL_CONFIG_FLAG\n1\ndense_fene")
+    p = tmp_path / "MD.in"
+    p.write_text(deck)
+    with pytest.raises(api.FlowmolError) as e:
+        api.read_input(str(p))
+    assert "DENSE_FENE" in str(e.value)
+    p.write_text(deck + "\nDENSE_FENE\n8\n30.0\n1.5\n0.85\n16\n16\n16\n")
+    x = api.read_input(str(p))
+    assert x.potential_flag == 1 and x.nmonomers == 8 and x.k_c == 30.0 and x.R_0 == 1.5
+    assert x.density == 0.85 and list(x.initialnunits) == [16, 16, 16] and x.rcutoff == 2.0 ** (1.0 / 6.0)
+    assert x.solvent_flag == 0
