@@ -686,3 +686,18 @@ def read_input(path) -> FmInput:
     x = FmInput()
     check(lib().fm_read_input(os.fsencode(path), C.byref(x)))
     return x
+
+
+def params_from_input(inp: FmInput, np_, domain, precision=PRECISION_FP64, **overrides) -> FmParams:
+    """fm_params for the run an MD.in deck describes (read_input), given the
+    molecule count and box -- from a restart header, or global_domain of the
+    deck's INITIALNUNITS and DENSITY for a lattice start.  Keyword arguments
+    override single fields (e.g. tplot, nlist_capacity)."""
+    kw = dict(delta_rneighbr=tuple(inp.delta_rneighbr), delta_t=inp.delta_t, tplot=inp.tplot,
+              density=inp.density, force_list=inp.force_list, potential_flag=inp.potential_flag,
+              rebuild_criteria=inp.rebuild_criteria, fixed_rebuild=max(1, inp.fixed_rebuild),
+              sLRC_flag=inp.sLRC_flag, precision=precision, k_c=inp.k_c, R_0=inp.R_0,
+              integration_algorithm=inp.integration_algorithm, solvent_flag=inp.solvent_flag,
+              eps=(inp.eps_pp, inp.eps_ps, inp.eps_ss))
+    kw.update(overrides)
+    return make_params(np_, domain, inp.rcutoff, **kw)

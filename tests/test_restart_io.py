@@ -138,3 +138,19 @@ def test_input_reader_dense_fene_special_case(tmp_path):
     assert x.potential_flag == 1 and x.nmonomers == 8 and x.k_c == 30.0 and x.R_0 == 1.5
     assert x.density == 0.85 and list(x.initialnunits) == [16, 16, 16] and x.rcutoff == 2.0 ** (1.0 / 6.0)
     assert x.solvent_flag == 0
+
+
+def test_params_from_input_deck_give_the_reference_geometry():
+    """fm_params built from default.in (8x8x8 FCC units at rho 0.8, WCA,
+    skin 0.3) give the oracle's cells, rneighbr2 and potshift."""
+    import oracle as O
+    x = api.read_input(os.path.join(GOLD, "default.in"))
+    dom = api.global_domain(list(x.initialnunits), x.density)
+    n = 4 * int(np.prod(list(x.initialnunits)))
+    p = api.params_from_input(x, n, dom)
+    assert p.np == n and p.tplot == x.tplot and p.delta_t == x.delta_t
+    rc, g = api.derive_geometry(p)
+    assert rc == 0
+    rco, nc, cs, rn2 = O.cells(dom, x.rcutoff, list(x.delta_rneighbr))
+    assert rco == 0 and g["ncells"] == list(nc) and g["cellside"] == list(cs) and g["rneighbr2"] == rn2
+    assert g["potshift"] == O.lib().orc_potshift(x.rcutoff)
