@@ -216,6 +216,9 @@ extern "C" int fm_create(const fm_params *p, fm_handle **out)
     if (p->potential_flag != 0 && p->potential_flag != 1) return fail(FM_ERR_ARG, "potential_flag must be 0 or 1");
     if (p->potential_flag == 1 && p->force_list == 0)
         return fail(FM_ERR_ARG, "potential flag/force_list incompatible - only LJ available with all pairs");
+    if (p->potential_flag == 1 && p->force_list == 2)  // simulation_compute_forces.f90:242-246
+        return fail(FM_ERR_ARG,
+                    "potential flag/force_list incompatible - only LJ available with full interaction neighbour lists");
     if (p->potential_flag == 1 && !(p->R_0 > 0.0 && p->k_c >= 0.0)) return fail(FM_ERR_ARG, "FENE needs R_0 > 0");
     if (p->solvent_flag != 0 && p->solvent_flag != 1) return fail(FM_ERR_ARG, "solvent_flag must be 0 or 1");
     if (p->solvent_flag == 1 && (p->potential_flag != 1 || p->force_list != 3))

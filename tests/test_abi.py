@@ -71,3 +71,25 @@ def test_create_without_device_is_an_error_code():
     p = api.make_params(100, [20.0, 20.0, 20.0], 2.5)
     h = C.c_void_p()
     assert api.lib().fm_create(C.byref(p), C.byref(h)) == 9  # FM_ERR_NODEVICE
+
+
+def test_combinations_the_reference_refuses_are_argument_errors():
+    """Parameter sets the reference stops on with error_abort come back as
+    FM_ERR_ARG from fm_create, before any device is touched: polymers with
+    all pairs or the full list (simulation_compute_forces.f90:206, 242-246),
+    the Soddemann solvent outside the half list, unknown flags."""
+    import ctypes as C
+    L = api.lib()
+    h = C.c_void_p()
+    cases = [
+        (dict(potential_flag=1, force_list=0), "all pairs"),
+        (dict(potential_flag=1, force_list=2), "full interaction"),
+        (dict(potential_flag=1, force_list=2, solvent_flag=1), "full interaction"),
+        (dict(potential_flag=0, solvent_flag=1), "solvent"),
+        (dict(rebuild_criteria=3), "rebuild_criteria"),
+        (dict(solvent_flag=2, potential_flag=1), "solvent_flag"),
+    ]
+    for kw, word in cases:
+        p = api.make_params(100, [10.0, 10.0, 10.0], 2.5, **kw)
+        assert L.fm_create(C.byref(p), C.byref(h)) == 1, kw
+        assert word in api.last_error(), (kw, api.last_error())
