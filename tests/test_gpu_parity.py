@@ -605,6 +605,62 @@ def test_two_molecules_in_the_cell_path(gpu_lib):
     s.close()
 
 
+def test_pressure_tensor_mie_mixture(liquid):
+    """The pressure tensor of a two-type Mie fluid with unequal masses: the
+    pair term uses the Mie accijmag, the kinetic term v v has no mass factor
+    (cumulative_pressure, simulation_record.f90:3170-3199), as in the oracle."""
+    from helpers import mie_mixture_tables
+    r, v, dom = liquid
+    mt = (np.arange(len(r)) % 2 + 1).astype(np.int32)
+    tab = mie_mixture_tables(2.5)
+    o = O.Oracle(r, v, dom, 2.5, tplot=10, density=0.8442)
+    o.set_mie(tab, mt)
+    o.set_pressure(1)
+    o.setup()
+    o.run_vv(50)
+    po, no = o.pressure_average()
+    s = gpu_system(r, v, dom, 2.5, tplot=10, density=0.8442)
+    s.set_mie(tab, mt)
+    s.set_pressure_outflag(1)
+    s.setup()
+    s.simulation_md(50)
+    pg, ng = s.pressure_tensor()
+    assert ng == no == 5
+    np.testing.assert_allclose(pg, po, rtol=1e-9, atol=1e-9 * np.abs(po).max())
+    s.close()
+
+
+@pytest.mark.parametrize("crit", [0, 2])
+def test_soddemann_leapfrog_trajectory(gpu_lib, crit):
+    """Soddemann polymer solution under leap-frog (INTEGRATION_ALGORITHM 0),
+    with the Rapaport and the exact-displacement rebuild criteria: the same
+    rebuilds as the oracle, records and positions after 80 steps."""
+    from flowmol_b200 import polymer
+    r, v, ch, sub, fy, bf, dom = polymer.fene_solution(96, targetconc=0.5)
+    r = lattice.jitter(r, 0.08, 94, dom)
+    eps = (1.5, 1.0, 0.5)
+    kw = dict(potential_flag=1, k_c=30.0, R_0=1.5, integration_algorithm=0, rebuild_criteria=crit)
+    o = O.Oracle(r, v, dom, WCA_RC, tplot=20, density=0.85, **kw)
+    o.set_monomers(ch, sub, fy, bf)
+    o.set_solvent(1, *eps)
+    o.setup()
+    recs_o = o.run_lfv(80)
+    s = gpu_system(r, v, dom, WCA_RC, tplot=20, density=0.85, solvent_flag=1, eps=eps, **kw)
+    s.upload_monomers(ch, sub, bf)
+    s.setup()
+    s.records()
+    s.simulation_md(80)
+    recs = s.records()
+    assert s.counters()["rebuilds"] == o.rebuild_count > 0
+    assert [x["iter"] for x in recs] == [int(x) for x in recs_o[:, 0]]
+    for row, ro in zip(recs, recs_o):
+        assert row["potenergy"] == pytest.approx(ro[5], rel=1e-9)
+        assert row["kinenergy"] == pytest.approx(ro[4], rel=1e-9)
+    rg, _, _, _ = s.download()
+    assert np.abs(wrap_diff(rg, o.r, dom)).max() < 1e-7
+    s.close()
+
+
 @pytest.mark.parametrize("case", ["wca", "lj", "fene", "faces"])
 def test_list_build_cells_equals_blocks(gpu_lib, case):
     """The per-cell and the 2x2x2-block list builds give identical rows (same
