@@ -93,3 +93,36 @@ def test_combinations_the_reference_refuses_are_argument_errors():
         p = api.make_params(100, [10.0, 10.0, 10.0], 2.5, **kw)
         assert L.fm_create(C.byref(p), C.byref(h)) == 1, kw
         assert word in api.last_error(), (kw, api.last_error())
+
+
+def test_plain_c_program_compiles_links_and_gets_codes(tmp_path):
+    """A C (not C++) caller: the header compiles under gcc -std=c99, the
+    library links, host-only calls answer, and fm_create reports a missing
+    device or succeeds -- never aborts."""
+    src = tmp_path / "caller.c"
+    src.write_text(r"""
+#include <stdio.h>
+#include "flowmol_b200.h"
+int main(void) {
+    fm_params p = {0};
+    p.np = 2048; p.domain[0] = p.domain[1] = p.domain[2] = 13.68; p.density = 0.8;
+    p.rcutoff = 1.12246204830937; p.delta_rneighbr[0] = p.delta_rneighbr[1] = p.delta_rneighbr[2] = 0.3;
+    p.delta_t = 0.005; p.tplot = 100; p.force_list = FM_FORCE_LIST_HALF;
+    int32_t nc[3]; double cs[3], rn2, rc2, ps;
+    int rc = fm_derive_geometry(&p, nc, cs, &rn2, &rc2, &ps);
+    fm_handle *h = NULL;
+    int rc2_ = fm_create(&p, &h);
+    char msg[256]; fm_last_error(msg, sizeof msg);
+    printf("%d %d %d %d %.17g %d\n", rc, nc[0], nc[1], nc[2], ps, rc2_);
+    if (h) fm_destroy(h);
+    return 0;
+}
+""")
+    exe = tmp_path / "caller"
+    libdir = os.path.join(ROOT, "flowmol_b200")
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(src),
+                    "-L", libdir, "-lflowmol_b200", "-Wl,-rpath," + libdir, "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
+    assert out[:4] == ["0", "9", "9", "9"]
+    assert float(out[4]) == pytest.approx(-1.0, abs=1e-12)  # WCA potshift
+    assert out[5] in ("0", "9")  # FM_OK with a GPU, FM_ERR_NODEVICE without
