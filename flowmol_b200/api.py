@@ -199,6 +199,7 @@ def lib():
             "fm_linklist_deallocateall": [h],
             "fm_sendmols": [h],
             "fm_sort_mols": [h],
+            "fm_rebuild_lists": [h],
             "fm_assign_to_cell": [h],
             "fm_assign_to_neighbourlist": [h],
             "fm_compute_forces": [h],
@@ -446,6 +447,10 @@ class MDSystem:
 
     def assign_to_cell(self):
         check(lib().fm_assign_to_cell(self.h))
+
+    def rebuild_lists(self):
+        """The whole rebuild branch of md_advance_vv in one call."""
+        check(lib().fm_rebuild_lists(self.h))
 
     def assign_to_neighbourlist(self):
         check(lib().fm_assign_to_neighbourlist(self.h))

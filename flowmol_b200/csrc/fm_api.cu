@@ -985,6 +985,17 @@ extern "C" int fm_assign_to_neighbourlist(fm_handle *h)
     return FM_OK;
 }
 
+// The rebuild branch of md_advance_vv (md.f90:150-157) in one call.
+extern "C" int fm_rebuild_lists(fm_handle *h)
+{
+    FM_TRY(fm_linklist_deallocateall(h));
+    FM_TRY(fm_sendmols(h));
+    FM_TRY(fm_sort_mols(h));
+    FM_TRY(fm_assign_to_cell(h));
+    FM_TRY(fm_update_borders(h, 1));
+    return fm_assign_to_neighbourlist(h);
+}
+
 extern "C" int fm_compute_forces(fm_handle *h)
 {
     FM_TRY(ready(h, 1));

@@ -223,6 +223,10 @@ FM_API int fm_assign_to_cell(fm_handle *h);
  * pair set of assign_to_neighbourlist_halfint_opt (660-804) stored in both
  * directions, built from shared-memory cell tiles. */
 FM_API int fm_assign_to_neighbourlist(fm_handle *h);
+/* The rebuild branch of md_advance_vv (md.f90:150-157) as one call:
+ * linklist_deallocateall, sendmols, sort_mols, assign_to_cell,
+ * messenger_updateborders(1), assign_to_neighbourlist. */
+FM_API int fm_rebuild_lists(fm_handle *h);
 /* simulation_compute_forces (simulation_compute_forces.f90:182-275): zeroes
  * and recomputes a; per-molecule PE and virial when mod(iter,tplot) == 0. */
 FM_API int fm_compute_forces(fm_handle *h);

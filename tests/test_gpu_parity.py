@@ -132,6 +132,42 @@ def test_subroutine_path_equals_fused_loop(liquid):
     assert a_sys.counters()["rebuilds"] == b_sys.counters()["rebuilds"]
 
 
+def test_rebuild_lists_equals_the_subroutine_sequence(liquid):
+    """fm_rebuild_lists (the rebuild branch in one call) leaves the same
+    state as the six subroutine mirrors called one by one: 40 iterations of
+    md_advance_vv with either, bit for bit."""
+    r, v, dom = liquid
+    sys_a = gpu_system(r, v, dom, 2.5, tplot=40, density=0.8442)
+    sys_a.setup()
+    sys_b = gpu_system(r, v, dom, 2.5, tplot=40, density=0.8442)
+    sys_b.setup()
+    nreb = 0
+    for _ in range(40):
+        for s, whole in ((sys_a, False), (sys_b, True)):
+            s.iter = s.iter + 1
+            s.simulation_move_particles_vv(1)
+            s.messenger_updateborders(0)
+            if s.simulation_checkrebuild():
+                nreb += whole
+                if whole:
+                    s.rebuild_lists()
+                else:
+                    s.linklist_deallocateall()
+                    s.sendmols()
+                    s.sort_mols()
+                    s.assign_to_cell()
+                    s.messenger_updateborders(1)
+                    s.assign_to_neighbourlist()
+            s.simulation_compute_forces()
+            s.simulation_move_particles_vv(2)
+    assert nreb > 0
+    ra, va, aa, _ = sys_a.download()
+    rb, vb, ab, _ = sys_b.download()
+    assert np.array_equal(ra, rb) and np.array_equal(va, vb) and np.array_equal(aa, ab)
+    sys_a.close()
+    sys_b.close()
+
+
 def test_all_pairs_matches_oracle(gpu_lib):
     r, v, dom = lattice.lj_fluid([3, 3, 3], 0.8, 1.0, 7)
     r = lattice.jitter(r, 0.08, 7, dom)
