@@ -970,7 +970,11 @@ void eng_tick(const EngDev &d, int tpm, const TickExtent &x, cudaStream_t st)
     const int slots = std::min(x.slots, d.nslots);
     const int gm = sgrid(std::min(x.mols, d.mol_cap), 256, 8);
     const int gc = sgrid(std::min(x.cells, d.cell_cap), 256, 8);
-    k_e_decide<<<1, EDEC, 0, st>>>(d);
+    // the slot loops (decision, all-pairs jobs) stop at the extent: every
+    // resident slot lies below it, the ones above are empty
+    EngDev dx = d;
+    dx.nslots = slots;
+    k_e_decide<<<1, EDEC, 0, st>>>(dx);
     k_e_wrap_bin<<<gm, 256, 0, st>>>(d);
     k_e_scan<<<slots, ESCAN, 0, st>>>(d);
     k_e_scatter<<<gm, 256, 0, st>>>(d);
@@ -981,8 +985,8 @@ void eng_tick(const EngDev &d, int tpm, const TickExtent &x, cudaStream_t st)
     k_e_build<<<sgrid(std::min(x.cells, d.cell_cap), NB_WARPS, 6), NB_THREADS, 0, st>>>(d);
     launch_force_any(d, tpm, std::min(x.mols, d.mol_cap), false, st);
     const dim3 gap(std::min(slots, EAP_XBLOCKS), EAP_YBLOCKS);
-    if (d.precision == 0) k_e_force_ap<0><<<gap, EAP_THREADS, 0, st>>>(d);
-    else k_e_force_ap<1><<<gap, EAP_THREADS, 0, st>>>(d);
+    if (d.precision == 0) k_e_force_ap<0><<<gap, EAP_THREADS, 0, st>>>(dx);
+    else k_e_force_ap<1><<<gap, EAP_THREADS, 0, st>>>(dx);
     k_e_thermo<<<dim3(slots, EY), ER, 0, st>>>(d);
     k_e_move_lfv<<<gm, 256, 0, st>>>(d);
     k_e_record<<<dim3(slots, EY), ER, 0, st>>>(d);
