@@ -12,6 +12,10 @@
 // file-scope __device__ array of fixed size instead of memory allocated per
 // handle.  It calls no cudaMalloc, cudaFree or allocating library routine.
 //
+// Positions outside [-L/2, L/2) are wrapped by one period on a private copy
+// before binning (the wrap sendmols applies at a rebuild), so the forces are
+// those fm_setup computes for the wrapped positions.
+//
 // Limits: at most FM_NOALLOC_MAX_MOLECULES molecules and
 // FM_NOALLOC_MAX_CELLS extended cells ((ncells+2)^3); larger inputs are
 // rejected with FM_ERR_ARG.  The array is about 3 MB and stays resident on
@@ -91,14 +95,27 @@ __global__ void k_na_zero(NaGeom g, NaScratch s)
     if (c == 0) *s.status = 0u;
 }
 
+// One period of wrap, as sendmols does at a rebuild (r >= L/2 -> r - L,
+// r < -L/2 -> r + L): the caller's positions are left as they are and the
+// wrapped copy is what gets binned and paired.
+__device__ __forceinline__ double na_wrap(double x, double hd, double L)
+{
+    if (x >= hd) x = __dsub_rn(x, L);
+    if (x < -hd) x = __dadd_rn(x, L);
+    return x;
+}
+
 __global__ void k_na_bin(NaGeom g, NaScratch s, const double *r3)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= g.n) return;
     bool bad = false;
-    int cx = na_bin(r3[3 * (size_t)i], g.hd[0], g.cs[0], g.ne[0], bad);
-    int cy = na_bin(r3[3 * (size_t)i + 1], g.hd[1], g.cs[1], g.ne[1], bad);
-    int cz = na_bin(r3[3 * (size_t)i + 2], g.hd[2], g.cs[2], g.ne[2], bad);
+    const double x = na_wrap(r3[3 * (size_t)i], g.hd[0], g.L[0]);
+    const double y = na_wrap(r3[3 * (size_t)i + 1], g.hd[1], g.L[1]);
+    const double z = na_wrap(r3[3 * (size_t)i + 2], g.hd[2], g.L[2]);
+    int cx = na_bin(x, g.hd[0], g.cs[0], g.ne[0], bad);
+    int cy = na_bin(y, g.hd[1], g.cs[1], g.ne[1], bad);
+    int cz = na_bin(z, g.hd[2], g.cs[2], g.ne[2], bad);
     if (bad) atomicOr(s.status, 1u);
     int c = cx + g.ne[0] * (cy + g.ne[1] * cz);
     s.cell_of[i] = c;
@@ -147,7 +164,9 @@ __global__ void k_na_scatter(NaGeom g, NaScratch s, const double *r3)
     if (i >= g.n) return;
     int c = s.cell_of[i];
     int slot = s.start[c] + atomicAdd(&s.count[c], 1);
-    s.spos[slot] = make_double4(r3[3 * (size_t)i], r3[3 * (size_t)i + 1], r3[3 * (size_t)i + 2], (double)i);
+    s.spos[slot] = make_double4(na_wrap(r3[3 * (size_t)i], g.hd[0], g.L[0]),
+                                na_wrap(r3[3 * (size_t)i + 1], g.hd[1], g.L[1]),
+                                na_wrap(r3[3 * (size_t)i + 2], g.hd[2], g.L[2]), (double)i);
 }
 
 // Deterministic in-cell order (by original index).
@@ -218,13 +237,14 @@ __global__ void k_na_force(NaGeom g, NaScratch s, double *a3, double *pe_out, do
                         pe += 4.0 * (s3 * s3 - s3) - g.potshift;
                         vir += acc * r2;
                     } else {
-                        const float sv = 1.0f / (float)r2, s2 = sv * sv, s4 = s2 * s2;
-                        const float acc = 48.0f * (s4 * s2 * sv - 0.5f * s4);
-                        fx += (double)(acc * (float)dx); fy += (double)(acc * (float)dy);
-                        fz += (double)(acc * (float)dz);
-                        const float s3 = s2 * sv;
-                        pe += (double)(4.0f * (s3 * s3 - s3)) - g.potshift;
-                        vir += (double)(acc * (float)r2);
+                        // the precision form of the main force kernel: FP32 pair
+                        // magnitude, scaled by the FP64 rij, sums in FP64
+                        const float sv = __frcp_rn((float)r2), s2 = sv * sv, s4 = s2 * s2;
+                        const double acc = (double)(48.0f * (s4 * s2 * sv - 0.5f * s4));
+                        fx = fma(acc, dx, fx); fy = fma(acc, dy, fy); fz = fma(acc, dz, fz);
+                        const float s3 = s2 * sv, s6 = s3 * s3;
+                        pe += (double)(4.0f * (s6 - s3)) - g.potshift;
+                        vir += acc * r2;
                     }
                 }
             }
@@ -292,7 +312,10 @@ extern "C" int fm_compute_forces_noalloc(const fm_params *p, int32_t n, const do
 
     // Set-up, once per device, with that device current: the address of the
     // scratch array as the device sees it.  The first call on a device does
-    // this (and should therefore come before any stream capture).
+    // this (and should therefore come before any stream capture).  The address
+    // is kept for the life of the process: the library must not be used on a
+    // device after that device was reset (cudaDeviceReset), which unloads the
+    // array and leaves the kept address stale.
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return na_fail(FM_ERR_NODEVICE, std::string("cudaGetDevice: ") + cudaGetErrorString(e));

@@ -213,7 +213,10 @@ FM_API int fm_sendmols(fm_handle *h);
  * Hilbert curve every sort_freq rebuilds for cache locality.  The device keeps
  * its molecules in cell order at every rebuild anyway, and state transfers use
  * upload order, so the order is invisible to the caller and this call only
- * validates the handle. */
+ * validates the handle.  A run started from an input with SORT_FLAG != 0
+ * therefore matches the reference run with SORT_FLAG 0: the caller's molecule
+ * order never changes, and the FP64 sums are not taken in the order that the
+ * reference's Hilbert renumbering would give (rounding-level differences). */
 FM_API int fm_sort_mols(fm_handle *h);
 /* assign_to_cell (linklist.f90:2645-2679) as a counting sort: histogram,
  * exclusive scan, scatter.  Molecules are also re-ordered by cell on the
@@ -448,11 +451,16 @@ FM_API int fm_get_launch_count(fm_handle *h, int64_t *launches);
  * fixed __device__ array (about 3 MB, resident on every GPU that loads the
  * library until exit) shared by all calls.  d_r, d_a are (3, n) column-major
  * FP64 device arrays; d_potenergymol and d_virialmol (n) may be NULL.  Uses
- * p->domain, rcutoff, delta_rneighbr, precision.  Limits: n <=
- * FM_NOALLOC_MAX_MOLECULES and (ncells+2)^3 <= FM_NOALLOC_MAX_CELLS, else
- * FM_ERR_ARG.  The first call on a device looks up the array's device
- * address, so make it before any stream capture.  Calls that overlap on the
- * GPU race on the shared scratch.  Blocks until the stream has drained. */
+ * p->domain, rcutoff, delta_rneighbr, precision.  Positions outside
+ * [-L/2, L/2) are wrapped by one period on a private copy first (d_r is not
+ * written), so the result is fm_setup's for the wrapped positions.  Limits:
+ * n <= FM_NOALLOC_MAX_MOLECULES and (ncells+2)^3 <= FM_NOALLOC_MAX_CELLS,
+ * else FM_ERR_ARG.  The first call on a device looks up the array's device
+ * address, so make it before any stream capture; the address is kept, so do
+ * not call this on a device after a cudaDeviceReset of that device.  Calls
+ * that overlap on the GPU race on the shared scratch.  Every call reads a
+ * status word back to the host and waits for cuda_stream to drain before it
+ * returns. */
 #define FM_NOALLOC_MAX_MOLECULES 65536
 #define FM_NOALLOC_MAX_CELLS 32768
 FM_API int fm_compute_forces_noalloc(const fm_params *p, int32_t n, const double *d_r, double *d_a,

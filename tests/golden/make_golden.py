@@ -1,7 +1,7 @@
 """Generates the golden fixtures in this folder from the reference checkout.
 
-Run in a container that has the reference at REFERENCE_ROOT (default
-/root/reference).  It reads, never writes, the reference:
+Run with the root of a reference checkout as the first argument (or in the
+REFERENCE_ROOT environment variable).  It reads, never writes, the reference:
   * runs/Intrinsic_Interface/results/simulation_header -- values the
     reference printed for its domain/cell geometry
     (setup_initial_record.f90:700-930);
@@ -23,7 +23,7 @@ import sys
 
 import numpy as np
 
-REF = os.environ.get("REFERENCE_ROOT", "/root/reference")
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REFERENCE_ROOT", "")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
@@ -37,6 +37,8 @@ def parse_header(path):
 
 
 def main():
+    if not REF or not os.path.isdir(REF):
+        sys.exit("usage: make_golden.py <reference checkout root>  (or set REFERENCE_ROOT)")
     hdr = parse_header(os.path.join(REF, "runs/Intrinsic_Interface/results/simulation_header"))
     sys.path.insert(0, os.path.join(REF, "src/reorder_restart"))
     import read_final_state as rfs  # the reference's own reader

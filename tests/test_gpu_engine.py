@@ -14,11 +14,13 @@ from flowmol_b200 import api, couette, lattice
 pytestmark = pytest.mark.gpu
 
 TPM = 4
+TOL32 = 1e-5       # FP32 pair forces: per molecule, relative to max(|F|, F_FLOOR32)
+F_FLOOR32 = 10.0
 
 
-def engine(max_mol=300000, slots=16, ticks=20, **kw):
+def engine(max_mol=300000, slots=16, ticks=20, tpm=TPM, **kw):
     return api.Engine(max_molecules=max_mol, max_cells=400000, max_list_entries=max_mol * 160,
-                      max_slots=slots, threads_per_molecule=TPM, ticks_per_chunk=ticks, **kw)
+                      max_slots=slots, threads_per_molecule=tpm, ticks_per_chunk=ticks, **kw)
 
 
 def lj_replica(nunits, rho, T, seed, jitter=0.03):
@@ -142,3 +144,122 @@ def test_failing_job_does_not_disturb_others(gpu_lib):
     res = {x["job_id"]: x for x in e.results()}
     assert res[jb]["status"] == 4  # FM_ERR_ESCAPE
     assert res[jg]["status"] == 0 and res[jg]["final_iter"] == 40
+
+
+# ---------------------------------------------------------------------------
+# The forms the bench runs: FP32 pair forces at 1 and 2 lanes per molecule.
+# ---------------------------------------------------------------------------
+
+# a sample of the uneven batched replicas: LJ rc 2.5 at densities 0.35-0.9 and
+# temperatures 0.7-1.4; the last box has fewer than 3 cells per axis and runs
+# all pairs with minimum image
+FP32_REPLICAS = [([5, 5, 5], 0.35, 1.4, 71), ([6, 6, 6], 0.9, 0.7, 72), ([7, 6, 5], 0.6, 1.0, 73),
+                 ([3, 3, 3], 0.8, 1.1, 74)]
+
+
+def _force_list(dom):
+    return 0 if min(np.floor(dom / 2.8)) < 3 else 3
+
+
+@pytest.mark.parametrize("tpm", [1, 2])
+def test_fp32_batch_replicas_follow_single_system(gpu_lib, tpm):
+    """FP32 engine replicas against the FP32 single-system path with the same
+    lanes per molecule: the same pair magnitudes summed in FP64, so the
+    trajectories agree to FP64 rounding (1e-9 after 150 steps)."""
+    nsteps = 150
+    e = engine(tpm=tpm, precision=1)
+    ids = []
+    for nu, rho, T, seed in FP32_REPLICAS:
+        r, v, dom = lj_replica(nu, rho, T, seed)
+        fl = _force_list(dom)
+        ids.append((e.submit(api.make_job(len(r), dom, 2.5, nsteps, tplot=50, force_list=fl), r, v), r, v, dom, fl))
+    e.run()
+    assert e.counters()["threads_per_molecule"] == tpm
+    res = {x["job_id"]: x for x in e.results()}
+    assert any(fl == 0 for *_x, fl in ids)
+    for jid, r, v, dom, fl in ids:
+        assert res[jid]["status"] == 0 and res[jid]["final_iter"] == nsteps
+        rg, vg = e.job_state(jid, len(r))
+        p = api.make_params(len(r), dom, 2.5, tplot=50, force_list=fl, threads_per_molecule=tpm, precision=1)
+        s = api.MDSystem(p)
+        s.upload(r, v)
+        s.setup()
+        s.simulation_md(nsteps)
+        rs, vs, _, _ = s.download()
+        np.testing.assert_allclose(rg, rs, rtol=0, atol=1e-9)
+        np.testing.assert_allclose(vg, vs, rtol=0, atol=1e-9)
+        last = s.records()[-1]
+        assert res[jid]["last"]["totenergy"] == pytest.approx(last["totenergy"], rel=1e-11)
+        s.close()
+
+
+def _min_image(d, dom):
+    return d - dom * np.round(d / dom)
+
+
+@pytest.mark.parametrize("tpm", [1, 2])
+def test_fp32_batch_forces_and_records_against_oracle(gpu_lib, tpm):
+    """FP32 engine replicas against the FP64 oracle directly.
+
+    Forces of iteration 0: a one-step velocity-Verlet job leaves
+    r1 = r0 + dt v0 + (dt^2/2) a0, so a0 = (r1 - r0 - dt v0) / (dt^2/2) to
+    ~1e-9 absolute (the rounding of r1, ~2e-15, over dt^2/2 = 1.25e-5) --
+    far below the FP32 tolerance 1e-5 * max(|F|, 10).  Records after 100
+    steps: kinetic, potential and total energy per molecule within 1e-5
+    relative and the pressure within 1e-4 absolute of the oracle's (FP32
+    forces move the trajectory by ~1e-6 over 100 steps)."""
+    dt = 0.005
+    for nu, rho, T, seed in FP32_REPLICAS:
+        r, v, dom = lj_replica(nu, rho, T, seed)
+        fl = _force_list(dom)
+        e = engine(tpm=tpm, precision=1)
+        j1 = e.submit(api.make_job(len(r), dom, 2.5, 1, tplot=1000, force_list=fl), r, v)
+        j100 = e.submit(api.make_job(len(r), dom, 2.5, 100, tplot=50, force_list=fl), r, v)
+        e.run()
+        res = {x["job_id"]: x for x in e.results()}
+        assert res[j1]["status"] == 0 and res[j100]["status"] == 0
+        r1, _ = e.job_state(j1, len(r))
+        a0 = _min_image(r1 - r - dt * v, dom) / (0.5 * dt * dt)
+        o = O.Oracle(r, v, dom, 2.5, tplot=50, force_list=fl)
+        o.setup()
+        err = rel_err_rows(a0, o.a, F_FLOOR32)
+        assert err.max() <= TOL32, (nu, rho, err.max())
+        rec = o.run_vv(100)
+        last_o = rec[-1]
+        last_g = res[j100]["last"]
+        assert last_g["iter"] == int(last_o[0]) == 100
+        m = o.macro()
+        for k in ("kinenergy", "potenergy", "totenergy"):
+            assert last_g[k] == pytest.approx(m[k], rel=TOL32, abs=TOL32), (k, nu, rho)
+        assert last_g["pressure"] == pytest.approx(m["pressure"], abs=1e-4)
+        e.close()
+
+
+def rel_err_rows(x, ref, floor):
+    d = np.linalg.norm(x - ref, axis=-1)
+    return d / np.maximum(np.linalg.norm(ref, axis=-1), floor)
+
+
+@pytest.mark.parametrize("tpm", [1, 2])
+def test_fp32_couette_job_follows_oracle(gpu_lib, tpm):
+    """One served Couette job (WCA, tethered sliding walls, thermostatted wall
+    regions, leap-frog) in FP32 against the FP64 oracle over 40 steps: the
+    time-averaged pressure tensor within 1e-5 relative (1e-5 absolute for the
+    small off-diagonal terms) and positions within 2e-6."""
+    job, r, v, tag, rt, sv, dom = couette_inputs(500, 1.0, 21)
+    nsteps = 40
+    e = engine(tpm=tpm, precision=1)
+    jid = e.submit(api.make_job(nsteps=nsteps, **job), r, v, tag, rt, sv)
+    e.run()
+    res = e.results()[0]
+    assert res["status"] == 0 and res["nsamples"] == nsteps // 10
+    rg, vg = e.job_state(jid, len(r))
+    o = O.Oracle(r, v, dom, couette.WCA_RC, tplot=10, integration_algorithm=0)
+    o.set_tags(6, tag, rt, sv, (0.0, 5000.0, 5.0e6), 2, (1.0, 1.0))
+    o.set_pressure(1)
+    o.setup()
+    o.run_lfv(nsteps)
+    P, ns = o.pressure_average()
+    assert ns == res["nsamples"]
+    np.testing.assert_allclose(res["ptensor"], P, rtol=1e-5, atol=1e-5)
+    np.testing.assert_allclose(rg, o.r, rtol=0, atol=2e-6)
