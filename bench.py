@@ -162,11 +162,11 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def run_form(api, torch, r, v, dom, precision, steps, warmup, dev, timing_pass=True, tpm=0):
+def run_form(api, torch, r, v, dom, precision, steps, warmup, dev, timing_pass=True, tpm=0, force_path=0):
     """Device-resident throughput of one precision form."""
     stream = torch.cuda.Stream(device=dev)
     p = api.make_params(len(r), dom, RC, (SKIN,) * 3, DT, TPLOT, density=DENSITY, precision=precision,
-                        threads_per_molecule=tpm)
+                        threads_per_molecule=tpm, force_path=force_path)
     s = api.MDSystem(p, stream=stream)
     s.upload(r, v)
     s.setup()
@@ -197,11 +197,12 @@ def run_form(api, torch, r, v, dom, precision, steps, warmup, dev, timing_pass=T
     out["records"] = s.records()
     out["capacity"] = s.counters()["nlist_capacity"]
     out["tpm"] = s.threads_per_molecule
+    out["force_path"] = "tiles" if s.force_path()[0] == api.FORCE_PATH_TILES else "gather"
     s.close()
     return out
 
 
-def run_e2e(api, torch, r, v, dom, precision, steps, dev):
+def run_e2e(api, torch, r, v, dom, precision, steps, dev, tpm=0, force_path=0):
     """Through the public API with host buffers: pinned upload, setup, steps,
     download of the final state and the records, all inside the timed region."""
     n = len(r)
@@ -210,7 +211,8 @@ def run_e2e(api, torch, r, v, dom, precision, steps, dev):
     ro = torch.empty((n, 3), dtype=torch.float64).pin_memory()
     vo = torch.empty((n, 3), dtype=torch.float64).pin_memory()
     ao = torch.empty((n, 3), dtype=torch.float64).pin_memory()
-    p = api.make_params(n, dom, RC, (SKIN,) * 3, DT, TPLOT, density=DENSITY, precision=precision)
+    p = api.make_params(n, dom, RC, (SKIN,) * 3, DT, TPLOT, density=DENSITY, precision=precision,
+                        threads_per_molecule=tpm, force_path=force_path)
     s = api.MDSystem(p)
     torch.cuda.synchronize(dev)
     import ctypes as C
@@ -308,9 +310,14 @@ def batch_replicas(nrep=256, seed=0x466D6F6C + 4):
 
 
 def run_batched(api, torch, dev, nsteps, nrep=256):
-    """All replicas in one engine (graph-captured ticks) vs the plain
-    single-system form run one replica at a time (bounded to plain_steps
-    per replica; throughput is per-step so the rates compare)."""
+    """All replicas in one engine (graph-captured ticks, admission and setup
+    inside the timed region) against the plain single-system form run one
+    replica at a time.  The plain form is measured per replica as its setup
+    (upload, binning, list, first forces) plus plain_steps steps timed apart
+    with CUDA events, and projected to the same nsteps the batch runs:
+    t = t_setup + nsteps * t_step.  Both sides therefore pay one setup per
+    replica over the same number of steps; the steps-only plain rate is
+    reported beside it."""
     reps = batch_replicas(nrep)
     tot = sum(len(x[0]) for x in reps)
     e = api.Engine(max_molecules=tot + 1024, max_cells=2_000_000, max_list_entries=(tot + 1024) * 160,
@@ -325,24 +332,36 @@ def run_batched(api, torch, dev, nsteps, nrep=256):
     c = e.counters()
     bad = [x for x in res if x["status"] != 0]
     e.close()
-    plain_steps = min(nsteps, 100)
-    t_plain = 0.0
+    plain_steps = min(nsteps, 200)
+    t_setup = t_steps = 0.0  # summed over the replicas; t_steps for plain_steps each
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    stream = torch.cuda.Stream(device=dev)
     for r, v, dom, rho, fl in reps:
         p = api.make_params(len(r), dom, RC, (SKIN,) * 3, DT, TPLOT, density=rho, force_list=fl,
                             precision=api.PRECISION_FP32)
-        s = api.MDSystem(p)
+        s = api.MDSystem(p, stream=stream)
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
         s.upload(r, v)
         s.setup()
-        s.simulation_md(plain_steps, blocking=True)
-        t_plain += time.perf_counter() - t0
+        s.sync()
+        t_setup += time.perf_counter() - t0
+        ev0.record(stream)
+        s.simulation_md(plain_steps, blocking=False)
+        ev1.record(stream)
+        ev1.synchronize()
+        s.sync()
+        t_steps += 1e-3 * ev0.elapsed_time(ev1)
         s.close()
     v_batch = tot * nsteps / t_batch
-    v_plain = tot * plain_steps / t_plain
+    v_plain = tot * nsteps / (t_setup + t_steps * nsteps / plain_steps)
+    v_plain_steps = tot * plain_steps / t_steps
     return {"value": v_batch, "unit": UNIT, "replicas": nrep, "molecules": tot, "steps_each": nsteps,
-            "seconds": t_batch, "plain_one_at_a_time": v_plain, "plain_steps_each": plain_steps,
-            "ratio_vs_plain": v_batch / v_plain, "failed": len(bad), "threads_per_molecule": c["threads_per_molecule"],
+            "seconds": t_batch, "plain_one_at_a_time": v_plain, "plain_steps_only": v_plain_steps,
+            "plain_setup_seconds": t_setup, "plain_steps_timed_each": plain_steps,
+            "ratio_vs_plain": v_batch / v_plain, "ratio_vs_plain_steps_only": v_batch / v_plain_steps,
+            "failed": len(bad), "threads_per_molecule": c["threads_per_molecule"],
             "gpu_launches": c["launches"],
             "workload": "256 periodic LJ replicas, N log-uniform 500-32000 (4 n^3 FCC), rho U(0.3,0.9), "
                         "T U(0.7,1.5), rc 2.5, skin 0.3, dt 0.005, VV, FP32 forces; boxes < 3 cells: all pairs"}
@@ -418,7 +437,21 @@ def run_served(api, torch, dev, njobs, seed=0x466D6F6C + 5):
     bad = [d for d in done if d["status"] != 0]
     c = e.counters()
     e.close()
+    # the same kind of jobs run one at a time (an engine with one slot: a job
+    # is admitted when the previous one has finished), on a sample of 64
+    sample = [make(200000 + k, np.random.Generator(np.random.Philox(seed + 2 + k))) for k in range(64)]
+    e1 = api.Engine(max_molecules=200_000, max_cells=400_000, max_list_entries=200_000 * 48, max_slots=1,
+                    precision=api.PRECISION_FP32, ticks_per_chunk=20, keep_states=False)
+    ts = time.perf_counter()
+    for j in sample:
+        e1.submit(*j)
+        e1.run()
+        e1.results()
+    t_one = time.perf_counter() - ts
+    e1.close()
+    v_one = sum(j[0].np * j[0].nsteps for j in sample) / t_one
     return {"value": work / t_total, "unit": UNIT, "jobs": njobs, "molecule_steps": work, "seconds": t_total,
+            "one_at_a_time": v_one, "one_at_a_time_jobs": len(sample), "ratio_vs_one_at_a_time": work / t_total / v_one,
             "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
             "arrival_rate_per_s": lam, "probe_service_rate": rate_work, "gpu_busy_frac": busy / t_total,
             "failed": len(bad), "threads_per_molecule": c["threads_per_molecule"],
@@ -488,6 +521,8 @@ def main():
                     help="NVE drift run of the 1M fluid per precision form (0: skip)")
     ap.add_argument("--tpm", type=int, default=0,
                     help="force-kernel lanes per molecule (0: the autotuner's choice)")
+    ap.add_argument("--force-path", type=int, default=0, choices=[0, 1, 2],
+                    help="force kernel of the 1M forms: 0 automatic, 1 one gather per list entry, 2 tiles")
     ap.add_argument("--profile-case", choices=["fp32", "fp64", "batched", "fene", "served"], default=None,
                     help="profiling workload, no timing: setup + 10 fused steps of the 1M system "
                          "(fp32, fp64) or of the FENE melt (fene), the batched replicas for "
@@ -558,7 +593,7 @@ def main():
         r, v, dom = make_state()
         prec = api.PRECISION_FP32 if args.profile_case == "fp32" else api.PRECISION_FP64
         p = api.make_params(len(r), dom, RC, (SKIN,) * 3, DT, TPLOT, density=DENSITY, precision=prec,
-                            threads_per_molecule=args.tpm)
+                            threads_per_molecule=args.tpm, force_path=args.force_path)
         s = api.MDSystem(p)
         s.upload(r, v)
         s.setup()
@@ -579,13 +614,16 @@ def main():
     max_over_ranks = ranks.max
 
     barrier()
-    f32 = run_form(api, torch, r, v, dom, api.PRECISION_FP32, args.steps, args.warmup, dev, tpm=args.tpm)
+    f32 = run_form(api, torch, r, v, dom, api.PRECISION_FP32, args.steps, args.warmup, dev, tpm=args.tpm,
+                   force_path=args.force_path)
     ms32 = max_over_ranks(f32["ms"])
     barrier()
-    f64 = run_form(api, torch, r, v, dom, api.PRECISION_FP64, args.steps, args.warmup, dev, tpm=args.tpm)
+    f64 = run_form(api, torch, r, v, dom, api.PRECISION_FP64, args.steps, args.warmup, dev, tpm=args.tpm,
+                   force_path=args.force_path)
     ms64 = max_over_ranks(f64["ms"])
     barrier()
-    e2e = None if args.no_e2e else run_e2e(api, torch, r, v, dom, api.PRECISION_FP32, args.steps, dev)
+    e2e = None if args.no_e2e else run_e2e(api, torch, r, v, dom, api.PRECISION_FP32, args.steps, dev,
+                                           tpm=args.tpm, force_path=args.force_path)
     if e2e is not None:
         e2e["value"] = world * n * args.steps / max_over_ranks(e2e["seconds"])
     barrier()
@@ -626,9 +664,11 @@ def main():
                        "rebuilds_in_timed_region": f32["rebuilds"], "parallelism": f"replicas x{world}"},
             "forms": {
                 "fp32_forces": {"value": value, "ms_per_step": ms32 / args.steps,
-                                "force_kernel_ms": f32["force_ms_avg"], "threads_per_molecule": f32["tpm"]},
+                                "force_kernel_ms": f32["force_ms_avg"], "threads_per_molecule": f32["tpm"],
+                                "force_path": f32["force_path"]},
                 "fp64_plain": {"value": world * n * args.steps / (ms64 * 1e-3), "ms_per_step": ms64 / args.steps,
-                               "force_kernel_ms": f64["force_ms_avg"], "threads_per_molecule": f64["tpm"]},
+                               "force_kernel_ms": f64["force_ms_avg"], "threads_per_molecule": f64["tpm"],
+                               "force_path": f64["force_path"]},
             },
             "roofline": {"bound": "hbm", "kernel": "k_force (fused forces + move(2) + next move(1))",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

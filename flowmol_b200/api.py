@@ -51,6 +51,7 @@ class FmParams(C.Structure):
         ("integration_algorithm", C.c_int32),
         ("list_build", C.c_int32),
         ("solvent_flag", C.c_int32),
+        ("force_path", C.c_int32),
         ("eps_pp", C.c_double),
         ("eps_ps", C.c_double),
         ("eps_ss", C.c_double),
@@ -85,6 +86,7 @@ class FmMieTables(C.Structure):
 
 
 LIST_BUILD_AUTO, LIST_BUILD_CELLS, LIST_BUILD_BLOCKS = 0, 1, 2
+FORCE_PATH_AUTO, FORCE_PATH_GATHER, FORCE_PATH_TILES = 0, 1, 2
 MIE_TABLE_KEYS = ("epsilon", "lambdar", "lambdaa", "C", "alpha", "potshift", "k_harmonic", "r0")
 
 
@@ -216,6 +218,7 @@ def lib():
             "fm_set_pressure_outflag": [h, C.c_int32],
             "fm_get_pressure_tensor": [h, P(C.c_double), P(C.c_int32), C.c_int32],
             "fm_get_threads_per_molecule": [h, P(C.c_int32)],
+            "fm_get_force_path": [h, P(C.c_int32), P(C.c_int32)],
             "fm_last_error": [C.c_char_p, C.c_int32],
             "fm_engine_create": [P(FmEngineParams), P(h)],
             "fm_engine_destroy": [h],
@@ -276,7 +279,7 @@ def make_params(np_, domain, rcutoff, delta_rneighbr=(0.3, 0.3, 0.3), delta_t=0.
                 density=None, initialstep=0, simtime=0.0, force_list=FORCE_LIST_HALF, potential_flag=0,
                 rebuild_criteria=0, fixed_rebuild=1, sLRC_flag=0, precision=PRECISION_FP64, k_c=30.0,
                 R_0=1.5, nlist_capacity=0, threads_per_molecule=0, integration_algorithm=1,
-                list_build=0, solvent_flag=0, eps=(1.0, 1.0, 1.0)) -> FmParams:
+                list_build=0, solvent_flag=0, eps=(1.0, 1.0, 1.0), force_path=0) -> FmParams:
     """`eps` = (eps_pp, eps_ps, eps_ss), the SOLVENT_INFO well depths used with
     solvent_flag 1."""
     p = FmParams()
@@ -303,6 +306,7 @@ def make_params(np_, domain, rcutoff, delta_rneighbr=(0.3, 0.3, 0.3), delta_t=0.
     p.integration_algorithm = int(integration_algorithm)
     p.list_build = int(list_build)
     p.solvent_flag = int(solvent_flag)
+    p.force_path = int(force_path)
     p.eps_pp, p.eps_ps, p.eps_ss = (float(x) for x in eps)
     return p
 
@@ -539,6 +543,12 @@ class MDSystem:
         t = C.c_int32()
         check(lib().fm_get_threads_per_molecule(self.h, C.byref(t)))
         return t.value
+
+    def force_path(self):
+        """(FORCE_PATH_GATHER or FORCE_PATH_TILES, staged capacity per block)."""
+        p = C.c_int32(); cap = C.c_int32()
+        check(lib().fm_get_force_path(self.h, C.byref(p), C.byref(cap)))
+        return p.value, cap.value
 
     def counters(self):
         rb = C.c_int64(); cap = C.c_int32(); mx = C.c_int32()

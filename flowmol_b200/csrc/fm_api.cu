@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "fm_common.cuh"
+#include "fm_tile.cuh"
 #include "flowmol_b200.h"
 
 using fm::FmDev;
@@ -164,7 +165,8 @@ static void release(fm_handle *h)
                     d.tax, d.tay, d.taz, d.cell_of, d.cell_count, d.cell_start, d.perm, d.tile_sum, d.nbr, d.nnbr,
                     d.pe, d.vir, d.partial, d.rec, d.sc, h->tpos, h->tuidx, h->glob, h->stage3, d.chain,
                     d.subchain, d.bflag, d.tchain, d.tsubchain, d.tbflag, d.bnd, d.nbond,
-                    (void *)d.mie_pair, (void *)d.mie_mass, (void *)d.mie_type_up, d.rdx, d.rdy, d.rdz, d.rf6};
+                    (void *)d.mie_pair, (void *)d.mie_mass, (void *)d.mie_type_up, d.rdx, d.rdy, d.rdz, d.rf6,
+                    d.blk_off, d.nbr16};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     d = FmDev{};
@@ -197,6 +199,48 @@ static int alloc_nlist(fm_handle *h, int maxn)
     d.maxn = maxn;
     FM_TRY(dalloc(&d.nbr, fm::nb_rows(d.n) * (size_t)maxn));
     return FM_OK;
+}
+
+// Rows of the tiled path: a multiple of 8 T entries (one 16-byte load per
+// lane per chunk).
+static int alloc_nlist16(fm_handle *h, int maxn)
+{
+    FmDev &d = h->d;
+    maxn = round_up(std::max(maxn, 8 * d.tile_T), 8 * d.tile_T);
+    if (d.nbr16) cudaFree(d.nbr16);
+    d.nbr16 = nullptr;
+    d.maxn16 = maxn;
+    FM_TRY(dalloc(&d.nbr16, (size_t)d.n * (size_t)maxn));
+    return FM_OK;
+}
+
+// Leaves the tiled path for the per-entry gather path (a block's staged
+// neighbourhood would no longer fit in shared memory): generic rows of the
+// same capacity; the caller builds them.
+static int leave_tiles(fm_handle *h)
+{
+    FmDev &d = h->d;
+    const int maxn = d.maxn16;
+    if (d.nbr16) cudaFree(d.nbr16);
+    d.nbr16 = nullptr;
+    d.tile = 0;
+    FM_TRY(alloc_nlist(h, maxn));
+    return FM_OK;
+}
+
+// Record partial rows the force kernel writes: one per CTA, or one per block
+// on the tiled path.
+static int force_rows(const fm_handle *h)
+{
+    return h->d.tile ? h->d.tile_nblk : fm::force_blocks(h->d.n, h->tpm);
+}
+
+// The list build of a rebuild: on the tiled path the blocks' staging table
+// first, then the rows.
+static void queue_build(fm_handle *h, int gated, int iter)
+{
+    if (h->d.tile) { fm::launch_blk_seg(h->d, gated, iter, h->st); h->launches += 1; }
+    fm::launch_build_nlist(h->d, gated, iter, h->st);
 }
 
 extern "C" int fm_create(const fm_params *p, fm_handle **out)
@@ -281,6 +325,39 @@ extern "C" int fm_create(const fm_params *p, fm_handle **out)
                      : p->list_build == FM_LIST_BUILD_CELLS ? 0 : (per_cell < 8.0 ? 1 : 0);
     int tpm = pick_tpm(*p, expected);
     if (tpm < 0) { delete h; return fail(FM_ERR_ARG, "threads_per_molecule must be 0, 1, 2, 4, 8 or 16"); }
+    if (p->force_path != FM_FORCE_PATH_AUTO && p->force_path != FM_FORCE_PATH_GATHER &&
+        p->force_path != FM_FORCE_PATH_TILES) {
+        delete h;
+        return fail(FM_ERR_ARG, "force_path must be FM_FORCE_PATH_AUTO, _GATHER or _TILES");
+    }
+    // tiled force path: dense systems (the list build's own choice of one warp
+    // per cell), lanes per molecule 4 or 8; a staged neighbourhood of 64 cells
+    // must fit in shared memory
+    {
+        const bool tpm_ok = p->threads_per_molecule == 0 || p->threads_per_molecule == 4 ||
+                            p->threads_per_molecule == 8;
+        const double est_union = 64.0 * std::max(per_cell, 0.25);
+        const bool fits = 1.25 * est_union + 64.0 < (double)fm::tile_ucap_limit(3);
+        // automatic keeps the gather kernel: on the 1M LJ liquid the tiled kernel
+        // measured 0.29-0.30 ms against 0.28 ms (its shared-memory reads are
+        // bank-conflicted and the neighbourhood is staged eight times); the
+        // tiled rows take half the list memory
+        const bool want = p->force_list != 0 && tpm_ok && fits && p->force_path == FM_FORCE_PATH_TILES;
+        if (p->force_path == FM_FORCE_PATH_TILES && !want) {
+            delete h;
+            return fail(FM_ERR_ARG, "force_path TILES needs a neighbour list, threads_per_molecule 0, 4 or 8, "
+                                    "and a 4x4x4-cell neighbourhood that fits in shared memory");
+        }
+        if (want) {
+            d.tile = 1;
+            d.tile_T = p->threads_per_molecule == 4 ? 4 : p->threads_per_molecule == 8 ? 8 : (expected > 24 ? 8 : 4);
+            d.tile_R = 3;  // (4 once Mie types or Soddemann bead flags are set; fixed at fm_setup)
+            for (int k = 0; k < 3; k++) d.tile_nb[k] = (d.ne[k] + 1) / 2;
+            d.tile_nblk = d.tile_nb[0] * d.tile_nb[1] * d.tile_nb[2];
+            d.tile_ucap = std::min(round_up((int)std::ceil(1.25 * est_union) + 64, 32), fm::tile_ucap_limit(3));
+            tpm = d.tile_T;
+        }
+    }
     h->tpm = tpm;
     h->expected_nbr = (int)std::lround(expected);
     int maxn = p->nlist_capacity > 0 ? p->nlist_capacity : round_up((int)std::ceil(1.3 * expected) + 16, 8);
@@ -307,19 +384,21 @@ extern "C" int fm_create(const fm_params *p, fm_handle **out)
         FM_ALLOC(d.bnd, 4 * n) FM_ALLOC(d.nbond, n)
     }
     int nb = std::max(std::max(fm::force_blocks(d.n, 16), fm::all_pairs_blocks(d.n)), fm::macro_blocks(d.n));
+    nb = std::max(nb, d.tile_nblk);
+    if (d.tile) { FM_ALLOC(d.blk_off, (size_t)d.tile_nblk * fm::TILE_NSEGP) }
     FM_ALLOC(d.partial, (size_t)nb * fm::RS_N)
     d.rec_cap = 4096;
     FM_ALLOC(d.rec, d.rec_cap)
     FM_ALLOC(d.sc, 1)
 #undef FM_ALLOC
-    if (rc == FM_OK && p->force_list != 0) rc = alloc_nlist(h, maxn);
+    if (rc == FM_OK && p->force_list != 0) rc = d.tile ? alloc_nlist16(h, maxn) : alloc_nlist(h, maxn);
     if (rc != FM_OK) {
         std::string msg = g_last_error;
         release(h);
         delete h;
         return fail(rc, msg);
     }
-    d.nblocks_force = fm::force_blocks(d.n, h->tpm);
+    d.nblocks_force = force_rows(h);
     cudaMemset(d.cell_count, 0, sizeof(int32_t) * (size_t)d.ncell);
     cudaMemset(d.cell_start, 0, sizeof(int32_t) * (size_t)(d.ncell + 1));
     cudaMemset(d.nnbr, 0, sizeof(int32_t) * n);
@@ -368,7 +447,7 @@ static int begin_state(fm_handle *h, int32_t n)
     h->list_valid = false;
     h->iter = h->p.initialstep;
     h->simtime = h->p.simtime;
-    h->d.nblocks_force = fm::force_blocks(h->d.n, h->tpm);
+    h->d.nblocks_force = force_rows(h);
     fm::launch_reset_scalars(h->d, h->st);
     FM_CUDA(cudaMemsetAsync(h->d.cell_count, 0, sizeof(int32_t) * (size_t)h->d.ncell, h->st));
     return FM_OK;
@@ -577,28 +656,57 @@ static int status_error(fm_handle *h, const fm::FmScalars &s)
         h->stage = 3;
         return fail(FM_ERR_BOND, buf);
     }
+    if (s.status & fm::ST_TILE) {
+        std::snprintf(buf, sizeof buf, "staged neighbourhood of %d molecules above the capacity %d at iteration %d",
+                      s.umax, h->d.tile_ucap, s.fail_iter);
+        h->stage = 3;
+        return fail(FM_ERR_NLIST, buf);
+    }
     if (s.status & fm::ST_NLIST) {
         std::snprintf(buf, sizeof buf, "neighbour list overflow at iteration %d (%d > %d)", s.fail_iter, s.max_nbr,
-                      h->d.maxn);
+                      h->d.tile ? h->d.maxn16 : h->d.maxn);
         h->stage = 3;
         return fail(FM_ERR_NLIST, buf);
     }
     return FM_OK;
 }
 
-// Grows the neighbour list to fit the largest list seen, clears the overflow
-// bit and rebuilds the list from the (frozen) current cells.
+// Status bits a larger capacity cures: the list (ST_NLIST) and, on the tiled
+// path, the staged neighbourhood (ST_TILE).
+static constexpr uint32_t GROWABLE = fm::ST_NLIST | fm::ST_TILE;
+static bool growable(const fm::FmScalars &s)
+{
+    return (s.status & GROWABLE) && !(s.status & (fm::ST_FATAL & ~GROWABLE));
+}
+
+// Grows the neighbour list to fit the largest list seen (and, on the tiled
+// path, the staging to fit the largest neighbourhood, leaving the tiled path
+// when that no longer fits in shared memory), clears the overflow bits and
+// rebuilds the list from the (frozen) current cells.
 static int grow_nlist(fm_handle *h, const fm::FmScalars &s, int iter)
 {
-    int want = round_up((int)std::ceil(1.2 * s.max_nbr) + 8, 8);
-    if ((size_t)want * (size_t)h->d.n > ((size_t)1 << 34)) return status_error(h, s);
-    FM_TRY(alloc_nlist(h, want));
+    FmDev &d = h->d;
+    if (d.tile && (s.status & fm::ST_TILE)) {
+        const int want_u = round_up((int)std::ceil(1.25 * s.umax) + 32, 32);
+        if (want_u > fm::tile_ucap_limit(d.tile_R)) {
+            FM_TRY(leave_tiles(h));
+            d.nblocks_force = force_rows(h);
+        } else {
+            d.tile_ucap = want_u;
+        }
+    }
+    if (s.status & fm::ST_NLIST) {
+        const int cur = d.tile ? d.maxn16 : d.maxn;
+        const int want = std::max(round_up((int)std::ceil(1.2 * s.max_nbr) + 8, 8), cur);
+        if ((size_t)want * (size_t)d.n > ((size_t)1 << 34)) return status_error(h, s);
+        FM_TRY(d.tile ? alloc_nlist16(h, want) : alloc_nlist(h, want));
+    }
     fm::FmScalars t = s;
     t.status = 0u;
     t.fail_iter = -1;
     t.max_nbr = 0;
-    FM_CUDA(cudaMemcpyAsync(h->d.sc, &t, sizeof t, cudaMemcpyHostToDevice, h->st));
-    fm::launch_build_nlist(h->d, 0, iter, h->st);
+    FM_CUDA(cudaMemcpyAsync(d.sc, &t, sizeof t, cudaMemcpyHostToDevice, h->st));
+    queue_build(h, 0, iter);
     FM_CUDA(cudaGetLastError());
     return FM_OK;
 }
@@ -652,7 +760,7 @@ static void queue_record(fm_handle *h, int iter, double simtime, bool pressure_s
 {
     FmDev d = h->d;
     if (!pressure_sample) d.pressure = 0;
-    d.nblocks_force = h->p.force_list == 0 ? fm::all_pairs_blocks(d.n) : fm::force_blocks(d.n, h->tpm);
+    d.nblocks_force = h->p.force_list == 0 ? fm::all_pairs_blocks(d.n) : force_rows(h);
     fm::launch_record(d, iter, simtime, h->st);
     h->launches += 1;
 }
@@ -671,14 +779,15 @@ static std::map<std::tuple<int, int, int>, int> g_tune_cache;
 
 static int autotune_tpm(fm_handle *h)
 {
-    if (h->p.threads_per_molecule > 0 || h->p.force_list == 0) return FM_OK;
+    // the tiled path's lanes per molecule are fixed by its row layout
+    if (h->p.threads_per_molecule > 0 || h->p.force_list == 0 || h->d.tile) return FM_OK;
     const auto key = std::make_tuple(h->d.n, h->expected_nbr, h->d.precision);
     {
         std::lock_guard<std::mutex> lk(g_tune_mutex);
         auto it = g_tune_cache.find(key);
         if (it != g_tune_cache.end()) {
             h->tpm = it->second;
-            h->d.nblocks_force = fm::force_blocks(h->d.n, h->tpm);
+            h->d.nblocks_force = force_rows(h);
             return FM_OK;
         }
     }
@@ -708,24 +817,35 @@ static int autotune_tpm(fm_handle *h)
     cudaEventDestroy(e1);
     FM_CUDA(cudaGetLastError());
     h->tpm = best_tpm;
-    h->d.nblocks_force = fm::force_blocks(h->d.n, h->tpm);
+    h->d.nblocks_force = force_rows(h);
     std::lock_guard<std::mutex> lk(g_tune_mutex);
     g_tune_cache[key] = best_tpm;
     return FM_OK;
+}
+
+// Staged rows of the tiled path: w (Mie type, Soddemann bead flag) is staged
+// when the potential reads it.
+static void set_tile_rows(fm_handle *h)
+{
+    FmDev &d = h->d;
+    if (!d.tile) return;
+    d.tile_R = (d.mie || d.solvent) ? 4 : 3;
+    if (d.tile_ucap > fm::tile_ucap_limit(d.tile_R)) d.tile_ucap = fm::tile_ucap_limit(d.tile_R);
 }
 
 extern "C" int fm_setup(fm_handle *h)
 {
     if (!h) return fail(FM_ERR_ARG, "null handle");
     if (h->stage < 1) return fail(FM_ERR_STATE, "fm_setup before fm_upload_state");
+    set_tile_rows(h);
     if (h->p.force_list != 0) {
         queue_cells(h, 0, 0);
-        fm::launch_build_nlist(h->d, 0, h->iter, h->st);
+        queue_build(h, 0, h->iter);
     }
     FM_CUDA(cudaGetLastError());
     fm::FmScalars s;
     FM_TRY(read_scalars(h, &s));
-    if (s.status & fm::ST_NLIST && !(s.status & (fm::ST_FATAL & ~fm::ST_NLIST))) {
+    for (int attempt = 0; attempt < 4 && growable(s); attempt++) {
         FM_TRY(grow_nlist(h, s, h->iter));
         FM_TRY(read_scalars(h, &s));
     }
@@ -759,7 +879,7 @@ static void queue_rebuild_check(fm_handle *h, int it, int flip)
     queue_decide(h, it, flip);
     if (p.force_list != 0) {
         queue_cells(h, 1, 1);
-        fm::launch_build_nlist(h->d, 1, it, h->st);
+        queue_build(h, 1, it);
         h->launches += 1;
     } else {
         fm::launch_wrap_bin(h->d, 1, 0, 1, it, h->st);
@@ -800,7 +920,7 @@ static int queue_steps(fm_handle *h, int first, int nsteps, int phase, const std
             queue_decide(h, it, fused_move1 ? 1 : 0);
             if (p.force_list != 0) {
                 queue_cells(h, 1, 1);
-                fm::launch_build_nlist(h->d, 1, it, h->st);
+                queue_build(h, 1, it);
                 h->launches += 1;
             } else {
                 fm::launch_wrap_bin(h->d, 1, 0, 1, it, h->st);
@@ -829,7 +949,7 @@ static int finish_range(fm_handle *h)
             h->q.active = false;
             return FM_OK;
         }
-        if (!h->q.active || (s.status & (fm::ST_FATAL & ~fm::ST_NLIST))) {
+        if (!h->q.active || (s.status & (fm::ST_FATAL & ~GROWABLE))) {
             h->q.active = false;
             return status_error(h, s);
         }
@@ -972,11 +1092,12 @@ extern "C" int fm_assign_to_neighbourlist(fm_handle *h)
     FM_TRY(ready(h, 1));
     if (h->p.force_list == 0) return FM_OK;
     if (!h->cells_valid) return fail(FM_ERR_STATE, "assign_to_neighbourlist needs assign_to_cell first");
-    fm::launch_build_nlist(h->d, 0, h->iter, h->st);
+    set_tile_rows(h);
+    queue_build(h, 0, h->iter);
     FM_CUDA(cudaGetLastError());
     fm::FmScalars s;
     FM_TRY(read_scalars(h, &s));
-    if ((s.status & fm::ST_NLIST) && !(s.status & (fm::ST_FATAL & ~fm::ST_NLIST))) {
+    for (int attempt = 0; attempt < 4 && growable(s); attempt++) {
         FM_TRY(grow_nlist(h, s, h->iter));
         FM_TRY(read_scalars(h, &s));
     }
@@ -1083,6 +1204,22 @@ extern "C" int fm_get_per_molecule(fm_handle *h, double *pe, double *vir)
     return FM_OK;
 }
 
+// The current rows in the generic int32 layout: the list itself, or on the
+// tiled path a temporary decoded copy (the caller frees it when it differs
+// from d.nbr).  Test hooks only.
+static int generic_rows(fm_handle *h, int32_t **out, int *maxn)
+{
+    if (!h->d.tile) { *out = h->d.nbr; *maxn = h->d.maxn; return FM_OK; }
+    int32_t *buf = nullptr;
+    FM_TRY(dalloc(&buf, fm::nb_rows(h->d.n) * (size_t)h->d.maxn16));
+    fm::launch_tile_to_generic(h->d, buf, h->d.maxn16, h->st);
+    cudaError_t ce = cudaGetLastError();
+    if (ce != cudaSuccess) { cudaFree(buf); FM_CUDA(ce); }
+    *out = buf;
+    *maxn = h->d.maxn16;
+    return FM_OK;
+}
+
 extern "C" int fm_get_pair_list(fm_handle *h, int32_t *owner, int32_t *partner, int8_t *code, int64_t cap,
                                 int64_t *n_out)
 {
@@ -1090,15 +1227,20 @@ extern "C" int fm_get_pair_list(fm_handle *h, int32_t *owner, int32_t *partner, 
     if (!n_out) return fail(FM_ERR_ARG, "null output");
     if (h->p.force_list == 0) { *n_out = 0; return FM_OK; }
     const size_t n = (size_t)h->d.n;
-    std::vector<int32_t> nnbr(n), slot(n), nbr(fm::nb_rows((int)n) * (size_t)h->d.maxn);
+    int32_t *dnbr = nullptr;
+    int maxn = 0;
+    FM_TRY(generic_rows(h, &dnbr, &maxn));
+    std::vector<int32_t> nnbr(n), slot(n), nbr(fm::nb_rows((int)n) * (size_t)maxn);
     FM_CUDA(cudaMemcpyAsync(nnbr.data(), h->d.nnbr, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, h->st));
     FM_CUDA(cudaMemcpyAsync(slot.data(), h->d.slot_of, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, h->st));
-    FM_CUDA(cudaMemcpyAsync(nbr.data(), h->d.nbr, sizeof(int32_t) * nbr.size(), cudaMemcpyDeviceToHost, h->st));
-    FM_CUDA(cudaStreamSynchronize(h->st));
+    cudaError_t ce = cudaMemcpyAsync(nbr.data(), dnbr, sizeof(int32_t) * nbr.size(), cudaMemcpyDeviceToHost, h->st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->st);
+    if (dnbr != h->d.nbr) cudaFree(dnbr);
+    FM_CUDA(ce);
     int64_t k = 0;
     for (size_t i = 0; i < n; i++) {
         for (int q = 0; q < nnbr[i]; q++) {
-            int32_t e = nbr[fm::nb_row((int)i, h->d.maxn) + fm::nb_col(q)];
+            int32_t e = nbr[fm::nb_row((int)i, maxn) + fm::nb_col(q)];
             int32_t j = e & fm::NB_INDEX_MASK;
             int c6 = (int)((uint32_t)e >> fm::NB_SHIFT_BITS);
             int sx = (c6 & 3) - 1, sy = ((c6 >> 2) & 3) - 1, sz = ((c6 >> 4) & 3) - 1;
@@ -1119,9 +1261,18 @@ extern "C" int fm_pair_digest(fm_handle *h, uint64_t *digest, int64_t *npairs)
     FM_TRY(ready(h, 1));
     if (!digest || !npairs) return fail(FM_ERR_ARG, "null output");
     if (h->p.force_list == 0) { *digest = 0; *npairs = 0; return FM_OK; }
+    int32_t *dnbr = nullptr;
+    int maxn = 0;
+    FM_TRY(generic_rows(h, &dnbr, &maxn));
+    FmDev d = h->d;
+    d.nbr = dnbr;
+    d.maxn = maxn;
     FM_CUDA(cudaMemsetAsync(&h->d.sc->digest, 0, sizeof(uint64_t) + sizeof(int64_t), h->st));
-    fm::launch_pair_digest(h->d, h->glob, h->st);
-    FM_CUDA(cudaGetLastError());
+    fm::launch_pair_digest(d, h->glob, h->st);
+    cudaError_t ce = cudaGetLastError();
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->st);
+    if (dnbr != h->d.nbr) cudaFree(dnbr);
+    FM_CUDA(ce);
     fm::FmScalars s;
     FM_TRY(read_scalars(h, &s));
     *digest = s.digest;
@@ -1136,13 +1287,21 @@ extern "C" int fm_get_threads_per_molecule(fm_handle *h, int32_t *tpm)
     return FM_OK;
 }
 
+extern "C" int fm_get_force_path(fm_handle *h, int32_t *path, int32_t *tile_capacity)
+{
+    if (!h) return fail(FM_ERR_ARG, "null handle");
+    if (path) *path = h->d.tile ? FM_FORCE_PATH_TILES : FM_FORCE_PATH_GATHER;
+    if (tile_capacity) *tile_capacity = h->d.tile ? h->d.tile_ucap : 0;
+    return FM_OK;
+}
+
 extern "C" int fm_get_counters(fm_handle *h, int64_t *rebuilds, int32_t *cap, int32_t *max_nbr)
 {
     FM_TRY(ready(h, 0));
     fm::FmScalars s;
     FM_TRY(read_scalars(h, &s));
     if (rebuilds) *rebuilds = s.rebuilds;
-    if (cap) *cap = h->d.maxn;
+    if (cap) *cap = h->d.tile ? h->d.maxn16 : h->d.maxn;
     if (max_nbr) *max_nbr = s.max_nbr;
     return FM_OK;
 }

@@ -35,9 +35,16 @@
 // whose subchain bit is set in the owner's bin_bflag words (get_bondflag,
 // modules.f90:602-610, 31 bits per word) is a bond partner.  Pruning is off
 // then (a stretched bond is still found, and fails at the force).
+//
+// With TILE the rows hold, instead of the entry bits, the candidate's 16-bit
+// word offset in the tiled force kernel's staging of the owner's block
+// (fm_tile.cuh): the segment's base in that staging (blk_off) plus the
+// candidate's place in its segment.  The pair set and the row order are the
+// same.
 #pragma once
 #include "fm_common.cuh"
 #include "fm_device.cuh"
+#include "fm_tile.cuh"
 
 namespace fm {
 
@@ -66,6 +73,12 @@ struct CellSys {
     const int32_t *chain, *subchain;
     const int4 *bflag;
     int32_t *bnd, *nbond;
+    // tiled force path (TILE only): rows of staging offsets
+    uint16_t *nbr16;
+    int maxn16, tT, tR;
+    int tdummy;                 // byte offset of the staging's dummy candidate (row padding)
+    const int32_t *blk_off;
+    int tnb[3];
 };
 
 // Per-warp shared staging.
@@ -79,6 +92,8 @@ struct BuildShared {
     int2 cs[POLY ? NB_STAGE : 1];  // chain, subchain of candidates
     int off[55];                // candidate offset of segment k (54 segments + total)
     int start[54], code[54];
+    int lbase[54];              // TILE: segment k's first candidate in the block staging
+    unsigned short loc[NB_STAGE];  // TILE: staged candidates' word offsets
     int ochain[POLY ? 32 : 1];
     alignas(16) int4 obf[POLY ? 32 : 1];
     unsigned hits[POLY ? 1 : 32];  // per owner: which of the 32 candidates hit (polymers: registers)
@@ -133,7 +148,7 @@ __device__ __forceinline__ bool exact_pair(const double4 *P, int io, int e, cons
 // Rows of every molecule of cell c (0-based extended index) of system y, by
 // one warp.  Returns BUILD_OVER_* bits when a row or a bond set overflowed
 // (the counts past the capacity are still reported through max_nbr).
-template <bool POLY>
+template <bool POLY, bool TILE = false>
 __device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY> &sh, int lane)
 {
     const int ne0 = y.ne[0], ne1 = y.ne[1], ne2 = y.ne[2];
@@ -141,7 +156,7 @@ __device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY> &sh, i
     const int ccount = y.cell_start[c + 1] - y.mol_off - cstart;
     if (ccount == 0) return 0u;  // uniform across the warp
     const double4 *P = y.P;
-    const int maxn = y.maxn;
+    const int maxn = TILE ? y.maxn16 : y.maxn;
     const unsigned lt = (1u << lane) - 1u;
     const double csmax = fmax(y.cs[0], fmax(y.cs[1], y.cs[2]));
     const float band = (float)(1e-4 * csmax * csmax) + 1e-6f;
@@ -157,8 +172,17 @@ __device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY> &sh, i
 
     // --- segments of neighbour cell q = lane ---
     int n_real = 0, b_real = 0, n_img = 0, b_img = 0, code_img = NB_NOSHIFT;
+    int lb_real = 0, lb_img = 0;
     if (lane < 27) {
         const int x2 = cx + lane % 3 - 1, y2 = cy + (lane / 3) % 3 - 1, z2 = cz + lane / 9 - 1;
+        if (TILE && x2 >= 0 && y2 >= 0 && z2 >= 0 && x2 < ne0 && y2 < ne1 && z2 < ne2) {
+            // union cell of (x2, y2, z2) around the owner's 2x2x2 block
+            const int blk = tile_block_of(y.tnb, cx, cy, cz);
+            const int u = (x2 - (cx & ~1) + 1) + TILE_UE * ((y2 - (cy & ~1) + 1) + TILE_UE * (z2 - (cz & ~1) + 1));
+            const int32_t *bo = y.blk_off + (size_t)blk * TILE_NSEGP + 2 * u;
+            lb_real = bo[0];
+            lb_img = bo[1];
+        }
         if (x2 >= 0 && y2 >= 0 && z2 >= 0 && x2 < ne0 && y2 < ne1 && z2 < ne2) {
             const bool h2 = is_halo(x2, ne0) || is_halo(y2, ne1) || is_halo(z2, ne2);
             if (!(chalo && h2)) {
@@ -200,6 +224,10 @@ __device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY> &sh, i
         sh.start[2 * lane + 1] = b_img;
         sh.code[2 * lane] = NB_NOSHIFT;
         sh.code[2 * lane + 1] = code_img;
+        if (TILE) {
+            sh.lbase[2 * lane] = lb_real;
+            sh.lbase[2 * lane + 1] = lb_img;
+        }
     }
     if (lane == 0) sh.off[54] = total;
     __syncwarp();
@@ -216,7 +244,8 @@ __device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY> &sh, i
         const float by0 = warp_min(yif), by1 = warp_max(yif);
         const float bz0 = warp_min(zif), bz1 = warp_max(zif);
         int cnt = 0, nb = 0;  // the owner lane's list and bond counts
-        int32_t *const row = y.nbr + nb_row(i, maxn);
+        int32_t *const row = TILE ? nullptr : y.nbr + nb_row(i, maxn);
+        uint16_t *const row16 = TILE ? y.nbr16 + tile_row16(i, maxn) : nullptr;
         const int self_e = i | (NB_NOSHIFT << NB_SHIFT_BITS);  // the owner's own entry
         const int nown = min(32, ccount - pass * 32);
         __syncwarp();
@@ -238,7 +267,7 @@ __device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY> &sh, i
                 const int t = t0 + lane;
                 bool keep = false;
                 float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
-                int j = 0;
+                int j = 0, loc = 0;
                 if (t < take) {
                     const int q = base + t;
                     int k = 0;  // segment containing q: largest k with off[k] <= q
@@ -246,6 +275,7 @@ __device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY> &sh, i
                     for (int step = 32; step > 0; step >>= 1)
                         if (k + step < 54 && sh.off[k + step] <= q) k += step;
                     j = sh.start[k] + (q - sh.off[k]);
+                    if (TILE) loc = tile_boff(sh.lbase[k] + (q - sh.off[k]), y.tR);
                     const int code = sh.code[k];
                     const double4 pj = ldg_pos(P + j);
                     const double xj = image(pj.x, (code & 3) - 1, y.L[0]);
@@ -264,6 +294,7 @@ __device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY> &sh, i
                 if (keep) {
                     const int pos = kept + __popc(m & lt);
                     sh.f[pos] = f;
+                    if (TILE) sh.loc[pos] = (unsigned short)loc;
                     if (POLY) sh.cs[pos] = make_int2(y.chain[j], y.subchain[j]);
                 }
                 kept += __popc(m);
@@ -349,12 +380,19 @@ __device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY> &sh, i
                     mine_hits &= mine_hits - 1u;
                     const int ent = __float_as_int(sh.f[t0 + b].w);
                     if (POLY || ent != self_e) {
-                        if (cnt < maxn) row[nb_col(cnt)] = ent;
+                        if (cnt < maxn) {
+                            if (TILE) row16[tile_pos16(cnt, y.tT)] = sh.loc[t0 + b];
+                            else row[nb_col(cnt)] = ent;
+                        }
                         cnt++;
                     }
                 }
                 if (!POLY) __syncwarp();
             }
+        }
+        if (TILE && own) {  // pad the last load of the row with the dummy candidate
+            const int lim = min((cnt + 4 * y.tT - 1) / (4 * y.tT) * (4 * y.tT), maxn);
+            for (int k = cnt; k < lim; k++) row16[tile_pos16(k, y.tT)] = (uint16_t)y.tdummy;
         }
         if (own) {
             y.nnbr[i] = cnt < maxn ? cnt : maxn;
@@ -394,6 +432,8 @@ struct BlockShared {
     int2 cs[POLY ? NB_STAGE : 1];
     int off[NB_BSEG + 1];
     int start[NB_BSEG], code[NB_BSEG];
+    int lbase[NB_BSEG];             // TILE: segment k's first candidate in the block staging
+    unsigned short loc[NB_STAGE];   // TILE: staged candidates' word offsets
     unsigned char segallow[NB_BSEG];
     int opre[9], ostart[8];         // owners by block cell: prefix counts, first molecule
     int ochain[POLY ? 32 : 1];
@@ -401,7 +441,7 @@ struct BlockShared {
     unsigned hits[POLY ? 1 : 32];   // per owner: which of the 32 candidates hit (polymers: registers)
 };
 
-template <bool POLY>
+template <bool POLY, bool TILE = false>
 __device__ uint32_t build_block(const CellSys &y, int blk, BlockShared<POLY> &sh, int lane)
 {
     const int ne0 = y.ne[0], ne1 = y.ne[1], ne2 = y.ne[2];
@@ -409,7 +449,7 @@ __device__ uint32_t build_block(const CellSys &y, int blk, BlockShared<POLY> &sh
     const int bx0 = 2 * (blk % nb0), by0 = 2 * ((blk / nb0) % nb1), bz0 = 2 * (blk / (nb0 * nb1));
     const unsigned lt = (1u << lane) - 1u;
     const double4 *P = y.P;
-    const int maxn = y.maxn;
+    const int maxn = TILE ? y.maxn16 : y.maxn;
 
     // --- the block's owner cells (lanes 0..7: a + 2b + 4c) ---
     int ocount = 0, ostart = 0;
@@ -509,6 +549,11 @@ __device__ uint32_t build_block(const CellSys &y, int blk, BlockShared<POLY> &sh
         sh.code[2 * u + 1] = seg_code[2 * h + 1];
         sh.segallow[2 * u] = (unsigned char)seg_allow[h];
         sh.segallow[2 * u + 1] = (unsigned char)seg_allow[h];
+        if (TILE) {  // the same block and segments as the tiled force staging
+            const int32_t *bo = y.blk_off + (size_t)blk * TILE_NSEGP + 2 * u;
+            sh.lbase[2 * u] = bo[0];
+            sh.lbase[2 * u + 1] = bo[1];
+        }
         carry += __shfl_sync(0xffffffffu, incl, 31);
     }
     const int total = carry;
@@ -530,7 +575,8 @@ __device__ uint32_t build_block(const CellSys &y, int blk, BlockShared<POLY> &sh
         const float by_lo = warp_min(own ? yif : 3e38f), by_hi = warp_max(own ? yif : -3e38f);
         const float bz_lo = warp_min(own ? zif : 3e38f), bz_hi = warp_max(own ? zif : -3e38f);
         int cnt = 0, nb = 0;
-        int32_t *const row = y.nbr + nb_row(i, maxn);
+        int32_t *const row = TILE ? nullptr : y.nbr + nb_row(i, maxn);
+        uint16_t *const row16 = TILE ? y.nbr16 + tile_row16(i, maxn) : nullptr;
         const int self_e = i | (NB_NOSHIFT << NB_SHIFT_BITS);  // the owner's own entry
         const int nown = min(32, nowners - pass * 32);
         __syncwarp();
@@ -552,7 +598,7 @@ __device__ uint32_t build_block(const CellSys &y, int blk, BlockShared<POLY> &sh
                 bool keep = false;
                 float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
                 unsigned al = 0u;
-                int j = 0;
+                int j = 0, loc = 0;
                 if (t < take) {
                     const int q = base + t;
                     int kk = 0;  // segment containing q: largest kk with off[kk] <= q
@@ -560,6 +606,7 @@ __device__ uint32_t build_block(const CellSys &y, int blk, BlockShared<POLY> &sh
                     for (int step = 64; step > 0; step >>= 1)
                         if (kk + step < NB_BSEG && sh.off[kk + step] <= q) kk += step;
                     j = sh.start[kk] + (q - sh.off[kk]);
+                    if (TILE) loc = tile_boff(sh.lbase[kk] + (q - sh.off[kk]), y.tR);
                     const int code = sh.code[kk];
                     al = sh.segallow[kk];
                     const double4 pj = ldg_pos(P + j);
@@ -578,6 +625,7 @@ __device__ uint32_t build_block(const CellSys &y, int blk, BlockShared<POLY> &sh
                     const int pos = kept + __popc(m & lt);
                     sh.f[pos] = f;
                     sh.allow[pos] = (unsigned char)al;
+                    if (TILE) sh.loc[pos] = (unsigned short)loc;
                     if (POLY) sh.cs[pos] = make_int2(y.chain[j], y.subchain[j]);
                 }
                 kept += __popc(m);
@@ -659,12 +707,19 @@ __device__ uint32_t build_block(const CellSys &y, int blk, BlockShared<POLY> &sh
                     mine_hits &= mine_hits - 1u;
                     const int ent = __float_as_int(sh.f[t0 + b].w);
                     if (POLY || ent != self_e) {
-                        if (cnt < maxn) row[nb_col(cnt)] = ent;
+                        if (cnt < maxn) {
+                            if (TILE) row16[tile_pos16(cnt, y.tT)] = sh.loc[t0 + b];
+                            else row[nb_col(cnt)] = ent;
+                        }
                         cnt++;
                     }
                 }
                 if (!POLY) __syncwarp();
             }
+        }
+        if (TILE && own) {  // pad the last load of the row with the dummy candidate
+            const int lim = min((cnt + 4 * y.tT - 1) / (4 * y.tT) * (4 * y.tT), maxn);
+            for (int k = cnt; k < lim; k++) row16[tile_pos16(k, y.tT)] = (uint16_t)y.tdummy;
         }
         if (own) {
             y.nnbr[i] = cnt < maxn ? cnt : maxn;

@@ -15,7 +15,8 @@ enum : uint32_t {
     ST_NLIST = 1u << 1,     // a neighbour list needed more than maxn slots
     ST_PE = 1u << 2,        // per-molecule PE above 10000 on a record step
     ST_BOND = 1u << 3,      // FENE bond at or beyond R_0
-    ST_FATAL = ST_ESCAPE | ST_NLIST | ST_PE | ST_BOND,
+    ST_TILE = 1u << 4,      // a block's staged neighbourhood exceeded the tiled force kernel's capacity
+    ST_FATAL = ST_ESCAPE | ST_NLIST | ST_PE | ST_BOND | ST_TILE,
 };
 
 // Device-resident scalars of the step loop (one per system).
@@ -37,6 +38,8 @@ struct FmScalars {
     unsigned long long dmax;  // rebuild criterion 2: bits of max |rdisp component| this step
     double pacc[6];           // pressure_outflag 1: sum over samples of P (xx yy zz xy xz yz)
     int32_t pcount;           // samples in pacc
+    int32_t tile_next;        // tiled force kernel: next block to hand out (the last taker resets it)
+    int32_t umax;             // tiled path: largest staged neighbourhood seen at the last build
 };
 
 // Partial sums of one record step, one row per force-kernel block.
@@ -113,6 +116,19 @@ struct FmDev {
     // Mie_potential 1: per-type-pair constants, per-type masses; a molecule's
     // type (1-based) rides in the w component of its position
     int build_blocks;            // list build: one warp per 2x2x2 cells (sparse systems)
+    // Tiled force path (tile = 1): the extended cell grid is cut into blocks of
+    // 2x2x2 cells; the force kernel stages the positions of a block's 4x4x4
+    // cell neighbourhood (images applied) in shared memory, and list entries
+    // are 16-bit offsets into that staging (fm_tile.cuh).
+    int tile;
+    int tile_T;                  // lanes per molecule (4 or 8); fixes the row layout
+    int tile_R;                  // staged rows per 32 candidates: 3 (x y z) or 4 (+ w)
+    int tile_nb[3];              // blocks per axis, ceil(ne / 2)
+    int tile_nblk;
+    int tile_ucap;               // staged candidates per block the force kernel holds
+    int32_t *blk_off;            // [tile_nblk][TILE_NSEGP] prefix of the staging segments
+    uint16_t *nbr16;             // rows of maxn16 entries (tile_pos16 layout)
+    int maxn16;
     // pressure_outflag 1: rf (xx yy zz xy xz yz) per molecule of the last
     // record step (pressure_tensor_forces, simulation_record.f90:6239-6256)
     int pressure;
@@ -175,6 +191,13 @@ void launch_scan_cells(const FmDev &d, int gated, cudaStream_t st);
 void launch_scatter(const FmDev &d, int gated, cudaStream_t st);
 void launch_reorder(const FmDev &d, int gated, double4 *tpos, int32_t *tuidx, cudaStream_t st);
 void launch_build_nlist(const FmDev &d, int gated, int iter, cudaStream_t st);
+// Tiled path: the staging segment table of every block (before the build).
+void launch_blk_seg(const FmDev &d, int gated, int iter, cudaStream_t st);
+size_t tile_smem_bytes(const FmDev &d);
+int tile_ucap_limit(int R);
+// Decodes the tiled rows into the generic int32 layout at `out` (rows of
+// d.maxn), for the pair-list and digest test hooks.
+void launch_tile_to_generic(const FmDev &d, int32_t *out, int maxn, cudaStream_t st);
 // Forces: mode 0 forces only, 1 forces + move(2), 2 forces + move(2) + next
 // move(1), 3 forces + leap-frog move.
 void launch_force(const FmDev &d, int record, int mode, int tpm, cudaStream_t st);

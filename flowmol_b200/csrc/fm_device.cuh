@@ -42,6 +42,23 @@ void pdl_launch(void (*k)(P...), dim3 grid, dim3 block, cudaStream_t st, A... ar
     cudaLaunchKernelEx(&c, k, args...);
 }
 
+// pdl_launch with dynamic shared memory.
+template <typename... P, typename... A>
+void pdl_launch_smem(void (*k)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, A... args)
+{
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t c = {};
+    c.gridDim = grid;
+    c.blockDim = block;
+    c.dynamicSmemBytes = smem;
+    c.stream = st;
+    c.attrs = at;
+    c.numAttrs = 1;
+    cudaLaunchKernelEx(&c, k, args...);
+}
+
 // Neighbour-list entries are read once per step and never again before the
 // next step: keep them out of L1, so that the partner positions they point at
 // stay cached there.

@@ -17,6 +17,7 @@
 #include "fm_common.cuh"
 #include "fm_device.cuh"
 #include "fm_build.cuh"
+#include "fm_tile.cuh"
 
 namespace fm {
 
@@ -73,6 +74,8 @@ __global__ void k_reset_scalars(FmDev d)
     s->dmax = 0ull;
     for (int q = 0; q < 6; q++) s->pacc[q] = 0.0;
     s->pcount = 0;
+    s->tile_next = 0;
+    s->umax = 0;
 }
 
 // r = (r + dt v) + (0.5 dt^2) a ; v = v + (0.5 dt) a   -- pass 1, in place.
@@ -423,10 +426,50 @@ __global__ void k_reorder_copy(FmDev d, int gated, const double4 *tpos, const in
 //  1118-1180, stored in both directions)
 // ---------------------------------------------------------------------------
 
+// Staging segment table of the tiled force path, one warp per block: the
+// exclusive prefix of the block's 128 segment sizes (fm_tile.cuh) and their
+// total.  A block whose total exceeds the force kernel's capacity raises
+// ST_TILE; the host grows the capacity and builds again.
+constexpr int BS_THREADS = 256;
+__global__ void __launch_bounds__(BS_THREADS) k_blk_seg(FmDev d, int gated, int iter)
+{
+    pdl_enter();
+    if (!gate(d, gated)) return;
+    const int lane = threadIdx.x & 31;
+    constexpr int WPB = BS_THREADS / 32;
+    int umax = 0;
+    for (int blk = blockIdx.x * WPB + (threadIdx.x >> 5); blk < d.tile_nblk; blk += gridDim.x * WPB) {
+        const int bx = blk % d.tile_nb[0], by = (blk / d.tile_nb[0]) % d.tile_nb[1];
+        const int bz = blk / (d.tile_nb[0] * d.tile_nb[1]);
+        int32_t *out = d.blk_off + (size_t)blk * TILE_NSEGP;
+        int carry = 0;
+#pragma unroll
+        for (int h = 0; h < TILE_NSEG / 32; h++) {
+            int st, cnt, code;
+            tile_segment(d.ne, d.cell_start, 2 * bx, 2 * by, 2 * bz, h * 32 + lane, st, cnt, code);
+            int incl = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            out[h * 32 + lane] = carry + incl - cnt;
+            carry += __shfl_sync(0xffffffffu, incl, 31);
+        }
+        if (lane == 0) out[TILE_NSEG] = carry;
+        umax = max(umax, carry);
+    }
+    umax = __reduce_max_sync(0xffffffffu, umax);
+    if (lane == 0 && umax > 0) {
+        atomicMax(&d.sc->umax, umax);
+        if (umax > d.tile_ucap) raise_status(d, ST_TILE, iter);
+    }
+}
+
 // Neighbour rows of every extended cell, one warp per cell or, for sparse
 // systems (BLOCKS), per block of 2x2x2 cells (grid-stride); the routines and
 // their pair-set argument are in fm_build.cuh.  Both give the same rows.
-template <bool POLY, bool BLOCKS>
+template <bool POLY, bool BLOCKS, bool TILE>
 __global__ void __launch_bounds__(NB_THREADS, 8) k_build_nlist(FmDev d, int gated, int iter)
 {
     pdl_enter();
@@ -446,6 +489,9 @@ __global__ void __launch_bounds__(NB_THREADS, 8) k_build_nlist(FmDev d, int gate
     y.max_nbr = &d.sc->max_nbr;
     y.chain = d.chain; y.subchain = d.subchain; y.bflag = d.bflag;
     y.bnd = d.bnd; y.nbond = d.nbond;
+    y.nbr16 = d.nbr16; y.maxn16 = d.maxn16; y.tT = d.tile_T; y.tR = d.tile_R; y.blk_off = d.blk_off;
+    y.tdummy = d.tile ? tile_boff(d.tile_ucap, d.tile_R) : 0;
+    for (int k = 0; k < 3; k++) y.tnb[k] = d.tile_nb[k];
     uint32_t over = 0u;
     const int nwork = BLOCKS ? ((d.ne[0] + 1) / 2) * ((d.ne[1] + 1) / 2) * ((d.ne[2] + 1) / 2) : d.ncell;
     // work units handed out NB_CHUNK at a time, so warps that meet empty or
@@ -457,8 +503,8 @@ __global__ void __launch_bounds__(NB_THREADS, 8) k_build_nlist(FmDev d, int gate
         if (u0 >= nwork) break;
         const int u1 = min(u0 + NB_CHUNK, nwork);
         for (int u = u0; u < u1; u++) {
-            if constexpr (BLOCKS) over |= build_block<POLY>(y, u, sh[warp], lane);
-            else over |= build_cell<POLY>(y, u, sh[warp], lane);
+            if constexpr (BLOCKS) over |= build_block<POLY, TILE>(y, u, sh[warp], lane);
+            else over |= build_cell<POLY, TILE>(y, u, sh[warp], lane);
         }
     }
     if (lane == 0) {
@@ -731,22 +777,45 @@ __device__ __forceinline__ void fene_bonds(const FmDev &d, const double4 *P, int
     }
 }
 
-// Block reduction of the record partials; row blockIdx.x of d.partial.
-__device__ __forceinline__ void block_partials(const FmDev &d, double v[RS_N])
+// (s, c) += (s2, c2): Neumaier merge of two compensated partial sums.
+__device__ __forceinline__ void nmerge(double &s, double &c, double s2, double c2)
 {
-    __shared__ double ws[RS_N][FORCE_THREADS / 32];
+    neumaier(s, c, s2);
+    c += c2;
+}
+
+// Block reduction of the record partials into row `row` of d.partial:
+// Neumaier-compensated sums in a fixed tree order (warp xor tree, then the
+// warps in index order), the row holding the compensated value rounded once;
+// PE max for the PE check.
+template <int NT = FORCE_THREADS>
+__device__ __forceinline__ void block_partials(const FmDev &d, double v[RS_N], int row)
+{
+    __shared__ double ws[RS_N][NT / 32], wc[RS_N][NT / 32];
     int w = threadIdx.x >> 5, l = threadIdx.x & 31;
 #pragma unroll
     for (int k = 0; k < RS_N; k++) {
-        double x = k == RS_PEMAX ? warp_max(v[k]) : warp_sum(v[k]);
-        if (l == 0) ws[k][w] = x;
+        double x = v[k], c = 0.0;
+        if (k == RS_PEMAX) {
+            x = warp_max(x);
+        } else {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double x2 = __shfl_xor_sync(0xffffffffu, x, o), c2 = __shfl_xor_sync(0xffffffffu, c, o);
+                nmerge(x, c, x2, c2);
+            }
+        }
+        if (l == 0) { ws[k][w] = x; wc[k][w] = c; }
     }
     __syncthreads();
     if (threadIdx.x < RS_N) {
         int k = threadIdx.x;
-        double acc = ws[k][0];
-        for (int q = 1; q < FORCE_THREADS / 32; q++) acc = k == RS_PEMAX ? fmax(acc, ws[k][q]) : acc + ws[k][q];
-        d.partial[(size_t)blockIdx.x * RS_N + k] = acc;
+        double acc = ws[k][0], cmp = wc[k][0];
+        for (int q = 1; q < NT / 32; q++) {
+            if (k == RS_PEMAX) acc = fmax(acc, ws[k][q]);
+            else nmerge(acc, cmp, ws[k][q], wc[k][q]);
+        }
+        d.partial[(size_t)row * RS_N + k] = k == RS_PEMAX ? acc : acc + cmp;
     }
 }
 
@@ -821,8 +890,282 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force(FmDev d)
     // a(:,i) = sum acc rij / mass (LJ_mass = 1; Mie_mass by type)
     if (active && lane == 0)
         m2 = epilogue<REC, MODE, (PREC & 2) != 0>(d, pset, i, P[i], fx, fy, fz, pe, vir, part, rf);
-    if (REC) block_partials(d, part);
+    if (REC) block_partials(d, part, blockIdx.x);
     if (MODE >= 2) block_vmax2(d, m2);
+}
+
+// ---------------------------------------------------------------------------
+// tiled forces: the same pair sums, partners read from a shared-memory
+// staging of the block's neighbourhood (fm_tile.cuh) instead of gathered
+// from global memory one list entry at a time
+// ---------------------------------------------------------------------------
+
+// One CTA takes a block of 2x2x2 cells at a time (handed out from an atomic
+// counter): it stages the positions of the block's 4x4x4-cell neighbourhood,
+// periodic images applied with the same single FP64 add as every other path
+// (image(): x_src +/- L), as FP64 rows of 32 candidates; then T lanes per
+// owner walk the owner's row of 16-bit staging offsets, T consecutive entries
+// at a time, and evaluate each pair exactly as k_force does (FP64 cutoff test
+// without contraction, the same pair_acc and epilogue).  Record partials are
+// written per block (a fixed row whatever CTA took it), so the record sums do
+// not depend on the hand-out order.
+constexpr int FT_THREADS = FORCE_THREADS;
+constexpr int FT_WARPS = FT_THREADS / 32;
+
+// FP32 LJ pair of the precision form on the tiled path: the pair magnitude
+// 48 s^7 - 24 s^4 = s^4 (48 s^3 - 24) in FP32 from an approximate reciprocal
+// (rcp.approx, relative error ~2^-23 -- far inside the form's 1e-5
+// tolerance), scaled by the FP64 rij; LJ_energy 4 (s^6 - s^3) - potshift on
+// record steps.
+template <bool REC>
+__device__ __forceinline__ double lj32_pair(double r2, double dx, double dy, double dz, double potshift,
+                                            double &fx, double &fy, double &fz, double &pe, double &vir)
+{
+    const float r2f = __double2float_rn(r2);
+    float s;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(s) : "f"(r2f));
+    const float s2 = s * s, s3 = s2 * s, s4 = s2 * s2;
+    const double acc = (double)(s4 * fmaf(48.0f, s3, -24.0f));
+    fx = fma(acc, dx, fx); fy = fma(acc, dy, fy); fz = fma(acc, dz, fz);
+    if (REC) {
+        pe += (double)(4.0f * (s3 * s3 - s3)) - potshift;
+        vir += acc * r2;
+    }
+    return acc;
+}
+
+__device__ __forceinline__ uint2 ld_stream_uint2(const uint2 *p)
+{
+    uint2 r;
+    asm("ld.global.nc.L1::no_allocate.v2.u32 {%0, %1}, [%2];" : "=r"(r.x), "=r"(r.y) : "l"(p));
+    return r;
+}
+
+template <int T, bool REC, int MODE, int PREC>
+__global__ void __launch_bounds__(FT_THREADS, REC ? 2 : 4) k_force_tile(FmDev d)
+{
+    constexpr bool MIE = (PREC & 2) != 0;
+    constexpr bool NEEDW = (PREC & 6) != 0;  // Mie types / Soddemann bead flags ride in w
+    constexpr bool LJ32 = PREC == 1;         // plain LJ, FP32 pair magnitude
+    constexpr int R = NEEDW ? 4 : 3;
+    constexpr int G = 32 / T;                // owners per warp per pass
+    extern __shared__ double stg[];
+    __shared__ int s_off[TILE_NSEGP];
+    __shared__ int s_start[TILE_NSEG];
+    __shared__ int s_code[TILE_NSEG];
+    __shared__ int s_opre[9], s_ostart[8];
+    __shared__ int s_blk, s_frozen, s_onext;
+    pdl_enter();
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) s_frozen = frozen(d) ? 1 : 0;
+    // the dummy candidate after the capacity: far from every owner (the
+    // staging below never writes index ucap)
+    if (tid < R) stg[tile_woff(d.tile_ucap, R) + 32 * tid] = tid < 3 ? 1e30 : 1.0;
+    __syncthreads();
+    if (s_frozen) return;
+    const int pset = d.sc->pset;
+    const double4 *__restrict__ P = cur_pos(d, pset);
+    const int sub = lane % T, og = lane / T;
+    const unsigned dummy = (unsigned)tile_boff(d.tile_ucap, R);
+    const unsigned lim2 = dummy | (dummy << 16);  // no byte offset beyond the dummy's
+    const char *sbase = reinterpret_cast<const char *>(stg);
+    const double Lx = d.L[0], Ly = d.L[1], Lz = d.L[2];
+    const double rc2 = d.rc2;
+    double m2max = 0.0;
+    for (;;) {
+        if (tid == 0) {
+            const int b = atomicAdd(&d.sc->tile_next, 1);
+            // every CTA takes exactly one number past the last block; the CTA
+            // that takes the very last one resets the counter for the next launch
+            if (b == d.tile_nblk + (int)gridDim.x - 1) d.sc->tile_next = 0;
+            s_blk = b;
+            s_onext = 0;
+        }
+        __syncthreads();
+        const int blk = s_blk;
+        if (blk >= d.tile_nblk) break;
+        const int bx = blk % d.tile_nb[0], by = (blk / d.tile_nb[0]) % d.tile_nb[1];
+        const int bz = blk / (d.tile_nb[0] * d.tile_nb[1]);
+        const int x0 = 2 * bx, y0 = 2 * by, z0 = 2 * bz;
+        if (tid < TILE_NSEG) {
+            int st, cnt, code;
+            tile_segment(d.ne, d.cell_start, x0, y0, z0, tid, st, cnt, code);
+            s_start[tid] = st;
+            s_code[tid] = code;
+        }
+        if (tid < TILE_NSEGP) s_off[tid] = d.blk_off[(size_t)blk * TILE_NSEGP + tid];
+        if (warp == FT_WARPS - 1) {  // the block's owner cells a + 2b + 4c and their prefix
+            int cnt = 0, st = 0;
+            if (lane < 8) {
+                const int x = x0 + (lane & 1), yy = y0 + ((lane >> 1) & 1), z = z0 + (lane >> 2);
+                if (x < d.ne[0] && yy < d.ne[1] && z < d.ne[2]) {
+                    const int c = x + d.ne[0] * (yy + d.ne[1] * z);
+                    st = d.cell_start[c];
+                    cnt = d.cell_start[c + 1] - st;
+                }
+            }
+            int incl = cnt;
+#pragma unroll
+            for (int o = 1; o < 8; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            if (lane < 8) { s_opre[lane + 1] = incl; s_ostart[lane] = st; }
+            if (lane == 0) s_opre[0] = 0;
+        }
+        __syncthreads();
+        // stage, two candidates per thread per pass (both loads in flight); a
+        // block above the capacity was refused by k_blk_seg before the build
+        const int U = min(s_off[TILE_NSEG], d.tile_ucap);
+        for (int c0 = tid; c0 < U; c0 += 2 * FT_THREADS) {
+            double4 p[2];
+            int code[2], cc[2];
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int c = min(c0 + h * FT_THREADS, U - 1);  // a repeat of the last is harmless
+                int k = 0;  // segment containing c: largest k with s_off[k] <= c
+#pragma unroll
+                for (int step = 64; step > 0; step >>= 1)
+                    if (k + step < TILE_NSEG && s_off[k + step] <= c) k += step;
+                p[h] = ldg_pos(P + s_start[k] + (c - s_off[k]));
+                code[h] = s_code[k];
+                cc[h] = c;
+            }
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int w = tile_woff(cc[h], R);
+                stg[w] = image(p[h].x, (code[h] & 3) - 1, Lx);
+                stg[w + 32] = image(p[h].y, ((code[h] >> 2) & 3) - 1, Ly);
+                stg[w + 64] = image(p[h].z, ((code[h] >> 4) & 3) - 1, Lz);
+                if (NEEDW) stg[w + 96] = p[h].w;
+            }
+        }
+        __syncthreads();
+        const int nown = s_opre[8];
+        double pacc[RS_N];
+#pragma unroll
+        for (int q = 0; q < RS_N; q++) pacc[q] = 0.0;
+        // owner groups: handed out from a shared counter (the warps of a block
+        // finish together), or in a fixed order on record steps so that the
+        // block's record partial is summed in the same order every time
+        for (int pass = 0;; pass++) {
+            int base;
+            if (REC) {
+                base = (warp + pass * FT_WARPS) * G;
+            } else {
+                if (lane == 0) base = atomicAdd(&s_onext, G);
+                base = __shfl_sync(0xffffffffu, base, 0);
+            }
+            if (base >= nown) break;
+            const int k = base + og;
+            const bool act = k < nown;
+            int i = 0;
+            if (act) {
+                int oc = 0;
+#pragma unroll
+                for (int q = 1; q < 8; q++) oc += k >= s_opre[q] ? 1 : 0;
+                i = s_ostart[oc] + (k - s_opre[oc]);
+            }
+            double fx = 0.0, fy = 0.0, fz = 0.0, pe = 0.0, vir = 0.0;
+            double rf[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+            double4 pi = make_double4(0.0, 0.0, 0.0, 0.0);
+            if (act) {
+                pi = ldg_pos(P + i);
+                const int nch = (d.nnbr[i] + 4 * T - 1) / (4 * T);  // rows are padded to whole chunks
+                const uint2 *row = reinterpret_cast<const uint2 *>(d.nbr16 + tile_row16(i, d.maxn16)) + sub;
+                for (int c = 0; c < nch; c++) {
+                    uint2 e = ld_stream_uint2(row + c * T);
+                    e.x = __vminu2(e.x, lim2);
+                    e.y = __vminu2(e.y, lim2);
+                    const unsigned off[4] = {e.x & 0xffffu, e.x >> 16, e.y & 0xffffu, e.y >> 16};
+                    double xj[4], yj[4], zj[4], wj[4];
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const double *pj = reinterpret_cast<const double *>(sbase + off[q]);
+                        xj[q] = pj[0];
+                        yj[q] = pj[32];
+                        zj[q] = pj[64];
+                        wj[q] = NEEDW ? pj[96] : 0.0;
+                    }
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const double dx = __dsub_rn(pi.x, xj[q]);
+                        const double dy = __dsub_rn(pi.y, yj[q]);
+                        const double dz = __dsub_rn(pi.z, zj[q]);
+                        const double r2 = norm2_rn(dx, dy, dz);
+                        if (r2 < rc2) {
+                            double acc;
+                            if (LJ32) acc = lj32_pair<REC>(r2, dx, dy, dz, d.potshift, fx, fy, fz, pe, vir);
+                            else acc = pair_acc<PREC, REC>(d, r2, dx, dy, dz, pi.w, wj[q], fx, fy, fz, pe, vir);
+                            if (REC && d.pressure) add_rf(rf, acc, dx, dy, dz);
+                        }
+                    }
+                }
+            }
+            if (T > 1) {
+#pragma unroll
+                for (int o = T / 2; o > 0; o >>= 1) {
+                    fx += __shfl_xor_sync(0xffffffffu, fx, o);
+                    fy += __shfl_xor_sync(0xffffffffu, fy, o);
+                    fz += __shfl_xor_sync(0xffffffffu, fz, o);
+                    if (REC) {
+                        pe += __shfl_xor_sync(0xffffffffu, pe, o);
+                        vir += __shfl_xor_sync(0xffffffffu, vir, o);
+                        if (d.pressure) {
+#pragma unroll
+                            for (int q = 0; q < 6; q++) rf[q] += __shfl_xor_sync(0xffffffffu, rf[q], o);
+                        }
+                    }
+                }
+            }
+            if (act && sub == 0) {
+                if (d.potential_flag == 1) fene_bonds<REC, MIE>(d, P, i, fx, fy, fz, pe, vir, rf);
+                double part[RS_N];
+#pragma unroll
+                for (int q = 0; q < RS_N; q++) part[q] = 0.0;
+                const double m2 = epilogue<REC, MODE, MIE>(d, pset, i, pi, fx, fy, fz, pe, vir, part, rf);
+                m2max = fmax(m2max, m2);
+                if (REC) {
+#pragma unroll
+                    for (int q = 0; q < RS_N; q++)
+                        pacc[q] = q == RS_PEMAX ? fmax(pacc[q], part[q]) : pacc[q] + part[q];
+                }
+            }
+        }
+        if (REC) block_partials(d, pacc, blk);
+        __syncthreads();  // the next block overwrites the staging
+    }
+    if (MODE >= 2) block_vmax2(d, m2max);
+}
+
+// Decodes tiled rows into the generic int32 layout (rows of maxn at out),
+// owner by owner: its block from its cell (cell_start), each offset back to
+// a staging position, its segment by the block's prefix, and the segment's
+// slot and image code (test hooks only).
+__global__ void k_tile_to_generic(FmDev d, int32_t *out, int maxn)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.n) return;
+    int lo = 0, hi = d.ncell - 1;  // largest c with cell_start[c] <= i
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (d.cell_start[mid] <= i) lo = mid; else hi = mid - 1;
+    }
+    const int c = lo;
+    const int cx = c % d.ne[0], cy = (c / d.ne[0]) % d.ne[1], cz = c / (d.ne[0] * d.ne[1]);
+    const int blk = tile_block_of(d.tile_nb, cx, cy, cz);
+    const int32_t *off = d.blk_off + (size_t)blk * TILE_NSEGP;
+    const int cnt = min(d.nnbr[i], maxn);
+    const uint16_t *row = d.nbr16 + tile_row16(i, d.maxn16);
+    for (int k = 0; k < cnt; k++) {
+        const int cand = tile_cand(row[tile_pos16(k, d.tile_T)], d.tile_R);
+        int s = 0;
+        for (int step = 64; step > 0; step >>= 1)
+            if (s + step < TILE_NSEG && off[s + step] <= cand) s += step;
+        int st, n, code;
+        tile_segment(d.ne, d.cell_start, cx & ~1, cy & ~1, cz & ~1, s, st, n, code);
+        out[nb_row(i, maxn) + nb_col(k)] = (st + (cand - off[s])) | (code << NB_SHIFT_BITS);
+    }
 }
 
 // Neumaier-compensated reduction of the per-block partials into one record
@@ -917,19 +1260,7 @@ __global__ void __launch_bounds__(MACRO_THREADS) k_macro_partials(FmDev d)
             pressure_part(part, vx, vy, vz, rf);
         }
     }
-    __shared__ double ws[RS_N][MACRO_THREADS / 32];
-    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    for (int k = 0; k < RS_N; k++) {
-        double x = k == RS_PEMAX ? warp_max(part[k]) : warp_sum(part[k]);
-        if (l == 0) ws[k][w] = x;
-    }
-    __syncthreads();
-    if (threadIdx.x < RS_N) {
-        int k = threadIdx.x;
-        double acc = ws[k][0];
-        for (int q = 1; q < MACRO_THREADS / 32; q++) acc = k == RS_PEMAX ? fmax(acc, ws[k][q]) : acc + ws[k][q];
-        d.partial[(size_t)blockIdx.x * RS_N + k] = acc;
-    }
+    block_partials<MACRO_THREADS>(d, part, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -975,22 +1306,7 @@ __global__ void __launch_bounds__(AP_THREADS) k_all_pairs(FmDev d)
     double m2 = 0.0;
     const double rf[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // simulation_compute_forces_LJ_AP records no rf
     if (active) m2 = epilogue<REC, MODE, (PREC & 2) != 0>(d, pset, i, pi, fx, fy, fz, pe, vir, part, rf);
-    if (REC) {
-        // AP blocks are AP_THREADS wide; reuse the generic reduction layout
-        __shared__ double ws[RS_N][AP_THREADS / 32];
-        int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-        for (int k = 0; k < RS_N; k++) {
-            double x = k == RS_PEMAX ? warp_max(part[k]) : warp_sum(part[k]);
-            if (l == 0) ws[k][w] = x;
-        }
-        __syncthreads();
-        if (threadIdx.x < RS_N) {
-            int k = threadIdx.x;
-            double acc = ws[k][0];
-            for (int q = 1; q < AP_THREADS / 32; q++) acc = k == RS_PEMAX ? fmax(acc, ws[k][q]) : acc + ws[k][q];
-            d.partial[(size_t)blockIdx.x * RS_N + k] = acc;
-        }
-    }
+    if (REC) block_partials<AP_THREADS>(d, part, blockIdx.x);
     if (MODE >= 2) block_vmax2(d, m2);
 }
 
@@ -1134,7 +1450,7 @@ void launch_reorder(const FmDev &d, int gated, double4 *tpos, int32_t *tuidx, cu
 }
 // The list build walks the cells grid-stride with every block resident (one
 // wave: a second partial wave would double the kernel's time).
-template <bool POLY, bool BLOCKS>
+template <bool POLY, bool BLOCKS, bool TILE>
 static int build_grid(int nwork)
 {
     static int resident = 0;
@@ -1142,23 +1458,93 @@ static int build_grid(int nwork)
         int dev = 0, nsm = kSMs, per_sm = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_build_nlist<POLY, BLOCKS>, NB_THREADS, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_build_nlist<POLY, BLOCKS, TILE>, NB_THREADS, 0);
         resident = std::max(nsm, 1) * std::max(per_sm, 1);
     }
     return std::min(nblk(nwork, NB_WARPS), resident);
+}
+
+template <bool POLY, bool BLOCKS, bool TILE>
+static void launch_build_t(const FmDev &d, int nwork, int gated, int iter, cudaStream_t st)
+{
+    pdl_launch(k_build_nlist<POLY, BLOCKS, TILE>, build_grid<POLY, BLOCKS, TILE>(nwork), NB_THREADS, st, d, gated,
+               iter);
 }
 
 void launch_build_nlist(const FmDev &d, int gated, int iter, cudaStream_t st)
 {
     cudaMemsetAsync(&d.sc->build_next, 0, sizeof(int32_t), st);
     const int nb = ((d.ne[0] + 1) / 2) * ((d.ne[1] + 1) / 2) * ((d.ne[2] + 1) / 2);
-    if (d.potential_flag == 1) {
-        if (d.build_blocks) pdl_launch(k_build_nlist<true, true>, build_grid<true, true>(nb), NB_THREADS, st, d, gated, iter);
-        else pdl_launch(k_build_nlist<true, false>, build_grid<true, false>(d.ncell), NB_THREADS, st, d, gated, iter);
-    } else {
-        if (d.build_blocks) pdl_launch(k_build_nlist<false, true>, build_grid<false, true>(nb), NB_THREADS, st, d, gated, iter);
-        else pdl_launch(k_build_nlist<false, false>, build_grid<false, false>(d.ncell), NB_THREADS, st, d, gated, iter);
+    const int nw = d.build_blocks ? nb : d.ncell;
+    switch ((d.potential_flag == 1 ? 4 : 0) + (d.build_blocks ? 2 : 0) + (d.tile ? 1 : 0)) {
+    case 0: launch_build_t<false, false, false>(d, nw, gated, iter, st); break;
+    case 1: launch_build_t<false, false, true>(d, nw, gated, iter, st); break;
+    case 2: launch_build_t<false, true, false>(d, nw, gated, iter, st); break;
+    case 3: launch_build_t<false, true, true>(d, nw, gated, iter, st); break;
+    case 4: launch_build_t<true, false, false>(d, nw, gated, iter, st); break;
+    case 5: launch_build_t<true, false, true>(d, nw, gated, iter, st); break;
+    case 6: launch_build_t<true, true, false>(d, nw, gated, iter, st); break;
+    default: launch_build_t<true, true, true>(d, nw, gated, iter, st); break;
     }
+}
+
+void launch_blk_seg(const FmDev &d, int gated, int iter, cudaStream_t st)
+{
+    pdl_launch(k_blk_seg, sgrid(d.tile_nblk, BS_THREADS / 32, 8), BS_THREADS, st, d, gated, iter);
+}
+
+// Staging capacity of the tiled force kernel: list entries are 16-bit byte
+// offsets into the staging, so it holds at most tile_ucap_max(R) candidates
+// (2720 for x y z, 2016 with w) plus the dummy -- at most ~64 KB.
+constexpr int TILE_SMEM_MAX = 232448 - 4096;
+int tile_ucap_limit(int R) { return tile_ucap_max(R); }
+size_t tile_smem_bytes(const FmDev &d) { return (size_t)tile_stage_doubles(d.tile_ucap, d.tile_R) * 8; }
+
+template <int T, bool REC, int MODE, int PREC>
+static void launch_force_tile_k(const FmDev &d, cudaStream_t st)
+{
+    auto k = k_force_tile<T, REC, MODE, PREC>;
+    static size_t smem_set = 0;
+    static int grid_for = -1, grid = 0;
+    const size_t smem = tile_smem_bytes(d);
+    if (smem_set == 0) {
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, TILE_SMEM_MAX);
+        smem_set = 1;
+    }
+    if (grid_for != (int)smem) {  // resident CTAs at this staging size
+        int dev = 0, nsm = kSMs, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, FT_THREADS, smem);
+        grid = std::max(nsm, 1) * std::max(per_sm, 1);
+        grid_for = (int)smem;
+    }
+    pdl_launch_smem(k, std::min(grid, d.tile_nblk), FT_THREADS, smem, st, d);
+}
+
+template <int T>
+static void launch_force_tile(const FmDev &d, int record, int mode, cudaStream_t st)
+{
+#define FM_TILE_CASE(R, M)                                                          \
+    if (record == R && mode == M) {                                                 \
+        switch (d.precision + 2 * d.mie + 4 * d.solvent) {                          \
+        case 0: launch_force_tile_k<T, R, M, 0>(d, st); break;                      \
+        case 1: launch_force_tile_k<T, R, M, 1>(d, st); break;                      \
+        case 2: launch_force_tile_k<T, R, M, 2>(d, st); break;                      \
+        case 3: launch_force_tile_k<T, R, M, 3>(d, st); break;                      \
+        case 4: launch_force_tile_k<T, R, M, 4>(d, st); break;                      \
+        default: launch_force_tile_k<T, R, M, 5>(d, st); break;                     \
+        }                                                                           \
+        return;                                                                     \
+    }
+    FM_TILE_CASE(0, 0) FM_TILE_CASE(0, 1) FM_TILE_CASE(0, 2) FM_TILE_CASE(0, 3)
+    FM_TILE_CASE(1, 0) FM_TILE_CASE(1, 1) FM_TILE_CASE(1, 2) FM_TILE_CASE(1, 3)
+#undef FM_TILE_CASE
+}
+
+void launch_tile_to_generic(const FmDev &d, int32_t *out, int maxn, cudaStream_t st)
+{
+    k_tile_to_generic<<<nblk(d.n, 128), 128, 0, st>>>(d, out, maxn);
 }
 
 int force_blocks(int n, int tpm) { return nblk(n * tpm, FORCE_THREADS); }
@@ -1187,6 +1573,11 @@ static void launch_force_tpm(const FmDev &d, int record, int mode, cudaStream_t 
 
 void launch_force(const FmDev &d, int record, int mode, int tpm, cudaStream_t st)
 {
+    if (d.tile) {
+        if (d.tile_T == 4) launch_force_tile<4>(d, record, mode, st);
+        else launch_force_tile<8>(d, record, mode, st);
+        return;
+    }
     switch (tpm) {
     case 1: launch_force_tpm<1>(d, record, mode, st); break;
     case 2: launch_force_tpm<2>(d, record, mode, st); break;

@@ -80,6 +80,8 @@ typedef struct fm_params {
     int32_t list_build;           /* FM_LIST_BUILD_*: one warp per cell or per 2x2x2 cells (same rows) */
     int32_t solvent_flag;         /* SOLVENT_INFO with potential_flag 1: 0 all beads alike (WCA + bonds),
                                      1 Soddemann solvent of variable quality (force_list 3 only) */
+    int32_t force_path;           /* FM_FORCE_PATH_*: how the neighbour-list force kernel reads partners
+                                     (same pairs and results to FP64 rounding; only the speed differs) */
     double eps_pp, eps_ps, eps_ss; /* SOLVENT_INFO well depths: polymer-polymer, polymer-solvent,
                                       solvent-solvent (solvent_flag 1) */
 } fm_params;
@@ -88,6 +90,15 @@ typedef struct fm_params {
  * cell), one warp per cell, one warp per block of 2x2x2 cells.  The rows are
  * identical; only the speed differs. */
 enum { FM_LIST_BUILD_AUTO = 0, FM_LIST_BUILD_CELLS = 1, FM_LIST_BUILD_BLOCKS = 2 };
+
+/* Force kernel of the neighbour-list modes: automatic (the gather kernel),
+ * one gather per list entry with threads_per_molecule lanes, or tiles -- one
+ * CTA per block of 2x2x2 cells stages the block's 4x4x4-cell neighbourhood
+ * (periodic images applied) in shared memory and the list holds 16-bit
+ * offsets into that staging (half the list memory), read by
+ * threads_per_molecule (4 or 8) lanes per molecule.  A handle on tiles leaves
+ * them for the gather kernel when a neighbourhood outgrows the staging. */
+enum { FM_FORCE_PATH_AUTO = 0, FM_FORCE_PATH_GATHER = 1, FM_FORCE_PATH_TILES = 2 };
 
 /* Macroscopic properties of one record step, the columns of
  * results/macroscopic_properties (parallel_io.MPI2.f90:4589-4646) plus the
@@ -273,6 +284,11 @@ FM_API int fm_get_pair_list(fm_handle *h, int32_t *owner, int32_t *partner, int8
 FM_API int fm_pair_digest(fm_handle *h, uint64_t *digest, int64_t *npairs);
 /* Force-kernel lanes per molecule in use (fixed, or chosen by the autotuner at fm_setup). */
 FM_API int fm_get_threads_per_molecule(fm_handle *h, int32_t *tpm);
+/* Force kernel in use (FM_FORCE_PATH_GATHER or FM_FORCE_PATH_TILES; a handle
+ * leaves the tiled path when a staged neighbourhood outgrows shared memory),
+ * and the staged-candidate capacity of a block on the tiled path (0 otherwise).
+ * No counterpart in the reference: a diagnostic of this implementation. */
+FM_API int fm_get_force_path(fm_handle *h, int32_t *path, int32_t *tile_capacity);
 /* Counters: rebuilds done, neighbour capacity in use, largest list seen. */
 FM_API int fm_get_counters(fm_handle *h, int64_t *rebuilds, int32_t *nlist_capacity, int32_t *max_neighbours);
 

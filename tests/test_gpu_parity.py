@@ -746,3 +746,133 @@ def test_list_build_cells_equals_blocks(gpu_lib, case):
         o.set_monomers(mono[0], mono[1], mono[3], mono[2])
     o.setup()
     assert np.array_equal(canonical_full(*b), canonical_oracle(*o.pair_list()))
+
+
+# ---------------------------------------------------------------------------
+# The two force kernels of the neighbour-list modes: one gather per list entry
+# (FORCE_PATH_GATHER, the automatic choice, which the tests above run) and the
+# tiled kernel (FORCE_PATH_TILES: the block's neighbourhood staged in shared
+# memory, 16-bit offsets in the rows).  These pin both explicitly.
+# ---------------------------------------------------------------------------
+
+@pytest.mark.parametrize("prec", [api.PRECISION_FP64, api.PRECISION_FP32], ids=["fp64", "fp32"])
+@pytest.mark.parametrize("path,tpm", [(api.FORCE_PATH_GATHER, 0), (api.FORCE_PATH_TILES, 4),
+                                      (api.FORCE_PATH_TILES, 8)], ids=["gather", "tiles4", "tiles8"])
+def test_force_paths_pairs_forces_energies(liquid, prec, path, tpm):
+    r, v, dom = liquid
+    o = O.Oracle(r, v, dom, 2.5, tplot=1, density=0.8442)
+    o.setup()
+    s = gpu_system(r, v, dom, 2.5, precision=prec, tplot=1, density=0.8442, force_path=path,
+                   threads_per_molecule=tpm)
+    s.setup()
+    assert s.force_path()[0] == path
+    assert np.array_equal(canonical_full(*s.pair_list()), canonical_oracle(*o.pair_list()))
+    _, _, a, _ = s.download()
+    pe, vir = s.per_molecule()
+    if prec == api.PRECISION_FP64:
+        assert rel_err(a, o.a, 1.0).max() <= TOL64
+        np.testing.assert_allclose(pe, o.potenergymol, rtol=TOL64, atol=TOL64)
+        np.testing.assert_allclose(vir, o.virialmol, rtol=TOL64, atol=TOL64)
+    else:
+        assert rel_err(a, o.a, F_FLOOR32).max() <= TOL32
+        assert (np.abs(pe - o.potenergymol) / np.maximum(np.abs(o.potenergymol), 1.0)).max() <= TOL32
+        assert (np.abs(vir - o.virialmol) / np.maximum(np.abs(o.virialmol), W_FLOOR32)).max() <= TOL32
+    m = s.records()[-1]
+    mo = o.macro()
+    tol = 1e-12 if prec == api.PRECISION_FP64 else TOL32
+    for k in ("kinenergy", "potenergy", "pressure", "virial"):
+        assert m[k] == pytest.approx(mo[k], rel=tol, abs=tol), k
+    s.close()
+
+
+def test_tiled_and_gather_trajectories_agree(liquid):
+    """300 velocity-Verlet steps with rebuilds and records: the tiled kernel
+    and the per-entry gather kernel sum the same pairs (in different orders),
+    so positions agree to 1e-9 and the records to 1e-10; the rebuild schedule
+    is identical."""
+    r, v, dom = liquid
+    runs = []
+    for path in (api.FORCE_PATH_GATHER, api.FORCE_PATH_TILES):
+        s = gpu_system(r, v, dom, 2.5, tplot=50, density=0.8442, force_path=path)
+        s.setup()
+        s.records()
+        s.simulation_md(300)
+        runs.append((s.download(), s.records(), s.counters()["rebuilds"]))
+        s.close()
+    (ra, va, _, _), reca, nra = runs[0]
+    (rb, vb, _, _), recb, nrb = runs[1]
+    assert nra == nrb and nra > 0
+    np.testing.assert_allclose(rb, ra, rtol=0, atol=1e-9)
+    np.testing.assert_allclose(vb, va, rtol=0, atol=1e-9)
+    assert len(reca) == len(recb)
+    for x, y in zip(reca, recb):
+        assert x["iter"] == y["iter"]
+        assert y["totenergy"] == pytest.approx(x["totenergy"], rel=1e-10)
+        assert y["pressure"] == pytest.approx(x["pressure"], rel=1e-9)
+
+
+def test_tiled_staging_grows_then_leaves_tiles(gpu_lib):
+    """A dense cube (rho 1.5, 10,976 molecules) in a dilute box with rc 4.5:
+    the staging capacity estimated from the mean density is too small (the
+    first build raises the staging overflow and the host grows it), and a
+    block whose 4x4x4 cells lie inside the cube holds ~10,600 candidates --
+    more than shared memory takes -- so the handle leaves the tiled path for
+    the gather path.  Pair set and forces still match the oracle."""
+    rc = 4.5
+    rr, _, _ = lattice.lj_fluid([14, 14, 14], 1.5, 1.0, 81)
+    dom = np.array([38.4, 38.4, 38.4])
+    rr = rr - rr.mean(axis=0)
+    rng = np.random.default_rng(81)
+    v = rng.normal(0.0, 1.0, rr.shape)
+    o = O.Oracle(rr, v, dom, rc, tplot=1)
+    o.setup()
+    s = gpu_system(rr, v, dom, rc, tplot=1, force_path=api.FORCE_PATH_TILES)
+    assert s.force_path()[0] == api.FORCE_PATH_TILES
+    s.setup()
+    assert s.force_path()[0] == api.FORCE_PATH_GATHER
+    assert np.array_equal(canonical_full(*s.pair_list()), canonical_oracle(*o.pair_list()))
+    _, _, a, _ = s.download()
+    assert rel_err(a, o.a, 1.0).max() <= TOL64
+    s.close()
+
+
+def test_tiled_staging_grows_on_a_liquid_vapour_slab(gpu_lib):
+    """Liquid and vapour in one box (a liquid slab at rho 0.8 filling a third
+    of the box, vapour elsewhere): the capacity estimated from the mean
+    density is below the slab's neighbourhoods, so the first build grows it;
+    the handle stays on the tiled path and matches the oracle."""
+    rl, _, doml = lattice.lj_fluid([8, 8, 8], 0.8, 1.0, 82)
+    dom = np.array([3.0 * doml[0], doml[1], doml[2]])
+    rl = lattice.jitter(rl, 0.03, 82, doml)
+    rng = np.random.default_rng(82)
+    v = rng.normal(0.0, 0.8, rl.shape)
+    s = gpu_system(rl, v, dom, 2.5, tplot=1, force_path=api.FORCE_PATH_TILES)
+    cap0 = s.force_path()[1]
+    s.setup()
+    path, cap = s.force_path()
+    assert path == api.FORCE_PATH_TILES and cap > cap0
+    o = O.Oracle(rl, v, dom, 2.5, tplot=1)
+    o.setup()
+    assert np.array_equal(canonical_full(*s.pair_list()), canonical_oracle(*o.pair_list()))
+    _, _, a, _ = s.download()
+    assert rel_err(a, o.a, 1.0).max() <= TOL64
+    s.close()
+
+
+def test_tiled_nlist_overflow_is_resized_and_resumed(liquid):
+    """A tiled handle whose rows overflow is grown and resumed from the
+    failing iteration, bit for bit as a run with enough capacity."""
+    r, v, dom = liquid
+    runs = []
+    for cap in (0, 8):
+        s = gpu_system(r, v, dom, 2.5, tplot=25, density=0.8442, nlist_capacity=cap,
+                       force_path=api.FORCE_PATH_TILES, threads_per_molecule=4)
+        s.setup()
+        s.simulation_md(80)
+        assert s.force_path()[0] == api.FORCE_PATH_TILES
+        runs.append((s.download(), s.counters()["nlist_capacity"]))
+        s.close()
+    (r1, v1, _, _), _ = runs[0]
+    (r2, v2, _, _), cap2 = runs[1]
+    assert cap2 > 8
+    assert np.array_equal(r1, r2) and np.array_equal(v1, v2)
