@@ -82,7 +82,7 @@ struct CellSys {
 };
 
 // Per-warp shared staging.
-template <bool POLY>
+template <bool POLY, bool TILE = false>
 struct BuildShared {
     float4 f[NB_STAGE];         // x, y, z offsets and the entry bits in w
     alignas(16) float ox[32];   // owners' offsets (+1e30 past the last owner),
@@ -92,8 +92,10 @@ struct BuildShared {
     int2 cs[POLY ? NB_STAGE : 1];  // chain, subchain of candidates
     int off[55];                // candidate offset of segment k (54 segments + total)
     int start[54], code[54];
-    int lbase[54];              // TILE: segment k's first candidate in the block staging
-    unsigned short loc[NB_STAGE];  // TILE: staged candidates' word offsets
+    int lbase[TILE ? 54 : 1];                   // segment k's first candidate in the block staging
+    unsigned short loc[TILE ? NB_STAGE : 1];    // staged candidates' staging offsets
+    alignas(16) int ob[TILE ? 1 : 32][8];       // owner lane's chunk being filled (generic rows)
+    alignas(16) unsigned short ob16[TILE ? 32 : 1][32];  // (tiled rows, 4 T <= 32 entries)
     int ochain[POLY ? 32 : 1];
     alignas(16) int4 obf[POLY ? 32 : 1];
     unsigned hits[POLY ? 1 : 32];  // per owner: which of the 32 candidates hit (polymers: registers)
@@ -145,11 +147,64 @@ __device__ __forceinline__ bool exact_pair(const double4 *P, int io, int e, cons
     return norm2_rn(__dsub_rn(po.x, xj), __dsub_rn(po.y, yj), __dsub_rn(po.z, zj)) < rn2;
 }
 
+// Appends entry cnt (< maxn) of the owner (slot i) of this lane: into the
+// lane's chunk buffer, and the chunk to the row once it is full, so that every
+// sector of the row is written whole.  Generic rows: a chunk is 8 entries
+// (32 bytes) at nb_col(8c).  Tiled rows: a chunk is the 4 T entries of one load
+// of the owner's T lanes, contiguous at tile_pos16(4Tc), entry k at place
+// (k % T) 4 + (k / T) % 4 of it.
+template <bool TILE, typename SH>
+__device__ __forceinline__ void append_entry(SH &sh, int lane, int T, int32_t *nbr, uint16_t *row16, int i,
+                                             int maxn, int cnt, int ent, unsigned short loc)
+{
+    if (TILE) {
+        const int ch = 4 * T, k = cnt % ch;
+        sh.ob16[lane][(k % T) * 4 + (k / T) % 4] = loc;
+        if (k == ch - 1) {
+            const uint4 *src = reinterpret_cast<const uint4 *>(sh.ob16[lane]);
+            uint4 *dst = reinterpret_cast<uint4 *>(row16 + (cnt - k));
+            for (int q = 0; q < ch / 8; q++) dst[q] = src[q];
+        }
+    } else {
+        sh.ob[lane][cnt & 7] = ent;
+        if ((cnt & 7) == 7) {
+            const int4 *src = reinterpret_cast<const int4 *>(sh.ob[lane]);
+            int4 *dst = reinterpret_cast<int4 *>(nbr + nb_row(i, maxn) + nb_col(cnt & ~7));
+            dst[0] = src[0];
+            dst[1] = src[1];
+        }
+    }
+}
+
+// Writes the owner's last, partial chunk (cnt entries in all, cnt < maxn; the
+// chunk lies inside the row because maxn is a whole number of chunks).  Tiled
+// rows are padded with the dummy candidate up to the chunk's end, the force
+// kernel's last load; generic rows leave the places past cnt unread.
+template <bool TILE, typename SH>
+__device__ __forceinline__ void flush_entries(SH &sh, int lane, int T, int32_t *nbr, uint16_t *row16, int i,
+                                              int maxn, int cnt, int dummy)
+{
+    if (TILE) {
+        const int ch = 4 * T, k0 = cnt % ch;
+        if (k0 == 0) return;
+        for (int k = k0; k < ch; k++) sh.ob16[lane][(k % T) * 4 + (k / T) % 4] = (unsigned short)dummy;
+        const uint4 *src = reinterpret_cast<const uint4 *>(sh.ob16[lane]);
+        uint4 *dst = reinterpret_cast<uint4 *>(row16 + (cnt - k0));
+        for (int q = 0; q < ch / 8; q++) dst[q] = src[q];
+    } else {
+        if ((cnt & 7) == 0) return;
+        const int4 *src = reinterpret_cast<const int4 *>(sh.ob[lane]);
+        int4 *dst = reinterpret_cast<int4 *>(nbr + nb_row(i, maxn) + nb_col(cnt & ~7));
+        dst[0] = src[0];
+        dst[1] = src[1];
+    }
+}
+
 // Rows of every molecule of cell c (0-based extended index) of system y, by
 // one warp.  Returns BUILD_OVER_* bits when a row or a bond set overflowed
 // (the counts past the capacity are still reported through max_nbr).
 template <bool POLY, bool TILE = false>
-__device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY> &sh, int lane)
+__device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY, TILE> &sh, int lane)
 {
     const int ne0 = y.ne[0], ne1 = y.ne[1], ne2 = y.ne[2];
     const int cstart = y.cell_start[c] - y.mol_off;
@@ -244,7 +299,6 @@ __device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY> &sh, i
         const float by0 = warp_min(yif), by1 = warp_max(yif);
         const float bz0 = warp_min(zif), bz1 = warp_max(zif);
         int cnt = 0, nb = 0;  // the owner lane's list and bond counts
-        int32_t *const row = TILE ? nullptr : y.nbr + nb_row(i, maxn);
         uint16_t *const row16 = TILE ? y.nbr16 + tile_row16(i, maxn) : nullptr;
         const int self_e = i | (NB_NOSHIFT << NB_SHIFT_BITS);  // the owner's own entry
         const int nown = min(32, ccount - pass * 32);
@@ -372,7 +426,8 @@ __device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY> &sh, i
                         nb += addb;
                     }
                 }
-                // the owner lane appends its hits in candidate order, all but itself
+                // the owner lane appends its hits in candidate order, all but
+                // itself, through its chunk buffer (whole sectors to the row)
                 if (!POLY) __syncwarp();
                 unsigned mine_hits = POLY ? mine_reg : (lane < nown ? sh.hits[lane] : 0u);
                 while (mine_hits) {
@@ -380,20 +435,15 @@ __device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY> &sh, i
                     mine_hits &= mine_hits - 1u;
                     const int ent = __float_as_int(sh.f[t0 + b].w);
                     if (POLY || ent != self_e) {
-                        if (cnt < maxn) {
-                            if (TILE) row16[tile_pos16(cnt, y.tT)] = sh.loc[t0 + b];
-                            else row[nb_col(cnt)] = ent;
-                        }
+                        if (cnt < maxn) append_entry<TILE>(sh, lane, y.tT, y.nbr, row16, i, maxn, cnt, ent,
+                                                           TILE ? sh.loc[t0 + b] : (unsigned short)0);
                         cnt++;
                     }
                 }
                 if (!POLY) __syncwarp();
             }
         }
-        if (TILE && own) {  // pad the last load of the row with the dummy candidate
-            const int lim = min((cnt + 4 * y.tT - 1) / (4 * y.tT) * (4 * y.tT), maxn);
-            for (int k = cnt; k < lim; k++) row16[tile_pos16(k, y.tT)] = (uint16_t)y.tdummy;
-        }
+        if (own && cnt < maxn) flush_entries<TILE>(sh, lane, y.tT, y.nbr, row16, i, maxn, cnt, y.tdummy);
         if (own) {
             y.nnbr[i] = cnt < maxn ? cnt : maxn;
             atomicMax(y.max_nbr, cnt);
@@ -420,7 +470,7 @@ __device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY> &sh, i
 
 constexpr int NB_BSEG = 128;  // 64 union cells x (real, images)
 
-template <bool POLY>
+template <bool POLY, bool TILE = false>
 struct BlockShared {
     float4 f[NB_STAGE];             // candidate offsets from the block centre, entry bits in w
     alignas(16) float ox[32];       // owners (+1e30 past the last owner)
@@ -432,8 +482,10 @@ struct BlockShared {
     int2 cs[POLY ? NB_STAGE : 1];
     int off[NB_BSEG + 1];
     int start[NB_BSEG], code[NB_BSEG];
-    int lbase[NB_BSEG];             // TILE: segment k's first candidate in the block staging
-    unsigned short loc[NB_STAGE];   // TILE: staged candidates' word offsets
+    int lbase[TILE ? NB_BSEG : 1];               // segment k's first candidate in the block staging
+    unsigned short loc[TILE ? NB_STAGE : 1];     // staged candidates' staging offsets
+    alignas(16) int ob[TILE ? 1 : 32][8];        // owner lane's chunk being filled (generic rows)
+    alignas(16) unsigned short ob16[TILE ? 32 : 1][32];  // (tiled rows, 4 T <= 32 entries)
     unsigned char segallow[NB_BSEG];
     int opre[9], ostart[8];         // owners by block cell: prefix counts, first molecule
     int ochain[POLY ? 32 : 1];
@@ -442,7 +494,7 @@ struct BlockShared {
 };
 
 template <bool POLY, bool TILE = false>
-__device__ uint32_t build_block(const CellSys &y, int blk, BlockShared<POLY> &sh, int lane)
+__device__ uint32_t build_block(const CellSys &y, int blk, BlockShared<POLY, TILE> &sh, int lane)
 {
     const int ne0 = y.ne[0], ne1 = y.ne[1], ne2 = y.ne[2];
     const int nb0 = (ne0 + 1) / 2, nb1 = (ne1 + 1) / 2;
@@ -575,7 +627,6 @@ __device__ uint32_t build_block(const CellSys &y, int blk, BlockShared<POLY> &sh
         const float by_lo = warp_min(own ? yif : 3e38f), by_hi = warp_max(own ? yif : -3e38f);
         const float bz_lo = warp_min(own ? zif : 3e38f), bz_hi = warp_max(own ? zif : -3e38f);
         int cnt = 0, nb = 0;
-        int32_t *const row = TILE ? nullptr : y.nbr + nb_row(i, maxn);
         uint16_t *const row16 = TILE ? y.nbr16 + tile_row16(i, maxn) : nullptr;
         const int self_e = i | (NB_NOSHIFT << NB_SHIFT_BITS);  // the owner's own entry
         const int nown = min(32, nowners - pass * 32);
@@ -700,6 +751,8 @@ __device__ uint32_t build_block(const CellSys &y, int blk, BlockShared<POLY> &sh
                         nb += addb;
                     }
                 }
+                // the owner lane appends its hits in candidate order, all but
+                // itself, through its chunk buffer (whole sectors to the row)
                 if (!POLY) __syncwarp();
                 unsigned mine_hits = POLY ? mine_reg : (lane < nown ? sh.hits[lane] : 0u);
                 while (mine_hits) {
@@ -707,20 +760,15 @@ __device__ uint32_t build_block(const CellSys &y, int blk, BlockShared<POLY> &sh
                     mine_hits &= mine_hits - 1u;
                     const int ent = __float_as_int(sh.f[t0 + b].w);
                     if (POLY || ent != self_e) {
-                        if (cnt < maxn) {
-                            if (TILE) row16[tile_pos16(cnt, y.tT)] = sh.loc[t0 + b];
-                            else row[nb_col(cnt)] = ent;
-                        }
+                        if (cnt < maxn) append_entry<TILE>(sh, lane, y.tT, y.nbr, row16, i, maxn, cnt, ent,
+                                                           TILE ? sh.loc[t0 + b] : (unsigned short)0);
                         cnt++;
                     }
                 }
                 if (!POLY) __syncwarp();
             }
         }
-        if (TILE && own) {  // pad the last load of the row with the dummy candidate
-            const int lim = min((cnt + 4 * y.tT - 1) / (4 * y.tT) * (4 * y.tT), maxn);
-            for (int k = cnt; k < lim; k++) row16[tile_pos16(k, y.tT)] = (uint16_t)y.tdummy;
-        }
+        if (own && cnt < maxn) flush_entries<TILE>(sh, lane, y.tT, y.nbr, row16, i, maxn, cnt, y.tdummy);
         if (own) {
             y.nnbr[i] = cnt < maxn ? cnt : maxn;
             atomicMax(y.max_nbr, cnt);

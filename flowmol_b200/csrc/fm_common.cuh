@@ -161,15 +161,18 @@ constexpr int32_t NB_INDEX_MASK = (1 << NB_SHIFT_BITS) - 1;
 constexpr int MAX_MOLECULES = NB_INDEX_MASK;
 
 // Neighbour list layout: molecules in groups of 32, each molecule's entries
-// in chunks of 4; chunk c of the 32 molecules of a group is one contiguous
-// 512-byte block (molecule i%32 at offset 16 (i%32) bytes), so a warp that
-// reads chunk c of its 32 molecules with 16-byte loads reads one segment.
-// The array holds ceil(n/32)*32 rows of maxn (a multiple of 8) entries.
+// in chunks of 8 (one 32-byte sector); chunk c of the 32 molecules of a group
+// is one contiguous 1 KB block (molecule i%32 at offset 32 (i%32) bytes), so a
+// warp that reads a 16-byte half of chunk c of its 32 molecules reads 32
+// sectors of one block, and the list build writes each sector whole (a
+// sector shared by two molecules written at different times would reach
+// DRAM half-written once the list outgrows L2).  The array holds
+// ceil(n/32)*32 rows of maxn (a multiple of 8) entries.
 __host__ __device__ inline size_t nb_row(int i, int maxn)
 {
-    return (size_t)(i >> 5) * (size_t)maxn * 32u + (size_t)(i & 31) * 4u;
+    return (size_t)(i >> 5) * (size_t)maxn * 32u + (size_t)(i & 31) * 8u;
 }
-__host__ __device__ inline size_t nb_col(int k) { return (size_t)(k & ~3) * 32u + (size_t)(k & 3); }
+__host__ __device__ inline size_t nb_col(int k) { return (size_t)(k & ~7) * 32u + (size_t)(k & 7); }
 inline size_t nb_rows(int n) { return ((size_t)n + 31u) / 32u * 32u; }
 
 // Sets the message fm_last_error returns on this thread (fm_api.cu).

@@ -585,7 +585,7 @@ __global__ void __launch_bounds__(EF_THREADS, REC ? 2 : 4) k_e_force(EngDev d)
             const int32_t *L = d.nbr + s.list_off + nb_row(i - s.mol_off, s.maxn);
             const double4 *Pj = P + s.mol_off;
             for (int k0 = lane * 4; k0 < cnt; k0 += 4 * TPM) {
-                const int4 e4 = ld_stream_int4(reinterpret_cast<const int4 *>(L + (size_t)k0 * 32));
+                const int4 e4 = ld_stream_int4(reinterpret_cast<const int4 *>(L + nb_col(k0)));
                 const int ev[4] = {e4.x, e4.y, e4.z, e4.w};
                 double4 pj[4];
 #pragma unroll

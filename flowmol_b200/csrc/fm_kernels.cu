@@ -475,8 +475,10 @@ __global__ void __launch_bounds__(NB_THREADS, 8) k_build_nlist(FmDev d, int gate
     pdl_enter();
     if (!gate(d, gated)) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    using Shared = typename std::conditional<BLOCKS, BlockShared<POLY>, BuildShared<POLY>>::type;
-    __shared__ Shared sh[NB_WARPS];
+    using Shared = typename std::conditional<BLOCKS, BlockShared<POLY, TILE>, BuildShared<POLY, TILE>>::type;
+    // per-warp staging in dynamic shared memory (the largest variants pass 48 KB)
+    extern __shared__ __align__(16) unsigned char build_smem[];
+    Shared *sh = reinterpret_cast<Shared *>(build_smem);
     CellSys y;
     y.P = cur_pos(d, d.sc->pset);
     y.cell_start = d.cell_start;
@@ -835,13 +837,13 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force(FmDev d)
     if (active) {
         const double4 pi = P[i];
         const int cnt = d.nnbr[i];
-        const int32_t *__restrict__ L = d.nbr + nb_row(i, d.maxn);  // chunk k0/4 at L + 32 k0 (16-byte aligned)
+        const int32_t *__restrict__ L = d.nbr + nb_row(i, d.maxn);  // entries k0..k0+3 at L + nb_col(k0) (16-byte aligned)
         const double Lx = d.L[0], Ly = d.L[1], Lz = d.L[2];
         const double rc2 = d.rc2;
         // each lane takes 4 consecutive entries per iteration (one 16-byte load)
         // and issues their 4 gathers before any arithmetic
         for (int k0 = lane * 4; k0 < cnt; k0 += 4 * TPM) {
-            const int4 e4 = ld_stream_int4(reinterpret_cast<const int4 *>(L + (size_t)k0 * 32));
+            const int4 e4 = ld_stream_int4(reinterpret_cast<const int4 *>(L + nb_col(k0)));
             const int ev[4] = {e4.x, e4.y, e4.z, e4.w};
             double4 pj[4];
 #pragma unroll
@@ -1451,6 +1453,13 @@ void launch_reorder(const FmDev &d, int gated, double4 *tpos, int32_t *tuidx, cu
 // The list build walks the cells grid-stride with every block resident (one
 // wave: a second partial wave would double the kernel's time).
 template <bool POLY, bool BLOCKS, bool TILE>
+static size_t build_smem_bytes()
+{
+    using Shared = typename std::conditional<BLOCKS, BlockShared<POLY, TILE>, BuildShared<POLY, TILE>>::type;
+    return sizeof(Shared) * NB_WARPS;
+}
+
+template <bool POLY, bool BLOCKS, bool TILE>
 static int build_grid(int nwork)
 {
     static int resident = 0;
@@ -1458,7 +1467,10 @@ static int build_grid(int nwork)
         int dev = 0, nsm = kSMs, per_sm = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_build_nlist<POLY, BLOCKS, TILE>, NB_THREADS, 0);
+        cudaFuncSetAttribute(k_build_nlist<POLY, BLOCKS, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)build_smem_bytes<POLY, BLOCKS, TILE>());
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_build_nlist<POLY, BLOCKS, TILE>, NB_THREADS,
+                                                      build_smem_bytes<POLY, BLOCKS, TILE>());
         resident = std::max(nsm, 1) * std::max(per_sm, 1);
     }
     return std::min(nblk(nwork, NB_WARPS), resident);
@@ -1467,8 +1479,9 @@ static int build_grid(int nwork)
 template <bool POLY, bool BLOCKS, bool TILE>
 static void launch_build_t(const FmDev &d, int nwork, int gated, int iter, cudaStream_t st)
 {
-    pdl_launch(k_build_nlist<POLY, BLOCKS, TILE>, build_grid<POLY, BLOCKS, TILE>(nwork), NB_THREADS, st, d, gated,
-               iter);
+    const int g = build_grid<POLY, BLOCKS, TILE>(nwork);  // (sets the kernel's shared-memory attribute once)
+    pdl_launch_smem(k_build_nlist<POLY, BLOCKS, TILE>, g, NB_THREADS, build_smem_bytes<POLY, BLOCKS, TILE>(), st, d,
+                    gated, iter);
 }
 
 void launch_build_nlist(const FmDev &d, int gated, int iter, cudaStream_t st)
