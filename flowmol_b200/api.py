@@ -195,6 +195,7 @@ def lib():
             "fm_move_lfv": [h],
             "fm_upload_monomers": [h, P(C.c_int32), P(C.c_int32), P(C.c_int32)],
             "fm_set_mie": [h, P(FmMieTables), P(C.c_int32)],
+            "fm_set_angular": [h, C.c_int32, P(C.c_double), P(C.c_double), P(C.c_int32)],
             "fm_get_bonds": [h, P(C.c_int32), P(C.c_int32), P(C.c_int8), C.c_int64, P(C.c_int64)],
             "fm_update_borders": [h, C.c_int32],
             "fm_check_rebuild": [h, P(C.c_int32)],
@@ -390,6 +391,18 @@ class MDSystem:
             setattr(t, k, a.ctypes.data_as(C.POINTER(C.c_double)))
         mt = np.ascontiguousarray(moltype, np.int32)
         check(lib().fm_set_mie(self.h, C.byref(t), mt.ctypes.data_as(C.POINTER(C.c_int32))))
+
+    def set_angular(self, k, theta0, funcy):
+        """angular_potential 1 (fm_set_angular): k and theta0 as (ntypes,
+        ntypes, ntypes) arrays indexed [i-1, j-1, k-1] -- the reference's
+        angular_k_lookup and angular_r0_lookup -- and funcy per molecule in
+        upload order.  After set_mie(), before setup()."""
+        kk = np.ascontiguousarray(np.asarray(k, np.float64).transpose(2, 1, 0)).reshape(-1)  # (i,j,k) at i+nt(j+nt k)
+        tt = np.ascontiguousarray(np.asarray(theta0, np.float64).transpose(2, 1, 0)).reshape(-1)
+        fy = np.ascontiguousarray(funcy, np.int32)
+        self._ang_keep = (kk, tt, fy)
+        check(lib().fm_set_angular(self.h, int(np.asarray(k).shape[0]), _dp(kk), _dp(tt),
+                                   fy.ctypes.data_as(C.POINTER(C.c_int32))))
 
     def bonds(self):
         n = C.c_int64()

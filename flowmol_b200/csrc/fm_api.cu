@@ -166,7 +166,7 @@ static void release(fm_handle *h)
                     d.pe, d.vir, d.partial, d.rec, d.sc, h->tpos, h->tuidx, h->glob, h->stage3, d.chain,
                     d.subchain, d.bflag, d.tchain, d.tsubchain, d.tbflag, d.bnd, d.nbond,
                     (void *)d.mie_pair, (void *)d.mie_mass, (void *)d.mie_type_up, d.rdx, d.rdy, d.rdz, d.rf6,
-                    d.blk_off, d.nbr16};
+                    d.blk_off, d.nbr16, (void *)d.ang_k, (void *)d.ang_t0, d.funcy, d.tfuncy};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     d = FmDev{};
@@ -241,6 +241,7 @@ static void queue_build(fm_handle *h, int gated, int iter)
 {
     if (h->d.tile) { fm::launch_blk_seg(h->d, gated, iter, h->st); h->launches += 1; }
     fm::launch_build_nlist(h->d, gated, iter, h->st);
+    if (h->d.angular) { fm::launch_angular_order(h->d, gated, iter, h->st); h->launches += 1; }
 }
 
 extern "C" int fm_create(const fm_params *p, fm_handle **out)
@@ -511,6 +512,49 @@ extern "C" int fm_upload_monomers(fm_handle *h, const int32_t *chainID, const in
 
 static int ready(fm_handle *h, int min_stage);
 
+extern "C" int fm_set_angular(fm_handle *h, int32_t ntypes, const double *k_lookup, const double *theta0_lookup,
+                              const int32_t *funcy)
+{
+    if (!h || !k_lookup || !theta0_lookup || !funcy) return fail(FM_ERR_ARG, "null argument");
+    if (h->stage != 1) return fail(FM_ERR_STATE, "set the angular tables after fm_set_mie and before fm_setup");
+    const fm_params &p = h->p;
+    if (p.force_list != 3 || p.potential_flag != 1 || p.solvent_flag != 0)
+        return fail(FM_ERR_ARG, "angular_potential needs force_list 3, potential_flag 1 and solvent_flag 0 "
+                                "(simulation_compute_forces.f90:257-259)");
+    FmDev &d = h->d;
+    if (!d.mie) return fail(FM_ERR_STATE, "angular_potential looks up the Mie types: call fm_set_mie first");
+    if (ntypes < 1 || ntypes > FM_MIE_MAXTYPES) return fail(FM_ERR_ARG, "ntypes out of range (1 .. FM_MIE_MAXTYPES)");
+    const size_t n3 = (size_t)ntypes * ntypes * ntypes, n = (size_t)d.n;
+    for (size_t u = 0; u < n; u++)
+        if (funcy[u] < 0 || funcy[u] > 4) return fail(FM_ERR_ARG, "funcy out of range (0 .. 4)");
+    if (!d.funcy) {
+        FM_TRY(dalloc(&d.funcy, n));
+        FM_TRY(dalloc(&d.tfuncy, n));
+        double *k = nullptr, *t = nullptr;
+        FM_TRY(dalloc(&k, (size_t)FM_MIE_MAXTYPES * FM_MIE_MAXTYPES * FM_MIE_MAXTYPES));
+        d.ang_k = k;
+        FM_TRY(dalloc(&t, (size_t)FM_MIE_MAXTYPES * FM_MIE_MAXTYPES * FM_MIE_MAXTYPES));
+        d.ang_t0 = t;
+    }
+    int32_t *fu = nullptr;
+    FM_TRY(dalloc(&fu, n));
+    cudaError_t ce = cudaMemcpyAsync(fu, funcy, sizeof(int32_t) * n, cudaMemcpyHostToDevice, h->st);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpyAsync((void *)d.ang_k, k_lookup, sizeof(double) * n3, cudaMemcpyHostToDevice, h->st);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpyAsync((void *)d.ang_t0, theta0_lookup, sizeof(double) * n3, cudaMemcpyHostToDevice, h->st);
+    if (ce == cudaSuccess) {
+        fm::launch_set_funcy(d, fu, h->st);  // slots still equal upload indices before the first binning
+        ce = cudaGetLastError();
+    }
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->st);
+    cudaFree(fu);
+    FM_CUDA(ce);
+    d.ang_nt = ntypes;
+    d.angular = 1;
+    return FM_OK;
+}
+
 extern "C" int fm_set_mie(fm_handle *h, const fm_mie_tables *t, const int32_t *moltype)
 {
     if (!h || !t || !moltype) return fail(FM_ERR_ARG, "null argument");
@@ -653,6 +697,13 @@ static int status_error(fm_handle *h, const fm::FmScalars &s)
     }
     if (s.status & fm::ST_BOND) {
         std::snprintf(buf, sizeof buf, "polymer bond beyond R_0 at iteration %d", s.fail_iter);
+        h->stage = 3;
+        return fail(FM_ERR_BOND, buf);
+    }
+    if (s.status & fm::ST_ANGLE) {
+        std::snprintf(buf, sizeof buf,
+                      "angular triple without a defined result (a middle bead without both bonds, or "
+                      "k_ijk < 1e-5) at iteration %d", s.fail_iter);
         h->stage = 3;
         return fail(FM_ERR_BOND, buf);
     }

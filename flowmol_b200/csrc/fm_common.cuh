@@ -16,7 +16,8 @@ enum : uint32_t {
     ST_PE = 1u << 2,        // per-molecule PE above 10000 on a record step
     ST_BOND = 1u << 3,      // FENE bond at or beyond R_0
     ST_TILE = 1u << 4,      // a block's staged neighbourhood exceeded the tiled force kernel's capacity
-    ST_FATAL = ST_ESCAPE | ST_NLIST | ST_PE | ST_BOND | ST_TILE,
+    ST_ANGLE = 1u << 5,     // angular triple with no defined result (missing bond, k_ijk < 1e-5)
+    ST_FATAL = ST_ESCAPE | ST_NLIST | ST_PE | ST_BOND | ST_TILE | ST_ANGLE,
 };
 
 // Device-resident scalars of the step loop (one per system).
@@ -142,6 +143,14 @@ struct FmDev {
     int solvent;
     double sod_eps[3];
     int mie;
+    // angular_potential (simulation_compute_forces_angular): k and theta_0 by
+    // the Mie types of a triple, [(ti-1) + nt ((tj-1) + nt (tk-1))]; funcy by
+    // slot (reordered with the chains); bonds of a middle bead (funcy 2)
+    // ordered as the reference discovers them (bnd[4 j] is its i, bnd[4 j + 1]
+    // its k)
+    int angular, ang_nt;
+    const double *ang_k, *ang_t0;
+    int32_t *funcy, *tfuncy;
     const FmMiePair *mie_pair;   // [(ti-1) + MIE_MAXT*(tj-1)]
     const double *mie_mass;      // [ti-1]
     const int32_t *mie_type_up;  // moltype by upload index (written into w at upload)
@@ -194,6 +203,10 @@ void launch_scan_cells(const FmDev &d, int gated, cudaStream_t st);
 void launch_scatter(const FmDev &d, int gated, cudaStream_t st);
 void launch_reorder(const FmDev &d, int gated, double4 *tpos, int32_t *tuidx, cudaStream_t st);
 void launch_build_nlist(const FmDev &d, int gated, int iter, cudaStream_t st);
+// angular_potential: orders each middle bead's two bonds as the reference's
+// list build discovers them (after every build).
+void launch_angular_order(const FmDev &d, int gated, int iter, cudaStream_t st);
+void launch_set_funcy(const FmDev &d, const int32_t *funcy_up, cudaStream_t st);
 // Tiled path: the staging segment table of every block (before the build).
 void launch_blk_seg(const FmDev &d, int gated, int iter, cudaStream_t st);
 size_t tile_smem_bytes(const FmDev &d);

@@ -400,6 +400,7 @@ __global__ void k_reorder_gather(FmDev d, int gated, double4 *tpos, int32_t *tui
         tuidx[s] = d.slot_of[o];
         if (d.potential_flag == 1) {
             d.tchain[s] = d.chain[o]; d.tsubchain[s] = d.subchain[o]; d.tbflag[s] = d.bflag[o];
+            if (d.funcy) d.tfuncy[s] = d.funcy[o];
         }
     }
 }
@@ -416,6 +417,7 @@ __global__ void k_reorder_copy(FmDev d, int gated, const double4 *tpos, const in
         d.slot_of[s] = tuidx[s];
         if (d.potential_flag == 1) {
             d.chain[s] = d.tchain[s]; d.subchain[s] = d.tsubchain[s]; d.bflag[s] = d.tbflag[s];
+            if (d.funcy) d.funcy[s] = d.tfuncy[s];
         }
     }
 }
@@ -779,6 +781,164 @@ __device__ __forceinline__ void fene_bonds(const FmDev &d, const double4 *P, int
     }
 }
 
+// ---------------------------------------------------------------------------
+// angular_potential (simulation_compute_forces_angular,
+// simulation_compute_forces.f90:981-1048; angular_harmonic_force,
+// setup_set_parameters.f90:441-489)
+// ---------------------------------------------------------------------------
+
+// The reference's triple of middle bead j: i = its first bond, k = its second
+// (in discovery order), rij = r_i - r_j, rjk = r_j - r_k with the partners'
+// periodic images (x_src +/- L, one rounding), theta = acos(rij.rjk /
+// (|rij| |rjk|)) and
+//   aForce(1) = -(k (theta - theta_0) / (|rij| sin theta)) (rjk/|rjk| - rij/|rij| cos theta)
+//   aForce(3) = -(k (theta - theta_0) / (|rjk| sin theta)) (rij/|rij| - rjk/|rjk| cos theta)
+//   aForce(2) = -aForce(1) - aForce(3)   (all zero when theta < 1e-5);
+// the reference then subtracts aForce(1), (2), (3) from the forces on i, j,
+// k.  Every molecule evaluates the triples it belongs to in the middle
+// bead's frame, so the three see the same numbers.  k_ijk < 1e-5 leaves the
+// reference's result unset: ST_ANGLE.
+__device__ __forceinline__ bool angular_triple(const FmDev &d, const double4 *P, int j, double (&f1)[3],
+                                               double (&f3)[3])
+{
+    const int e0 = d.bnd[(size_t)j * 4], e1 = d.bnd[(size_t)j * 4 + 1];
+    const double4 pj = P[j], pi = P[e0 & NB_INDEX_MASK], pk = P[e1 & NB_INDEX_MASK];
+    const int c0 = e0 >> NB_SHIFT_BITS, c1 = e1 >> NB_SHIFT_BITS;
+    const double ri[3] = {image(pi.x, (c0 & 3) - 1, d.L[0]), image(pi.y, ((c0 >> 2) & 3) - 1, d.L[1]),
+                          image(pi.z, ((c0 >> 4) & 3) - 1, d.L[2])};
+    const double rk[3] = {image(pk.x, (c1 & 3) - 1, d.L[0]), image(pk.y, ((c1 >> 2) & 3) - 1, d.L[1]),
+                          image(pk.z, ((c1 >> 4) & 3) - 1, d.L[2])};
+    const double rj[3] = {pj.x, pj.y, pj.z};
+    const int nt = d.ang_nt;
+    const int q = ((int)pi.w - 1) + nt * (((int)pj.w - 1) + nt * ((int)pk.w - 1));
+    const double kk = d.ang_k[q], t0 = d.ang_t0[q];
+    f1[0] = f1[1] = f1[2] = 0.0;
+    f3[0] = f3[1] = f3[2] = 0.0;
+    if (kk < 1e-5) return false;
+    double rij[3], rjk[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) { rij[c] = __dsub_rn(ri[c], rj[c]); rjk[c] = __dsub_rn(rj[c], rk[c]); }
+    const double mij = sqrt(norm2_rn(rij[0], rij[1], rij[2]));
+    const double mjk = sqrt(norm2_rn(rjk[0], rjk[1], rjk[2]));
+    const double dot = __dadd_rn(__dadd_rn(__dmul_rn(rij[0], rjk[0]), __dmul_rn(rij[1], rjk[1])),
+                                 __dmul_rn(rij[2], rjk[2]));
+    const double th = acos(dot / (mij * mjk));
+    if (th < 1e-5) return true;
+    const double ct = cos(th), stt = sin(th);
+    const double a1 = kk * (th - t0) / (mij * stt), a3 = kk * (th - t0) / (mjk * stt);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        f1[c] = -a1 * (rjk[c] / mjk - rij[c] / mij * ct);
+        f3[c] = -a3 * (rij[c] / mij - rjk[c] / mjk * ct);
+    }
+    return true;
+}
+
+// The angular forces on molecule m (added to its force sum before the
+// division by its mass): -aForce(2) of its own triple when it is a middle
+// bead, and -aForce(1) or -aForce(3) of each bonded middle bead's triple in
+// which it is the bead i or k.
+__device__ __forceinline__ void angular_forces(const FmDev &d, const double4 *P, int m, double &fx, double &fy,
+                                               double &fz)
+{
+    double f1[3], f3[3];
+    bool ok = true;
+    if (d.funcy[m] == 2) {
+        ok &= angular_triple(d, P, m, f1, f3);
+        fx += f1[0] + f3[0]; fy += f1[1] + f3[1]; fz += f1[2] + f3[2];  // -aForce(2)
+    }
+    const int nb = d.nbond[m];
+    for (int b = 0; b < nb; b++) {
+        const int e = d.bnd[(size_t)m * 4 + b];
+        const int p = e & NB_INDEX_MASK;
+        if (d.funcy[p] != 2) continue;
+        const int c = e >> NB_SHIFT_BITS;  // m as p sees it: the opposite image
+        const int back = m | (((2 - (c & 3)) | ((2 - ((c >> 2) & 3)) << 2) | ((2 - ((c >> 4) & 3)) << 4))
+                              << NB_SHIFT_BITS);
+        ok &= angular_triple(d, P, p, f1, f3);
+        if (d.bnd[(size_t)p * 4] == back) { fx -= f1[0]; fy -= f1[1]; fz -= f1[2]; }
+        else if (d.bnd[(size_t)p * 4 + 1] == back) { fx -= f3[0]; fy -= f3[1]; fz -= f3[2]; }
+        else ok = false;
+    }
+    if (!ok) {
+        uint32_t old = atomicOr(&d.sc->status, ST_ANGLE);
+        if ((old & ST_FATAL) == 0u) d.sc->fail_iter = -3;
+    }
+}
+
+// Discovery key of the bond (j, entry) in the reference's list build
+// (assign_to_neighbourlist_halfint_opt, linklist.f90:660-804, where
+// check_update_adjacentbeadinfo appends each bonded pair to both rows as it is
+// met): interior cells in (x, y, z) loop order with z fastest; in each cell
+// first the in-cell pairs (list order, the later member after the earlier),
+// then the 13 forward shifts (shift, owner, partner); the cells' lists are in
+// decreasing molecule number (head insertion, assign_to_cell loops 1..np).
+// A pair across the periodic boundary is met only in the halo sweeps that
+// follow (:778-802): after every interior pair, ordered here by the partner's
+// molecule number.
+__device__ int ang_cell_of(const FmDev &d, int s)
+{
+    int lo = 0, hi = d.ncell - 1;  // largest c with cell_start[c] <= s
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (d.cell_start[mid] <= s) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+__device__ int ang_list_pos(const FmDev &d, int c, int s)
+{
+    const int me = d.slot_of[s];
+    int pos = 0;
+    for (int t = d.cell_start[c]; t < d.cell_start[c + 1]; t++) pos += d.slot_of[t] > me ? 1 : 0;
+    return pos;
+}
+__device__ unsigned long long ang_key(const FmDev &d, int j, int e)
+{
+    const int p = e & NB_INDEX_MASK, code = e >> NB_SHIFT_BITS;
+    if (code != NB_NOSHIFT) return (1ull << 62) | (unsigned long long)d.slot_of[p];
+    const int SX[13] = {1, 1, 0, -1, 0, 1, 1, 0, -1, -1, -1, 0, 1};  // the 13 forward shifts (:686-688)
+    const int SY[13] = {0, 1, 1, 1, 0, 0, 1, 1, 1, 0, -1, -1, -1};
+    const int SZ[13] = {0, 0, 0, 0, 1, 1, 1, 1, 1, 1, 1, 1, 1};
+    const int cj = ang_cell_of(d, j), cp = ang_cell_of(d, p);
+    const int ne0 = d.ne[0], ne1 = d.ne[1];
+    const int jx = cj % ne0, jy = (cj / ne0) % ne1, jz = cj / (ne0 * ne1);
+    const int px = cp % ne0, py = (cp / ne0) % ne1, pz = cp / (ne0 * ne1);
+    const int pj = ang_list_pos(d, cj, j), pp = ang_list_pos(d, cp, p);
+    int oc = cj, sub = 0, pa = min(pj, pp), pb = max(pj, pp);
+    if (cj != cp) {
+        const int dx = px - jx, dy = py - jy, dz = pz - jz;
+        for (int k = 0; k < 13; k++) {
+            if (SX[k] == dx && SY[k] == dy && SZ[k] == dz) { oc = cj; sub = 1 + k; pa = pj; pb = pp; }
+            if (SX[k] == -dx && SY[k] == -dy && SZ[k] == -dz) { oc = cp; sub = 1 + k; pa = pp; pb = pj; }
+        }
+    }
+    const int ox = oc % ne0, oy = (oc / ne0) % ne1, oz = oc / (ne0 * ne1);
+    const unsigned long long rank = ((unsigned long long)(ox - 1) * (unsigned)(d.nc[1]) + (unsigned)(oy - 1)) *
+                                        (unsigned)(d.nc[2]) + (unsigned)(oz - 1);
+    return (rank << 34) | ((unsigned long long)sub << 30) | ((unsigned long long)pa << 15) | (unsigned long long)pb;
+}
+
+__global__ void k_angular_order(FmDev d, int gated, int iter)
+{
+    pdl_enter();
+    if (!gate(d, gated)) return;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < d.n; j += gridDim.x * blockDim.x) {
+        if (d.funcy[j] != 2) continue;
+        if (d.nbond[j] != 2) { raise_status(d, ST_ANGLE, iter); continue; }
+        const int e0 = d.bnd[(size_t)j * 4], e1 = d.bnd[(size_t)j * 4 + 1];
+        if (ang_key(d, j, e1) < ang_key(d, j, e0)) {
+            d.bnd[(size_t)j * 4] = e1;
+            d.bnd[(size_t)j * 4 + 1] = e0;
+        }
+    }
+}
+
+__global__ void k_set_funcy(FmDev d, const int32_t *funcy_up)
+{
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u < d.n) d.funcy[u] = funcy_up[u];  // slots still equal upload indices
+}
+
 // (s, c) += (s2, c2): Neumaier merge of two compensated partial sums.
 __device__ __forceinline__ void nmerge(double &s, double &c, double s2, double c2)
 {
@@ -889,6 +1049,9 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force(FmDev d)
     double m2 = 0.0;
     if (active && lane == 0 && d.potential_flag == 1)
         fene_bonds<REC, (PREC & 2) != 0>(d, P, i, fx, fy, fz, pe, vir, rf);
+    if constexpr ((PREC & 2) != 0) {  // angular_potential needs the Mie types
+        if (active && lane == 0 && d.angular) angular_forces(d, P, i, fx, fy, fz);
+    }
     // a(:,i) = sum acc rij / mass (LJ_mass = 1; Mie_mass by type)
     if (active && lane == 0)
         m2 = epilogue<REC, MODE, (PREC & 2) != 0>(d, pset, i, P[i], fx, fy, fz, pe, vir, part, rf);
@@ -1122,6 +1285,9 @@ __global__ void __launch_bounds__(FT_THREADS, REC ? 2 : 4) k_force_tile(FmDev d)
             }
             if (act && sub == 0) {
                 if (d.potential_flag == 1) fene_bonds<REC, MIE>(d, P, i, fx, fy, fz, pe, vir, rf);
+                if constexpr (MIE) {
+                    if (d.angular) angular_forces(d, P, i, fx, fy, fz);
+                }
                 double part[RS_N];
 #pragma unroll
                 for (int q = 0; q < RS_N; q++) part[q] = 0.0;
@@ -1499,6 +1665,16 @@ void launch_build_nlist(const FmDev &d, int gated, int iter, cudaStream_t st)
     case 6: launch_build_t<true, true, false>(d, nw, gated, iter, st); break;
     default: launch_build_t<true, true, true>(d, nw, gated, iter, st); break;
     }
+}
+
+void launch_angular_order(const FmDev &d, int gated, int iter, cudaStream_t st)
+{
+    pdl_launch(k_angular_order, sgrid(d.n, 256, 8), 256, st, d, gated, iter);
+}
+
+void launch_set_funcy(const FmDev &d, const int32_t *funcy_up, cudaStream_t st)
+{
+    k_set_funcy<<<nblk(d.n, 256), 256, 0, st>>>(d, funcy_up);
 }
 
 void launch_blk_seg(const FmDev &d, int gated, int iter, cudaStream_t st)

@@ -187,6 +187,22 @@ typedef struct fm_mie_tables {
     const double *k_harmonic, *r0;      /* k_lookup, r0_lookup (bonds) */
 } fm_mie_tables;
 FM_API int fm_set_mie(fm_handle *h, const fm_mie_tables *t, const int32_t *moltype);
+/* angular_potential 1 (simulation_compute_forces_angular,
+ * simulation_compute_forces.f90:981-1048, called at :257-259 with force_list
+ * 3, potential_flag 1, solvent_flag 0): the bond-angle force of every middle
+ * bead (funcy 2) and its two bonded partners, by the Mie types of the triple.
+ * k_lookup, theta0_lookup: angular_k_lookup and angular_r0_lookup
+ * (setup_set_parameters.f90:890-907), ntypes^3 each, (i,j,k) at
+ * [(i-1) + ntypes*((j-1) + ntypes*(k-1))]; funcy per molecule (monomer%funcy).
+ * The force is the reference's angular_harmonic_force (:441-489) with its i
+ * and k in the order the reference's list build discovers the middle bead's
+ * bonds, computed in the middle bead's frame (periodic images as the halo
+ * copies form them) and applied to the three molecules.  No energy is
+ * recorded (the reference records none).  Where the reference has no defined
+ * result the step fails with FM_ERR_BOND: a middle bead without both bonds, or
+ * a triple whose k_ijk < 1e-5.  After fm_set_mie, before fm_setup. */
+FM_API int fm_set_angular(fm_handle *h, int32_t ntypes, const double *k_lookup, const double *theta0_lookup,
+                          const int32_t *funcy);
 /* Bonds of the last list build as (owner glob_no, partner glob_no, image
  * code) triplets, like fm_get_pair_list.  Test hook. */
 FM_API int fm_get_bonds(fm_handle *h, int32_t *owner, int32_t *partner, int8_t *code, int64_t cap, int64_t *n);

@@ -93,6 +93,10 @@ typedef struct orc {
     int *moltype;
     double mie_mass[16], mie_eps[256], mie_lr[256], mie_la[256], mie_C[256], mie_alpha[256], mie_shift[256],
         mie_k[256], mie_r0[256];
+    /* angular_potential: angular_k_lookup / angular_r0_lookup (ntypes^3,
+     * (i,j,k) at [(i-1) + ang_nt*((j-1) + ang_nt*(k-1))]) */
+    int angular, ang_nt;
+    double *ang_k, *ang_t0;
     double vsum, mv2sum, potenergysum, virial;
     double kinenergy, potenergy, totenergy, temperature, pressure;
     int rebuild_count;
@@ -320,6 +324,7 @@ void orc_free(orc *s)
     free(s->chainID); free(s->subchainID); free(s->funcy); free(s->bflag); free(s->bond);
     free(s->bondcount);
     free(s->tag); free(s->rtether); free(s->slidev); free(s->rfmol); free(s->moltype);
+    free(s->ang_k); free(s->ang_t0);
     free(s->cellnp); free(s->cellhead); free(s->cn_molno); free(s->cn_next);
     free(s->Nlist); free(s->nhead); free(s->nn_molno); free(s->nn_next);
     free(s);
@@ -1070,6 +1075,80 @@ static int forces_poly(orc *s)
     return ORC_OK;
 }
 
+/* simulation_compute_forces_angular (simulation_compute_forces.f90:981-1048)
+ * with angular_harmonic_force (setup_set_parameters.f90:441-489), for every
+ * real middle bead j (funcy 2): i = bond(1,j), k = bond(2,j) in the order the
+ * list build discovered the bonds (a cross-boundary partner is its halo
+ * image), rij = r_i - r_j, rjk = r_j - r_k, theta = acos(rij.rjk/(|rij||rjk|)),
+ *   aForce(1) = -(k (theta - theta_0) / (|rij| sin theta)) (rjk/|rjk| - rij/|rij| cos theta)
+ *   aForce(3) = -(k (theta - theta_0) / (|rjk| sin theta)) (rij/|rij| - rjk/|rjk| cos theta)
+ *   aForce(2) = -aForce(1) - aForce(3), zero when theta < 1e-5,
+ * and a(i) -= aForce(1)/m_i, a(j) -= aForce(2)/m_j, a(k) -= aForce(3)/m_k
+ * (the rows of halo images are not returned).  No energy is recorded.
+ * Where the reference has no defined result this returns ORC_ERR_BOND: a
+ * middle bead without both bonds (its fallbacks read bond(3:4) or a stale
+ * index), a triple whose k_ijk < 1e-5 (the function returns its result
+ * unset), and a middle bead that has a halo image (the reference also loops
+ * over halo beads, whose bond rows hold only the partners found from interior
+ * cells). */
+static int forces_angular(orc *s)
+{
+    const int nt = s->ang_nt;
+    for (int n = s->np + 1; n <= s->np + s->halo_np; n++)
+        if (s->funcy[s->halo_src[n - 1] - 1] == 2) return ORC_ERR_BOND;
+    for (int j = 1; j <= s->np; j++) {
+        if (s->funcy[j - 1] != 2) continue;
+        const int i = s->bond[(size_t)(j - 1) * s->max_funcy + 0];
+        const int k = s->bond[(size_t)(j - 1) * s->max_funcy + 1];
+        if (i == 0 || k == 0) return ORC_ERR_BOND;
+        const int q = (type_of(s, i) - 1) + nt * ((type_of(s, j) - 1) + nt * (type_of(s, k) - 1));
+        const double kk = s->ang_k[q], t0 = s->ang_t0[q];
+        if (kk < 1e-5) return ORC_ERR_BOND;
+        const double *ri = &s->r[3 * (size_t)(i - 1)], *rj = &s->r[3 * (size_t)(j - 1)],
+                     *rk = &s->r[3 * (size_t)(k - 1)];
+        double rij[3], rjk[3];
+        for (int c = 0; c < 3; c++) { rij[c] = ri[c] - rj[c]; rjk[c] = rj[c] - rk[c]; }
+        const double mag_ij = sqrt(rij[0] * rij[0] + rij[1] * rij[1] + rij[2] * rij[2]);
+        const double mag_jk = sqrt(rjk[0] * rjk[0] + rjk[1] * rjk[1] + rjk[2] * rjk[2]);
+        const double th = acos((rij[0] * rjk[0] + rij[1] * rjk[1] + rij[2] * rjk[2]) / (mag_ij * mag_jk));
+        double f1[3] = {0.0, 0.0, 0.0}, f3[3] = {0.0, 0.0, 0.0}, f2[3];
+        if (!(th < 1e-5)) {
+            const double ct = cos(th), st = sin(th);
+            const double c1 = kk * (th - t0) / (mag_ij * st), c3 = kk * (th - t0) / (mag_jk * st);
+            for (int c = 0; c < 3; c++) {
+                f1[c] = -c1 * (rjk[c] / mag_jk - rij[c] / mag_ij * ct);
+                f3[c] = -c3 * (rij[c] / mag_ij - rjk[c] / mag_jk * ct);
+            }
+        }
+        for (int c = 0; c < 3; c++) f2[c] = -f1[c] - f3[c];
+        const double mi = mass_of(s, i), mj = mass_of(s, j), mk = mass_of(s, k);
+        double *ai = &s->a[3 * (size_t)(i - 1)], *aj = &s->a[3 * (size_t)(j - 1)], *ak = &s->a[3 * (size_t)(k - 1)];
+        for (int c = 0; c < 3; c++) {
+            ai[c] = ai[c] - f1[c] / mi;
+            aj[c] = aj[c] - f2[c] / mj;
+            ak[c] = ak[c] - f3[c] / mk;
+        }
+    }
+    return ORC_OK;
+}
+
+/* angular_potential on (simulation_compute_forces.f90:257-259: force_list 3,
+ * potential_flag 1, solvent_flag 0); the types are the Mie moltypes. */
+int orc_set_angular(orc *s, int ntypes, const double *k, const double *theta0)
+{
+    if (!s->mie || ntypes < 1 || ntypes > MIET) return ORC_ERR_PARAM;
+    if (s->force_list != 3 || s->potential_flag != 1 || s->solvent_flag != 0) return ORC_ERR_PARAM;
+    size_t n3 = (size_t)ntypes * ntypes * ntypes;
+    free(s->ang_k); free(s->ang_t0);
+    s->ang_k = (double *)xcalloc(n3, sizeof(double));
+    s->ang_t0 = (double *)xcalloc(n3, sizeof(double));
+    memcpy(s->ang_k, k, n3 * sizeof(double));
+    memcpy(s->ang_t0, theta0, n3 * sizeof(double));
+    s->ang_nt = ntypes;
+    s->angular = 1;
+    return ORC_OK;
+}
+
 /* simulation_compute_forces dispatcher (:182-275). */
 int orc_compute_forces(orc *s)
 {
@@ -1087,6 +1166,7 @@ int orc_compute_forces(orc *s)
         int rc = forces_poly(s);
         if (rc) return rc;
         for (int n = 0; n < s->np + s->halo_np; n++) s->potenergymol[n] += s->potenergymol_POLY[n];
+        if (s->angular && s->force_list == 3 && s->solvent_flag == 0 && (rc = forces_angular(s))) return rc;
     }
     return ORC_OK;
 }

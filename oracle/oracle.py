@@ -84,6 +84,8 @@ def lib():
         L.orc_set_monomers.argtypes = [C.c_void_p, i3, i3, i3, i3]
         d8 = C.POINTER(C.c_double)
         L.orc_set_mie.argtypes = [C.c_void_p, C.c_int] + [d8] * 9 + [i3]
+        L.orc_set_angular.restype = C.c_int
+        L.orc_set_angular.argtypes = [C.c_void_p, C.c_int, d8, d8]
         L.orc_set_tags.argtypes = [C.c_void_p, C.c_int, i3, d3, d3, C.c_double, C.c_double, C.c_double, C.c_int,
                                    C.c_double, C.c_double]
         L.orc_set_pressure.argtypes = [C.c_void_p, C.c_int]
@@ -210,6 +212,15 @@ class Oracle:
             keep.append(np.ascontiguousarray(np.asarray(tables[k], np.float64).T).reshape(-1))  # (i,j) at i + nt*j
         mt = np.ascontiguousarray(moltype, np.int32)
         _check(lib().orc_set_mie(self.h, nt, *[_dp(a) for a in keep], _ip(mt)))
+
+    def set_angular(self, k, theta0):
+        """angular_potential on: k and theta0 as (ntypes, ntypes, ntypes)
+        arrays indexed [i-1, j-1, k-1] (angular_k_lookup, angular_r0_lookup).
+        After set_mie(), before setup()."""
+        kk = np.ascontiguousarray(np.asarray(k, np.float64).transpose(2, 1, 0)).reshape(-1)  # (i,j,k) at i+nt(j+nt k)
+        tt = np.ascontiguousarray(np.asarray(theta0, np.float64).transpose(2, 1, 0)).reshape(-1)
+        self._ang = (kk, tt)
+        _check(lib().orc_set_angular(self.h, int(np.asarray(k).shape[0]), _dp(kk), _dp(tt)))
 
     @property
     def potenergymol(self):

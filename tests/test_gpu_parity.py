@@ -876,3 +876,67 @@ def test_tiled_nlist_overflow_is_resized_and_resumed(liquid):
     (r2, v2, _, _), cap2 = runs[1]
     assert cap2 > 8
     assert np.array_equal(r1, r2) and np.array_equal(v1, v2)
+
+
+def _angular_melt():
+    """A bead-spring melt (512 chains of 8, rho 0.85) whose chains with any bead
+    within 2.2 cells of a box face are turned to solvent, so no bead of an
+    angular triple has a halo image (where the reference's routine reads
+    incomplete halo bond rows); types alternate along a chain (1, 2, 1, 2, ...;
+    solvent 1), masses 1 and 1.5, harmonic bonds (Mie_potential 1)."""
+    from flowmol_b200 import polymer
+    from helpers import mie_tables
+    r, v, ch, sub, fy, bf, dom = polymer.fene_melt(512)
+    _, nc, cs, _ = O.cells(dom, WCA_RC, (0.3, 0.3, 0.3), potential_flag=1, R_0=1.5)
+    lim = 0.5 * dom - 2.2 * cs
+    near = np.any(np.abs(r) > lim, axis=1)
+    drop = np.unique(ch[near])
+    ch, sub, fy, bf = polymer.mark_solvent(ch, sub, fy, bf, drop)
+    mt = np.where((ch != 0) & (sub % 2 == 0), 2, 1).astype(np.int32)
+    tab = mie_tables(WCA_RC, np.ones((2, 2)), np.full((2, 2), 12.0), np.full((2, 2), 6.0), [1.0, 1.5],
+                     k=np.full((2, 2), 295.3322), r0=np.ones((2, 2)))
+    kk = np.zeros((2, 2, 2)); tt = np.zeros((2, 2, 2))
+    kk[0, 1, 0], tt[0, 1, 0] = 4.3196, 2.7751
+    kk[1, 0, 1], tt[1, 0, 1] = 3.1, 2.5
+    return r, v, ch, sub, fy, bf, dom, mt, tab, kk, tt
+
+
+def test_angular_potential_forces_and_trajectory(gpu_lib):
+    """angular_potential 1 on interior chains: the angular forces with the
+    reference's i/k roles (its bond discovery order), forces to 1e-12 and
+    positions to 1e-9 after 100 velocity-Verlet steps against the oracle."""
+    r, v, ch, sub, fy, bf, dom, mt, tab, kk, tt = _angular_melt()
+    assert np.sum(fy == 2) > 300  # enough middle beads left
+    o = O.Oracle(r, v, dom, WCA_RC, tplot=20, potential_flag=1, k_c=30.0, R_0=1.5, density=0.85)
+    o.set_monomers(ch, sub, fy, bf)
+    o.set_mie(tab, mt)
+    o.set_angular(kk, tt)
+    o.setup()
+    s = gpu_system(r, v, dom, WCA_RC, tplot=20, density=0.85, potential_flag=1, k_c=30.0, R_0=1.5)
+    s.upload_monomers(ch, sub, bf)
+    s.set_mie(tab, mt)
+    s.set_angular(kk, tt, fy)
+    s.setup()
+    _, _, a, _ = s.download()
+    assert rel_err(a, o.a, 1.0).max() <= TOL64
+    o.run_vv(100)
+    s.simulation_md(100)
+    rg, vg, _, _ = s.download()
+    np.testing.assert_allclose(rg, o.r, rtol=0, atol=1e-9)
+    np.testing.assert_allclose(vg, o.v, rtol=0, atol=1e-9)
+    s.close()
+
+
+def test_angular_potential_without_constants_is_an_error(gpu_lib):
+    """A triple whose k_ijk < 1e-5 (the reference returns an unset result):
+    FM_ERR_BOND."""
+    r, v, ch, sub, fy, bf, dom, mt, tab, kk, tt = _angular_melt()
+    kk[1, 0, 1] = 0.0
+    s = gpu_system(r, v, dom, WCA_RC, tplot=20, density=0.85, potential_flag=1, k_c=30.0, R_0=1.5)
+    s.upload_monomers(ch, sub, bf)
+    s.set_mie(tab, mt)
+    s.set_angular(kk, tt, fy)
+    with pytest.raises(api.FlowmolError) as e:
+        s.setup()
+    assert e.value.code == 8  # FM_ERR_BOND
+    s.close()

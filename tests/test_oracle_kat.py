@@ -297,3 +297,93 @@ def test_pressure_tensor_sampling_follows_the_reference_routines():
     vnew = o0.v
     kin = np.einsum("ni,nj->ij", vnew, vnew) / np.prod(dom)
     np.testing.assert_allclose(p0, kin, rtol=1e-12, atol=1e-15)
+
+
+def _trimer_oracle(angular, k=4.3196, t0=2.7751, kz=0.0):
+    """A lone trimer (chain 1: beads 1-2-3, the middle one funcy 2) in the
+    middle of a periodic box, Mie 12-6 types 1-2-1 with masses 1 and 1.5,
+    harmonic bonds; the angle between the bonds ~150 degrees."""
+    from helpers import mie_tables
+    from flowmol_b200 import polymer
+    r = np.array([[-0.95, 0.05, 0.0], [0.0, 0.0, 0.02], [0.82, 0.47, -0.1]])
+    v = np.zeros_like(r)
+    dom = np.array([10.0, 10.0, 10.0])
+    o = O.Oracle(r, v, dom, WCA_RC, tplot=1, potential_flag=1, k_c=30.0, R_0=1.5)
+    bf = np.array([polymer.bflag_words([2]), polymer.bflag_words([1, 3]), polymer.bflag_words([2])], np.int32)
+    o.set_monomers([1, 1, 1], [1, 2, 3], [1, 2, 1], bf)
+    tab = mie_tables(WCA_RC, np.ones((2, 2)), np.full((2, 2), 12.0), np.full((2, 2), 6.0), [1.0, 1.5],
+                     k=np.full((2, 2), 295.3322), r0=np.ones((2, 2)))
+    o.set_mie(tab, np.array([1, 2, 1], np.int32))
+    if angular:
+        kk = np.zeros((2, 2, 2)); tt = np.zeros((2, 2, 2))
+        kk[0, 1, 0] = k; tt[0, 1, 0] = t0
+        kk[1, 0, 1] = kz
+        o.set_angular(kk, tt)
+    return o, r
+
+
+def test_angular_force_follows_the_reference_routine():
+    """The oracle's angular term equals a separate restatement of
+    simulation_compute_forces_angular / angular_harmonic_force for a lone
+    trimer, with i and k the middle bead's first and second bond."""
+    import math
+    plain, r = _trimer_oracle(False)
+    plain.setup()
+    o, _ = _trimer_oracle(True)
+    o.setup()
+    da = o.a - plain.a
+    own, par, _code = o.bond_list()
+    row = [int(p) for w, p in zip(own, par) if w == 2]
+    i, k = row[0] - 1, row[1] - 1
+    j = 1
+    rij = r[i] - r[j]; rjk = r[j] - r[k]
+    mij = math.sqrt(rij @ rij); mjk = math.sqrt(rjk @ rjk)
+    th = math.acos((rij @ rjk) / (mij * mjk))
+    kk, t0 = 4.3196, 2.7751
+    f1 = -(kk * (th - t0) / (mij * math.sin(th))) * (rjk / mjk - rij / mij * math.cos(th))
+    f3 = -(kk * (th - t0) / (mjk * math.sin(th))) * (rij / mij - rjk / mjk * math.cos(th))
+    f2 = -f1 - f3
+    mass = {0: 1.0, 1: 1.5, 2: 1.0}
+    want = np.zeros((3, 3))
+    want[i] -= f1 / mass[i]; want[j] -= f2 / mass[j]; want[k] -= f3 / mass[k]
+    np.testing.assert_allclose(da, want, rtol=1e-12, atol=1e-13)
+    assert np.abs(da).max() > 1e-3
+
+
+def test_angular_force_is_not_the_gradient_on_bead_k():
+    """The reference's routine applies -grad U to bead i but +grad U to bead k
+    (U = k/2 (theta - theta_0)^2, theta between rij and rjk), so its angular
+    force is not conservative; the restatement keeps that, and the total
+    force stays zero (the reference's own balance check)."""
+    import math
+    plain, r = _trimer_oracle(False)
+    plain.setup()
+    o, _ = _trimer_oracle(True)
+    o.setup()
+    mass = np.array([1.0, 1.5, 1.0])
+    f = (o.a - plain.a) * mass[:, None]
+    own, par, _code = o.bond_list()
+    row = [int(p) for w, p in zip(own, par) if w == 2]
+    i, k = row[0] - 1, row[1] - 1
+
+    def U(x):
+        rij = x[i] - x[1]; rjk = x[1] - x[k]
+        th = math.acos((rij @ rjk) / math.sqrt((rij @ rij) * (rjk @ rjk)))
+        return 0.5 * 4.3196 * (th - 2.7751) ** 2
+
+    g = np.zeros((3, 3))
+    for a in range(3):
+        for c in range(3):
+            xp = r.copy(); xm = r.copy(); xp[a, c] += 1e-6; xm[a, c] -= 1e-6
+            g[a, c] = (U(xp) - U(xm)) / 2e-6
+    np.testing.assert_allclose(f[i], -g[i], rtol=1e-6, atol=1e-8)
+    np.testing.assert_allclose(f[k], g[k], rtol=1e-6, atol=1e-8)
+    np.testing.assert_allclose(f.sum(axis=0), 0.0, atol=1e-12)
+
+
+def test_angular_undefined_cases_are_errors():
+    """k_ijk < 1e-5 leaves the reference's result unset: an error, not a
+    number."""
+    o, _ = _trimer_oracle(True, k=0.0)
+    with pytest.raises(O.OracleError):
+        o.setup()
