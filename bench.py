@@ -330,6 +330,7 @@ def run_batched(api, torch, dev, nsteps, nrep=256):
     t_batch = time.perf_counter() - t0
     res = e.results()
     c = e.counters()
+    tune_bb = e.tuning()[1]
     bad = [x for x in res if x["status"] != 0]
     e.close()
     plain_steps = min(nsteps, 200)
@@ -362,7 +363,7 @@ def run_batched(api, torch, dev, nsteps, nrep=256):
             "plain_setup_seconds": t_setup, "plain_steps_timed_each": plain_steps,
             "ratio_vs_plain": v_batch / v_plain, "ratio_vs_plain_steps_only": v_batch / v_plain_steps,
             "failed": len(bad), "threads_per_molecule": c["threads_per_molecule"],
-            "gpu_launches": c["launches"],
+            "list_build_blocks_below": tune_bb, "gpu_launches": c["launches"],
             "workload": "256 periodic LJ replicas, N log-uniform 500-32000 (4 n^3 FCC), rho U(0.3,0.9), "
                         "T U(0.7,1.5), rc 2.5, skin 0.3, dt 0.005, VV, FP32 forces; boxes < 3 cells: all pairs"}
 
@@ -436,6 +437,7 @@ def run_served(api, torch, dev, njobs, seed=0x466D6F6C + 5):
     lat = np.array([d["finish_time"] - (t0 + t_arr[d["job_id"] - 1]) for d in done])
     bad = [d for d in done if d["status"] != 0]
     c = e.counters()
+    tune_bb = e.tuning()[1]
     e.close()
     # the same kind of jobs run one at a time (an engine with one slot: a job
     # is admitted when the previous one has finished), on a sample of 64
@@ -455,6 +457,7 @@ def run_served(api, torch, dev, njobs, seed=0x466D6F6C + 5):
             "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
             "arrival_rate_per_s": lam, "probe_service_rate": rate_work, "gpu_busy_frac": busy / t_total,
             "failed": len(bad), "threads_per_molecule": c["threads_per_molecule"],
+            "list_build_blocks_below": tune_bb,
             "workload": "Couette channels (WCA fluid between tethered, thermostatted FCC walls, top wall "
                         "sliding U(0.5,2.0)), N log-uniform 256-65536, 200-2000 steps, leap-frog + tags, "
                         "time-averaged virial pressure tensor, FP32 forces"}

@@ -74,7 +74,7 @@ class FmEngineParams(C.Structure):
     _fields_ = [
         ("max_molecules", C.c_int64), ("max_cells", C.c_int64), ("max_list_entries", C.c_int64),
         ("max_slots", C.c_int32), ("precision", C.c_int32), ("threads_per_molecule", C.c_int32),
-        ("ticks_per_chunk", C.c_int32), ("keep_states", C.c_int32), ("pad_", C.c_int32),
+        ("ticks_per_chunk", C.c_int32), ("keep_states", C.c_int32), ("list_build", C.c_int32),
         ("delta_t", C.c_double),
     ]
 
@@ -87,6 +87,7 @@ class FmMieTables(C.Structure):
 
 LIST_BUILD_AUTO, LIST_BUILD_CELLS, LIST_BUILD_BLOCKS = 0, 1, 2
 FORCE_PATH_AUTO, FORCE_PATH_GATHER, FORCE_PATH_TILES = 0, 1, 2
+LIST_BUILD_AUTO, LIST_BUILD_CELLS, LIST_BUILD_BLOCKS = 0, 1, 2
 MIE_TABLE_KEYS = ("epsilon", "lambdar", "lambdaa", "C", "alpha", "potshift", "k_harmonic", "r0")
 
 
@@ -231,6 +232,7 @@ def lib():
             "fm_engine_take_results": [h, P(FmJobResult), C.c_int32, P(C.c_int32)],
             "fm_engine_job_state": [h, C.c_int64, P(C.c_double), P(C.c_double)],
             "fm_engine_counters": [h, P(C.c_int64), P(C.c_int64), P(C.c_int32), P(C.c_int64)],
+            "fm_engine_tuning": [h, P(C.c_int32), P(C.c_double)],
             "fm_read_final_state": [C.c_char_p, P(FmRestartHeader), C.c_int32, P(C.c_double), P(C.c_double),
                                     P(C.c_int32), P(C.c_double), P(C.c_int32), P(C.c_double), P(C.c_int32),
                                     P(C.c_double)],
@@ -611,7 +613,7 @@ class Engine:
     """Multi-job slot engine (batched replicas, served jobs)."""
 
     def __init__(self, max_molecules, max_cells, max_list_entries, max_slots, delta_t=0.005, precision=0,
-                 threads_per_molecule=0, ticks_per_chunk=20, keep_states=True):
+                 threads_per_molecule=0, ticks_per_chunk=20, keep_states=True, list_build=0):
         p = FmEngineParams()
         p.max_molecules = int(max_molecules)
         p.max_cells = int(max_cells)
@@ -621,6 +623,7 @@ class Engine:
         p.threads_per_molecule = int(threads_per_molecule)
         p.ticks_per_chunk = int(ticks_per_chunk)
         p.keep_states = 1 if keep_states else 0
+        p.list_build = int(list_build)
         p.delta_t = float(delta_t)
         hp = C.c_void_p()
         check(lib().fm_engine_create(C.byref(p), C.byref(hp)))
@@ -676,6 +679,12 @@ class Engine:
         t = C.c_int64(); m = C.c_int64(); tp = C.c_int32(); la = C.c_int64()
         check(lib().fm_engine_counters(self.h, C.byref(t), C.byref(m), C.byref(tp), C.byref(la)))
         return dict(ticks=t.value, molecule_steps=m.value, threads_per_molecule=tp.value, launches=la.value)
+
+    def tuning(self):
+        """(threads per molecule, blocks_below): the autotuner's choices."""
+        tp = C.c_int32(); bb = C.c_double()
+        check(lib().fm_engine_tuning(self.h, C.byref(tp), C.byref(bb)))
+        return tp.value, bb.value
 
 
 def _ip32(a):

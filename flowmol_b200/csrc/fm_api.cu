@@ -85,6 +85,18 @@ struct fm_handle {
     size_t ev_used = 0;
     int64_t launches = 0;
     int expected_nbr = 0;  // (4/3) pi r_n^3 rho, rounded: the autotuner's key
+    int cap = 0;           // molecules the arrays hold: np, or a subdomain's capacity
+    // subdomain of a spatial decomposition (d.dd = 1)
+    fm::DdDev x{};
+    int nranks = 0;
+    bool planned = false;
+    int n_own = 0, n_halo = 0;  // after the last sort: owned molecules and halo copies (d.n = both)
+    int n_kept = 0;             // owned molecules kept by the last classification
+    int n_pending = 0;          // array entries before the sort (old entries + arrivals)
+    int dd_phase = 0;           // rebuild: 0 idle, 1 classified, 2 immigrated, 3 halo counted
+    int32_t *dd_dev = nullptr;  // device block behind x (plan and counters)
+    double *dd_sums = nullptr;  // device [RS_N]
+    std::vector<int32_t> dd_counts;
 };
 
 // ---------------------------------------------------------------------------
@@ -166,11 +178,13 @@ static void release(fm_handle *h)
                     d.pe, d.vir, d.partial, d.rec, d.sc, h->tpos, h->tuidx, h->glob, h->stage3, d.chain,
                     d.subchain, d.bflag, d.tchain, d.tsubchain, d.tbflag, d.bnd, d.nbond,
                     (void *)d.mie_pair, (void *)d.mie_mass, (void *)d.mie_type_up, d.rdx, d.rdy, d.rdz, d.rf6,
-                    d.blk_off, d.nbr16, (void *)d.ang_k, (void *)d.ang_t0, d.funcy, d.tfuncy};
+                    d.blk_off, d.nbr16, (void *)d.ang_k, (void *)d.ang_t0, d.funcy, d.tfuncy, h->dd_dev,
+                    h->dd_sums};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     d = FmDev{};
     h->tpos = nullptr; h->tuidx = nullptr; h->glob = nullptr; h->stage3 = nullptr;
+    h->dd_dev = nullptr; h->dd_sums = nullptr;
 }
 
 static int pick_tpm(const fm_params &p, double expected_full)
@@ -197,7 +211,7 @@ static int alloc_nlist(fm_handle *h, int maxn)
     if (d.nbr) cudaFree(d.nbr);
     d.nbr = nullptr;
     d.maxn = maxn;
-    FM_TRY(dalloc(&d.nbr, fm::nb_rows(d.n) * (size_t)maxn));
+    FM_TRY(dalloc(&d.nbr, fm::nb_rows(h->cap) * (size_t)maxn));
     return FM_OK;
 }
 
@@ -210,7 +224,7 @@ static int alloc_nlist16(fm_handle *h, int maxn)
     if (d.nbr16) cudaFree(d.nbr16);
     d.nbr16 = nullptr;
     d.maxn16 = maxn;
-    FM_TRY(dalloc(&d.nbr16, (size_t)d.n * (size_t)maxn));
+    FM_TRY(dalloc(&d.nbr16, (size_t)h->cap * (size_t)maxn));
     return FM_OK;
 }
 
@@ -244,7 +258,13 @@ static void queue_build(fm_handle *h, int gated, int iter)
     if (h->d.angular) { fm::launch_angular_order(h->d, gated, iter, h->st); h->launches += 1; }
 }
 
-extern "C" int fm_create(const fm_params *p, fm_handle **out)
+// A subdomain's block of the undivided system's cells (fm_dd_create).
+struct DdGeom {
+    int32_t nglob[3], org[3], nloc[3];
+    int32_t capacity;
+};
+
+static int create_impl(const fm_params *p, const DdGeom *g, fm_handle **out)
 {
     if (!p || !out) return fail(FM_ERR_ARG, "null argument");
     *out = nullptr;
@@ -279,19 +299,40 @@ extern "C" int fm_create(const fm_params *p, fm_handle **out)
     double cs[3], rn2, rc2, ps;
     int grc = derive(p, nc, cs, &rn2, &rc2, &ps);
     if (grc != FM_OK && !(grc == FM_ERR_FEWCELLS && p->force_list == 0)) return grc;
+    if (g) {
+        // subdomain: the LJ neighbour-list path with velocity Verlet and rebuild
+        // criteria 0/1, per-entry gather kernel
+        if (p->force_list == 0) return fail(FM_ERR_ARG, "a subdomain needs a neighbour list (force_list 2 or 3)");
+        if (p->potential_flag != 0 || p->solvent_flag != 0)
+            return fail(FM_ERR_ARG, "a subdomain runs the LJ/WCA pair potential (potential_flag 0)");
+        if (p->integration_algorithm != 1) return fail(FM_ERR_ARG, "a subdomain integrates with velocity Verlet");
+        if (p->rebuild_criteria != 0 && p->rebuild_criteria != 1)
+            return fail(FM_ERR_ARG, "a subdomain takes rebuild_criteria 0 (vmax) or 1 (fixed)");
+        if (p->force_path == FM_FORCE_PATH_TILES) return fail(FM_ERR_ARG, "a subdomain uses the gather force path");
+        for (int k = 0; k < 3; k++) {
+            if (g->nglob[k] != nc[k])
+                return fail(FM_ERR_ARG, "ncells_global differs from the cells fm_derive_geometry gives");
+            if (g->nloc[k] < 1 || g->org[k] < 0 || g->org[k] + g->nloc[k] > g->nglob[k])
+                return fail(FM_ERR_ARG, "subdomain cells outside the global grid");
+        }
+        if (g->capacity < 1 || g->capacity > fm::MAX_MOLECULES) return fail(FM_ERR_ARG, "capacity out of range");
+    }
 
     fm_handle *h = new fm_handle();
     h->p = *p;
     FM_CUDA(cudaGetDevice(&h->device));
     FmDev &d = h->d;
-    d.n = p->np;
+    d.n = g ? 0 : p->np;
+    h->cap = g ? g->capacity : p->np;
     for (int k = 0; k < 3; k++) {
         d.L[k] = p->domain[k];
         d.hd[k] = 0.5 * p->domain[k];
         d.cs[k] = cs[k];
-        d.nc[k] = p->force_list == 0 ? 1 : nc[k];
+        d.nc[k] = p->force_list == 0 ? 1 : (g ? g->nloc[k] : nc[k]);
         d.ne[k] = d.nc[k] + 2;
+        if (g) { d.org[k] = g->org[k]; d.gne[k] = g->nglob[k] + 2; }
     }
+    d.dd = g ? 1 : 0;
     d.ncell = d.ne[0] * d.ne[1] * d.ne[2];
     d.rc2 = rc2;
     d.rn2 = rn2;
@@ -325,6 +366,7 @@ extern "C" int fm_create(const fm_params *p, fm_handle **out)
     d.build_blocks = p->list_build == FM_LIST_BUILD_BLOCKS ? 1
                      : p->list_build == FM_LIST_BUILD_CELLS ? 0 : (per_cell < 8.0 ? 1 : 0);
     int tpm = pick_tpm(*p, expected);
+    if (g && p->threads_per_molecule == 0) h->p.threads_per_molecule = tpm;  // every rank the same kernel
     if (tpm < 0) { delete h; return fail(FM_ERR_ARG, "threads_per_molecule must be 0, 1, 2, 4, 8 or 16"); }
     if (p->force_path != FM_FORCE_PATH_AUTO && p->force_path != FM_FORCE_PATH_GATHER &&
         p->force_path != FM_FORCE_PATH_TILES) {
@@ -363,7 +405,7 @@ extern "C" int fm_create(const fm_params *p, fm_handle **out)
     h->expected_nbr = (int)std::lround(expected);
     int maxn = p->nlist_capacity > 0 ? p->nlist_capacity : round_up((int)std::ceil(1.3 * expected) + 16, 8);
 
-    const size_t n = (size_t)d.n;
+    const size_t n = (size_t)h->cap;
     int rc = FM_OK;
 #define FM_ALLOC(ptr, cnt)                                   \
     if (rc == FM_OK) rc = dalloc(&(ptr), (size_t)(cnt));
@@ -384,7 +426,7 @@ extern "C" int fm_create(const fm_params *p, fm_handle **out)
         FM_ALLOC(d.tchain, n) FM_ALLOC(d.tsubchain, n) FM_ALLOC(d.tbflag, n)
         FM_ALLOC(d.bnd, 4 * n) FM_ALLOC(d.nbond, n)
     }
-    int nb = std::max(std::max(fm::force_blocks(d.n, 16), fm::all_pairs_blocks(d.n)), fm::macro_blocks(d.n));
+    int nb = std::max(std::max(fm::force_blocks(h->cap, 16), fm::all_pairs_blocks(h->cap)), fm::macro_blocks(h->cap));
     nb = std::max(nb, d.tile_nblk);
     if (d.tile) { FM_ALLOC(d.blk_off, (size_t)d.tile_nblk * fm::TILE_NSEGP) }
     FM_ALLOC(d.partial, (size_t)nb * fm::RS_N)
@@ -419,6 +461,8 @@ extern "C" int fm_create(const fm_params *p, fm_handle **out)
     return FM_OK;
 }
 
+extern "C" int fm_create(const fm_params *p, fm_handle **out) { return create_impl(p, nullptr, out); }
+
 extern "C" int fm_destroy(fm_handle *h)
 {
     if (!h) return FM_OK;
@@ -442,6 +486,7 @@ extern "C" int fm_set_stream(fm_handle *h, void *stream)
 static int begin_state(fm_handle *h, int32_t n)
 {
     if (!h) return fail(FM_ERR_ARG, "null handle");
+    if (h->d.dd) return fail(FM_ERR_STATE, "a subdomain handle takes its molecules through fm_dd_upload");
     if (n != h->d.n) return fail(FM_ERR_ARG, "n differs from the np the handle was created with");
     h->q.active = false;
     h->cells_valid = false;
@@ -713,6 +758,13 @@ static int status_error(fm_handle *h, const fm::FmScalars &s)
         h->stage = 3;
         return fail(FM_ERR_NLIST, buf);
     }
+    if (s.status & fm::ST_MIGRATE) {
+        std::snprintf(buf, sizeof buf,
+                      "subdomain at iteration %d: a molecule moved beyond the neighbouring subdomains, or more "
+                      "molecules arrived than the capacity holds", s.fail_iter);
+        h->stage = 3;
+        return fail(FM_ERR_ESCAPE, buf);
+    }
     if (s.status & fm::ST_NLIST) {
         std::snprintf(buf, sizeof buf, "neighbour list overflow at iteration %d (%d > %d)", s.fail_iter, s.max_nbr,
                       h->d.tile ? h->d.maxn16 : h->d.maxn);
@@ -887,6 +939,7 @@ static void set_tile_rows(fm_handle *h)
 extern "C" int fm_setup(fm_handle *h)
 {
     if (!h) return fail(FM_ERR_ARG, "null handle");
+    if (h->d.dd) return fail(FM_ERR_STATE, "a subdomain handle is driven by the fm_dd_* calls");
     if (h->stage < 1) return fail(FM_ERR_STATE, "fm_setup before fm_upload_state");
     set_tile_rows(h);
     if (h->p.force_list != 0) {
@@ -1022,6 +1075,7 @@ static int finish_range(fm_handle *h)
 extern "C" int fm_step(fm_handle *h, int32_t nsteps, int32_t blocking)
 {
     if (!h) return fail(FM_ERR_ARG, "null handle");
+    if (h->d.dd) return fail(FM_ERR_STATE, "a subdomain handle is driven by the fm_dd_* calls");
     if (h->stage != 2) return fail(FM_ERR_STATE, "fm_step needs fm_setup (or a failed state was not re-uploaded)");
     if (h->p.force_list != 0 && !(h->cells_valid && h->list_valid))
         return fail(FM_ERR_STATE, "fm_step needs current cell and neighbour lists (call fm_setup)");
@@ -1061,6 +1115,7 @@ extern "C" int fm_sync(fm_handle *h)
 static int ready(fm_handle *h, int min_stage)
 {
     if (!h) return fail(FM_ERR_ARG, "null handle");
+    if (h->d.dd) return fail(FM_ERR_STATE, "a subdomain handle is driven by the fm_dd_* calls");
     if (h->stage == 3) return fail(FM_ERR_STATE, "state is broken; re-upload it");
     if (h->stage < min_stage) return fail(FM_ERR_STATE, "call order: upload, setup, then step");
     if (h->q.active) FM_TRY(finish_range(h));
@@ -1427,5 +1482,449 @@ extern "C" int fm_get_launch_count(fm_handle *h, int64_t *launches)
 {
     if (!h || !launches) return fail(FM_ERR_ARG, "null argument");
     *launches = h->launches;
+    return FM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// spatial decomposition: one rank's subdomain (messenger.MPI.f90)
+//
+// The caller (one process per GPU, or several subdomains in one process)
+// runs the exchanges between the calls: counts and flat record buffers in
+// device memory, rank to rank (an all-to-all).  A rebuild is
+//   fm_dd_classify -> exchange counts -> fm_dd_pack_emigrants -> exchange
+//   -> fm_dd_immigrate -> fm_dd_halo_counts -> exchange counts
+//   -> fm_dd_pack_halo -> exchange -> fm_dd_receive_halo (sort + list build);
+// a step without a rebuild refreshes the halo positions
+// (fm_dd_gather_positions -> exchange -> fm_dd_scatter_positions).
+// ---------------------------------------------------------------------------
+
+extern "C" int fm_dd_create(const fm_params *p, const int32_t ncells_global[3], const int32_t origin[3],
+                            const int32_t ncells_local[3], int32_t capacity, fm_handle **out)
+{
+    if (!ncells_global || !origin || !ncells_local) return fail(FM_ERR_ARG, "null argument");
+    DdGeom g;
+    for (int k = 0; k < 3; k++) { g.nglob[k] = ncells_global[k]; g.org[k] = origin[k]; g.nloc[k] = ncells_local[k]; }
+    g.capacity = capacity;
+    return create_impl(p, &g, out);
+}
+
+static int dd_ready(fm_handle *h, bool planned, int min_stage)
+{
+    if (!h) return fail(FM_ERR_ARG, "null handle");
+    if (!h->d.dd) return fail(FM_ERR_STATE, "not a subdomain handle (fm_dd_create)");
+    if (planned && !h->planned) return fail(FM_ERR_STATE, "fm_dd_set_plan first");
+    if (h->stage == 3) return fail(FM_ERR_STATE, "state is broken; re-upload it");
+    if (h->stage < min_stage) return fail(FM_ERR_STATE, "call order: fm_dd_upload, a rebuild, then forces");
+    return FM_OK;
+}
+
+extern "C" int fm_dd_set_plan(fm_handle *h, int32_t rank, const int32_t dims[3], const int32_t *owner_axis,
+                              const int32_t *need_off, const int32_t *need_rank, const int32_t *need_code,
+                              const int32_t *need_cell)
+{
+    FM_TRY(dd_ready(h, false, 0));
+    if (!dims || !owner_axis || !need_off) return fail(FM_ERR_ARG, "null argument");
+    const FmDev &d = h->d;
+    const int nranks = dims[0] * dims[1] * dims[2];
+    if (dims[0] < 1 || dims[1] < 1 || dims[2] < 1 || rank < 0 || rank >= nranks)
+        return fail(FM_ERR_ARG, "rank outside the process grid");
+    const int G = (d.gne[0] - 2) + (d.gne[1] - 2) + (d.gne[2] - 2);
+    const int nc = d.ncell;
+    for (int k = 0; k < G; k++) {
+        const int ax = k < d.gne[0] - 2 ? 0 : (k < d.gne[0] - 2 + d.gne[1] - 2 ? 1 : 2);
+        if (owner_axis[k] < 0 || owner_axis[k] >= dims[ax]) return fail(FM_ERR_ARG, "owner_axis out of range");
+    }
+    if (need_off[0] != 0) return fail(FM_ERR_ARG, "need_off[0] must be 0");
+    for (int c = 0; c < nc; c++)
+        if (need_off[c + 1] < need_off[c]) return fail(FM_ERR_ARG, "need_off must be non-decreasing");
+    const int nneed = need_off[nc];
+    if (nneed > 0 && (!need_rank || !need_code || !need_cell)) return fail(FM_ERR_ARG, "null argument");
+    for (int k = 0; k < nneed; k++)
+        if (need_rank[k] < 0 || need_rank[k] >= nranks || need_code[k] < 0 || need_code[k] > 63 ||
+            need_cell[k] < 0)
+            return fail(FM_ERR_ARG, "need entries out of range");
+    // one device block: owner_axis | need_off | need_rank | need_code | need_cell
+    //                   | count | offset | cursor | nlist | list_idx | list_aux
+    const size_t total = (size_t)G + (size_t)nc + 1 + 3 * (size_t)nneed + 3 * (size_t)nranks + 1 + 2 * (size_t)h->cap;
+    if (h->dd_dev) cudaFree(h->dd_dev);
+    h->dd_dev = nullptr;
+    FM_TRY(dalloc(&h->dd_dev, total));
+    if (!h->dd_sums) FM_TRY(dalloc(&h->dd_sums, (size_t)fm::RS_N));
+    int32_t *b = h->dd_dev;
+    fm::DdDev &x = h->x;
+    x.rank = rank;
+    for (int k = 0; k < 3; k++) x.dims[k] = dims[k];
+    x.owner_axis = b; b += G;
+    x.need_off = b; b += nc + 1;
+    x.need_rank = b; b += nneed;
+    x.need_code = b; b += nneed;
+    x.need_cell = b; b += nneed;
+    x.count = b; b += nranks;
+    x.offset = b; b += nranks;
+    x.cursor = b; b += nranks;
+    x.nlist = b; b += 1;
+    x.list_idx = b; b += h->cap;
+    x.list_aux = b; b += h->cap;
+    x.list_cap = h->cap;
+    FM_CUDA(cudaMemcpyAsync((void *)x.owner_axis, owner_axis, sizeof(int32_t) * G, cudaMemcpyHostToDevice, h->st));
+    FM_CUDA(cudaMemcpyAsync((void *)x.need_off, need_off, sizeof(int32_t) * (nc + 1), cudaMemcpyHostToDevice, h->st));
+    if (nneed > 0) {
+        FM_CUDA(cudaMemcpyAsync((void *)x.need_rank, need_rank, sizeof(int32_t) * nneed, cudaMemcpyHostToDevice, h->st));
+        FM_CUDA(cudaMemcpyAsync((void *)x.need_code, need_code, sizeof(int32_t) * nneed, cudaMemcpyHostToDevice, h->st));
+        FM_CUDA(cudaMemcpyAsync((void *)x.need_cell, need_cell, sizeof(int32_t) * nneed, cudaMemcpyHostToDevice, h->st));
+    }
+    FM_CUDA(cudaStreamSynchronize(h->st));
+    h->nranks = nranks;
+    h->dd_counts.assign((size_t)nranks, 0);
+    h->planned = true;
+    return FM_OK;
+}
+
+extern "C" int fm_dd_upload(fm_handle *h, int32_t n, const double *r, const double *v, const int32_t *gid)
+{
+    FM_TRY(dd_ready(h, false, 0));
+    if (n < 0 || n > h->cap) return fail(FM_ERR_ARG, "n outside 0 .. capacity");
+    if (n > 0 && (!r || !v || !gid)) return fail(FM_ERR_ARG, "null argument");
+    for (int i = 0; i < n; i++)
+        if (gid[i] < 0 || gid[i] >= fm::MAX_MOLECULES) return fail(FM_ERR_ARG, "global numbers must be 0 .. 2^26-2");
+    FmDev &d = h->d;
+    h->iter = h->p.initialstep;
+    h->simtime = h->p.simtime;
+    fm::launch_reset_scalars(d, h->st);
+    FM_CUDA(cudaMemsetAsync(d.cell_count, 0, sizeof(int32_t) * (size_t)d.ncell, h->st));
+    d.n = n;
+    if (n > 0) {
+        const size_t n3 = 3 * (size_t)n;
+        FM_CUDA(cudaMemcpyAsync(h->stage3, r, sizeof(double) * n3, cudaMemcpyHostToDevice, h->st));
+        FM_CUDA(cudaMemcpyAsync(h->stage3 + n3, v, sizeof(double) * n3, cudaMemcpyHostToDevice, h->st));
+        fm::launch_scatter_state(d, h->stage3, h->stage3 + n3, nullptr, h->st);  // w = 0, a = 0
+        FM_CUDA(cudaMemcpyAsync(d.slot_of, gid, sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice, h->st));
+    }
+    FM_CUDA(cudaGetLastError());
+    FM_CUDA(cudaStreamSynchronize(h->st));
+    h->n_own = n;
+    h->n_halo = 0;
+    h->dd_phase = 0;
+    h->stage = 1;
+    h->cells_valid = h->list_valid = false;
+    h->has_pe = false;
+    return FM_OK;
+}
+
+// Counts per destination rank from the device, their offsets back.
+static int dd_fetch_counts(fm_handle *h, int32_t *counts, int *total)
+{
+    fm::DdDev &x = h->x;
+    FM_CUDA(cudaMemcpyAsync(h->dd_counts.data(), x.count, sizeof(int32_t) * h->nranks, cudaMemcpyDeviceToHost, h->st));
+    FM_CUDA(cudaStreamSynchronize(h->st));
+    std::vector<int32_t> off((size_t)h->nranks);
+    int t = 0;
+    for (int r = 0; r < h->nranks; r++) {
+        off[(size_t)r] = t;
+        t += h->dd_counts[(size_t)r];
+        if (counts) counts[r] = h->dd_counts[(size_t)r];
+    }
+    FM_CUDA(cudaMemcpyAsync(x.offset, off.data(), sizeof(int32_t) * h->nranks, cudaMemcpyHostToDevice, h->st));
+    FM_CUDA(cudaMemsetAsync(x.cursor, 0, sizeof(int32_t) * h->nranks, h->st));
+    FM_CUDA(cudaStreamSynchronize(h->st));  // `off` is a stack buffer
+    *total = t;
+    return FM_OK;
+}
+
+extern "C" int fm_dd_classify(fm_handle *h, int32_t wrap, int32_t *counts)
+{
+    FM_TRY(dd_ready(h, true, 1));
+    if (!counts) return fail(FM_ERR_ARG, "null argument");
+    FmDev &d = h->d;
+    fm::DdDev &x = h->x;
+    FM_CUDA(cudaMemsetAsync(d.cell_count, 0, sizeof(int32_t) * (size_t)d.ncell, h->st));
+    FM_CUDA(cudaMemsetAsync(x.count, 0, sizeof(int32_t) * h->nranks, h->st));
+    FM_CUDA(cudaMemsetAsync(x.nlist, 0, sizeof(int32_t), h->st));
+    fm::launch_dd_classify(d, x, d.n, wrap ? 1 : 0, h->iter, h->st);
+    h->launches += 1;
+    FM_CUDA(cudaGetLastError());
+    int total = 0;
+    FM_TRY(dd_fetch_counts(h, counts, &total));
+    fm::FmScalars s;
+    FM_TRY(read_scalars(h, &s));
+    FM_TRY(status_error(h, s));
+    h->n_kept = h->n_own - total;
+    h->cells_valid = h->list_valid = false;
+    h->dd_phase = 1;
+    return FM_OK;
+}
+
+extern "C" int fm_dd_pack_emigrants(fm_handle *h, double *d_send)
+{
+    FM_TRY(dd_ready(h, true, 1));
+    if (h->dd_phase != 1) return fail(FM_ERR_STATE, "fm_dd_pack_emigrants follows fm_dd_classify");
+    int total = h->n_own - h->n_kept;
+    if (total > 0 && !d_send) return fail(FM_ERR_ARG, "null send buffer");
+    fm::launch_dd_pack_emigrants(h->d, h->x, total, d_send, h->st);
+    h->launches += total > 0;
+    FM_CUDA(cudaGetLastError());
+    return FM_OK;
+}
+
+extern "C" int fm_dd_immigrate(fm_handle *h, const double *d_recv, int32_t n)
+{
+    FM_TRY(dd_ready(h, true, 1));
+    if (h->dd_phase != 1) return fail(FM_ERR_STATE, "fm_dd_immigrate follows fm_dd_pack_emigrants");
+    if (n < 0 || (n > 0 && !d_recv)) return fail(FM_ERR_ARG, "bad arrivals");
+    FmDev &d = h->d;
+    const int base = d.n;
+    if ((int64_t)base + n > h->cap) return fail(FM_ERR_ARG, "arrivals exceed the subdomain's capacity");
+    fm::launch_dd_append_immigrants(d, h->x, d_recv, n, base, h->iter, h->st);
+    h->launches += n > 0;
+    FM_CUDA(cudaGetLastError());
+    h->n_pending = base + n;
+    h->n_kept += n;
+    h->dd_phase = 2;
+    return FM_OK;
+}
+
+extern "C" int fm_dd_halo_counts(fm_handle *h, int32_t *counts)
+{
+    FM_TRY(dd_ready(h, true, 1));
+    if (h->dd_phase != 2) return fail(FM_ERR_STATE, "fm_dd_halo_counts follows fm_dd_immigrate");
+    if (!counts) return fail(FM_ERR_ARG, "null argument");
+    FmDev d = h->d;
+    FM_CUDA(cudaMemsetAsync(h->x.count, 0, sizeof(int32_t) * h->nranks, h->st));
+    fm::launch_dd_halo_records(d, h->x, h->n_pending, 0, nullptr, h->st);
+    h->launches += 1;
+    FM_CUDA(cudaGetLastError());
+    int total = 0;
+    FM_TRY(dd_fetch_counts(h, counts, &total));
+    fm::FmScalars s;
+    FM_TRY(read_scalars(h, &s));
+    FM_TRY(status_error(h, s));
+    h->dd_phase = 3;
+    return FM_OK;
+}
+
+extern "C" int fm_dd_pack_halo(fm_handle *h, double *d_send)
+{
+    FM_TRY(dd_ready(h, true, 1));
+    if (h->dd_phase != 3) return fail(FM_ERR_STATE, "fm_dd_pack_halo follows fm_dd_halo_counts");
+    fm::launch_dd_halo_records(h->d, h->x, h->n_pending, 1, d_send, h->st);
+    h->launches += 1;
+    FM_CUDA(cudaGetLastError());
+    return FM_OK;
+}
+
+// Neighbour rows of the sorted subdomain; a row overflow grows the rows and
+// builds again.
+static int dd_build(fm_handle *h)
+{
+    FmDev &d = h->d;
+    for (int attempt = 0; attempt < 6; attempt++) {
+        fm::launch_build_nlist(d, 0, h->iter, h->st);
+        h->launches += 1;
+        FM_CUDA(cudaGetLastError());
+        fm::FmScalars s;
+        FM_TRY(read_scalars(h, &s));
+        if (!(s.status & fm::ST_NLIST) || (s.status & (fm::ST_FATAL & ~fm::ST_NLIST))) return status_error(h, s);
+        const int want = round_up((int)std::ceil(1.2 * s.max_nbr) + 8, 8);
+        if ((size_t)want * fm::nb_rows(h->cap) > ((size_t)1 << 34)) return status_error(h, s);
+        FM_TRY(alloc_nlist(h, want));
+        s.status &= ~fm::ST_NLIST;
+        s.max_nbr = 0;
+        FM_CUDA(cudaMemcpyAsync(&d.sc->status, &s.status, sizeof(uint32_t), cudaMemcpyHostToDevice, h->st));
+        FM_CUDA(cudaMemcpyAsync(&d.sc->max_nbr, &s.max_nbr, sizeof(int32_t), cudaMemcpyHostToDevice, h->st));
+        FM_CUDA(cudaStreamSynchronize(h->st));
+    }
+    return fail(FM_ERR_NLIST, "subdomain neighbour rows kept overflowing");
+}
+
+extern "C" int fm_dd_receive_halo(fm_handle *h, const double *d_recv, int32_t n)
+{
+    FM_TRY(dd_ready(h, true, 1));
+    if (h->dd_phase != 3) return fail(FM_ERR_STATE, "fm_dd_receive_halo follows fm_dd_pack_halo");
+    if (n < 0 || (n > 0 && !d_recv)) return fail(FM_ERR_ARG, "bad halo records");
+    FmDev &d = h->d;
+    const int base = h->n_pending;
+    if ((int64_t)base + n > h->cap) return fail(FM_ERR_ARG, "halo copies exceed the subdomain's capacity");
+    fm::launch_dd_append_halo(d, d_recv, n, base, h->st);
+    // counting sort of every entry with a cell (owned kept, arrivals, halo
+    // copies), in-cell by global number; then the rows
+    FmDev old = d;
+    old.n = base + n;
+    fm::launch_scan_cells(old, 0, h->st);
+    fm::launch_scatter(old, 0, h->st);
+    d.n = h->n_kept + n;
+    fm::launch_reorder(d, 0, h->tpos, h->tuidx, h->st);
+    h->launches += 6;
+    FM_CUDA(cudaGetLastError());
+    h->n_own = h->n_kept;
+    h->n_halo = n;
+    h->cells_valid = true;
+    d.nblocks_force = force_rows(h);
+    FM_TRY(dd_build(h));
+    h->list_valid = true;
+    h->dd_phase = 0;
+    if (h->stage < 2) h->stage = 2;
+    return FM_OK;
+}
+
+extern "C" int fm_dd_counts(fm_handle *h, int32_t *n_owned, int32_t *n_halo)
+{
+    FM_TRY(dd_ready(h, false, 0));
+    if (n_owned) *n_owned = h->n_own;
+    if (n_halo) *n_halo = h->n_halo;
+    return FM_OK;
+}
+
+extern "C" int fm_dd_cell_starts(fm_handle *h, int32_t *starts)
+{
+    FM_TRY(dd_ready(h, true, 2));
+    if (!starts) return fail(FM_ERR_ARG, "null argument");
+    FM_CUDA(cudaMemcpyAsync(starts, h->d.cell_start, sizeof(int32_t) * ((size_t)h->d.ncell + 1), cudaMemcpyDeviceToHost,
+                            h->st));
+    FM_CUDA(cudaStreamSynchronize(h->st));
+    return FM_OK;
+}
+
+extern "C" int fm_dd_gather_positions(fm_handle *h, const int32_t *d_idx, const int8_t *d_code, int32_t n,
+                                      double *d_out)
+{
+    FM_TRY(dd_ready(h, true, 2));
+    if (n < 0 || (n > 0 && (!d_idx || !d_code || !d_out))) return fail(FM_ERR_ARG, "bad gather list");
+    fm::launch_dd_gather_positions(h->d, d_idx, d_code, n, d_out, h->st);
+    h->launches += n > 0;
+    FM_CUDA(cudaGetLastError());
+    return FM_OK;
+}
+
+extern "C" int fm_dd_scatter_positions(fm_handle *h, const int32_t *d_idx, const double *d_in, int32_t n)
+{
+    FM_TRY(dd_ready(h, true, 2));
+    if (n < 0 || (n > 0 && (!d_idx || !d_in))) return fail(FM_ERR_ARG, "bad scatter list");
+    fm::launch_dd_scatter_positions(h->d, d_idx, d_in, n, h->st);
+    h->launches += n > 0;
+    FM_CUDA(cudaGetLastError());
+    return FM_OK;
+}
+
+extern "C" int fm_dd_move1(fm_handle *h)
+{
+    FM_TRY(dd_ready(h, true, 2));
+    fm::launch_move1(h->d, h->st);
+    h->launches += 1;
+    FM_CUDA(cudaGetLastError());
+    return FM_OK;
+}
+
+extern "C" int fm_dd_vmax2(fm_handle *h, uint64_t *vmax2)
+{
+    FM_TRY(dd_ready(h, true, 2));
+    if (!vmax2) return fail(FM_ERR_ARG, "null argument");
+    unsigned long long v = 0ull;
+    FM_CUDA(cudaMemcpyAsync(&v, &h->d.sc->vmax2, sizeof v, cudaMemcpyDeviceToHost, h->st));
+    FM_CUDA(cudaStreamSynchronize(h->st));
+    *vmax2 = (uint64_t)v;
+    return FM_OK;
+}
+
+extern "C" int fm_dd_decide(fm_handle *h, uint64_t vmax2_global, int32_t iter, int32_t flip, int32_t *rebuild)
+{
+    FM_TRY(dd_ready(h, true, 2));
+    if (!rebuild) return fail(FM_ERR_ARG, "null argument");
+    const unsigned long long v = (unsigned long long)vmax2_global;
+    FM_CUDA(cudaMemcpyAsync(&h->d.sc->vmax2, &v, sizeof v, cudaMemcpyHostToDevice, h->st));
+    h->iter = iter;
+    fm::launch_decide(h->d, iter, flip ? 1 : 0, h->p.rebuild_criteria, h->p.fixed_rebuild, h->half_min_delta, h->st);
+    h->launches += 1;
+    FM_CUDA(cudaGetLastError());
+    fm::FmScalars s;
+    FM_TRY(read_scalars(h, &s));  // (also keeps `v` alive until the copy is done)
+    FM_TRY(status_error(h, s));
+    *rebuild = s.rebuild;
+    return FM_OK;
+}
+
+extern "C" int fm_dd_forces(fm_handle *h, int32_t iter, int32_t record, int32_t mode)
+{
+    FM_TRY(dd_ready(h, true, 2));
+    if (!(h->cells_valid && h->list_valid)) return fail(FM_ERR_STATE, "forces need a rebuild after the upload");
+    if (mode < 0 || mode > 2) return fail(FM_ERR_ARG, "mode must be 0, 1 or 2");
+    h->iter = iter;
+    h->d.nblocks_force = force_rows(h);
+    queue_force(h, record ? 1 : 0, mode);
+    FM_CUDA(cudaGetLastError());
+    if (record) h->has_pe = true;
+    return FM_OK;
+}
+
+extern "C" int fm_dd_sums(fm_handle *h, double *sums)
+{
+    FM_TRY(dd_ready(h, true, 2));
+    if (!sums) return fail(FM_ERR_ARG, "null argument");
+    if (!h->has_pe) return fail(FM_ERR_STATE, "no record step has been computed");
+    fm::launch_dd_sums(h->d, h->dd_sums, h->st);
+    h->launches += 1;
+    FM_CUDA(cudaGetLastError());
+    FM_CUDA(cudaMemcpyAsync(sums, h->dd_sums, sizeof(double) * fm::RS_N, cudaMemcpyDeviceToHost, h->st));
+    fm::FmScalars s;
+    FM_TRY(read_scalars(h, &s));
+    FM_TRY(status_error(h, s));
+    return FM_OK;
+}
+
+extern "C" int fm_dd_macro(fm_handle *h, const double *sums, int32_t iter, double simtime, fm_macro *out)
+{
+    FM_TRY(dd_ready(h, false, 0));
+    if (!sums || !out) return fail(FM_ERR_ARG, "null argument");
+    const FmDev &d = h->d;
+    // evaluate_macroscopic_properties (simulation_record.f90:1205-1314), as the
+    // single-system record kernel forms it, over the whole system's sums
+    const double gnp = (double)h->p.np;
+    fm_macro r;
+    std::memset(&r, 0, sizeof r);
+    r.iter = iter;
+    r.simtime = simtime;
+    r.vsum = sums[fm::RS_VSUM];
+    r.mv2sum = sums[fm::RS_MV2];
+    r.virial = sums[fm::RS_VIR];
+    r.kinenergy = (0.5 * r.mv2sum) / gnp;
+    r.potenergy = (0.5 * sums[fm::RS_PE]) / gnp + d.pot_slrc;
+    r.totenergy = r.kinenergy + r.potenergy;
+    r.temperature = r.mv2sum / (3.0 * gnp);
+    r.pressure = (d.density / (gnp * 3.0)) * (r.mv2sum + r.virial / 2.0) + d.p_slrc;
+    *out = r;
+    if (sums[fm::RS_PEMAX] > 10000.0) return fail(FM_ERR_PE, "max(potenergymol) > 10000");
+    return FM_OK;
+}
+
+extern "C" int fm_dd_download(fm_handle *h, int32_t cap, int32_t *n_owned, double *r, double *v, int32_t *gid)
+{
+    FM_TRY(dd_ready(h, false, 1));
+    if (!n_owned) return fail(FM_ERR_ARG, "null argument");
+    const FmDev &d = h->d;
+    const size_t n = (size_t)d.n;
+    std::vector<double4> pos(n);
+    std::vector<double> vx(n), vy(n), vz(n);
+    std::vector<int32_t> ids(n);
+    fm::FmScalars s;
+    FM_TRY(read_scalars(h, &s));
+    if (n > 0) {
+        FM_CUDA(cudaMemcpyAsync(pos.data(), fm::cur_pos(d, s.pset), sizeof(double4) * n, cudaMemcpyDeviceToHost, h->st));
+        FM_CUDA(cudaMemcpyAsync(vx.data(), d.vx, sizeof(double) * n, cudaMemcpyDeviceToHost, h->st));
+        FM_CUDA(cudaMemcpyAsync(vy.data(), d.vy, sizeof(double) * n, cudaMemcpyDeviceToHost, h->st));
+        FM_CUDA(cudaMemcpyAsync(vz.data(), d.vz, sizeof(double) * n, cudaMemcpyDeviceToHost, h->st));
+        FM_CUDA(cudaMemcpyAsync(ids.data(), d.slot_of, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, h->st));
+        FM_CUDA(cudaStreamSynchronize(h->st));
+    }
+    int m = 0;
+    for (size_t i = 0; i < n; i++) {
+        if (pos[i].w != 0.0) continue;  // halo copy
+        if (m < cap) {
+            if (r) { r[3 * m] = pos[i].x; r[3 * m + 1] = pos[i].y; r[3 * m + 2] = pos[i].z; }
+            if (v) { v[3 * m] = vx[i]; v[3 * m + 1] = vy[i]; v[3 * m + 2] = vz[i]; }
+            if (gid) gid[m] = ids[i];
+        }
+        m++;
+    }
+    *n_owned = m;
+    if (m > cap) return fail(FM_ERR_ARG, "more owned molecules than cap");
     return FM_OK;
 }

@@ -79,6 +79,10 @@ struct CellSys {
     int tdummy;                 // byte offset of the staging's dummy candidate (row padding)
     const int32_t *blk_off;
     int tnb[3];
+    // subdomain (dd = 1): halo cells hold explicit copies (no images, no
+    // rows); cell x of this grid is global extended cell x + org[0]
+    int dd;
+    int org[3];
 };
 
 // Per-warp shared staging.
@@ -221,9 +225,13 @@ __device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY, TILE> 
     const float prune2 = (float)(y.rn2 * 1.0001 + 1e-4);
     const int cx = c % ne0, cy = (c / ne0) % ne1, cz = c / (ne0 * ne1);
     const bool chalo = is_halo(cx, ne0) || is_halo(cy, ne1) || is_halo(cz, ne2);
-    const double refx = (cx - 0.5) * y.cs[0] - y.hd[0];
-    const double refy = (cy - 0.5) * y.cs[1] - y.hd[1];
-    const double refz = (cz - 0.5) * y.cs[2] - y.hd[2];
+    if (y.dd && chalo) {  // a subdomain's halo copies are partners only: no rows
+        for (int k = lane; k < ccount; k += 32) y.nnbr[cstart + k] = 0;
+        return 0u;
+    }
+    const double refx = (cx + y.org[0] - 0.5) * y.cs[0] - y.hd[0];
+    const double refy = (cy + y.org[1] - 0.5) * y.cs[1] - y.hd[1];
+    const double refz = (cz + y.org[2] - 0.5) * y.cs[2] - y.hd[2];
 
     // --- segments of neighbour cell q = lane ---
     int n_real = 0, b_real = 0, n_img = 0, b_img = 0, code_img = NB_NOSHIFT;
@@ -244,7 +252,7 @@ __device__ uint32_t build_cell(const CellSys &y, int c, BuildShared<POLY, TILE> 
                 const int c2 = x2 + ne0 * (y2 + ne1 * z2);
                 b_real = y.cell_start[c2] - y.mol_off;
                 n_real = y.cell_start[c2 + 1] - y.mol_off - b_real;
-                if (h2) {
+                if (h2 && !y.dd) {
                     // images in a halo cell come from the interior cell on the far
                     // side: low halo <- last interior cell shifted by -domain, high
                     // halo <- first interior cell shifted by +domain
@@ -513,6 +521,10 @@ __device__ uint32_t build_block(const CellSys &y, int blk, BlockShared<POLY, TIL
             ostart = y.cell_start[c] - y.mol_off;
             ocount = y.cell_start[c + 1] - y.mol_off - ostart;
             ohalo = is_halo(x, ne0) || is_halo(yy, ne1) || is_halo(z, ne2);
+            if (y.dd && ohalo) {  // a subdomain's halo copies: no rows
+                for (int k = 0; k < ocount; k++) y.nnbr[ostart + k] = 0;
+                ocount = 0;
+            }
         }
     }
     int oincl = ocount;
@@ -532,9 +544,9 @@ __device__ uint32_t build_block(const CellSys &y, int blk, BlockShared<POLY, TIL
     const float band = (float)(1e-4 * csmax * csmax) + 1e-6f;
     const float lo32 = (float)y.rn2 - band, hi32 = (float)y.rn2 + band;
     const float prune2 = (float)(y.rn2 * 1.0001 + 1e-4);
-    const double refx = bx0 * y.cs[0] - y.hd[0];  // centre of the 2x2x2 block
-    const double refy = by0 * y.cs[1] - y.hd[1];
-    const double refz = bz0 * y.cs[2] - y.hd[2];
+    const double refx = (bx0 + y.org[0]) * y.cs[0] - y.hd[0];  // centre of the 2x2x2 block
+    const double refy = (by0 + y.org[1]) * y.cs[1] - y.hd[1];
+    const double refz = (bz0 + y.org[2]) * y.cs[2] - y.hd[2];
 
     // --- segments of the union cells u = lane and u = lane + 32 ---
     int seg_n[4], seg_b[4], seg_code[4];
@@ -563,7 +575,7 @@ __device__ uint32_t build_block(const CellSys &y, int blk, BlockShared<POLY, TIL
                 const int c2 = x2 + ne0 * (y2 + ne1 * z2);
                 seg_b[2 * h] = y.cell_start[c2] - y.mol_off;
                 seg_n[2 * h] = y.cell_start[c2 + 1] - y.mol_off - seg_b[2 * h];
-                if (h2) {
+                if (h2 && !y.dd) {
                     // images of the interior cell on the far side, as in build_cell
                     const int ssx = x2 == 0 ? -1 : (x2 == ne0 - 1 ? 1 : 0);
                     const int ssy = y2 == 0 ? -1 : (y2 == ne1 - 1 ? 1 : 0);

@@ -17,7 +17,8 @@ enum : uint32_t {
     ST_BOND = 1u << 3,      // FENE bond at or beyond R_0
     ST_TILE = 1u << 4,      // a block's staged neighbourhood exceeded the tiled force kernel's capacity
     ST_ANGLE = 1u << 5,     // angular triple with no defined result (missing bond, k_ijk < 1e-5)
-    ST_FATAL = ST_ESCAPE | ST_NLIST | ST_PE | ST_BOND | ST_TILE | ST_ANGLE,
+    ST_MIGRATE = 1u << 6,   // subdomain: a molecule left the neighbouring subdomains, or the capacity ran out
+    ST_FATAL = ST_ESCAPE | ST_NLIST | ST_PE | ST_BOND | ST_TILE | ST_ANGLE | ST_MIGRATE,
 };
 
 // Device-resident scalars of the step loop (one per system).
@@ -154,6 +155,16 @@ struct FmDev {
     const FmMiePair *mie_pair;   // [(ti-1) + MIE_MAXT*(tj-1)]
     const double *mie_mass;      // [ti-1]
     const int32_t *mie_type_up;  // moltype by upload index (written into w at upload)
+    // Subdomain of a spatial decomposition (dd = 1): the extended grid above is
+    // this rank's interior cells nc plus one halo layer; interior cell x = 1
+    // is global interior cell org[0] (0-based) of the global grid of gne - 2
+    // cells per axis, whose cell size and box (L, hd, cs) are the ones above.
+    // Positions are global coordinates.  The halo cells hold explicit copies
+    // of the neighbouring subdomains' boundary molecules (periodic shift
+    // applied by the sender), marked by w = 1 (owned molecules: w = 0), with
+    // v = a = 0 and no rows; images are never formed.
+    int dd;
+    int org[3], gne[3];
     // record partials [nblocks][RS_N] and finished rows
     double *partial;
     int nblocks_force;
@@ -183,6 +194,31 @@ __host__ __device__ inline size_t nb_row(int i, int maxn)
 }
 __host__ __device__ inline size_t nb_col(int k) { return (size_t)(k & ~7) * 32u + (size_t)(k & 7); }
 inline size_t nb_rows(int n) { return ((size_t)n + 31u) / 32u * 32u; }
+
+// Subdomain bookkeeping of the decomposition kernels (fm_dd_kernels.cu).
+constexpr int DD_MREC = 10;  // migrating molecule: r, v, a, global number
+constexpr int DD_HREC = 5;   // halo copy: shifted r, global number, destination halo cell
+struct DdDev {
+    int rank, dims[3];
+    const int32_t *owner_axis;  // process coordinate of each global interior cell, x then y then z
+    // needs of this rank's cells: for cell c, entries [need_off[c], need_off[c+1])
+    // of (rank whose halo holds it, image code it is seen with, that rank's halo cell)
+    const int32_t *need_off, *need_rank, *need_code, *need_cell;
+    int32_t *count, *offset, *cursor;  // per destination rank
+    int32_t *nlist;                    // emigrants listed
+    int32_t *list_idx, *list_aux;      // emigrant slot and destination
+    int list_cap;
+};
+void launch_dd_classify(const FmDev &d, const DdDev &x, int n, int wrap, int iter, cudaStream_t st);
+void launch_dd_pack_emigrants(const FmDev &d, const DdDev &x, int n, double *out, cudaStream_t st);
+void launch_dd_append_immigrants(const FmDev &d, const DdDev &x, const double *in, int n, int base, int iter,
+                                 cudaStream_t st);
+void launch_dd_halo_records(const FmDev &d, const DdDev &x, int n, int pass, double *out, cudaStream_t st);
+void launch_dd_append_halo(const FmDev &d, const double *in, int n, int base, cudaStream_t st);
+void launch_dd_gather_positions(const FmDev &d, const int32_t *idx, const int8_t *code, int n, double *out,
+                                cudaStream_t st);
+void launch_dd_scatter_positions(const FmDev &d, const int32_t *idx, const double *in, int n, cudaStream_t st);
+void launch_dd_sums(const FmDev &d, double *out, cudaStream_t st);
 
 // Sets the message fm_last_error returns on this thread (fm_api.cu).
 void set_last_error(const char *msg);

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstddef>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -122,6 +123,10 @@ struct fm_engine {
     int64_t next_id = 1;
     int tpm = 0;
     bool tuned = false;
+    // list-build tile: jobs below this many molecules per cell are built by
+    // 2x2x2-cell blocks (FM_LIST_BUILD_AUTO: chosen by tune_build)
+    double blocks_below = 8.0;
+    bool tuned_build = false;
     cudaGraphExec_t graph = nullptr;
     int graph_tpm = -1;
     fm::TickExtent graph_x{0, 0, 0};  // launch extents the graph was captured with
@@ -236,6 +241,12 @@ Footprint footprint(const fm_job &j, int maxn_override)
     return f;
 }
 
+// Molecules per cell of a job (its mean density times the cell volume).
+double per_cell(const fm::EngSlot &s, int nmol)
+{
+    return (double)nmol / (s.L[0] * s.L[1] * s.L[2]) * s.cs[0] * s.cs[1] * s.cs[2];
+}
+
 bool can_admit(fm_engine *e, const Job &jb, const Footprint &f)
 {
     if (!e->mol.fits(jb.p.np)) return false;
@@ -277,10 +288,9 @@ int admit(fm_engine *e, Job &jb, int slot)
     s.nmol = j.np;
     s.list_off = jb.list_off;
     s.maxn = jb.maxn;
-    // sparse cells (a few molecules each) are built 2x2x2 at a time (same rows)
-    s.build_blocks = f.mode == fm::MODE_LIST && (double)j.np / (j.domain[0] * j.domain[1] * j.domain[2]) *
-                                                        s.cs[0] * s.cs[1] * s.cs[2] < 8.0
-                         ? 1 : 0;
+    // sparse cells (a few molecules each) are built 2x2x2 at a time (same rows);
+    // the threshold is the autotuner's
+    s.build_blocks = f.mode == fm::MODE_LIST && per_cell(s, j.np) < e->blocks_below ? 1 : 0;
     s.tplot = std::max(1, j.tplot);
     s.integrator = j.integration_algorithm == 0 ? 0 : 1;
     s.ensemble = j.ensemble;
@@ -392,14 +402,107 @@ int retire(fm_engine *e, int slot)
     return FM_OK;
 }
 
+// Times the list build of every resident list job with the tile each
+// candidate threshold gives it (one cell per warp, or 2x2x2 cells), into
+// scratch rows and a scratch copy of the slot table, so the jobs' own lists
+// and state are untouched (both tiles give the same rows); keeps the fastest
+// threshold and applies it to the resident and later jobs.
+int tune_build(fm_engine *e)
+{
+    std::vector<int> ks;
+    for (size_t k = 0; k < e->table.size(); k++)
+        if (e->table[k].state == fm::SLOT_RUN && e->table[k].mode == fm::MODE_LIST) ks.push_back((int)k);
+    if (ks.empty()) return FM_OK;
+    fm::EngFlags saved{};
+    EN_CUDA(cudaMemcpyAsync(&saved, e->d.flags, sizeof saved, cudaMemcpyDeviceToHost, e->st));
+    EN_CUDA(cudaStreamSynchronize(e->st));
+    fm::EngDev dd = e->d;
+    int32_t *snbr = nullptr, *snnbr = nullptr;
+    fm::EngSlot *sslots = nullptr;
+    EN_TRY(dal(&snbr, (size_t)e->p.max_list_entries));
+    int rc = dal(&snnbr, (size_t)e->d.mol_cap);
+    if (rc == FM_OK) rc = dal(&sslots, (size_t)e->d.nslots);
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (rc == FM_OK && (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess))
+        rc = efail(FM_ERR_CUDA, "cudaEventCreate");
+    dd.nbr = snbr;
+    dd.nnbr = snnbr;
+    dd.slots = sslots;
+    const double cands[5] = {0.0, 4.0, 8.0, 16.0, 1e30};
+    double best_t = e->blocks_below;
+    float best = 1e30f;
+    std::vector<fm::EngSlot> tmp(e->table);
+    std::vector<int32_t> rb_slot(ks.size()), rb_upre(ks.size() + 1);
+    fm::EngFlags fl = saved;
+    for (int c = 0; c < 5 && rc == FM_OK; c++) {
+        int tot = 0, cells = 0;
+        for (size_t q = 0; q < ks.size(); q++) {
+            fm::EngSlot &s = tmp[(size_t)ks[q]];
+            s.build_blocks = per_cell(s, s.nmol) < cands[c] ? 1 : 0;
+            rb_slot[q] = ks[q];
+            rb_upre[q] = tot;
+            tot += s.build_blocks ? ((s.ne[0] + 1) / 2) * ((s.ne[1] + 1) / 2) * ((s.ne[2] + 1) / 2) : s.ncell;
+            cells += s.ncell;
+        }
+        rb_upre[ks.size()] = tot;
+        fl.any_rebuild = 1;
+        fl.rb_n = (int)ks.size();
+        fl.rb_utot = tot;
+        cudaError_t ce = cudaMemcpyAsync(sslots, tmp.data(), sizeof(fm::EngSlot) * tmp.size(),
+                                         cudaMemcpyHostToDevice, e->st);
+        if (ce == cudaSuccess)
+            ce = cudaMemcpyAsync(e->d.rb_slot, rb_slot.data(), sizeof(int32_t) * ks.size(), cudaMemcpyHostToDevice,
+                                 e->st);
+        if (ce == cudaSuccess)
+            ce = cudaMemcpyAsync(e->d.rb_upre, rb_upre.data(), sizeof(int32_t) * (ks.size() + 1),
+                                 cudaMemcpyHostToDevice, e->st);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(e->d.flags, &fl, sizeof fl, cudaMemcpyHostToDevice, e->st);
+        if (ce != cudaSuccess) { rc = efail(FM_ERR_CUDA, cudaGetErrorString(ce)); break; }
+        fm::eng_build_only(dd, cells, e->st);  // warm-up
+        cudaEventRecord(a, e->st);
+        for (int rep = 0; rep < 2; rep++) fm::eng_build_only(dd, cells, e->st);
+        cudaEventRecord(b, e->st);
+        // also keeps the host buffers above alive until the copies are done
+        if ((ce = cudaEventSynchronize(b)) != cudaSuccess) { rc = efail(FM_ERR_CUDA, cudaGetErrorString(ce)); break; }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        if (ms < best) { best = ms; best_t = cands[c]; }
+        e->launches += 3;
+    }
+    cudaStreamSynchronize(e->st);
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    cudaFree(snbr);
+    cudaFree(snnbr);
+    cudaFree(sslots);
+    if (rc != FM_OK) return rc;
+    EN_CUDA(cudaGetLastError());
+    EN_CUDA(cudaMemcpyAsync(e->d.flags, &saved, sizeof saved, cudaMemcpyHostToDevice, e->st));
+    e->blocks_below = best_t;
+    e->tuned_build = true;
+    for (int k : ks) {  // the same rows either way: switching a running job is invisible
+        fm::EngSlot &s = e->table[(size_t)k];
+        s.build_blocks = per_cell(s, s.nmol) < best_t ? 1 : 0;
+        EN_CUDA(cudaMemcpyAsync(reinterpret_cast<char *>(e->d.slots + k) + offsetof(fm::EngSlot, build_blocks),
+                                &s.build_blocks, sizeof(int), cudaMemcpyHostToDevice, e->st));
+    }
+    EN_CUDA(cudaStreamSynchronize(e->st));
+    return FM_OK;
+}
+
 int autotune(fm_engine *e)
 {
     if (e->tuned) return FM_OK;
-    if (e->p.threads_per_molecule > 0) { e->tpm = e->p.threads_per_molecule; e->tuned = true; return FM_OK; }
+    if (e->p.list_build == FM_LIST_BUILD_AUTO && !e->tuned_build) EN_TRY(tune_build(e));
+    if (e->p.threads_per_molecule > 0) {
+        e->tpm = e->p.threads_per_molecule;
+        e->tuned = e->p.list_build != FM_LIST_BUILD_AUTO || e->tuned_build;  // until a list job runs
+        return FM_OK;
+    }
     bool any = false;
     for (size_t k = 0; k < e->table.size(); k++)
         if (e->table[k].state == fm::SLOT_RUN && e->table[k].mode == fm::MODE_LIST) any = true;
-    if (!any) return FM_OK;
+    if (!any) return FM_OK;  // tune_build found none either
     cudaEvent_t a, b;
     EN_CUDA(cudaEventCreate(&a));
     EN_CUDA(cudaEventCreate(&b));
@@ -476,6 +579,9 @@ extern "C" int fm_engine_create(const fm_engine_params *p, fm_engine **out)
     int t = p->threads_per_molecule;
     if (t != 0 && t != 1 && t != 2 && t != 4 && t != 8 && t != 16)
         return efail(FM_ERR_ARG, "threads_per_molecule must be 0, 1, 2, 4, 8 or 16");
+    if (p->list_build != FM_LIST_BUILD_AUTO && p->list_build != FM_LIST_BUILD_CELLS &&
+        p->list_build != FM_LIST_BUILD_BLOCKS)
+        return efail(FM_ERR_ARG, "list_build must be FM_LIST_BUILD_AUTO, _CELLS or _BLOCKS");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return efail(FM_ERR_NODEVICE, "no CUDA device");
     fm_engine *e = new fm_engine();
@@ -531,6 +637,7 @@ extern "C" int fm_engine_create(const fm_engine_params *p, fm_engine **out)
     e->resident.assign((size_t)p->max_slots, Job());
     e->table.assign((size_t)p->max_slots, fm::EngSlot{});
     e->tpm = p->threads_per_molecule > 0 ? p->threads_per_molecule : 4;
+    e->blocks_below = p->list_build == FM_LIST_BUILD_CELLS ? 0.0 : (p->list_build == FM_LIST_BUILD_BLOCKS ? 1e30 : 8.0);
     cudaError_t err = cudaDeviceSynchronize();
     if (err != cudaSuccess) {
         free_all(e);
@@ -671,6 +778,14 @@ extern "C" int fm_engine_job_state(fm_engine *e, int64_t job_id, double *r, doub
     if (r) std::memcpy(r, it->second.first.data(), it->second.first.size() * 8);
     if (v) std::memcpy(v, it->second.second.data(), it->second.second.size() * 8);
     e->states.erase(it);
+    return FM_OK;
+}
+
+extern "C" int fm_engine_tuning(fm_engine *e, int32_t *tpm, double *blocks_below)
+{
+    if (!e) return efail(FM_ERR_ARG, "null engine");
+    if (tpm) *tpm = e->tpm;
+    if (blocks_below) *blocks_below = e->blocks_below;
     return FM_OK;
 }
 

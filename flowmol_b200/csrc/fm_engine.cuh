@@ -120,6 +120,8 @@ struct TickExtent {
 
 // Launchers (fm_engine.cu); `tpm` = lanes per molecule of the force kernel.
 void eng_tick(const EngDev &d, int tpm, const TickExtent &x, cudaStream_t st);
+// The list build of the work list in d.flags / d.rb_* (autotuner timing runs).
+void eng_build_only(const EngDev &d, int cells, cudaStream_t st);
 void eng_force_only(const EngDev &d, int tpm, int mols, cudaStream_t st);  // autotuner: forces of running list jobs
 void eng_scatter_job(const EngDev &d, int slot, int mol_off, int n, const double *r3, const double *v3,
                      const int32_t *tag, const double *rteth3, const double *slidev3, cudaStream_t st);

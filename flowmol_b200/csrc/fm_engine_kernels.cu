@@ -422,6 +422,8 @@ __global__ void __launch_bounds__(NB_THREADS, 6) k_e_build(EngDev d)
             y.chain = y.subchain = nullptr;
             y.bflag = nullptr;
             y.bnd = y.nbond = nullptr;
+            y.dd = 0;
+            y.org[0] = y.org[1] = y.org[2] = 0;
         }
         __syncwarp();
         r_loaded = r;
@@ -990,6 +992,11 @@ void eng_tick(const EngDev &d, int tpm, const TickExtent &x, cudaStream_t st)
     k_e_thermo<<<dim3(slots, EY), ER, 0, st>>>(d);
     k_e_move_lfv<<<gm, 256, 0, st>>>(d);
     k_e_record<<<dim3(slots, EY), ER, 0, st>>>(d);
+}
+
+void eng_build_only(const EngDev &d, int cells, cudaStream_t st)
+{
+    k_e_build<<<sgrid(std::min(cells, d.cell_cap), NB_WARPS, 6), NB_THREADS, 0, st>>>(d);
 }
 
 void eng_force_only(const EngDev &d, int tpm, int mols, cudaStream_t st)

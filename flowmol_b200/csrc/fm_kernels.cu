@@ -341,14 +341,19 @@ __global__ void k_scatter(FmDev d, int gated)
     if (!gate(d, gated)) return;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < d.n; i += gridDim.x * blockDim.x) {
         int c = d.cell_of[i];
+        if (c < 0) continue;  // a subdomain's departed molecule or stale halo copy
         int slot = d.cell_start[c] + atomicAdd(&d.cell_count[c], 1);
         d.perm[slot] = i;
     }
 }
 
-// Atomics make the in-cell order arbitrary; sorting each cell by old slot
-// makes the whole rebuild deterministic.  One warp per cell: up to 32 members
-// by a bitonic sort in registers, larger cells by lane 0 (insertion sort).
+// Atomics make the in-cell order arbitrary; sorting each cell by the
+// molecules' identity (slot_of: upload index, or global number in a
+// subdomain) makes the whole rebuild deterministic and independent of the
+// previous order, so that a subdomain lays out a cell's molecules exactly as
+// the undivided system does.  One warp per cell: up to 32 members by a
+// bitonic sort of (identity, old slot) keys in registers, larger cells by
+// lane 0 (insertion sort).
 constexpr int SORT_WARPS = 8;
 __global__ void __launch_bounds__(32 * SORT_WARPS) k_sort_cells(FmDev d, int gated)
 {
@@ -359,26 +364,31 @@ __global__ void __launch_bounds__(32 * SORT_WARPS) k_sort_cells(FmDev d, int gat
         const int b = d.cell_start[c], e = d.cell_start[c + 1];
         const int m = e - b;  // uniform across the warp
         if (m <= 32) {
-            int key = lane < m ? d.perm[b + lane] : 0x7fffffff;
+            unsigned long long key = ~0ull;
+            if (lane < m) {
+                const int o = d.perm[b + lane];
+                key = ((unsigned long long)(unsigned)d.slot_of[o] << 32) | (unsigned)o;
+            }
 #pragma unroll
             for (int k = 2; k <= 32; k <<= 1) {
 #pragma unroll
                 for (int j = k >> 1; j > 0; j >>= 1) {
-                    const int other = __shfl_xor_sync(0xffffffffu, key, j);
+                    const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, j);
                     const bool keep_min = ((lane & j) == 0) == ((lane & k) == 0);
-                    key = keep_min ? min(key, other) : max(key, other);
+                    key = keep_min ? (key < other ? key : other) : (key > other ? key : other);
                 }
             }
-            if (lane < m) d.perm[b + lane] = key;
+            if (lane < m) d.perm[b + lane] = (int)(unsigned)(key & 0xffffffffull);
         } else if (lane == 0) {
             for (int x = b + 1; x < e; x++) {
-                const int key = d.perm[x];
+                const int o = d.perm[x];
+                const int key = d.slot_of[o];
                 int y = x - 1;
-                while (y >= b && d.perm[y] > key) {
+                while (y >= b && d.slot_of[d.perm[y]] > key) {
                     d.perm[y + 1] = d.perm[y];
                     y--;
                 }
-                d.perm[y + 1] = key;
+                d.perm[y + 1] = o;
             }
         }
         if (lane == 0) d.cell_count[c] = 0;  // leave counts zeroed for the next histogram
@@ -496,6 +506,8 @@ __global__ void __launch_bounds__(NB_THREADS, 8) k_build_nlist(FmDev d, int gate
     y.nbr16 = d.nbr16; y.maxn16 = d.maxn16; y.tT = d.tile_T; y.tR = d.tile_R; y.blk_off = d.blk_off;
     y.tdummy = d.tile ? tile_boff(d.tile_ucap, d.tile_R) : 0;
     for (int k = 0; k < 3; k++) y.tnb[k] = d.tile_nb[k];
+    y.dd = d.dd;
+    for (int k = 0; k < 3; k++) y.org[k] = d.dd ? d.org[k] : 0;
     uint32_t over = 0u;
     const int nwork = BLOCKS ? ((d.ne[0] + 1) / 2) * ((d.ne[1] + 1) / 2) * ((d.ne[2] + 1) / 2) : d.ncell;
     // work units handed out NB_CHUNK at a time, so warps that meet empty or

@@ -383,7 +383,8 @@ typedef struct fm_engine_params {
     int32_t threads_per_molecule; /* 0 = autotuned on the first resident jobs */
     int32_t ticks_per_chunk;      /* steps per graph launch between admission points */
     int32_t keep_states;          /* keep final r, v of finished jobs for fm_engine_job_state */
-    int32_t pad_;
+    int32_t list_build;           /* FM_LIST_BUILD_*: the list build's tile, one cell or 2x2x2 cells per
+                                     warp (same rows); AUTO = chosen by timing the resident jobs */
     double delta_t;               /* DELTA_T shared by every job */
 } fm_engine_params;
 
@@ -450,6 +451,12 @@ FM_API int fm_engine_take_results(fm_engine *e, fm_job_result *out, int32_t cap,
 FM_API int fm_engine_job_state(fm_engine *e, int64_t job_id, double *r, double *v);
 FM_API int fm_engine_counters(fm_engine *e, int64_t *ticks, int64_t *molecule_steps, int32_t *threads_per_molecule,
                               int64_t *launches);
+/* The autotuner's choices: force-kernel lanes per molecule, and the list
+ * build's tile -- jobs with fewer than `blocks_below` molecules per cell are
+ * built by 2x2x2-cell blocks, the rest one cell per warp (0: every job by
+ * cells).  Both are chosen on the first resident jobs by timing the force
+ * kernel and the list build over them (no counterpart in the reference). */
+FM_API int fm_engine_tuning(fm_engine *e, int32_t *threads_per_molecule, double *blocks_below);
 
 /* ---- instrumentation -------------------------------------------------- */
 /* When enabled, every force-kernel launch is bracketed by CUDA events on the
@@ -499,6 +506,78 @@ FM_API int fm_compute_forces_noalloc(const fm_params *p, int32_t n, const double
                                      double *d_potenergymol, double *d_virialmol, void *cuda_stream);
 /* Message of the last failing fm_compute_forces_noalloc call on this thread. */
 FM_API int fm_noalloc_last_error(char *buf, int32_t len);
+
+/* ---- spatial decomposition: one rank's subdomain ---------------------- */
+/* The reference's MPI build splits the box over a process grid
+ * (messenger_init, messenger.MPI.f90:222-550), refreshes every rank's halo of
+ * the neighbours' boundary cells each step (messenger_updateborders,
+ * :594-628, faces/edges/corners :882-1380) and moves molecules to the rank
+ * whose subdomain they entered on rebuilds (sendmols, :1383-1421).  Here a
+ * subdomain is a block of the UNDIVIDED system's cells in global coordinates:
+ * interior cells origin .. origin + ncells_local - 1 (0-based, per axis) of
+ * the ncells_global that fm_derive_geometry gives for p (p->np is the whole
+ * system's count).  Molecules are binned, ordered (by global number) and
+ * paired exactly as in the undivided system, so forces and trajectories are
+ * bit-identical to one fm_handle over the whole box; records differ only in
+ * the order the ranks' sums are added.  Scope: force_list 2/3, LJ/WCA
+ * (potential_flag 0), velocity Verlet, rebuild_criteria 0/1.
+ *
+ * The caller moves the data between ranks: flat FP64 record buffers in device
+ * memory (FM_DD_MREC doubles per migrating molecule, FM_DD_HREC per halo
+ * copy, 3 per refreshed position), grouped by destination rank in rank
+ * order, with counts per destination (an all-to-all; NCCL or gloo).  A
+ * rebuild (at setup: wrap = 0; on a step: wrap = 1):
+ *   fm_dd_classify(counts) -> all-to-all counts -> fm_dd_pack_emigrants
+ *   -> all-to-all records -> fm_dd_immigrate -> fm_dd_halo_counts(counts)
+ *   -> all-to-all counts -> fm_dd_pack_halo -> all-to-all records
+ *   -> fm_dd_receive_halo (counting sort + neighbour rows).
+ * Between rebuilds the halo positions are refreshed from lists the caller
+ * derives from fm_dd_cell_starts and the plan: fm_dd_gather_positions ->
+ * all-to-all -> fm_dd_scatter_positions.  A velocity-Verlet step:
+ * fm_dd_vmax2 -> max over ranks -> fm_dd_decide -> (rebuild | refresh) ->
+ * fm_dd_forces(mode 2) -> on record steps fm_dd_sums -> sum over ranks ->
+ * fm_dd_macro.  No call here communicates. */
+#define FM_DD_MREC 10
+#define FM_DD_HREC 5
+#define FM_DD_NSUMS 11 /* pe, virial, mv2, vsum, max pe, 6 pressure terms (0 here) */
+FM_API int fm_dd_create(const fm_params *p, const int32_t ncells_global[3], const int32_t origin[3],
+                        const int32_t ncells_local[3], int32_t capacity, fm_handle **out);
+/* The process grid (rank = (px dims[1] + py) dims[2] + pz, as MPI_Cart_create
+ * numbers it), the process coordinate owning each global interior cell
+ * (owner_axis: x cells, then y, then z), and per local extended cell c the
+ * needs [need_off[c], need_off[c+1]): the rank whose halo holds it, the image
+ * code it is seen with ((sx+1) | (sy+1)<<2 | (sz+1)<<4) and that rank's local
+ * halo cell. */
+FM_API int fm_dd_set_plan(fm_handle *h, int32_t rank, const int32_t dims[3], const int32_t *owner_axis,
+                          const int32_t *need_off, const int32_t *need_rank, const int32_t *need_code,
+                          const int32_t *need_cell);
+/* The rank's molecules (r, v host (3, n) column-major; gid 0-based global numbers). */
+FM_API int fm_dd_upload(fm_handle *h, int32_t n, const double *r, const double *v, const int32_t *gid);
+FM_API int fm_dd_classify(fm_handle *h, int32_t wrap, int32_t *counts);
+FM_API int fm_dd_pack_emigrants(fm_handle *h, double *d_send);
+FM_API int fm_dd_immigrate(fm_handle *h, const double *d_recv, int32_t n);
+FM_API int fm_dd_halo_counts(fm_handle *h, int32_t *counts);
+FM_API int fm_dd_pack_halo(fm_handle *h, double *d_send);
+FM_API int fm_dd_receive_halo(fm_handle *h, const double *d_recv, int32_t n);
+FM_API int fm_dd_counts(fm_handle *h, int32_t *n_owned, int32_t *n_halo);
+/* ncells + 1 starts of the local extended cells after the last sort. */
+FM_API int fm_dd_cell_starts(fm_handle *h, int32_t *starts);
+FM_API int fm_dd_gather_positions(fm_handle *h, const int32_t *d_idx, const int8_t *d_code, int32_t n,
+                                  double *d_out);
+FM_API int fm_dd_scatter_positions(fm_handle *h, const int32_t *d_idx, const double *d_in, int32_t n);
+/* Velocity-Verlet pass 1 in place (the first step after a rebuild at setup). */
+FM_API int fm_dd_move1(fm_handle *h);
+FM_API int fm_dd_vmax2(fm_handle *h, uint64_t *vmax2);
+/* simulation_checkrebuild with the ranks' largest |v|^2 (bits of the double);
+ * flip = 1 when the last force call moved the molecules (mode 2). */
+FM_API int fm_dd_decide(fm_handle *h, uint64_t vmax2_global, int32_t iter, int32_t flip, int32_t *rebuild);
+/* Forces of the owned molecules: mode 0 forces only, 1 + move(2), 2 + move(2)
+ * and the next move(1); record = 1 on tplot steps (partials for fm_dd_sums). */
+FM_API int fm_dd_forces(fm_handle *h, int32_t iter, int32_t record, int32_t mode);
+FM_API int fm_dd_sums(fm_handle *h, double *sums);
+FM_API int fm_dd_macro(fm_handle *h, const double *sums, int32_t iter, double simtime, fm_macro *out);
+/* The owned molecules in slot order (r, v (3, n) column-major, gid). */
+FM_API int fm_dd_download(fm_handle *h, int32_t cap, int32_t *n_owned, double *r, double *v, int32_t *gid);
 
 /* ---- errors --------------------------------------------------------- */
 /* Copies the message of the last failing call on this thread. */

@@ -263,3 +263,35 @@ def test_fp32_couette_job_follows_oracle(gpu_lib, tpm):
     assert ns == res["nsamples"]
     np.testing.assert_allclose(res["ptensor"], P, rtol=1e-5, atol=1e-5)
     np.testing.assert_allclose(rg, o.r, rtol=0, atol=2e-6)
+
+
+@pytest.mark.parametrize("tpm", [0, 4])
+def test_list_build_tiles_give_identical_jobs(gpu_lib, tpm):
+    """The list build's tile (one cell per warp, 2x2x2 cells per warp, or the
+    autotuner's choice per job density) changes no result bit: dense and
+    sparse jobs run to the same trajectories under all three."""
+    reps = [([8, 8, 8], 0.85, 1.0, 51), ([7, 7, 7], 0.3, 1.4, 52), ([9, 6, 7], 0.1, 1.2, 53),
+            ([6, 6, 6], 0.8, 0.9, 54)]
+    out = {}
+    for lb in (api.LIST_BUILD_CELLS, api.LIST_BUILD_BLOCKS, api.LIST_BUILD_AUTO):
+        e = engine(tpm=tpm, list_build=lb, ticks=10)
+        ids = []
+        for nu, rho, T, seed in reps:
+            r, v, dom = lj_replica(nu, rho, T, seed)
+            ids.append((e.submit(api.make_job(len(r), dom, 2.5, 120, tplot=40), r, v), len(r)))
+        e.run()
+        res = {x["job_id"]: x for x in e.results()}
+        out[lb] = [(res[j]["status"], res[j]["last"], res[j]["rebuilds"]) + e.job_state(j, n) for j, n in ids]
+        t, bb = e.tuning()
+        if lb == api.LIST_BUILD_CELLS:
+            assert bb == 0.0
+        elif lb == api.LIST_BUILD_BLOCKS:
+            assert bb >= 1e30
+        else:
+            assert bb in (0.0, 4.0, 8.0, 16.0, 1e30)
+        assert t in ((1, 2, 4, 8, 16) if tpm == 0 else (tpm,))
+        e.close()
+    for lb in (api.LIST_BUILD_BLOCKS, api.LIST_BUILD_AUTO):
+        for a, b in zip(out[api.LIST_BUILD_CELLS], out[lb]):
+            assert a[0] == b[0] == 0 and a[1] == b[1] and a[2] == b[2]
+            assert np.array_equal(a[3], b[3]) and np.array_equal(a[4], b[4])
