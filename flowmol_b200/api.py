@@ -242,6 +242,28 @@ def lib():
             "fm_force_kernel_timing": [h, C.c_int32],
             "fm_get_force_kernel_time": [h, P(C.c_double), P(C.c_int64)],
             "fm_get_launch_count": [h, P(C.c_int64)],
+            "fm_dd_create": [P(FmParams), P(C.c_int32), P(C.c_int32), P(C.c_int32), C.c_int32, P(h)],
+            "fm_dd_set_plan": [h, C.c_int32, P(C.c_int32), P(C.c_int32), P(C.c_int32), P(C.c_int32),
+                               P(C.c_int32), P(C.c_int32)],
+            "fm_dd_upload": [h, C.c_int32, P(C.c_double), P(C.c_double), P(C.c_int32)],
+            "fm_dd_classify": [h, C.c_int32, P(C.c_int32)],
+            "fm_dd_pack_emigrants": [h, C.c_void_p],
+            "fm_dd_immigrate": [h, C.c_void_p, C.c_int32],
+            "fm_dd_halo_counts": [h, P(C.c_int32)],
+            "fm_dd_pack_halo": [h, C.c_void_p],
+            "fm_dd_receive_halo": [h, C.c_void_p, C.c_int32],
+            "fm_dd_counts": [h, P(C.c_int32), P(C.c_int32)],
+            "fm_dd_cell_starts": [h, P(C.c_int32)],
+            "fm_dd_gather_positions": [h, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p],
+            "fm_dd_scatter_positions": [h, C.c_void_p, C.c_void_p, C.c_int32],
+            "fm_dd_move1": [h],
+            "fm_dd_vmax2": [h, P(C.c_uint64)],
+            "fm_dd_decide": [h, C.c_uint64, C.c_int32, C.c_int32, P(C.c_int32)],
+            "fm_dd_forces": [h, C.c_int32, C.c_int32, C.c_int32],
+            "fm_dd_sums": [h, P(C.c_double)],
+            "fm_dd_macro": [h, P(C.c_double), C.c_int32, C.c_double, P(FmMacro)],
+            "fm_dd_download": [h, C.c_int32, P(C.c_int32), P(C.c_double), P(C.c_double), P(C.c_int32)],
+            "fm_dd_pair_list": [h, P(C.c_int32), P(C.c_int32), P(C.c_int32), C.c_int64, P(C.c_int64)],
         }
         for name, args in sig.items():
             f = getattr(L, name)

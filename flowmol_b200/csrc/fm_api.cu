@@ -1928,3 +1928,33 @@ extern "C" int fm_dd_download(fm_handle *h, int32_t cap, int32_t *n_owned, doubl
     if (m > cap) return fail(FM_ERR_ARG, "more owned molecules than cap");
     return FM_OK;
 }
+
+extern "C" int fm_dd_pair_list(fm_handle *h, int32_t *owner, int32_t *partner, int32_t *partner_cell, int64_t cap,
+                               int64_t *n_out)
+{
+    FM_TRY(dd_ready(h, true, 2));
+    if (!n_out) return fail(FM_ERR_ARG, "null output");
+    const FmDev &d = h->d;
+    const size_t n = (size_t)d.n;
+    std::vector<int32_t> nnbr(n), slot(n), start((size_t)d.ncell + 1), nbr(fm::nb_rows((int)n) * (size_t)d.maxn);
+    FM_CUDA(cudaMemcpyAsync(nnbr.data(), d.nnbr, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, h->st));
+    FM_CUDA(cudaMemcpyAsync(slot.data(), d.slot_of, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, h->st));
+    FM_CUDA(cudaMemcpyAsync(start.data(), d.cell_start, sizeof(int32_t) * start.size(), cudaMemcpyDeviceToHost, h->st));
+    FM_CUDA(cudaMemcpyAsync(nbr.data(), d.nbr, sizeof(int32_t) * nbr.size(), cudaMemcpyDeviceToHost, h->st));
+    FM_CUDA(cudaStreamSynchronize(h->st));
+    int64_t k = 0;
+    for (size_t i = 0; i < n; i++) {
+        for (int q = 0; q < nnbr[i]; q++) {
+            const int32_t j = nbr[fm::nb_row((int)i, d.maxn) + fm::nb_col(q)] & fm::NB_INDEX_MASK;
+            if (k < cap) {
+                if (owner) owner[k] = slot[i];
+                if (partner) partner[k] = slot[(size_t)j];
+                if (partner_cell)
+                    partner_cell[k] = (int32_t)(std::upper_bound(start.begin(), start.end(), j) - start.begin()) - 1;
+            }
+            k++;
+        }
+    }
+    *n_out = k;
+    return FM_OK;
+}

@@ -578,6 +578,10 @@ FM_API int fm_dd_sums(fm_handle *h, double *sums);
 FM_API int fm_dd_macro(fm_handle *h, const double *sums, int32_t iter, double simtime, fm_macro *out);
 /* The owned molecules in slot order (r, v (3, n) column-major, gid). */
 FM_API int fm_dd_download(fm_handle *h, int32_t cap, int32_t *n_owned, double *r, double *v, int32_t *gid);
+/* Neighbour rows as (owner, partner) global numbers and the partner's local
+ * extended cell (a halo cell's image code is the plan's), for tests. */
+FM_API int fm_dd_pair_list(fm_handle *h, int32_t *owner, int32_t *partner, int32_t *partner_cell, int64_t cap,
+                           int64_t *n_out);
 
 /* ---- errors --------------------------------------------------------- */
 /* Copies the message of the last failing call on this thread. */
