@@ -71,6 +71,17 @@ __device__ __forceinline__ int4 ld_stream_int4(const int4 *p)
     return r;
 }
 
+// FP32 reciprocal of the precision form's pair magnitudes (s = 1/r^2): the
+// hardware's approximate reciprocal (rcp.approx.ftz.f32, about 1 ulp; r^2 is
+// never subnormal here), one instruction where a correctly rounded
+// reciprocal takes a short sequence with a slow path.
+__device__ __forceinline__ float rcp_f32(float x)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // Read-only gather of one double4 (32-byte aligned) as a single 256-bit load:
 // one L1 request per partner instead of two.
 __device__ __forceinline__ double4 ldg_pos(const double4 *p)

@@ -462,7 +462,7 @@ __device__ __forceinline__ void lj_pair(PairAcc &a, double dx, double dy, double
         }
     } else {
         // FP32 pair magnitude; the FP64 rij scales it (one conversion)
-        const float s = __frcp_rn((float)r2), s2 = s * s, s4 = s2 * s2;
+        const float s = rcp_f32((float)r2), s2 = s * s, s4 = s2 * s2;
         const double acc = (double)(48.0f * (s4 * s2 * s - 0.5f * s4));
         a.fx = fma(acc, dx, a.fx); a.fy = fma(acc, dy, a.fy); a.fz = fma(acc, dz, a.fz);
         if (rec) {
@@ -597,9 +597,15 @@ __global__ void __launch_bounds__(EF_THREADS, REC ? 2 : 4) k_e_force(EngDev d)
                 for (int q = 0; q < 4; q++) {
                     if (k0 + q >= cnt) break;
                     const int code = ev[q] >> NB_SHIFT_BITS;
-                    const double dx = __dsub_rn(pi.x, image(pj[q].x, (code & 3) - 1, s.L[0]));
-                    const double dy = __dsub_rn(pi.y, image(pj[q].y, ((code >> 2) & 3) - 1, s.L[1]));
-                    const double dz = __dsub_rn(pi.z, image(pj[q].z, ((code >> 4) & 3) - 1, s.L[2]));
+                    double xj = pj[q].x, yj = pj[q].y, zj = pj[q].z;
+                    if (code != NB_NOSHIFT) {  // rows of boundary cells only
+                        xj = image(xj, (code & 3) - 1, s.L[0]);
+                        yj = image(yj, ((code >> 2) & 3) - 1, s.L[1]);
+                        zj = image(zj, ((code >> 4) & 3) - 1, s.L[2]);
+                    }
+                    const double dx = __dsub_rn(pi.x, xj);
+                    const double dy = __dsub_rn(pi.y, yj);
+                    const double dz = __dsub_rn(pi.z, zj);
                     const double r2 = norm2_rn(dx, dy, dz);
                     if (r2 < s.rc2) lj_pair<PREC>(a, dx, dy, dz, r2, s.potshift, rec, ptens);
                 }

@@ -575,7 +575,7 @@ __device__ __forceinline__ double pair_acc(const FmDev &d, double r2, double dx,
                 vir += acc * r2;
             }
         } else {
-            const float s = __frcp_rn((float)r2);
+            const float s = rcp_f32((float)r2);
             const float s2 = s * s;
             float accf;
             if (wca) {
@@ -610,7 +610,7 @@ __device__ __forceinline__ double pair_acc(const FmDev &d, double r2, double dx,
             }
             return acc;
         } else {
-            const float s = __frcp_rn((float)r2);
+            const float s = rcp_f32((float)r2);
             const double acc = (double)((float)m.ceps * ((float)m.lr * powf(s, (float)m.er1) -
                                                          (float)m.ala * powf(s, (float)m.ea1)));
             fx = fma(acc, dx, fx); fy = fma(acc, dy, fy); fz = fma(acc, dz, fz);
@@ -633,7 +633,7 @@ __device__ __forceinline__ double pair_acc(const FmDev &d, double r2, double dx,
         return acc;
     } else {
         // FP32 pair magnitude; the FP64 rij scales it (one conversion)
-        const float s = __frcp_rn((float)r2);
+        const float s = rcp_f32((float)r2);
         const float s2 = s * s, s4 = s2 * s2;
         const double acc = (double)(48.0f * (s4 * s2 * s - 0.5f * s4));
         fx = fma(acc, dx, fx); fy = fma(acc, dy, fy); fz = fma(acc, dz, fz);
@@ -993,6 +993,65 @@ __device__ __forceinline__ void block_partials(const FmDev &d, double v[RS_N], i
     }
 }
 
+// Pair sum of molecule i over its list row: lane `lane` of the molecule's
+// TPM lanes takes 4 consecutive entries per iteration (one 16-byte load) and
+// issues their 4 gathers before any arithmetic.  Entries without an image
+// shift (all but the rows of boundary cells) skip the shift decoding.
+template <int TPM, bool REC, int PREC>
+__device__ __forceinline__ void list_pairs(const FmDev &d, const double4 *__restrict__ P, int i, int lane,
+                                           const double4 &pi, double &fx, double &fy, double &fz, double &pe,
+                                           double &vir, double (&rf)[6])
+{
+    const int cnt = d.nnbr[i];
+    const int32_t *__restrict__ L = d.nbr + nb_row(i, d.maxn);  // entries k0..k0+3 at L + nb_col(k0) (16-byte aligned)
+    const double Lx = d.L[0], Ly = d.L[1], Lz = d.L[2];
+    const double rc2 = d.rc2;
+    for (int k0 = lane * 4; k0 < cnt; k0 += 4 * TPM) {
+        const int4 e4 = ld_stream_int4(reinterpret_cast<const int4 *>(L + nb_col(k0)));
+        const int ev[4] = {e4.x, e4.y, e4.z, e4.w};
+        double4 pj[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+            if (k0 + q < cnt) pj[q] = ldg_pos(P + (ev[q] & NB_INDEX_MASK));
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            if (k0 + q >= cnt) break;
+            const int code = ev[q] >> NB_SHIFT_BITS;
+            double xj = pj[q].x, yj = pj[q].y, zj = pj[q].z;
+            if (code != NB_NOSHIFT) {
+                const int ssx = (code & 3) - 1, ssy = ((code >> 2) & 3) - 1, ssz = ((code >> 4) & 3) - 1;
+                xj = ssx ? __dadd_rn(xj, ssx > 0 ? Lx : -Lx) : xj;
+                yj = ssy ? __dadd_rn(yj, ssy > 0 ? Ly : -Ly) : yj;
+                zj = ssz ? __dadd_rn(zj, ssz > 0 ? Lz : -Lz) : zj;
+            }
+            const double dx = __dsub_rn(pi.x, xj);
+            const double dy = __dsub_rn(pi.y, yj);
+            const double dz = __dsub_rn(pi.z, zj);
+            const double r2 = norm2_rn(dx, dy, dz);
+            if (r2 < rc2) {
+                const double acc = pair_acc<PREC, REC>(d, r2, dx, dy, dz, pi.w, pj[q].w, fx, fy, fz, pe, vir);
+                // every partner of i in the full list: the half list's i and j sides
+                if (REC && d.pressure) add_rf(rf, acc, dx, dy, dz);
+            }
+        }
+    }
+}
+
+// Bonded terms and the integrator epilogue of molecule i once its pair sum is
+// complete; returns |v|^2 after a position update (epilogue()).
+template <bool REC, int MODE, int PREC>
+__device__ __forceinline__ double owner_finish(const FmDev &d, int pset, const double4 *__restrict__ P, int i,
+                                               double fx, double fy, double fz, double pe, double vir,
+                                               double (&part)[RS_N], double (&rf)[6])
+{
+    if (d.potential_flag == 1) fene_bonds<REC, (PREC & 2) != 0>(d, P, i, fx, fy, fz, pe, vir, rf);
+    if constexpr ((PREC & 2) != 0) {  // angular_potential needs the Mie types
+        if (d.angular) angular_forces(d, P, i, fx, fy, fz);
+    }
+    // a(:,i) = sum acc rij / mass (LJ_mass = 1; Mie_mass by type)
+    return epilogue<REC, MODE, (PREC & 2) != 0>(d, pset, i, P[i], fx, fy, fz, pe, vir, part, rf);
+}
+
 template <int TPM, bool REC, int MODE, int PREC>
 __global__ void __launch_bounds__(FORCE_THREADS) k_force(FmDev d)
 {
@@ -1006,41 +1065,7 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force(FmDev d)
     const bool active = i < d.n;
     double fx = 0.0, fy = 0.0, fz = 0.0, pe = 0.0, vir = 0.0;
     double rf[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    if (active) {
-        const double4 pi = P[i];
-        const int cnt = d.nnbr[i];
-        const int32_t *__restrict__ L = d.nbr + nb_row(i, d.maxn);  // entries k0..k0+3 at L + nb_col(k0) (16-byte aligned)
-        const double Lx = d.L[0], Ly = d.L[1], Lz = d.L[2];
-        const double rc2 = d.rc2;
-        // each lane takes 4 consecutive entries per iteration (one 16-byte load)
-        // and issues their 4 gathers before any arithmetic
-        for (int k0 = lane * 4; k0 < cnt; k0 += 4 * TPM) {
-            const int4 e4 = ld_stream_int4(reinterpret_cast<const int4 *>(L + nb_col(k0)));
-            const int ev[4] = {e4.x, e4.y, e4.z, e4.w};
-            double4 pj[4];
-#pragma unroll
-            for (int q = 0; q < 4; q++)
-                if (k0 + q < cnt) pj[q] = ldg_pos(P + (ev[q] & NB_INDEX_MASK));
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                if (k0 + q >= cnt) break;
-                const int code = ev[q] >> NB_SHIFT_BITS;
-                const int ssx = (code & 3) - 1, ssy = ((code >> 2) & 3) - 1, ssz = ((code >> 4) & 3) - 1;
-                const double xj = ssx ? __dadd_rn(pj[q].x, ssx > 0 ? Lx : -Lx) : pj[q].x;
-                const double yj = ssy ? __dadd_rn(pj[q].y, ssy > 0 ? Ly : -Ly) : pj[q].y;
-                const double zj = ssz ? __dadd_rn(pj[q].z, ssz > 0 ? Lz : -Lz) : pj[q].z;
-                const double dx = __dsub_rn(pi.x, xj);
-                const double dy = __dsub_rn(pi.y, yj);
-                const double dz = __dsub_rn(pi.z, zj);
-                const double r2 = norm2_rn(dx, dy, dz);
-                if (r2 < rc2) {
-                    const double acc = pair_acc<PREC, REC>(d, r2, dx, dy, dz, pi.w, pj[q].w, fx, fy, fz, pe, vir);
-                    // every partner of i in the full list: the half list's i and j sides
-                    if (REC && d.pressure) add_rf(rf, acc, dx, dy, dz);
-                }
-            }
-        }
-    }
+    if (active) list_pairs<TPM, REC, PREC>(d, P, i, lane, P[i], fx, fy, fz, pe, vir, rf);
     if (TPM > 1) {
 #pragma unroll
         for (int o = TPM / 2; o > 0; o >>= 1) {
@@ -1059,14 +1084,7 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force(FmDev d)
     }
     double part[RS_N] = {};
     double m2 = 0.0;
-    if (active && lane == 0 && d.potential_flag == 1)
-        fene_bonds<REC, (PREC & 2) != 0>(d, P, i, fx, fy, fz, pe, vir, rf);
-    if constexpr ((PREC & 2) != 0) {  // angular_potential needs the Mie types
-        if (active && lane == 0 && d.angular) angular_forces(d, P, i, fx, fy, fz);
-    }
-    // a(:,i) = sum acc rij / mass (LJ_mass = 1; Mie_mass by type)
-    if (active && lane == 0)
-        m2 = epilogue<REC, MODE, (PREC & 2) != 0>(d, pset, i, P[i], fx, fy, fz, pe, vir, part, rf);
+    if (active && lane == 0) m2 = owner_finish<REC, MODE, PREC>(d, pset, P, i, fx, fy, fz, pe, vir, part, rf);
     if (REC) block_partials(d, part, blockIdx.x);
     if (MODE >= 2) block_vmax2(d, m2);
 }

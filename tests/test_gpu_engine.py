@@ -269,10 +269,13 @@ def test_fp32_couette_job_follows_oracle(gpu_lib, tpm):
 def test_list_build_tiles_give_identical_jobs(gpu_lib, tpm):
     """The list build's tile (one cell per warp, 2x2x2 cells per warp, or the
     autotuner's choice per job density) changes no result bit: dense and
-    sparse jobs run to the same trajectories under all three."""
+    sparse jobs run to the same trajectories under all three.  With the lanes
+    per molecule autotuned as well (tpm 0), two engines may time their way to
+    different lane counts, which sum each row in a different order: such a
+    pair is compared to FP64 rounding instead."""
     reps = [([8, 8, 8], 0.85, 1.0, 51), ([7, 7, 7], 0.3, 1.4, 52), ([9, 6, 7], 0.1, 1.2, 53),
             ([6, 6, 6], 0.8, 0.9, 54)]
-    out = {}
+    out, lanes = {}, {}
     for lb in (api.LIST_BUILD_CELLS, api.LIST_BUILD_BLOCKS, api.LIST_BUILD_AUTO):
         e = engine(tpm=tpm, list_build=lb, ticks=10)
         ids = []
@@ -283,6 +286,7 @@ def test_list_build_tiles_give_identical_jobs(gpu_lib, tpm):
         res = {x["job_id"]: x for x in e.results()}
         out[lb] = [(res[j]["status"], res[j]["last"], res[j]["rebuilds"]) + e.job_state(j, n) for j, n in ids]
         t, bb = e.tuning()
+        lanes[lb] = t
         if lb == api.LIST_BUILD_CELLS:
             assert bb == 0.0
         elif lb == api.LIST_BUILD_BLOCKS:
@@ -292,6 +296,14 @@ def test_list_build_tiles_give_identical_jobs(gpu_lib, tpm):
         assert t in ((1, 2, 4, 8, 16) if tpm == 0 else (tpm,))
         e.close()
     for lb in (api.LIST_BUILD_BLOCKS, api.LIST_BUILD_AUTO):
+        same_lanes = lanes[lb] == lanes[api.LIST_BUILD_CELLS]
         for a, b in zip(out[api.LIST_BUILD_CELLS], out[lb]):
-            assert a[0] == b[0] == 0 and a[1] == b[1] and a[2] == b[2]
-            assert np.array_equal(a[3], b[3]) and np.array_equal(a[4], b[4])
+            assert a[0] == b[0] == 0 and a[2] == b[2]
+            if same_lanes:
+                assert a[1] == b[1]
+                assert np.array_equal(a[3], b[3]) and np.array_equal(a[4], b[4])
+            else:
+                assert a[1]["iter"] == b[1]["iter"]
+                assert a[1]["totenergy"] == pytest.approx(b[1]["totenergy"], rel=1e-11)
+                np.testing.assert_allclose(a[3], b[3], rtol=0, atol=1e-9)
+                np.testing.assert_allclose(a[4], b[4], rtol=0, atol=1e-9)
