@@ -5,7 +5,10 @@
 // and move(2), and the record reduction on tplot steps.  Move(2) of one
 // iteration and move(1) of the next are fused into the force kernel, so a
 // non-rebuild step is one force launch plus the small decision kernel and
-// the gated no-op rebuild launches.
+// the rebuild branch.  Where CUDA graphs with conditional nodes are available
+// the rebuild branch of a step is one graph launch: the decision kernel sets
+// the condition of an IF node whose body holds the rebuild kernels, so a step
+// without a rebuild launches the decision and the force kernel only.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -97,6 +100,13 @@ struct fm_handle {
     int32_t *dd_dev = nullptr;  // device block behind x (plan and counters)
     double *dd_sums = nullptr;  // device [RS_N]
     std::vector<int32_t> dd_counts;
+    // rebuild branch as a CUDA graph, per `flip` (whether the previous force
+    // kernel already did this step's move(1)); rebuilt when the device state
+    // it was captured with (FmDev) changes
+    cudaGraphExec_t rbx[2] = {nullptr, nullptr};
+    FmDev rbd[2]{};
+    bool rb_off = false;          // graphs unavailable here: per-kernel launches
+    cudaStream_t cap_st = nullptr;
 };
 
 // ---------------------------------------------------------------------------
@@ -168,8 +178,19 @@ static int dalloc(T **ptr, size_t count)
     return FM_OK;
 }
 
+static void release_graphs(fm_handle *h)
+{
+    for (int f = 0; f < 2; f++) {
+        if (h->rbx[f]) cudaGraphExecDestroy(h->rbx[f]);
+        h->rbx[f] = nullptr;
+    }
+}
+
 static void release(fm_handle *h)
 {
+    release_graphs(h);
+    if (h->cap_st) cudaStreamDestroy(h->cap_st);
+    h->cap_st = nullptr;
     for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
     h->ev.clear();
     FmDev &d = h->d;
@@ -977,18 +998,107 @@ static void queue_decide(fm_handle *h, int it, int flip)
     h->launches += 1;
 }
 
+static void queue_rebuild_branch(fm_handle *h, int it, int flip);
+
 static void queue_rebuild_check(fm_handle *h, int it, int flip)
 {
     const fm_params &p = h->p;
-    queue_decide(h, it, flip);
     if (p.force_list != 0) {
-        queue_cells(h, 1, 1);
-        queue_build(h, 1, it);
-        h->launches += 1;
+        queue_rebuild_branch(h, it, flip);
     } else {
+        queue_decide(h, it, flip);
         fm::launch_wrap_bin(h->d, 1, 0, 1, it, h->st);
         h->launches += 1;
     }
+}
+
+// The rebuild branch of one iteration as a graph: k_decide_graph (the
+// iteration from the device counter g_iter) and an IF node whose body is the
+// rebuild pipeline of queue_cells + queue_build, captured on a private stream
+// without programmatic launch edges.  Returns null (and the caller launches
+// the kernels one by one) where the graph cannot be made.
+static cudaGraphExec_t rebuild_graph(fm_handle *h, int flip)
+{
+    if (h->rb_off) return nullptr;
+    if (h->rbx[flip] && std::memcmp(&h->rbd[flip], &h->d, sizeof(FmDev)) == 0) return h->rbx[flip];
+    if (h->rbx[flip]) { cudaGraphExecDestroy(h->rbx[flip]); h->rbx[flip] = nullptr; }
+    const FmDev &d = h->d;
+    const fm_params &p = h->p;
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ex = nullptr;
+    bool ok = (h->cap_st || cudaStreamCreateWithFlags(&h->cap_st, cudaStreamNonBlocking) == cudaSuccess) &&
+              cudaGraphCreate(&g, 0) == cudaSuccess;
+    cudaGraphConditionalHandle cond{};
+    cudaGraphNode_t dec = nullptr, ifn = nullptr;
+    if (ok) ok = cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault) == cudaSuccess;
+    const int body_kernels = 8 + (d.tile ? 1 : 0) + (d.angular ? 1 : 0);
+    fm::pdl_capture = true;
+    if (ok && cudaStreamBeginCaptureToGraph(h->cap_st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) ==
+                  cudaSuccess) {
+        fm::launch_decide_graph(d, flip, p.rebuild_criteria, p.fixed_rebuild, h->half_min_delta, cond, body_kernels,
+                                h->cap_st);
+        ok = cudaStreamEndCapture(h->cap_st, &g) == cudaSuccess;
+    } else {
+        ok = false;
+    }
+    if (ok) {  // the decision is the graph's only node
+        size_t n = 1;
+        ok = cudaGraphGetNodes(g, &dec, &n) == cudaSuccess && n == 1;
+    }
+    cudaGraph_t body = nullptr;
+    if (ok) {
+        cudaGraphNodeParams cp{};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = cond;
+        cp.conditional.type = cudaGraphCondTypeIf;
+        cp.conditional.size = 1;
+        ok = cudaGraphAddNode(&ifn, g, &dec, 1, &cp) == cudaSuccess;
+        if (ok) body = cp.conditional.phGraph_out[0];
+    }
+    if (ok && cudaStreamBeginCaptureToGraph(h->cap_st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) ==
+                  cudaSuccess) {
+        fm::launch_wrap_bin(d, 1, 1, 1, fm::ITER_DEVICE, h->cap_st);
+        fm::launch_scan_cells(d, 1, h->cap_st);
+        fm::launch_scatter(d, 1, h->cap_st);
+        fm::launch_reorder(d, 1, h->tpos, h->tuidx, h->cap_st);
+        if (d.tile) fm::launch_blk_seg(d, 1, fm::ITER_DEVICE, h->cap_st);
+        fm::launch_build_nlist(d, 1, fm::ITER_DEVICE, h->cap_st);
+        if (d.angular) fm::launch_angular_order(d, 1, fm::ITER_DEVICE, h->cap_st);
+        ok = cudaStreamEndCapture(h->cap_st, &body) == cudaSuccess;
+    } else {
+        ok = false;
+    }
+    fm::pdl_capture = false;
+    if (ok) ok = cudaGraphInstantiate(&ex, g, 0) == cudaSuccess;
+    if (g) cudaGraphDestroy(g);
+    if (!ok) {
+        if (ex) cudaGraphExecDestroy(ex);
+        cudaGetLastError();  // the per-kernel path takes over
+        h->rb_off = true;
+        return nullptr;
+    }
+    h->rbx[flip] = ex;
+    h->rbd[flip] = h->d;
+    return ex;
+}
+
+// The rebuild check of iteration `it` on the cell path: the graph when there
+// is one (g_iter set by the caller at the start of its range), else the
+// decision and the gated rebuild kernels one launch each.
+static void queue_rebuild_branch(fm_handle *h, int it, int flip)
+{
+    const fm_params &p = h->p;
+    cudaGraphExec_t ex = rebuild_graph(h, flip);
+    if (ex) {
+        if (p.rebuild_criteria == 2) { fm::launch_disp(h->d, h->st); h->launches += 1; }
+        cudaGraphLaunch(ex, h->st);
+        h->launches += 1;  // the decision; the body's kernels are counted on the device
+        return;
+    }
+    queue_decide(h, it, flip);
+    queue_cells(h, 1, 1);
+    queue_build(h, 1, it);
+    h->launches += 1;
 }
 
 // Leap-frog iterations [first, first + nsteps): forces + record + move fused,
@@ -996,6 +1106,7 @@ static void queue_rebuild_check(fm_handle *h, int it, int flip)
 static int queue_steps_lfv(fm_handle *h, int first, int nsteps, const std::vector<double> &simtime_after,
                            int range_offset)
 {
+    if (h->p.force_list != 0 && nsteps > 0) fm::launch_set_graph_iter(h->d, first, h->st);
     for (int s = 0; s < nsteps; s++) {
         const int it = first + s;
         h->iter = it;
@@ -1016,17 +1127,17 @@ static int queue_steps(fm_handle *h, int first, int nsteps, int phase, const std
     const fm_params &p = h->p;
     if (p.integration_algorithm == 0) return queue_steps_lfv(h, first, nsteps, simtime_after, range_offset);
     bool fused_move1 = false;  // the previous force kernel already did move(1)
+    if (p.force_list != 0 && nsteps > (phase == 1 ? 1 : 0))  // the first decision's iteration
+        fm::launch_set_graph_iter(h->d, phase == 1 ? first + 1 : first, h->st);
     for (int s = 0; s < nsteps; s++) {
         const int it = first + s;
         h->iter = it;
         if (!(s == 0 && phase == 1)) {
             if (!fused_move1) { fm::launch_move1(h->d, h->st); h->launches += 1; }
-            queue_decide(h, it, fused_move1 ? 1 : 0);
             if (p.force_list != 0) {
-                queue_cells(h, 1, 1);
-                queue_build(h, 1, it);
-                h->launches += 1;
+                queue_rebuild_branch(h, it, fused_move1 ? 1 : 0);
             } else {
+                queue_decide(h, it, fused_move1 ? 1 : 0);
                 fm::launch_wrap_bin(h->d, 1, 0, 1, it, h->st);
                 h->launches += 1;
             }
@@ -1481,7 +1592,13 @@ extern "C" int fm_get_force_kernel_time(fm_handle *h, double *ms, int64_t *launc
 extern "C" int fm_get_launch_count(fm_handle *h, int64_t *launches)
 {
     if (!h || !launches) return fail(FM_ERR_ARG, "null argument");
-    *launches = h->launches;
+    int64_t body = 0;  // kernels run inside the rebuild graph's conditional body
+    if (h->d.sc) {
+        fm::FmScalars s;
+        FM_TRY(read_scalars(h, &s));
+        body = s.graph_kernels;
+    }
+    *launches = h->launches + body;
     return FM_OK;
 }
 

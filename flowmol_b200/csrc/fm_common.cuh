@@ -42,7 +42,14 @@ struct FmScalars {
     int32_t pcount;           // samples in pacc
     int32_t tile_next;        // tiled force kernel: next block to hand out (the last taker resets it)
     int32_t umax;             // tiled path: largest staged neighbourhood seen at the last build
+    int32_t g_iter;           // rebuild graph: iteration its next decision is for
+    int32_t cur_iter;         // rebuild graph: iteration of the last decision (errors in its body)
+    int64_t graph_kernels;    // rebuild graph: kernels its conditional body has run
 };
+
+// Iteration argument of a kernel inside the rebuild graph's body: the
+// iteration of the decision that opened the body (FmScalars::cur_iter).
+constexpr int ITER_DEVICE = -2147483647 - 1;
 
 // Partial sums of one record step, one row per force-kernel block.
 // With pressure_outflag 1 the six distinct components of v v + rf/2 follow
@@ -231,6 +238,10 @@ void launch_move2(const FmDev &d, cudaStream_t st);          // pass 2 in place
 void launch_vmax(const FmDev &d, cudaStream_t st);           // vmax2 of current v
 void launch_move_lfv(const FmDev &d, cudaStream_t st);       // leap-frog move in place + vmax2
 void launch_disp(const FmDev &d, cudaStream_t st);            // criterion 2: rdisp += v dt, max component
+extern thread_local bool pdl_capture;  // set while a graph is captured: launches without PDL edges
+void launch_decide_graph(const FmDev &d, int flip, int rebuild_criteria, int fixed_rebuild, double half_min_delta,
+                         cudaGraphConditionalHandle cond, int body_kernels, cudaStream_t st);
+void launch_set_graph_iter(const FmDev &d, int iter, cudaStream_t st);
 void launch_decide(const FmDev &d, int iter, int flip, int rebuild_criteria, int fixed_rebuild,
                    double half_min_delta, cudaStream_t st);
 // Rebuild pipeline; gated = 1 makes each kernel a no-op unless sc->rebuild.

@@ -22,6 +22,10 @@ __device__ __forceinline__ void pdl_enter()
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
+// Set while a CUDA graph is being captured on this thread: its kernels are
+// ordered by the graph's edges, launched without the attribute below.
+extern thread_local bool pdl_capture;
+
 // Launches k with programmatic stream serialization: the next kernel of the
 // step may be launched while k's last blocks run, and waits in pdl_enter for
 // k to complete before it reads anything (so the chain of small, often gated
@@ -38,7 +42,7 @@ void pdl_launch(void (*k)(P...), dim3 grid, dim3 block, cudaStream_t st, A... ar
     c.dynamicSmemBytes = 0;
     c.stream = st;
     c.attrs = at;
-    c.numAttrs = 1;
+    c.numAttrs = pdl_capture ? 0 : 1;
     cudaLaunchKernelEx(&c, k, args...);
 }
 
@@ -55,7 +59,7 @@ void pdl_launch_smem(void (*k)(P...), dim3 grid, dim3 block, size_t smem, cudaSt
     c.dynamicSmemBytes = smem;
     c.stream = st;
     c.attrs = at;
-    c.numAttrs = 1;
+    c.numAttrs = pdl_capture ? 0 : 1;
     cudaLaunchKernelEx(&c, k, args...);
 }
 

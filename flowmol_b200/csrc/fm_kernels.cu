@@ -21,12 +21,15 @@
 
 namespace fm {
 
+thread_local bool pdl_capture = false;
+
 namespace {
 
 __device__ __forceinline__ bool frozen(const FmDev &d) { return (d.sc->status & ST_FATAL) != 0u; }
 
 __device__ __forceinline__ void raise_status(const FmDev &d, uint32_t bit, int iter)
 {
+    if (iter == ITER_DEVICE) iter = d.sc->cur_iter;
     uint32_t old = atomicOr(&d.sc->status, bit);
     if ((old & ST_FATAL) == 0u) d.sc->fail_iter = iter;
 }
@@ -183,11 +186,10 @@ __global__ void k_disp(FmDev d)
 // rebuild decision (simulation_checkrebuild.f90:34, 83-99, 101-103, 106-121, 148-155)
 // ---------------------------------------------------------------------------
 
-__global__ void k_decide(FmDev d, int iter, int flip, int crit, int fixed_rebuild, double half_min_delta)
+__device__ __forceinline__ int decide(const FmDev &d, int iter, int flip, int crit, int fixed_rebuild,
+                                      double half_min_delta)
 {
-    pdl_enter();
     FmScalars *s = d.sc;
-    if (s->status & ST_FATAL) return;
     if (flip) s->pset ^= 1;
     int rebuild = ((iter + 1) % d.tplot) == 0 ? 1 : 0;
     if (crit == 0) {
@@ -208,7 +210,35 @@ __global__ void k_decide(FmDev d, int iter, int flip, int crit, int fixed_rebuil
         s->rebuilds += 1;
     }
     s->rebuild = rebuild;
+    return rebuild;
 }
+
+__global__ void k_decide(FmDev d, int iter, int flip, int crit, int fixed_rebuild, double half_min_delta)
+{
+    pdl_enter();
+    if (d.sc->status & ST_FATAL) return;
+    decide(d, iter, flip, crit, fixed_rebuild, half_min_delta);
+}
+
+// The decision as the first node of the rebuild graph (fm_api.cu): the
+// iteration comes from the device (g_iter, set by the host at the start of a
+// range and advanced here), and the outcome opens the graph's conditional
+// body -- the rebuild kernels -- or skips it without launching anything.  A
+// frozen state skips it (the handle's default, 0).
+__global__ void k_decide_graph(FmDev d, int flip, int crit, int fixed_rebuild, double half_min_delta,
+                               cudaGraphConditionalHandle cond, int body_kernels)
+{
+    FmScalars *s = d.sc;
+    const int iter = s->g_iter;
+    s->g_iter = iter + 1;
+    s->cur_iter = iter;
+    if (s->status & ST_FATAL) return;
+    const int rebuild = decide(d, iter, flip, crit, fixed_rebuild, half_min_delta);
+    if (rebuild) s->graph_kernels += body_kernels;
+    cudaGraphSetConditional(cond, rebuild ? 1u : 0u);
+}
+
+__global__ void k_set_graph_iter(FmDev d, int iter) { d.sc->g_iter = iter; }
 
 // ---------------------------------------------------------------------------
 // cell binning by counting sort (linklist.f90:2645-2679; sendmols wrap
@@ -1615,6 +1645,15 @@ void launch_move2(const FmDev &d, cudaStream_t st) { pdl_launch(k_move2, nblk(d.
 void launch_vmax(const FmDev &d, cudaStream_t st) { pdl_launch(k_vmax, nblk(d.n, 256), 256, st, d); }
 void launch_move_lfv(const FmDev &d, cudaStream_t st) { pdl_launch(k_move_lfv, nblk(d.n, 256), 256, st, d); }
 void launch_disp(const FmDev &d, cudaStream_t st) { pdl_launch(k_disp, nblk(d.n, 256), 256, st, d); }
+
+void launch_decide_graph(const FmDev &d, int flip, int crit, int fixed_rebuild, double half_min_delta,
+                         cudaGraphConditionalHandle cond, int body_kernels, cudaStream_t st)
+{
+    k_decide_graph<<<1, 1, 0, st>>>(d, flip, crit, fixed_rebuild > 0 ? fixed_rebuild : 1, half_min_delta, cond,
+                                    body_kernels);
+}
+
+void launch_set_graph_iter(const FmDev &d, int iter, cudaStream_t st) { k_set_graph_iter<<<1, 1, 0, st>>>(d, iter); }
 
 void launch_decide(const FmDev &d, int iter, int flip, int crit, int fixed_rebuild, double half_min_delta,
                    cudaStream_t st)

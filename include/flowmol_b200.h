@@ -477,7 +477,9 @@ FM_API int fm_get_force_kernel_time(fm_handle *h, double *ms, int64_t *launches)
  * samples. */
 FM_API int fm_set_pressure_outflag(fm_handle *h, int32_t flag);
 FM_API int fm_get_pressure_tensor(fm_handle *h, double P[9], int32_t *nsamples, int32_t reset);
-/* Kernels this handle has launched since creation. */
+/* Kernels this handle has launched since creation: the host's launches plus
+ * the rebuild kernels that the device ran inside the rebuild graph of a step
+ * (waits for the handle's stream). */
 FM_API int fm_get_launch_count(fm_handle *h, int64_t *launches);
 
 /* ---- forces without device allocation -------------------------------- */
