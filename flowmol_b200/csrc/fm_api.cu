@@ -103,10 +103,12 @@ struct fm_handle {
     // rebuild branch as a CUDA graph, per `flip` (whether the previous force
     // kernel already did this step's move(1)); rebuilt when the device state
     // it was captured with (FmDev) changes
-    cudaGraphExec_t rbx[2] = {nullptr, nullptr};
-    FmDev rbd[2]{};
+    // [flip] rebuild branch, [2 + flip] STEP_GRAPH_K whole iterations
+    cudaGraphExec_t rbx[4] = {nullptr, nullptr, nullptr, nullptr};
+    FmDev rbd[4]{};
+    int rbt[4] = {0, 0, 0, 0};    // lanes per molecule the force kernels were captured with
     bool rb_off = false;          // graphs unavailable here: per-kernel launches
-    cudaStream_t cap_st = nullptr;
+    cudaStream_t cap_st = nullptr, cap_st2 = nullptr;
 };
 
 // ---------------------------------------------------------------------------
@@ -180,7 +182,7 @@ static int dalloc(T **ptr, size_t count)
 
 static void release_graphs(fm_handle *h)
 {
-    for (int f = 0; f < 2; f++) {
+    for (int f = 0; f < 4; f++) {
         if (h->rbx[f]) cudaGraphExecDestroy(h->rbx[f]);
         h->rbx[f] = nullptr;
     }
@@ -190,7 +192,8 @@ static void release(fm_handle *h)
 {
     release_graphs(h);
     if (h->cap_st) cudaStreamDestroy(h->cap_st);
-    h->cap_st = nullptr;
+    if (h->cap_st2) cudaStreamDestroy(h->cap_st2);
+    h->cap_st = h->cap_st2 = nullptr;
     for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
     h->ev.clear();
     FmDev &d = h->d;
@@ -1012,59 +1015,91 @@ static void queue_rebuild_check(fm_handle *h, int it, int flip)
     }
 }
 
-// The rebuild branch of one iteration as a graph: k_decide_graph (the
-// iteration from the device counter g_iter) and an IF node whose body is the
-// rebuild pipeline of queue_cells + queue_build, captured on a private stream
-// without programmatic launch edges.  Returns null (and the caller launches
-// the kernels one by one) where the graph cannot be made.
-static cudaGraphExec_t rebuild_graph(fm_handle *h, int flip)
+// The rebuild branch of an iteration, appended to the graph being captured
+// on h->cap_st: k_decide_graph (the iteration from the device counter g_iter)
+// and an IF node whose body is the rebuild pipeline of queue_cells +
+// queue_build, captured on h->cap_st2 with programmatic edges between its
+// kernels as the stream launches have.
+static bool capture_branch(fm_handle *h, int flip)
 {
-    if (h->rb_off) return nullptr;
-    if (h->rbx[flip] && std::memcmp(&h->rbd[flip], &h->d, sizeof(FmDev)) == 0) return h->rbx[flip];
-    if (h->rbx[flip]) { cudaGraphExecDestroy(h->rbx[flip]); h->rbx[flip] = nullptr; }
     const FmDev &d = h->d;
     const fm_params &p = h->p;
+    cudaStreamCaptureStatus cst;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    if (cudaStreamGetCaptureInfo(h->cap_st, &cst, nullptr, &g, nullptr, nullptr) != cudaSuccess || !g) return false;
+    cudaGraphConditionalHandle cond{};
+    if (cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault) != cudaSuccess) return false;
+    const int body_kernels = 8 + (d.tile ? 1 : 0) + (d.angular ? 1 : 0);
+    fm::launch_decide_graph(d, flip, p.rebuild_criteria, p.fixed_rebuild, h->half_min_delta, cond, body_kernels,
+                            h->cap_st);
+    if (cudaStreamGetCaptureInfo(h->cap_st, &cst, nullptr, nullptr, &deps, &nd) != cudaSuccess) return false;
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t ifn = nullptr;
+    if (cudaGraphAddNode(&ifn, g, deps, nd, &cp) != cudaSuccess) return false;
+    if (cudaStreamUpdateCaptureDependencies(h->cap_st, &ifn, 1, cudaStreamSetCaptureDependencies) != cudaSuccess)
+        return false;
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    if (cudaStreamBeginCaptureToGraph(h->cap_st2, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) !=
+        cudaSuccess)
+        return false;
+    fm::pdl_capture = true;  // the body's first kernel has no predecessor to overlap
+    fm::launch_wrap_bin(d, 1, 1, 1, fm::ITER_DEVICE, h->cap_st2);
+    fm::pdl_capture = false;
+    fm::launch_scan_cells(d, 1, h->cap_st2);
+    fm::launch_scatter(d, 1, h->cap_st2);
+    fm::launch_reorder(d, 1, h->tpos, h->tuidx, h->cap_st2);
+    if (d.tile) fm::launch_blk_seg(d, 1, fm::ITER_DEVICE, h->cap_st2);
+    fm::launch_build_nlist(d, 1, fm::ITER_DEVICE, h->cap_st2);
+    if (d.angular) fm::launch_angular_order(d, 1, fm::ITER_DEVICE, h->cap_st2);
+    fm::pdl_capture = true;
+    return cudaStreamEndCapture(h->cap_st2, &body) == cudaSuccess;
+}
+
+// Iterations per graph launch in the middle of a range.
+constexpr int STEP_GRAPH_K = 8;
+
+// No iteration of [it, it + k) is a record step.
+static bool no_record_in(int it, int k, int tplot)
+{
+    for (int j = 0; j < k; j++)
+        if (((it + j) % tplot) == 0) return false;
+    return true;
+}
+
+// Graph of `k` iterations (k = 0: the rebuild branch of one iteration only):
+// per iteration the rebuild branch and, for k > 0, the non-recording force
+// kernel with move(2) and the next move(1) (mode 2), as queue_steps launches
+// them for an iteration in the middle of a range.  The first branch takes
+// `flip`, the later ones 1 (move(1) was fused into the force kernel before
+// them).  Cached per (flip, k) until the device state it was captured with
+// (FmDev) or the lanes per molecule change; null where graphs cannot be made.
+static cudaGraphExec_t step_graph(fm_handle *h, int flip, int k)
+{
+    if (h->rb_off) return nullptr;
+    const int slot = 2 * (k > 0) + flip;
+    if (h->rbx[slot] && h->rbt[slot] == h->tpm && std::memcmp(&h->rbd[slot], &h->d, sizeof(FmDev)) == 0)
+        return h->rbx[slot];
+    if (h->rbx[slot]) { cudaGraphExecDestroy(h->rbx[slot]); h->rbx[slot] = nullptr; }
+    bool ok = (h->cap_st || cudaStreamCreateWithFlags(&h->cap_st, cudaStreamNonBlocking) == cudaSuccess) &&
+              (h->cap_st2 || cudaStreamCreateWithFlags(&h->cap_st2, cudaStreamNonBlocking) == cudaSuccess);
     cudaGraph_t g = nullptr;
     cudaGraphExec_t ex = nullptr;
-    bool ok = (h->cap_st || cudaStreamCreateWithFlags(&h->cap_st, cudaStreamNonBlocking) == cudaSuccess) &&
-              cudaGraphCreate(&g, 0) == cudaSuccess;
-    cudaGraphConditionalHandle cond{};
-    cudaGraphNode_t dec = nullptr, ifn = nullptr;
-    if (ok) ok = cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault) == cudaSuccess;
-    const int body_kernels = 8 + (d.tile ? 1 : 0) + (d.angular ? 1 : 0);
     fm::pdl_capture = true;
-    if (ok && cudaStreamBeginCaptureToGraph(h->cap_st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) ==
-                  cudaSuccess) {
-        fm::launch_decide_graph(d, flip, p.rebuild_criteria, p.fixed_rebuild, h->half_min_delta, cond, body_kernels,
-                                h->cap_st);
-        ok = cudaStreamEndCapture(h->cap_st, &g) == cudaSuccess;
-    } else {
-        ok = false;
-    }
-    if (ok) {  // the decision is the graph's only node
-        size_t n = 1;
-        ok = cudaGraphGetNodes(g, &dec, &n) == cudaSuccess && n == 1;
-    }
-    cudaGraph_t body = nullptr;
-    if (ok) {
-        cudaGraphNodeParams cp{};
-        cp.type = cudaGraphNodeTypeConditional;
-        cp.conditional.handle = cond;
-        cp.conditional.type = cudaGraphCondTypeIf;
-        cp.conditional.size = 1;
-        ok = cudaGraphAddNode(&ifn, g, &dec, 1, &cp) == cudaSuccess;
-        if (ok) body = cp.conditional.phGraph_out[0];
-    }
-    if (ok && cudaStreamBeginCaptureToGraph(h->cap_st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) ==
-                  cudaSuccess) {
-        fm::launch_wrap_bin(d, 1, 1, 1, fm::ITER_DEVICE, h->cap_st);
-        fm::launch_scan_cells(d, 1, h->cap_st);
-        fm::launch_scatter(d, 1, h->cap_st);
-        fm::launch_reorder(d, 1, h->tpos, h->tuidx, h->cap_st);
-        if (d.tile) fm::launch_blk_seg(d, 1, fm::ITER_DEVICE, h->cap_st);
-        fm::launch_build_nlist(d, 1, fm::ITER_DEVICE, h->cap_st);
-        if (d.angular) fm::launch_angular_order(d, 1, fm::ITER_DEVICE, h->cap_st);
-        ok = cudaStreamEndCapture(h->cap_st, &body) == cudaSuccess;
+    if (ok && cudaStreamBeginCapture(h->cap_st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        for (int s = 0; ok && s < std::max(k, 1); s++) {
+            ok = capture_branch(h, s == 0 ? flip : 1);
+            if (ok && k > 0) fm::launch_force(h->d, 0, 2, h->tpm, h->cap_st);
+        }
+        cudaGraph_t got = nullptr;
+        const bool ended = cudaStreamEndCapture(h->cap_st, &got) == cudaSuccess;
+        g = got;
+        ok = ok && ended && g;
     } else {
         ok = false;
     }
@@ -1077,8 +1112,9 @@ static cudaGraphExec_t rebuild_graph(fm_handle *h, int flip)
         h->rb_off = true;
         return nullptr;
     }
-    h->rbx[flip] = ex;
-    h->rbd[flip] = h->d;
+    h->rbx[slot] = ex;
+    h->rbd[slot] = h->d;
+    h->rbt[slot] = h->tpm;
     return ex;
 }
 
@@ -1088,7 +1124,7 @@ static cudaGraphExec_t rebuild_graph(fm_handle *h, int flip)
 static void queue_rebuild_branch(fm_handle *h, int it, int flip)
 {
     const fm_params &p = h->p;
-    cudaGraphExec_t ex = rebuild_graph(h, flip);
+    cudaGraphExec_t ex = step_graph(h, flip, 0);
     if (ex) {
         if (p.rebuild_criteria == 2) { fm::launch_disp(h->d, h->st); h->launches += 1; }
         cudaGraphLaunch(ex, h->st);
@@ -1132,6 +1168,20 @@ static int queue_steps(fm_handle *h, int first, int nsteps, int phase, const std
     for (int s = 0; s < nsteps; s++) {
         const int it = first + s;
         h->iter = it;
+        // STEP_GRAPH_K middle iterations in one graph launch: none records,
+        // none is the range's last, move(1) of the first is already done
+        if (fused_move1 && p.force_list != 0 && p.rebuild_criteria != 2 && !h->timing && s + STEP_GRAPH_K < nsteps &&
+            no_record_in(it, STEP_GRAPH_K, p.tplot)) {
+            cudaGraphExec_t ex = step_graph(h, 1, STEP_GRAPH_K);
+            if (ex) {
+                cudaGraphLaunch(ex, h->st);
+                h->launches += 2 * STEP_GRAPH_K;  // decisions and force kernels
+                s += STEP_GRAPH_K - 1;
+                h->iter = first + s;
+                h->simtime = simtime_after[(size_t)(range_offset + s)];
+                continue;
+            }
+        }
         if (!(s == 0 && phase == 1)) {
             if (!fused_move1) { fm::launch_move1(h->d, h->st); h->launches += 1; }
             if (p.force_list != 0) {
