@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -426,6 +427,10 @@ static int create_impl(const fm_params *p, const DdGeom *g, fm_handle **out)
         }
     }
     h->tpm = tpm;
+    // FM_STEP_GRAPHS=0: every kernel of a step is launched on its own (the
+    // same kernels and results); Nsight Compute does not profile kernel nodes
+    // of graphs that hold conditional nodes
+    if (const char *e = std::getenv("FM_STEP_GRAPHS")) h->rb_off = std::strcmp(e, "0") == 0;
     h->expected_nbr = (int)std::lround(expected);
     int maxn = p->nlist_capacity > 0 ? p->nlist_capacity : round_up((int)std::ceil(1.3 * expected) + 16, 8);
 
@@ -628,7 +633,6 @@ extern "C" int fm_set_mie(fm_handle *h, const fm_mie_tables *t, const int32_t *m
 {
     if (!h || !t || !moltype) return fail(FM_ERR_ARG, "null argument");
     if (h->stage != 1) return fail(FM_ERR_STATE, "set the Mie tables after fm_upload_state and before fm_setup");
-    if (h->d.solvent) return fail(FM_ERR_ARG, "the Mie potential is not combined with the Soddemann solvent here");
     const int nt = t->ntypes;
     if (nt < 1 || nt > FM_MIE_MAXTYPES) return fail(FM_ERR_ARG, "ntypes out of range (1 .. FM_MIE_MAXTYPES)");
     if (!t->mass || !t->epsilon || !t->lambdar || !t->lambdaa || !t->C || !t->alpha || !t->potshift ||

@@ -27,6 +27,12 @@ namespace {
 
 __device__ __forceinline__ bool frozen(const FmDev &d) { return (d.sc->status & ST_FATAL) != 0u; }
 
+// w of a position: the Mie type (1-based), the Soddemann bead flag (1 for a
+// chain bead), or with both the type plus 32 times the flag.
+__device__ __forceinline__ int mie_type(double w) { return ((int)w) & 31; }
+template <bool MIE>
+__device__ __forceinline__ int bead_flag(double w) { return MIE ? ((int)w) >> 5 : (int)w; }
+
 __device__ __forceinline__ void raise_status(const FmDev &d, uint32_t bit, int iter)
 {
     if (iter == ITER_DEVICE) iter = d.sc->cur_iter;
@@ -581,14 +587,19 @@ __device__ __forceinline__ double pair_acc(const FmDev &d, double r2, double dx,
     if (SOD) {
         // simulation_compute_forces_Soddemann_neigbr_halfint (:793-888): WCA
         // inside wca_cut2, the cosine well eps a s^2 sin(a s + b) beyond it
-        // (the reference's expression, s = 1/r^2); no potshift
-        const double eps = d.sod_eps[(int)wi + (int)wj];
+        // (the reference's expression, s = 1/r^2); no potshift.  The WCA force
+        // is get_accijmag: Mie_accijmag of the pair's types with
+        // Mie_potential 1, its energy the LJ-WCA expression either way.
+        const double eps = d.sod_eps[bead_flag<MIE>(wi) + bead_flag<MIE>(wj)];
         const bool wca = r2 < SOD_WCA_CUT2;
         if (!F32) {
             const double s = __drcp_rn(r2);
             const double s2 = s * s;
             double acc;
-            if (wca) {
+            if (wca && MIE) {
+                const FmMiePair &m = d.mie_pair[(mie_type(wi) - 1) + MIE_MAXT * (mie_type(wj) - 1)];
+                acc = m.ceps * (m.lr * pow(s, m.er1) - m.ala * pow(s, m.ea1));
+            } else if (wca) {
                 const double s4 = s2 * s2;
                 acc = 48.0 * (s4 * s2 * s - 0.5 * s4);  // get_accijmag = LJ_accijmag
             } else {
@@ -608,7 +619,10 @@ __device__ __forceinline__ double pair_acc(const FmDev &d, double r2, double dx,
             const float s = rcp_f32((float)r2);
             const float s2 = s * s;
             float accf;
-            if (wca) {
+            if (wca && MIE) {
+                const FmMiePair &m = d.mie_pair[(mie_type(wi) - 1) + MIE_MAXT * (mie_type(wj) - 1)];
+                accf = (float)m.ceps * ((float)m.lr * powf(s, (float)m.er1) - (float)m.ala * powf(s, (float)m.ea1));
+            } else if (wca) {
                 const float s4 = s2 * s2;
                 accf = 48.0f * (s4 * s2 * s - 0.5f * s4);
             } else {
@@ -629,7 +643,7 @@ __device__ __forceinline__ double pair_acc(const FmDev &d, double r2, double dx,
         return 0.0;  // the Soddemann routine records no pressure-tensor term
     }
     if (MIE) {
-        const FmMiePair &m = d.mie_pair[((int)wi - 1) + MIE_MAXT * ((int)wj - 1)];
+        const FmMiePair &m = d.mie_pair[(mie_type(wi) - 1) + MIE_MAXT * (mie_type(wj) - 1)];
         if (!F32) {
             const double s = __drcp_rn(r2);  // == 1.0 / r2
             const double acc = m.ceps * (m.lr * pow(s, m.er1) - m.ala * pow(s, m.ea1));
@@ -703,7 +717,10 @@ __device__ __forceinline__ void pressure_part(double (&part)[RS_N], double wx, d
 // The record partials use v after move(2) for velocity Verlet and v + a dt/2
 // for leap-frog (simulation_record.f90:1236-1252).  Returns |v|^2 after a
 // position update (modes 2, 3), else 0.
-template <bool REC, int MODE, bool MIE = false>
+// DIV false: the forces are accelerations already (the Soddemann pairs and
+// the mass-divided bonds of a Mie + Soddemann system); the kinetic terms are
+// still mass-weighted.
+template <bool REC, int MODE, bool MIE = false, bool DIV = true>
 __device__ __forceinline__ double epilogue(const FmDev &d, int pset, int i, double4 p, double fx, double fy,
                                            double fz, double pe, double vir, double (&part)[RS_N],
                                            const double (&rf)[6])
@@ -715,8 +732,8 @@ __device__ __forceinline__ double epilogue(const FmDev &d, int pset, int i, doub
     }
     double mass = 1.0;  // LJ_mass; Mie_mass = mass_lookup(moltype)
     if (MIE) {
-        mass = d.mie_mass[(int)p.w - 1];
-        fx = fx / mass; fy = fy / mass; fz = fz / mass;
+        mass = d.mie_mass[mie_type(p.w) - 1];
+        if (DIV) { fx = fx / mass; fy = fy / mass; fz = fz / mass; }
     }
     d.ax[i] = fx; d.ay[i] = fy; d.az[i] = fz;
     if (REC) { d.pe[i] = pe; d.vir[i] = vir; }
@@ -796,7 +813,7 @@ __device__ __forceinline__ void fene_bonds(const FmDev &d, const double4 *P, int
         if (MIE) {
             // harmonic_accijmag / harmonic_energy (setup_set_parameters.f90:384-437):
             // -k (|r| - r0)/|r| and k/2 (|r| - r0)^2, constants by type pair
-            const FmMiePair &m = d.mie_pair[((int)pi.w - 1) + MIE_MAXT * ((int)pj.w - 1)];
+            const FmMiePair &m = d.mie_pair[(mie_type(pi.w) - 1) + MIE_MAXT * (mie_type(pj.w) - 1)];
             const double rm = sqrt(r2), dr = rm - m.r0;
             const double acc = -m.k * dr / rm;
             fx += acc * dx; fy += acc * dy; fz += acc * dz;
@@ -852,7 +869,7 @@ __device__ __forceinline__ bool angular_triple(const FmDev &d, const double4 *P,
                           image(pk.z, ((c1 >> 4) & 3) - 1, d.L[2])};
     const double rj[3] = {pj.x, pj.y, pj.z};
     const int nt = d.ang_nt;
-    const int q = ((int)pi.w - 1) + nt * (((int)pj.w - 1) + nt * ((int)pk.w - 1));
+    const int q = (mie_type(pi.w) - 1) + nt * ((mie_type(pj.w) - 1) + nt * (mie_type(pk.w) - 1));
     const double kk = d.ang_k[q], t0 = d.ang_t0[q];
     f1[0] = f1[1] = f1[2] = 0.0;
     f3[0] = f3[1] = f3[2] = 0.0;
@@ -1074,12 +1091,24 @@ __device__ __forceinline__ double owner_finish(const FmDev &d, int pset, const d
                                                double fx, double fy, double fz, double pe, double vir,
                                                double (&part)[RS_N], double (&rf)[6])
 {
-    if (d.potential_flag == 1) fene_bonds<REC, (PREC & 2) != 0>(d, P, i, fx, fy, fz, pe, vir, rf);
-    if constexpr ((PREC & 2) != 0) {  // angular_potential needs the Mie types
-        if (d.angular) angular_forces(d, P, i, fx, fy, fz);
+    if constexpr ((PREC & 6) == 6) {
+        // Mie + Soddemann: the Soddemann pairs are not divided by a mass
+        // (:852-860), the bonds of simulation_compute_forces_poly are
+        // (:752-754)
+        const double4 pi = P[i];
+        double bx = 0.0, by = 0.0, bz = 0.0;
+        if (d.potential_flag == 1) fene_bonds<REC, true>(d, P, i, bx, by, bz, pe, vir, rf);
+        const double mass = d.mie_mass[mie_type(pi.w) - 1];
+        fx += bx / mass; fy += by / mass; fz += bz / mass;
+        return epilogue<REC, MODE, true, false>(d, pset, i, pi, fx, fy, fz, pe, vir, part, rf);
+    } else {
+        if (d.potential_flag == 1) fene_bonds<REC, (PREC & 2) != 0>(d, P, i, fx, fy, fz, pe, vir, rf);
+        if constexpr ((PREC & 2) != 0) {  // angular_potential needs the Mie types
+            if (d.angular) angular_forces(d, P, i, fx, fy, fz);
+        }
+        // a(:,i) = sum acc rij / mass (LJ_mass = 1; Mie_mass by type)
+        return epilogue<REC, MODE, (PREC & 2) != 0>(d, pset, i, P[i], fx, fy, fz, pe, vir, part, rf);
     }
-    // a(:,i) = sum acc rij / mass (LJ_mass = 1; Mie_mass by type)
-    return epilogue<REC, MODE, (PREC & 2) != 0>(d, pset, i, P[i], fx, fy, fz, pe, vir, part, rf);
 }
 
 template <int TPM, bool REC, int MODE, int PREC>
@@ -1169,7 +1198,6 @@ __device__ __forceinline__ uint2 ld_stream_uint2(const uint2 *p)
 template <int T, bool REC, int MODE, int PREC>
 __global__ void __launch_bounds__(FT_THREADS, REC ? 2 : 4) k_force_tile(FmDev d)
 {
-    constexpr bool MIE = (PREC & 2) != 0;
     constexpr bool NEEDW = (PREC & 6) != 0;  // Mie types / Soddemann bead flags ride in w
     constexpr bool LJ32 = PREC == 1;         // plain LJ, FP32 pair magnitude
     constexpr int R = NEEDW ? 4 : 3;
@@ -1344,14 +1372,10 @@ __global__ void __launch_bounds__(FT_THREADS, REC ? 2 : 4) k_force_tile(FmDev d)
                 }
             }
             if (act && sub == 0) {
-                if (d.potential_flag == 1) fene_bonds<REC, MIE>(d, P, i, fx, fy, fz, pe, vir, rf);
-                if constexpr (MIE) {
-                    if (d.angular) angular_forces(d, P, i, fx, fy, fz);
-                }
                 double part[RS_N];
 #pragma unroll
                 for (int q = 0; q < RS_N; q++) part[q] = 0.0;
-                const double m2 = epilogue<REC, MODE, MIE>(d, pset, i, pi, fx, fy, fz, pe, vir, part, rf);
+                const double m2 = owner_finish<REC, MODE, PREC>(d, pset, P, i, fx, fy, fz, pe, vir, part, rf);
                 m2max = fmax(m2max, m2);
                 if (REC) {
 #pragma unroll
@@ -1476,7 +1500,7 @@ __global__ void __launch_bounds__(MACRO_THREADS) k_macro_partials(FmDev d)
             vy = __dadd_rn(vy, __dmul_rn(__dmul_rn(0.5, d.ay[i]), d.dt));
             vz = __dadd_rn(vz, __dmul_rn(__dmul_rn(0.5, d.az[i]), d.dt));
         }
-        const double mass = d.mie ? d.mie_mass[(int)cur_pos(d, d.sc->pset)[i].w - 1] : 1.0;
+        const double mass = d.mie ? d.mie_mass[mie_type(cur_pos(d, d.sc->pset)[i].w) - 1] : 1.0;
         part[RS_PE] = d.pe[i];
         part[RS_VIR] = d.vir[i];
         part[RS_MV2] = mass * norm2_rn(vx, vy, vz);
@@ -1585,20 +1609,18 @@ __global__ void k_pair_digest(FmDev d, const int32_t *glob_of_upload)
 }
 
 // Types of an uploaded state (slots still equal upload indices).
-__global__ void k_set_types(FmDev d)
+// w of each position from the Mie type (moltype) and the Soddemann bead flag
+// (solvent_flag 1: 1 for a chain bead, 0 for a solvent molecule, chainID 0):
+// the type, the flag, or the type + 32 x the flag with both.  Run after either
+// is uploaded, while slots still equal upload indices; a part not uploaded
+// yet reads as 0 (type) or the zeroed chain ids.
+__global__ void k_set_w(FmDev d)
 {
     int u = blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= d.n) return;
-    cur_pos(d, d.sc->pset)[u].w = (double)d.mie_type_up[u];
-}
-
-// solvent_flag 1: w = 1 for a chain bead, 0 for a solvent molecule (chainID
-// 0); the chain ids are still in upload order = slot order here
-__global__ void k_set_bead_flags(FmDev d)
-{
-    int u = blockIdx.x * blockDim.x + threadIdx.x;
-    if (u >= d.n) return;
-    cur_pos(d, d.sc->pset)[u].w = d.chain[u] != 0 ? 1.0 : 0.0;
+    const int type = d.mie && d.mie_type_up ? d.mie_type_up[u] : 0;
+    const int flag = d.solvent ? (d.chain[u] != 0 ? 1 : 0) : 0;
+    cur_pos(d, d.sc->pset)[u].w = (double)(type + (d.mie ? 32 : 1) * flag);
 }
 
 // upload order u -> slot u (uploads start in upload order)
@@ -1791,7 +1813,9 @@ static void launch_force_tile(const FmDev &d, int record, int mode, cudaStream_t
         case 2: launch_force_tile_k<T, R, M, 2>(d, st); break;                      \
         case 3: launch_force_tile_k<T, R, M, 3>(d, st); break;                      \
         case 4: launch_force_tile_k<T, R, M, 4>(d, st); break;                      \
-        default: launch_force_tile_k<T, R, M, 5>(d, st); break;                     \
+        case 5: launch_force_tile_k<T, R, M, 5>(d, st); break;                      \
+        case 6: launch_force_tile_k<T, R, M, 6>(d, st); break;                      \
+        default: launch_force_tile_k<T, R, M, 7>(d, st); break;                     \
         }                                                                           \
         return;                                                                     \
     }
@@ -1820,7 +1844,9 @@ static void launch_force_tpm(const FmDev &d, int record, int mode, cudaStream_t 
         case 2: pdl_launch(k_force<TPM, R, M, 2>, g, FORCE_THREADS, st, d); break;                   \
         case 3: pdl_launch(k_force<TPM, R, M, 3>, g, FORCE_THREADS, st, d); break;                   \
         case 4: pdl_launch(k_force<TPM, R, M, 4>, g, FORCE_THREADS, st, d); break;                   \
-        default: pdl_launch(k_force<TPM, R, M, 5>, g, FORCE_THREADS, st, d); break;                  \
+        case 5: pdl_launch(k_force<TPM, R, M, 5>, g, FORCE_THREADS, st, d); break;                   \
+        case 6: pdl_launch(k_force<TPM, R, M, 6>, g, FORCE_THREADS, st, d); break;                   \
+        default: pdl_launch(k_force<TPM, R, M, 7>, g, FORCE_THREADS, st, d); break;                  \
         }                                                                                       \
         return;                                                                                 \
     }
@@ -1879,12 +1905,9 @@ void launch_pair_digest(const FmDev &d, const int32_t *glob_of_upload, cudaStrea
     k_pair_digest<<<nblk(d.n, 256), 256, 0, st>>>(d, glob_of_upload);
 }
 
-void launch_set_types(const FmDev &d, cudaStream_t st) { k_set_types<<<nblk(d.n, 256), 256, 0, st>>>(d); }
+void launch_set_types(const FmDev &d, cudaStream_t st) { k_set_w<<<nblk(d.n, 256), 256, 0, st>>>(d); }
 
-void launch_set_bead_flags(const FmDev &d, cudaStream_t st)
-{
-    k_set_bead_flags<<<nblk(d.n, 256), 256, 0, st>>>(d);
-}
+void launch_set_bead_flags(const FmDev &d, cudaStream_t st) { k_set_w<<<nblk(d.n, 256), 256, 0, st>>>(d); }
 
 void launch_scatter_state(const FmDev &d, const double *r3, const double *v3, const double *a3, cudaStream_t st)
 {

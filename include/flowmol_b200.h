@@ -173,9 +173,14 @@ FM_API int fm_upload_monomers(fm_handle *h, const int32_t *chainID, const int32_
  * simulation_record.f90:1236-1252).  The tables are the reference's own
  * lookup arrays after setup_mie_potential (:566-1092): ntypes x ntypes,
  * entry (i,j) at [(i-1) + ntypes*(j-1)], types 1-based; mass has ntypes
- * entries.  moltype(n) is in upload order.  Call after fm_upload_state (and
- * fm_upload_monomers), before fm_setup.  No counterpart entry point in the
- * reference, whose tables are module globals. */
+ * entries.  moltype(n) is in upload order.  With the Soddemann solvent
+ * (solvent_flag 1) the WCA branch of its pair force is Mie_accijmag of the
+ * pair's types (get_accijmag), its energy stays the LJ-WCA expression, the
+ * pair accelerations are not divided by a mass and the harmonic bonds are
+ * (simulation_compute_forces.f90:839-872, 752-754).  Call after
+ * fm_upload_state (and fm_upload_monomers), before fm_setup.  No
+ * counterpart entry point in the reference, whose tables are module
+ * globals. */
 #define FM_MIE_MAXTYPES 16
 typedef struct fm_mie_tables {
     int32_t ntypes, pad_;

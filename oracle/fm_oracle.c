@@ -922,7 +922,9 @@ static void forces_halfint(orc *s)
 }
 
 /* simulation_compute_forces_Soddemann_neigbr_halfint (:793-888): half list;
- * WCA (get_accijmag, LJ) below wca_cut2 and the reference's cosine-well
+ * WCA (get_accijmag: LJ_accijmag, or Mie_accijmag of the pair's types with
+ * Mie_potential 1; the energy is the LJ-WCA expression either way) below
+ * wca_cut2 and the reference's cosine-well
  * expression out to sod_cut2, the well depth by how many of the pair are
  * chain beads (chainID != 0; an image has its source's).  The minimum-image
  * line (:821) leaves rij as it is for every listed pair (|rij| < L/2, as
@@ -946,7 +948,7 @@ static void forces_soddemann(orc *s)
             const double eps = s->sod_eps[ptot];
             const double inv = 1.0 / r2;
             double acc;
-            if (r2 < W2) acc = lj_accijmag(inv);
+            if (r2 < W2) acc = pair_accijmag(s, inv, i, j); /* get_accijmag (:839) */
             else acc = (eps * A * (inv * inv)) * sin(inv * A + B);
             double *ai = &s->a[3 * (size_t)(i - 1)], *aj = &s->a[3 * (size_t)(j - 1)];
             for (int k = 0; k < 3; k++) {

@@ -132,6 +132,34 @@ def test_subroutine_path_equals_fused_loop(liquid):
     assert a_sys.counters()["rebuilds"] == b_sys.counters()["rebuilds"]
 
 
+@pytest.mark.parametrize("integration", [1, 0])
+@pytest.mark.parametrize("crit", [0, 2])
+def test_step_graphs_equal_per_kernel_launches(liquid, monkeypatch, integration, crit):
+    """The step graphs (the decision setting the condition of a rebuild body,
+    eight middle iterations per launch) change no result bit against
+    launching every kernel of a step on its own (FM_STEP_GRAPHS=0, read when a
+    handle is created): 150 iterations with rebuilds and records, velocity
+    Verlet and leap-frog, rebuild criteria 0 and 2.  The graphs launch fewer
+    kernels: the rebuild kernels run only on rebuild steps."""
+    r, v, dom = liquid
+    out = []
+    for env in ("1", "0"):
+        monkeypatch.setenv("FM_STEP_GRAPHS", env)
+        s = gpu_system(r, v, dom, 2.5, tplot=40, density=0.8442, integration_algorithm=integration,
+                       rebuild_criteria=crit)
+        s.setup()
+        s.records()
+        s.simulation_md(150)
+        out.append((s.download(), s.records(), s.counters()["rebuilds"], s.launch_count()))
+        s.close()
+    (sa, ra, na, la), (sb, rb, nb, lb) = out
+    for x, y in zip(sa, sb):
+        assert np.array_equal(x, y)
+    assert ra == rb and len(ra) == 3
+    assert na == nb and na > 2
+    assert la < lb
+
+
 def test_rebuild_lists_equals_the_subroutine_sequence(liquid):
     """fm_rebuild_lists (the rebuild branch in one call) leaves the same
     state as the six subroutine mirrors called one by one: 40 iterations of
@@ -511,6 +539,57 @@ def test_soddemann_polymer_solution(gpu_lib, prec):
     recs = s.records()
     assert [x["iter"] for x in recs] == [int(x) for x in recs_o[:, 0]]
     for row, ro in zip(recs, recs_o):
+        assert row["potenergy"] == pytest.approx(ro[5], rel=1e-9)
+    rg, _, _, _ = s.download()
+    assert np.abs(wrap_diff(rg, o.r, dom)).max() < 1e-7
+    s.close()
+
+
+@pytest.mark.parametrize("prec", [api.PRECISION_FP64, api.PRECISION_FP32])
+def test_mie_soddemann_polymer_solution(gpu_lib, prec):
+    """Mie_potential 1 with SOLVENT_INFO 1 (simulation_compute_forces.f90
+    :839-872): the WCA branch of the Soddemann force is Mie_accijmag of the
+    pair's types (get_accijmag) while its energy stays the LJ-WCA
+    expression, the pair accelerations are not divided by a mass but the
+    harmonic bonds are (:752-754), and the kinetic sums are mass-weighted.
+    A two-type solution (types alternate over the molecules, masses 1 and
+    1.5): bonds and pair set bit-exact, forces to 1e-12 (FP64) or 1e-5 (FP32
+    pair magnitudes), per-molecule PE, and 100 steps in FP64."""
+    from flowmol_b200 import polymer
+    from helpers import mie_mixture_tables
+    r, v, ch, sub, fy, bf, dom = polymer.fene_solution(192, targetconc=0.5)
+    r = lattice.jitter(r, 0.08, 93, dom)
+    eps = (1.5, 1.0, 0.5)
+    tab = mie_mixture_tables(WCA_RC)
+    mt = (np.arange(len(r)) % 2 + 1).astype(np.int32)
+    o = O.Oracle(r, v, dom, WCA_RC, tplot=20, potential_flag=1, k_c=30.0, R_0=1.5, density=0.85)
+    o.set_monomers(ch, sub, fy, bf)
+    o.set_solvent(1, *eps)
+    o.set_mie(tab, mt)
+    o.setup()
+    s = gpu_system(r, v, dom, WCA_RC, precision=prec, tplot=20, density=0.85, potential_flag=1, k_c=30.0,
+                   R_0=1.5, solvent_flag=1, eps=eps)
+    s.upload_monomers(ch, sub, bf)
+    s.set_mie(tab, mt)
+    s.setup()
+    key = lambda t: np.sort((t[0].astype(np.int64) << 32) | (t[1].astype(np.int64) << 5) | t[2])  # noqa: E731
+    assert np.array_equal(key(s.bonds()), key(o.bond_list()))
+    assert np.array_equal(canonical_full(*s.pair_list()), canonical_oracle(*o.pair_list()))
+    _, _, a, _ = s.download()
+    pe, _ = s.per_molecule()
+    if prec == api.PRECISION_FP32:
+        assert rel_err(a, o.a, F_FLOOR32).max() <= TOL32
+        s.close()
+        return
+    assert rel_err(a, o.a, 1.0).max() <= TOL64
+    np.testing.assert_allclose(pe, o.potenergymol, rtol=TOL64, atol=TOL64)
+    recs_o = o.run_vv(100)
+    s.records()
+    s.simulation_md(100)
+    recs = s.records()
+    assert [x["iter"] for x in recs] == [int(x) for x in recs_o[:, 0]]
+    for row, ro in zip(recs, recs_o):
+        assert row["kinenergy"] == pytest.approx(ro[4], rel=1e-9)
         assert row["potenergy"] == pytest.approx(ro[5], rel=1e-9)
     rg, _, _, _ = s.download()
     assert np.abs(wrap_diff(rg, o.r, dom)).max() < 1e-7

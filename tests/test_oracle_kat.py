@@ -248,6 +248,39 @@ def test_soddemann_two_body_analytic(dist, beads):
     np.testing.assert_allclose(o.potenergymol, [pe, pe], rtol=1e-13)
 
 
+@pytest.mark.parametrize("dist", [1.05, 1.3])
+def test_mie_soddemann_two_body(dist):
+    """Mie_potential 1 with the Soddemann solvent: inside wca_cut2 the force
+    is get_accijmag = Mie_accijmag of the two types (setup_set_parameters.f90
+    :149-168), the energy the LJ-WCA expression of the Soddemann routine
+    (:864-866), and the accelerations are not divided by the masses
+    (:852-860); beyond it the cosine well as without Mie."""
+    from helpers import mie_mixture_tables
+    eps = (1.7, 1.3, 0.6)
+    tab = mie_mixture_tables(WCA_RC)
+    r = np.array([[-dist / 2, 0.1, 0.2], [dist / 2, 0.1, 0.2]])
+    o = O.Oracle(r, np.zeros((2, 3)), [8.0, 8.0, 8.0], WCA_RC, tplot=1, potential_flag=1, k_c=30.0, R_0=1.5)
+    o.set_monomers(np.array([1, 0], np.int32), np.ones(2, np.int32), np.zeros(2, np.int32),
+                   np.zeros((2, 4), np.int32))
+    o.set_solvent(1, *eps)
+    o.set_mie(tab, np.array([1, 2], np.int32))
+    o.setup()
+    r2 = (-dist / 2 - dist / 2) ** 2
+    s = 1.0 / r2
+    e = eps[1]  # one chain bead in the pair: eps_ps
+    if r2 < WCA_CUT2_SOD:
+        lr, la = tab["lambdar"][0, 1], tab["lambdaa"][0, 1]
+        C, ep, al = tab["C"][0, 1], tab["epsilon"][0, 1], tab["alpha"][0, 1]
+        acc = C * ep * (lr * s ** (0.5 * lr + 1) - al * la * s ** (0.5 * la + 1))
+        pe = 4.0 * ((s * s * s) * (s * s * s) - s * s * s + 0.25) - e
+    else:
+        acc = (e * SOD_A * (s * s)) * np.sin(s * SOD_A + SOD_B)
+        pe = 0.5 * e * (np.cos(SOD_A * r2 + SOD_B) - 1.0)
+    a = o.a
+    assert a[0, 0] == pytest.approx(acc * -dist, rel=1e-13) and a[1, 0] == pytest.approx(acc * dist, rel=1e-13)
+    np.testing.assert_allclose(o.potenergymol, [pe, pe], rtol=1e-13)
+
+
 def test_soddemann_pairs_beyond_rneighbr_are_not_seen():
     """A pair inside sod_cut but beyond rneighbr (1.42246) is not in the list
     the forces walk: no force, as in the reference, where rneighbr2 keeps its
