@@ -310,8 +310,9 @@ def batch_replicas(nrep=256, seed=0x466D6F6C + 4):
 
 
 def run_batched(api, torch, dev, nsteps, nrep=256):
-    """All replicas in one engine (graph-captured ticks, admission and setup
-    inside the timed region) against the plain single-system form run one
+    """All replicas in one engine (admission and setup inside the timed
+    region; the ticks loop on the device in one graph launch, until the
+    replicas are done) against the plain single-system form run one
     replica at a time.  The plain form is measured per replica as its setup
     (upload, binning, list, first forces) plus plain_steps steps timed apart
     with CUDA events, and projected to the same nsteps the batch runs:
@@ -321,7 +322,7 @@ def run_batched(api, torch, dev, nsteps, nrep=256):
     reps = batch_replicas(nrep)
     tot = sum(len(x[0]) for x in reps)
     e = api.Engine(max_molecules=tot + 1024, max_cells=2_000_000, max_list_entries=(tot + 1024) * 160,
-                   max_slots=nrep, precision=api.PRECISION_FP32, ticks_per_chunk=50, keep_states=False)
+                   max_slots=nrep, precision=api.PRECISION_FP32, ticks_per_chunk=4096, keep_states=False)
     for r, v, dom, rho, fl in reps:
         e.submit(api.make_job(len(r), dom, RC, nsteps, density=rho, tplot=TPLOT, force_list=fl), r, v)
     torch.cuda.synchronize(dev)

@@ -7,6 +7,7 @@
 #include <cstddef>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <iterator>
@@ -128,6 +129,9 @@ struct fm_engine {
     double blocks_below = 8.0;
     bool tuned_build = false;
     cudaGraphExec_t graph = nullptr;
+    bool graph_loop = false;          // the graph is the device-driven tick loop (WHILE node)
+    bool loop_off = false;            // conditional nodes unavailable: fixed chunks of ticks
+    cudaStream_t cap_st = nullptr;    // capture of the loop's body
     int graph_tpm = -1;
     fm::TickExtent graph_x{0, 0, 0};  // launch extents the graph was captured with
     fm::TickExtent need_x{0, 0, 0};   // extents the resident jobs call for
@@ -159,6 +163,7 @@ void free_all(fm_engine *e)
     for (void *q : ptrs)
         if (q) cudaFree(q);
     if (e->graph) cudaGraphExecDestroy(e->graph);
+    if (e->cap_st) cudaStreamDestroy(e->cap_st);
     if (e->own_stream && e->st) cudaStreamDestroy(e->st);
 }
 
@@ -179,9 +184,78 @@ int ensure_stage(fm_engine *e, size_t ndouble, size_t nint)
     return FM_OK;
 }
 
+// Ticks per iteration of the tick loop: enough that the WHILE node's own cost
+// per iteration is spread thin, at most one chunk.
+constexpr int LOOP_BODY_TICKS = 32;
+int loop_body_ticks(const fm_engine *e) { return std::max(1, std::min(e->p.ticks_per_chunk, LOOP_BODY_TICKS)); }
+
+// The chunk as one graph that loops ticks on the device: a WHILE node whose
+// body is loop_body_ticks ticks followed by k_e_continue, which ends the loop
+// when no job is left running, after ticks_per_chunk ticks, or -- while jobs
+// wait in the queue -- once a job has finished or failed, so the host retires
+// it and admits the next without waiting for the rest of the chunk.  A batch
+// that fits the engine is one launch.  False when the graph cannot be made
+// (the caller captures fixed chunks instead).
+bool capture_loop(fm_engine *e)
+{
+    if (e->loop_off) return false;
+    if (!e->cap_st && cudaStreamCreateWithFlags(&e->cap_st, cudaStreamNonBlocking) != cudaSuccess) return false;
+    cudaGraph_t g = nullptr, body = nullptr;
+    cudaGraphExec_t ex = nullptr;
+    cudaGraphConditionalHandle cond{};
+    cudaGraphNode_t wn = nullptr;
+    bool ok = cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+        cudaStreamCaptureStatus cs;
+        const cudaGraphNode_t *deps = nullptr;
+        size_t nd = 0;
+        fm::eng_loop_reset(e->d, e->st);
+        ok = cudaStreamGetCaptureInfo(e->st, &cs, nullptr, &g, &deps, &nd) == cudaSuccess && g &&
+             cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+        cudaGraphNodeParams cp{};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = cond;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        if (ok) ok = cudaGraphAddNode(&wn, g, deps, nd, &cp) == cudaSuccess;
+        if (ok) ok = cudaStreamUpdateCaptureDependencies(e->st, &wn, 1, cudaStreamSetCaptureDependencies) == cudaSuccess;
+        if (ok) {
+            body = cp.conditional.phGraph_out[0];
+            ok = cudaStreamBeginCaptureToGraph(e->cap_st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) ==
+                 cudaSuccess;
+            if (ok) {
+                const int k = loop_body_ticks(e);
+                for (int t = 0; t < k; t++) fm::eng_tick(e->d, e->tpm, e->need_x, e->cap_st);
+                fm::eng_loop_continue(e->d, e->need_x.slots, cond, k, std::max(e->p.ticks_per_chunk, 1),
+                                      e->cap_st);
+                ok = cudaStreamEndCapture(e->cap_st, &body) == cudaSuccess;
+            }
+        }
+        cudaGraph_t got = nullptr;
+        const bool ended = cudaStreamEndCapture(e->st, &got) == cudaSuccess;
+        ok = ok && ended && got;
+        g = got;
+    }
+    if (ok) ok = cudaGraphInstantiate(&ex, g, 0) == cudaSuccess;
+    if (g) cudaGraphDestroy(g);
+    if (!ok) {
+        if (ex) cudaGraphExecDestroy(ex);
+        cudaGetLastError();
+        e->loop_off = true;
+        return false;
+    }
+    e->graph = ex;
+    e->graph_loop = true;
+    e->graph_tpm = e->tpm;
+    e->graph_x = e->need_x;
+    return true;
+}
+
 int capture(fm_engine *e)
 {
     if (e->graph) { cudaGraphExecDestroy(e->graph); e->graph = nullptr; }
+    e->graph_loop = false;
+    if (capture_loop(e)) return FM_OK;
     cudaGraph_t g;
     EN_CUDA(cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
     for (int t = 0; t < e->p.ticks_per_chunk; t++) fm::eng_tick(e->d, e->tpm, e->need_x, e->st);
@@ -587,6 +661,9 @@ extern "C" int fm_engine_create(const fm_engine_params *p, fm_engine **out)
     fm_engine *e = new fm_engine();
     e->p = *p;
     if (e->p.ticks_per_chunk <= 0) e->p.ticks_per_chunk = 20;
+    // FM_STEP_GRAPHS=0: fixed chunks of ticks_per_chunk ticks in a plain graph
+    // (no conditional node), which Nsight Compute can profile kernel by kernel
+    if (const char *ev = std::getenv("FM_STEP_GRAPHS")) e->loop_off = std::strcmp(ev, "0") == 0;
     fm::EngDev &d = e->d;
     d.nslots = p->max_slots;
     d.mol_cap = (int)p->max_molecules;
@@ -729,10 +806,34 @@ extern "C" int fm_engine_step_chunk(fm_engine *e, int32_t *resident_out, int32_t
     EN_TRY(update_hwm(e));
     if (nres > 0) {
         if (!e->tuned) EN_TRY(autotune(e));
+        if (!e->tuned && !e->loop_off) {
+            // the resident jobs are still in their setup: one tick on its own,
+            // so that the autotuner times them running before the tick loop --
+            // which may run a whole batch in one launch -- is captured with its
+            // choice
+            fm::eng_tick(e->d, e->tpm, e->need_x, e->st);
+            e->ticks += 1;
+            e->launches += fm::eng_kernels_per_tick();
+            EN_TRY(sync_table(e));
+            EN_TRY(autotune(e));
+        }
         if (!e->graph || e->graph_tpm != e->tpm || !extent_ok(e->graph_x, e->need_x)) EN_TRY(capture(e));
+        if (e->graph_loop) {
+            const int waiting = e->queue.empty() ? 0 : 1;
+            EN_CUDA(cudaMemcpyAsync(&e->d.flags->queue_waiting, &waiting, sizeof waiting, cudaMemcpyHostToDevice,
+                                    e->st));
+        }
         EN_CUDA(cudaGraphLaunch(e->graph, e->st));
-        e->ticks += e->p.ticks_per_chunk;
-        e->launches += (int64_t)fm::eng_kernels_per_tick() * e->p.ticks_per_chunk;
+        if (e->graph_loop) {  // the device counted the ticks of this launch
+            int t = 0;
+            EN_CUDA(cudaMemcpyAsync(&t, &e->d.flags->loop_ticks, sizeof t, cudaMemcpyDeviceToHost, e->st));
+            EN_CUDA(cudaStreamSynchronize(e->st));
+            e->ticks += t;
+            e->launches += (int64_t)fm::eng_kernels_per_tick() * t + t / loop_body_ticks(e) + 1;
+        } else {
+            e->ticks += e->p.ticks_per_chunk;
+            e->launches += (int64_t)fm::eng_kernels_per_tick() * e->p.ticks_per_chunk;
+        }
         EN_TRY(sync_table(e));
         for (size_t k = 0; k < e->resident.size(); k++) {
             if (e->resident[k].slot < 0) continue;

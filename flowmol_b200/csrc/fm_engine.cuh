@@ -62,6 +62,9 @@ struct EngFlags {
     // this tick's rebuilding jobs (slot order): count, their molecules, their
     // cells, their list-build units (cells or 2x2x2 blocks)
     int rb_n, rb_mtot, rb_ctot, rb_utot;
+    // ticks run by the current launch of the tick loop (the graph's WHILE node),
+    // and whether jobs wait in the host's queue (written before each launch)
+    int loop_ticks, queue_waiting;
 };
 
 struct EngDev {
@@ -129,5 +132,12 @@ void eng_claim_cells(const EngDev &d, int slot, int cell_off, int ncell, cudaStr
 void eng_gather_job(const EngDev &d, int slot, int mol_off, int n, double *r3, double *v3, cudaStream_t st);
 void eng_release_job(const EngDev &d, int mol_off, int n, int cell_off, int ncell, cudaStream_t st);
 int eng_kernels_per_tick();
+// The tick loop's bookkeeping: the counter reset before the WHILE node, and
+// the kernel that ends each tick by setting the node's condition -- go on
+// while some resident job runs, fewer than max_ticks ticks have run, and no
+// job has finished or failed while others wait in the queue for its slot.
+void eng_loop_reset(const EngDev &d, cudaStream_t st);
+void eng_loop_continue(const EngDev &d, int slots, cudaGraphConditionalHandle cond, int body_ticks, int max_ticks,
+                       cudaStream_t st);
 
 }  // namespace fm

@@ -973,6 +973,38 @@ void launch_force_any(const EngDev &d, int tpm, int mols, bool force_only, cudaS
 
 int eng_kernels_per_tick() { return 15; }
 
+__global__ void k_e_loop_reset(EngDev d) { d.flags->loop_ticks = 0; }
+
+// Ends an iteration (body_ticks ticks) of the loop: the WHILE node runs
+// another while a resident job is set up or running and the launch has run
+// fewer than max_ticks ticks, unless a job is done or failed (the host
+// retires those between launches) while queued jobs wait for a slot.
+__global__ void k_e_continue(EngDev d, int slots, cudaGraphConditionalHandle cond, int body_ticks, int max_ticks)
+{
+    int live = 0, ended = 0;
+    for (int k = threadIdx.x; k < slots; k += blockDim.x) {
+        const int st = d.slots[k].state;
+        live |= st == SLOT_SETUP || st == SLOT_RUN;
+        ended |= st == SLOT_DONE || st == SLOT_FAILED;
+    }
+    live = __syncthreads_or(live);
+    ended = __syncthreads_or(ended);
+    if (threadIdx.x == 0) {
+        const int t = d.flags->loop_ticks + body_ticks;
+        d.flags->loop_ticks = t;
+        const bool make_room = ended && d.flags->queue_waiting;
+        cudaGraphSetConditional(cond, (live && !make_room && t < max_ticks) ? 1u : 0u);
+    }
+}
+
+void eng_loop_reset(const EngDev &d, cudaStream_t st) { k_e_loop_reset<<<1, 1, 0, st>>>(d); }
+
+void eng_loop_continue(const EngDev &d, int slots, cudaGraphConditionalHandle cond, int body_ticks, int max_ticks,
+                       cudaStream_t st)
+{
+    k_e_continue<<<1, 256, 0, st>>>(d, std::min(slots, d.nslots), cond, body_ticks, max_ticks);
+}
+
 void eng_tick(const EngDev &d, int tpm, const TickExtent &x, cudaStream_t st)
 {
     const int slots = std::min(x.slots, d.nslots);

@@ -386,7 +386,8 @@ typedef struct fm_engine_params {
     int32_t max_slots;            /* jobs resident at once */
     int32_t precision;            /* FM_PRECISION_* for every job */
     int32_t threads_per_molecule; /* 0 = autotuned on the first resident jobs */
-    int32_t ticks_per_chunk;      /* steps per graph launch between admission points */
+    int32_t ticks_per_chunk;      /* most steps per graph launch between admission points (a launch
+                                     ends earlier when a job finishes while others are queued) */
     int32_t keep_states;          /* keep final r, v of finished jobs for fm_engine_job_state */
     int32_t list_build;           /* FM_LIST_BUILD_*: the list build's tile, one cell or 2x2x2 cells per
                                      warp (same rows); AUTO = chosen by timing the resident jobs */
@@ -445,8 +446,11 @@ FM_API int fm_engine_set_stream(fm_engine *e, void *cuda_stream);
 FM_API int fm_engine_submit(fm_engine *e, const fm_job *job, const double *r, const double *v, const int32_t *tag,
                             const double *rtether, const double *slidev, int64_t *job_id);
 /* One admission point (retire finished jobs, admit queued ones that fit)
- * followed by one chunk of ticks; reports how many jobs are resident and
- * queued afterwards. */
+ * followed by one chunk of ticks: one graph launch whose ticks loop on the
+ * device, min(ticks_per_chunk, 32) per iteration, until no job is left
+ * running, ticks_per_chunk ticks have run, or -- while jobs wait in the
+ * queue -- a job has finished or failed; reports how many jobs are resident
+ * and queued afterwards. */
 FM_API int fm_engine_step_chunk(fm_engine *e, int32_t *resident, int32_t *queued);
 /* Chunks until nothing is resident or queued (max_chunks <= 0: no limit). */
 FM_API int fm_engine_run(fm_engine *e, int32_t max_chunks);

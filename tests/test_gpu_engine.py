@@ -67,6 +67,37 @@ def couette_inputs(n_target, speed, seed):
     return job, r, v, tag, rt, sv, dom
 
 
+def test_tick_loop_runs_a_batch_in_one_launch(gpu_lib):
+    """The chunk's ticks loop on the device (a graph WHILE node): a batch that
+    fits the engine runs from admission to its last step in one
+    fm_engine_step_chunk -- one graph launch, however large ticks_per_chunk
+    -- and the loop stops when the jobs are done, not at the chunk's bound.
+    While jobs wait in the queue, a job that finishes ends the launch, so the
+    host retires it and admits the next one at once."""
+    reps = [([6, 6, 6], 0.8, 1.0, 21), ([7, 5, 6], 0.6, 1.3, 22), ([3, 3, 3], 0.9, 1.0, 23)]
+    e = engine(ticks=100000)
+    for k, (nu, rho, T, seed) in enumerate(reps):
+        r, v, dom = lj_replica(nu, rho, T, seed)
+        fl = 0 if min(np.floor(dom / 2.8)) < 3 else 3
+        e.submit(api.make_job(len(r), dom, 2.5, 60 * (k + 1), tplot=40, force_list=fl), r, v)
+    res, q = e.step_chunk()
+    assert res == 0 and q == 0
+    out = e.results()
+    assert sorted(x["final_iter"] for x in out) == [60, 120, 180] and all(x["status"] == 0 for x in out)
+    assert e.counters()["ticks"] <= 181 + 32  # whole iterations of the loop (32 ticks each)
+    e.close()
+    e = engine(slots=2, ticks=100000)
+    for k, (nu, rho, T, seed) in enumerate(reps[:2] + reps[:1]):
+        r, v, dom = lj_replica(nu, rho, T, seed)
+        e.submit(api.make_job(len(r), dom, 2.5, 120 if k == 1 else 60, tplot=40), r, v)
+    res, q = e.step_chunk()  # the third job waits: the first launch ends when the 60-step job is done
+    assert (res, q) == (1, 1) and [x["final_iter"] for x in e.results()] == [60]
+    res, q = e.step_chunk()
+    assert (res, q) == (0, 0) and sorted(x["final_iter"] for x in e.results()) == [60, 120]
+    assert e.counters()["ticks"] <= 64 + 96
+    e.close()
+
+
 def test_couette_job_follows_oracle(gpu_lib):
     job, r, v, tag, rt, sv, dom = couette_inputs(500, 1.0, 21)
     nsteps = 200
