@@ -481,12 +481,26 @@ int retire(fm_engine *e, int slot)
 // scratch rows and a scratch copy of the slot table, so the jobs' own lists
 // and state are untouched (both tiles give the same rows); keeps the fastest
 // threshold and applies it to the resident and later jobs.
+// The autotuners time kernels on the running neighbour-list jobs.  Below
+// this many of their molecules a kernel's time is mostly launch latency and
+// the candidates cannot be told apart, so tuning waits for a larger load
+// (a served stream's first chunk may hold one small job).
+constexpr int64_t TUNE_MIN_MOLECULES = 65536;
+
+int64_t running_list_molecules(const fm_engine *e)
+{
+    int64_t m = 0;
+    for (const fm::EngSlot &s : e->table)
+        if (s.state == fm::SLOT_RUN && s.mode == fm::MODE_LIST) m += s.nmol;
+    return m;
+}
+
 int tune_build(fm_engine *e)
 {
     std::vector<int> ks;
     for (size_t k = 0; k < e->table.size(); k++)
         if (e->table[k].state == fm::SLOT_RUN && e->table[k].mode == fm::MODE_LIST) ks.push_back((int)k);
-    if (ks.empty()) return FM_OK;
+    if (ks.empty() || running_list_molecules(e) < TUNE_MIN_MOLECULES) return FM_OK;
     fm::EngFlags saved{};
     EN_CUDA(cudaMemcpyAsync(&saved, e->d.flags, sizeof saved, cudaMemcpyDeviceToHost, e->st));
     EN_CUDA(cudaStreamSynchronize(e->st));
@@ -573,10 +587,7 @@ int autotune(fm_engine *e)
         e->tuned = e->p.list_build != FM_LIST_BUILD_AUTO || e->tuned_build;  // until a list job runs
         return FM_OK;
     }
-    bool any = false;
-    for (size_t k = 0; k < e->table.size(); k++)
-        if (e->table[k].state == fm::SLOT_RUN && e->table[k].mode == fm::MODE_LIST) any = true;
-    if (!any) return FM_OK;  // tune_build found none either
+    if (running_list_molecules(e) < TUNE_MIN_MOLECULES) return FM_OK;  // tune_build waits too
     cudaEvent_t a, b;
     EN_CUDA(cudaEventCreate(&a));
     EN_CUDA(cudaEventCreate(&b));
@@ -806,9 +817,11 @@ extern "C" int fm_engine_step_chunk(fm_engine *e, int32_t *resident_out, int32_t
     EN_TRY(update_hwm(e));
     if (nres > 0) {
         if (!e->tuned) EN_TRY(autotune(e));
-        if (!e->tuned && !e->loop_off) {
-            // the resident jobs are still in their setup: one tick on its own,
-            // so that the autotuner times them running before the tick loop --
+        bool setup_pending = false;
+        for (const fm::EngSlot &sl : e->table) setup_pending |= sl.state == fm::SLOT_SETUP;
+        if (!e->tuned && !e->loop_off && setup_pending) {
+            // the new jobs are still in their setup: one tick on its own, so
+            // that the autotuner times them running before the tick loop --
             // which may run a whole batch in one launch -- is captured with its
             // choice
             fm::eng_tick(e->d, e->tpm, e->need_x, e->st);
