@@ -369,16 +369,20 @@ def run_batched(api, torch, dev, nsteps, nrep=256):
                         "T U(0.7,1.5), rc 2.5, skin 0.3, dt 0.005, VV, FP32 forces; boxes < 3 cells: all pairs"}
 
 
+# Poisson arrivals at this fraction of the service rate probed with 48 jobs resident at once.
+ARRIVAL_FRACTION = 0.6
+
+
 def run_served(api, torch, dev, njobs, seed=0x466D6F6C + 5):
     """Poisson-arriving Couette jobs through the engine's admission loop.
     Job sizes log-uniform in 256-65536 molecules, 200-2000 steps, wall speed
-    U(0.5, 2.0); the arrival rate is 0.5 x the service rate measured with 48
-    jobs resident at once.  Served jobs overlap less than the probe's, so each
-    tick carries fewer molecules and its fixed launch cost weighs more: at 0.6x
-    the queue grows over a 4096-job run, at 0.4x the engine idles ~22% of the
-    time; 0.5x keeps it >80% busy (`gpu_busy_frac`: wall time inside graphs of
-    ticks / total) with a bounded queue.  Latency = finish time - scheduled
-    arrival time."""
+    U(0.5, 2.0); the arrival rate is ARRIVAL_FRACTION x the service rate
+    measured with 48 jobs resident at once.  Served jobs overlap less than the
+    probe's, so each tick carries fewer molecules and its fixed launch cost
+    weighs more: 0.5x left the engine ~77% busy, 0.55x ~79%, 0.6x ~81%
+    (`gpu_busy_frac`: wall time inside graphs of ticks / total), each with a
+    bounded queue (p50 ~0.2 s, p99 ~0.5 s).  Latency = finish time -
+    scheduled arrival time."""
     from flowmol_b200 import couette
     rng = np.random.Generator(np.random.Philox(seed))
 
@@ -415,7 +419,7 @@ def run_served(api, torch, dev, njobs, seed=0x466D6F6C + 5):
     e = new_engine()
     arrivals = np.cumsum(rng.exponential(1.0, njobs))
     mean_work = work / njobs
-    lam = 0.5 * rate_work / mean_work
+    lam = ARRIVAL_FRACTION * rate_work / mean_work
     t_arr = arrivals / lam
     t0 = time.monotonic()
     nxt = 0
