@@ -191,11 +191,12 @@ int loop_body_ticks(const fm_engine *e) { return std::max(1, std::min(e->p.ticks
 
 // The chunk as one graph that loops ticks on the device: a WHILE node whose
 // body is loop_body_ticks ticks followed by k_e_continue, which ends the loop
-// when no job is left running, after ticks_per_chunk ticks, or -- while jobs
-// wait in the queue -- once a job has finished or failed, so the host retires
-// it and admits the next without waiting for the rest of the chunk.  A batch
-// that fits the engine is one launch.  False when the graph cannot be made
-// (the caller captures fixed chunks instead).
+// when no job is left running, after ticks_per_chunk ticks, once a job has
+// failed (the host retires it, or re-queues it after a list overflow), or --
+// while jobs wait in the queue -- once a job has finished, so the host
+// retires it and admits the next without waiting for the rest of the chunk.
+// A batch that fits the engine is one launch.  False when the graph cannot be
+// made (the caller captures fixed chunks instead).
 bool capture_loop(fm_engine *e)
 {
     if (e->loop_off) return false;

@@ -133,9 +133,9 @@ void eng_gather_job(const EngDev &d, int slot, int mol_off, int n, double *r3, d
 void eng_release_job(const EngDev &d, int mol_off, int n, int cell_off, int ncell, cudaStream_t st);
 int eng_kernels_per_tick();
 // The tick loop's bookkeeping: the counter reset before the WHILE node, and
-// the kernel that ends each tick by setting the node's condition -- go on
-// while some resident job runs, fewer than max_ticks ticks have run, and no
-// job has finished or failed while others wait in the queue for its slot.
+// the kernel that ends each iteration by setting the node's condition -- go
+// on while some resident job runs and fewer than max_ticks ticks have run,
+// unless a job has failed or has finished while others wait in the queue.
 void eng_loop_reset(const EngDev &d, cudaStream_t st);
 void eng_loop_continue(const EngDev &d, int slots, cudaGraphConditionalHandle cond, int body_ticks, int max_ticks,
                        cudaStream_t st);

@@ -977,23 +977,26 @@ __global__ void k_e_loop_reset(EngDev d) { d.flags->loop_ticks = 0; }
 
 // Ends an iteration (body_ticks ticks) of the loop: the WHILE node runs
 // another while a resident job is set up or running and the launch has run
-// fewer than max_ticks ticks, unless a job is done or failed (the host
-// retires those between launches) while queued jobs wait for a slot.
+// fewer than max_ticks ticks, unless a job has failed (the host retires it,
+// and re-queues it after a list overflow) or a job is done while queued jobs
+// wait for a slot.
 __global__ void k_e_continue(EngDev d, int slots, cudaGraphConditionalHandle cond, int body_ticks, int max_ticks)
 {
-    int live = 0, ended = 0;
+    int live = 0, done = 0, failed = 0;
     for (int k = threadIdx.x; k < slots; k += blockDim.x) {
         const int st = d.slots[k].state;
         live |= st == SLOT_SETUP || st == SLOT_RUN;
-        ended |= st == SLOT_DONE || st == SLOT_FAILED;
+        done |= st == SLOT_DONE;
+        failed |= st == SLOT_FAILED;
     }
     live = __syncthreads_or(live);
-    ended = __syncthreads_or(ended);
+    done = __syncthreads_or(done);
+    failed = __syncthreads_or(failed);
     if (threadIdx.x == 0) {
         const int t = d.flags->loop_ticks + body_ticks;
         d.flags->loop_ticks = t;
-        const bool make_room = ended && d.flags->queue_waiting;
-        cudaGraphSetConditional(cond, (live && !make_room && t < max_ticks) ? 1u : 0u);
+        const bool to_host = failed || (done && d.flags->queue_waiting);
+        cudaGraphSetConditional(cond, (live && !to_host && t < max_ticks) ? 1u : 0u);
     }
 }
 

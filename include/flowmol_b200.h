@@ -448,9 +448,9 @@ FM_API int fm_engine_submit(fm_engine *e, const fm_job *job, const double *r, co
 /* One admission point (retire finished jobs, admit queued ones that fit)
  * followed by one chunk of ticks: one graph launch whose ticks loop on the
  * device, min(ticks_per_chunk, 32) per iteration, until no job is left
- * running, ticks_per_chunk ticks have run, or -- while jobs wait in the
- * queue -- a job has finished or failed; reports how many jobs are resident
- * and queued afterwards. */
+ * running, ticks_per_chunk ticks have run, a job has failed, or -- while
+ * jobs wait in the queue -- a job has finished; reports how many jobs are
+ * resident and queued afterwards. */
 FM_API int fm_engine_step_chunk(fm_engine *e, int32_t *resident, int32_t *queued);
 /* Chunks until nothing is resident or queued (max_chunks <= 0: no limit). */
 FM_API int fm_engine_run(fm_engine *e, int32_t max_chunks);

@@ -96,6 +96,18 @@ def test_tick_loop_runs_a_batch_in_one_launch(gpu_lib):
     assert (res, q) == (0, 0) and sorted(x["final_iter"] for x in e.results()) == [60, 120]
     assert e.counters()["ticks"] <= 64 + 96
     e.close()
+    # a job whose list overflows ends the launch at once (it is re-queued with
+    # more room) instead of waiting for a long job beside it to finish
+    e = engine(ticks=100000)
+    r, v, dom = lj_replica(*reps[0])
+    e.submit(api.make_job(len(r), dom, 2.5, 60, tplot=20, nlist_capacity=8), r, v)
+    r2, v2, dom2 = lj_replica(*reps[1])
+    e.submit(api.make_job(len(r2), dom2, 2.5, 600, tplot=200), r2, v2)
+    e.run()
+    out = e.results()
+    assert all(x["status"] == 0 for x in out) and max(x["retries"] for x in out) >= 1
+    assert e.counters()["ticks"] <= 600 + 64
+    e.close()
 
 
 def test_couette_job_follows_oracle(gpu_lib):
