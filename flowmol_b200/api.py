@@ -149,6 +149,7 @@ class FmInput(C.Structure):
         ("slidedistbottom", C.c_double * 3), ("fixdisttop", C.c_double * 3), ("fixdistbottom", C.c_double * 3),
         ("wallslidev", C.c_double * 3), ("teth_k", C.c_double * 3), ("thermostattemperature", C.c_double * 2),
         ("targetconc", C.c_double), ("eps_pp", C.c_double), ("eps_ps", C.c_double), ("eps_ss", C.c_double),
+        ("sort_freq", C.c_int32), ("sortblocksize", C.c_int32),
     ]
 
     def as_dict(self):
@@ -203,6 +204,9 @@ def lib():
             "fm_linklist_deallocateall": [h],
             "fm_sendmols": [h],
             "fm_sort_mols": [h],
+            "fm_set_sort": [h, C.c_int32, C.c_int32, C.c_int32],
+            "fm_get_sort_state": [h, P(C.c_int64), P(C.c_int64), P(C.c_int32), P(C.c_double), P(C.c_int32)],
+            "fm_sort_table": [C.c_int32, P(C.c_int32), P(C.c_int32), C.c_int64],
             "fm_rebuild_lists": [h],
             "fm_assign_to_cell": [h],
             "fm_assign_to_neighbourlist": [h],
@@ -481,10 +485,20 @@ class MDSystem:
     def sendmols(self):
         check(lib().fm_sendmols(self.h))
 
+    def set_sort(self, sort_flag, sort_freq=1, sortblocksize=1):
+        """SORT_FLAG: 0 off, 1 x-fastest blocks, 2 Hilbert-ordered blocks of
+        sortblocksize^3 cells, every sort_freq-th rebuild."""
+        check(lib().fm_set_sort(self.h, int(sort_flag), int(sort_freq), int(sortblocksize)))
+
     def sort_mols(self):
-        """The device keeps molecules in cell order internally; transfers use
-        upload order, so the reference's Hilbert re-order is invisible."""
+        """Every sort_freq-th call re-numbers the molecules by sort block
+        (linklist.f90:2744-2869); downloads report the new order."""
         check(lib().fm_sort_mols(self.h))
+
+    def sort_state(self):
+        so = C.c_int64(); sk = C.c_int64(); nr = C.c_int32(); f1 = C.c_double(); f2 = C.c_int32()
+        check(lib().fm_get_sort_state(self.h, C.byref(so), C.byref(sk), C.byref(nr), C.byref(f1), C.byref(f2)))
+        return dict(sorts=so.value, skipped=sk.value, nrebuilds=nr.value, sf1=f1.value, sf2=f2.value)
 
     def assign_to_cell(self):
         check(lib().fm_assign_to_cell(self.h))
@@ -739,6 +753,14 @@ def write_final_state(path, h, r, v, tag=None, rtether=None, glob_no=None, rtrue
     monomer = arr(monomer, np.float64)
     check(lib().fm_write_final_state(os.fsencode(path), C.byref(h), _dpn(r), _dpn(v), _ip32(tag), _dpn(rtether),
                                      _ip32(glob_no), _dpn(rtrue), _ip32(moltype), _dpn(monomer)))
+
+
+def sort_table(sort_flag, nblocks):
+    """Hcurve over nblocks sort blocks per axis, flat and x fastest."""
+    nb = (C.c_int32 * 3)(*[int(x) for x in nblocks])
+    out = np.zeros(int(np.prod(nblocks)), np.int32)
+    check(lib().fm_sort_table(int(sort_flag), nb, out.ctypes.data_as(C.POINTER(C.c_int32)), out.size))
+    return out
 
 
 def read_input(path) -> FmInput:

@@ -13,7 +13,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libflowmol_b200.so")
-SOURCES = ["fm_kernels.cu", "fm_dd_kernels.cu", "fm_api.cu", "fm_noalloc.cu", "fm_engine_kernels.cu", "fm_engine.cu", "fm_io.cpp"]
+SOURCES = ["fm_kernels.cu", "fm_dd_kernels.cu", "fm_sort.cu", "fm_api.cu", "fm_noalloc.cu", "fm_engine_kernels.cu", "fm_engine.cu", "fm_io.cpp"]
 HEADERS = ["fm_common.cuh", "fm_device.cuh", "fm_build.cuh", "fm_engine.cuh", "fm_tile.cuh"]
 
 NVCC_FLAGS = [

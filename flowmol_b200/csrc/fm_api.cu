@@ -110,6 +110,10 @@ struct fm_handle {
     int rbt[4] = {0, 0, 0, 0};    // lanes per molecule the force kernels were captured with
     bool rb_off = false;          // graphs unavailable here: per-kernel launches
     cudaStream_t cap_st = nullptr, cap_st2 = nullptr;
+    // sort_mols (fm_sort.cu): sort_flag 0 leaves the numbering alone
+    int sort_flag = 0;
+    fm::FmSortDev sdev{};
+    bool glob_moved = false;      // a sort was configured: global numbers live on the device
 };
 
 // ---------------------------------------------------------------------------
@@ -189,9 +193,23 @@ static void release_graphs(fm_handle *h)
     }
 }
 
+// Kernels of one launch_sort (the radix sort's own are the library's).
+constexpr int SORT_KERNELS = 5;
+
+static void free_sort(fm_handle *h)
+{
+    fm::FmSortDev &s = h->sdev;
+    void *ptrs[] = {(void *)s.hc, s.key, s.key_out, s.val, s.val_out, s.cnt, s.newv, s.gtmp, s.tmp, s.ss};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    s = fm::FmSortDev{};
+    h->sort_flag = 0;
+}
+
 static void release(fm_handle *h)
 {
     release_graphs(h);
+    free_sort(h);
     if (h->cap_st) cudaStreamDestroy(h->cap_st);
     if (h->cap_st2) cudaStreamDestroy(h->cap_st2);
     h->cap_st = h->cap_st2 = nullptr;
@@ -633,6 +651,7 @@ extern "C" int fm_set_mie(fm_handle *h, const fm_mie_tables *t, const int32_t *m
 {
     if (!h || !t || !moltype) return fail(FM_ERR_ARG, "null argument");
     if (h->stage != 1) return fail(FM_ERR_STATE, "set the Mie tables after fm_upload_state and before fm_setup");
+    if (h->sort_flag) return fail(FM_ERR_ARG, "Sort should be turned off - Not developed for Mie potential");
     const int nt = t->ntypes;
     if (nt < 1 || nt > FM_MIE_MAXTYPES) return fail(FM_ERR_ARG, "ntypes out of range (1 .. FM_MIE_MAXTYPES)");
     if (!t->mass || !t->epsilon || !t->lambdar || !t->lambdaa || !t->C || !t->alpha || !t->potshift ||
@@ -717,6 +736,17 @@ extern "C" int fm_get_bonds(fm_handle *h, int32_t *owner, int32_t *partner, int8
     return FM_OK;
 }
 
+// Global numbers by upload index: once a sort was configured they are
+// renumbered on the device, and the host copy is refreshed before each use.
+static int pull_glob(fm_handle *h)
+{
+    if (!h->glob_moved || h->glob_host.empty()) return FM_OK;
+    FM_CUDA(cudaMemcpyAsync(h->glob_host.data(), h->glob, sizeof(int32_t) * h->glob_host.size(),
+                            cudaMemcpyDeviceToHost, h->st));
+    FM_CUDA(cudaStreamSynchronize(h->st));
+    return FM_OK;
+}
+
 extern "C" int fm_download_state(fm_handle *h, double *r, double *v, double *a, int32_t *glob_no)
 {
     if (!h) return fail(FM_ERR_ARG, "null handle");
@@ -731,7 +761,10 @@ extern "C" int fm_download_state(fm_handle *h, double *r, double *v, double *a, 
     if (a) FM_CUDA(cudaMemcpyAsync(a, da, bytes, cudaMemcpyDeviceToHost, h->st));
     FM_CUDA(cudaGetLastError());
     FM_CUDA(cudaStreamSynchronize(h->st));
-    if (glob_no) std::memcpy(glob_no, h->glob_host.data(), sizeof(int32_t) * n);
+    if (glob_no) {
+        FM_TRY(pull_glob(h));
+        std::memcpy(glob_no, h->glob_host.data(), sizeof(int32_t) * n);
+    }
     return FM_OK;
 }
 
@@ -846,10 +879,20 @@ static int grow_nlist(fm_handle *h, const fm::FmScalars &s, int iter)
 // pieces of the step
 // ---------------------------------------------------------------------------
 
+// sort_mols of a rebuild, after the periodic wrap and before the cell sort
+// orders each cell's members by the (new) upload index.
+static void queue_sort(fm_handle *h, int gated, cudaStream_t st)
+{
+    if (!h->sort_flag) return;
+    fm::launch_sort(h->d, h->sdev, gated, st);
+    h->launches += SORT_KERNELS;
+}
+
 static void queue_cells(fm_handle *h, int wrap, int gated)
 {
     const FmDev &d = h->d;
     fm::launch_wrap_bin(d, wrap, 1, gated, h->iter, h->st);
+    if (wrap) queue_sort(h, gated, h->st);
     fm::launch_scan_cells(d, gated, h->st);
     fm::launch_scatter(d, gated, h->st);
     fm::launch_reorder(d, gated, h->tpos, h->tuidx, h->st);
@@ -1016,6 +1059,7 @@ static void queue_rebuild_check(fm_handle *h, int it, int flip)
         queue_decide(h, it, flip);
         fm::launch_wrap_bin(h->d, 1, 0, 1, it, h->st);
         h->launches += 1;
+        queue_sort(h, 1, h->st);
     }
 }
 
@@ -1035,7 +1079,7 @@ static bool capture_branch(fm_handle *h, int flip)
     if (cudaStreamGetCaptureInfo(h->cap_st, &cst, nullptr, &g, nullptr, nullptr) != cudaSuccess || !g) return false;
     cudaGraphConditionalHandle cond{};
     if (cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault) != cudaSuccess) return false;
-    const int body_kernels = 8 + (d.tile ? 1 : 0) + (d.angular ? 1 : 0);
+    const int body_kernels = 8 + (d.tile ? 1 : 0) + (d.angular ? 1 : 0) + (h->sort_flag ? SORT_KERNELS : 0);
     fm::launch_decide_graph(d, flip, p.rebuild_criteria, p.fixed_rebuild, h->half_min_delta, cond, body_kernels,
                             h->cap_st);
     if (cudaStreamGetCaptureInfo(h->cap_st, &cst, nullptr, nullptr, &deps, &nd) != cudaSuccess) return false;
@@ -1054,6 +1098,7 @@ static bool capture_branch(fm_handle *h, int flip)
         return false;
     fm::pdl_capture = true;  // the body's first kernel has no predecessor to overlap
     fm::launch_wrap_bin(d, 1, 1, 1, fm::ITER_DEVICE, h->cap_st2);
+    if (h->sort_flag) fm::launch_sort(d, h->sdev, 1, h->cap_st2);
     fm::pdl_capture = false;
     fm::launch_scan_cells(d, 1, h->cap_st2);
     fm::launch_scatter(d, 1, h->cap_st2);
@@ -1194,6 +1239,7 @@ static int queue_steps(fm_handle *h, int first, int nsteps, int phase, const std
                 queue_decide(h, it, fused_move1 ? 1 : 0);
                 fm::launch_wrap_bin(h->d, 1, 0, 1, it, h->st);
                 h->launches += 1;
+                queue_sort(h, 1, h->st);
             }
         }
         const int record = (it % p.tplot) == 0;
@@ -1334,7 +1380,89 @@ extern "C" int fm_check_rebuild(fm_handle *h, int32_t *rebuild)
     return FM_OK;
 }
 
-extern "C" int fm_sort_mols(fm_handle *h) { return ready(h, 1); }
+extern "C" int fm_set_sort(fm_handle *h, int32_t sort_flag, int32_t sort_freq, int32_t sortblocksize)
+{
+    FM_TRY(ready(h, 1));  // refuses a subdomain handle: its molecules are named by global number
+    if (sort_flag < 0 || sort_flag > 2) return fail(FM_ERR_ARG, "Incorrect value of sort_flag");
+    if (sort_flag != 0 && h->p.potential_flag == 1)
+        return fail(FM_ERR_ARG, "Sort should be turned off - Not developed for polymers");
+    if (sort_flag != 0 && h->d.mie) return fail(FM_ERR_ARG, "Sort should be turned off - Not developed for Mie potential");
+    if (sort_flag != 0 && sortblocksize < 1) return fail(FM_ERR_ARG, "sortblocksize must be at least 1");
+    FM_TRY(fm_sync(h));
+    release_graphs(h);  // recaptured with or without the sort kernels
+    free_sort(h);
+    if (sort_flag == 0) return FM_OK;
+    fm::FmSortDev s{};
+    long long blocks = 1;
+    for (int k = 0; k < 3; k++) {
+        s.bsl[k] = (double)sortblocksize * h->d.cs[k];  // blocksidelength (linklist.f90:2790-2791)
+        s.nb[k] = (int)std::ceil(h->d.L[k] / s.bsl[k]);
+        blocks *= s.nb[k];
+    }
+    if (blocks > (1ll << 26)) return fail(FM_ERR_ARG, "sort blocks: more than 2^26");
+    std::vector<int32_t> hc((size_t)blocks);
+    const char *why = nullptr;
+    if (fm::sort_table(sort_flag, s.nb, hc.data(), &why) != 0) return fail(FM_ERR_ARG, why);
+    s.freq = sort_freq;
+    s.blocks = (int)blocks;
+    s.end_bit = 1;
+    while ((1ll << s.end_bit) < blocks) s.end_bit++;
+    const int n = h->d.n;
+    int32_t *hcd = nullptr;
+    std::vector<int32_t> iota((size_t)n);
+    for (int i = 0; i < n; i++) iota[(size_t)i] = i;
+    fm::FmSortScalars q{};
+    q.nrebuilds = 1;
+    q.sf1 = 1.5;
+    q.sf2 = 5;
+    s.tmp_bytes = fm::sort_scratch_bytes(n, s.end_bit);
+    h->sdev = s;  // free_sort releases whatever the allocations below got
+    fm::FmSortDev &t = h->sdev;
+    FM_TRY(dalloc(&hcd, (size_t)blocks));
+    t.hc = hcd;
+    FM_TRY(dalloc(&t.key, n)); FM_TRY(dalloc(&t.key_out, n)); FM_TRY(dalloc(&t.val, n));
+    FM_TRY(dalloc(&t.val_out, n)); FM_TRY(dalloc(&t.cnt, (size_t)blocks)); FM_TRY(dalloc(&t.newv, n));
+    FM_TRY(dalloc(&t.gtmp, n)); FM_TRY(dalloc(&t.ss, 1));
+    FM_CUDA(cudaMalloc(&t.tmp, std::max<size_t>(t.tmp_bytes, 16)));
+    t.glob = h->glob;
+    FM_CUDA(cudaMemcpyAsync(hcd, hc.data(), sizeof(int32_t) * (size_t)blocks, cudaMemcpyHostToDevice, h->st));
+    FM_CUDA(cudaMemcpyAsync(t.val, iota.data(), sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice, h->st));
+    FM_CUDA(cudaMemsetAsync(t.key, 0, sizeof(int32_t) * (size_t)n, h->st));
+    FM_CUDA(cudaMemsetAsync(t.cnt, 0, sizeof(int32_t) * (size_t)blocks, h->st));
+    FM_CUDA(cudaMemcpyAsync(t.ss, &q, sizeof(q), cudaMemcpyHostToDevice, h->st));
+    FM_CUDA(cudaStreamSynchronize(h->st));  // the host vectors go out of scope
+    h->sort_flag = sort_flag;
+    h->glob_moved = true;
+    return FM_OK;
+}
+
+extern "C" int fm_get_sort_state(fm_handle *h, int64_t *sorts, int64_t *skipped, int32_t *nrebuilds, double *sf1,
+                                 int32_t *sf2)
+{
+    FM_TRY(ready(h, 1));
+    fm::FmSortScalars q{};
+    q.nrebuilds = 1;
+    q.sf1 = 1.5;
+    q.sf2 = 5;
+    if (h->sort_flag) {
+        FM_CUDA(cudaMemcpyAsync(&q, h->sdev.ss, sizeof(q), cudaMemcpyDeviceToHost, h->st));
+        FM_CUDA(cudaStreamSynchronize(h->st));
+    }
+    if (sorts) *sorts = q.sorts;
+    if (skipped) *skipped = q.skipped;
+    if (nrebuilds) *nrebuilds = q.nrebuilds;
+    if (sf1) *sf1 = q.sf1;
+    if (sf2) *sf2 = q.sf2;
+    return FM_OK;
+}
+
+extern "C" int fm_sort_mols(fm_handle *h)
+{
+    FM_TRY(ready(h, 1));
+    queue_sort(h, 0, h->st);
+    FM_CUDA(cudaGetLastError());
+    return FM_OK;
+}
 
 extern "C" int fm_sendmols(fm_handle *h)
 {
@@ -1508,6 +1636,7 @@ extern "C" int fm_get_pair_list(fm_handle *h, int32_t *owner, int32_t *partner, 
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->st);
     if (dnbr != h->d.nbr) cudaFree(dnbr);
     FM_CUDA(ce);
+    FM_TRY(pull_glob(h));
     int64_t k = 0;
     for (size_t i = 0; i < n; i++) {
         for (int q = 0; q < nnbr[i]; q++) {

@@ -283,4 +283,44 @@ void launch_scatter_state(const FmDev &d, const double *r3, const double *v3, co
 void launch_gather_state(const FmDev &d, double *r3, double *v3, double *a3, int32_t *gid,
                          double *pe, double *vir, cudaStream_t st);
 
+// ---- sort_mols (fm_sort.cu) ------------------------------------------------
+// Device scalars of sort_mols (linklist.f90:2744-2869): its save variables
+// nrebuilds (starts at 1), sf1 (1.5) and sf2 (5), and the current sort.
+struct FmSortScalars {
+    int32_t nrebuilds;
+    int32_t due;       // this rebuild sorts
+    int32_t ave;       // ave_molperblock of this sort, safety factors applied
+    int32_t overflow;  // a block holds more than ave: this sort is skipped
+    double sf1;
+    int32_t sf2;
+    int32_t pad_;
+    int64_t sorts, skipped;
+};
+// Sort blocks of sortblocksize^3 cells, their Hcurve order and the buffers of
+// the stable (block, upload index) sort.  Keys and values are by upload index.
+struct FmSortDev {
+    int freq, blocks, end_bit;
+    int nb[3];
+    double bsl[3];                // blocksidelength
+    const int32_t *hc;            // Hcurve, x fastest, values 1..blocks
+    int32_t *key, *key_out;       // block (0-based Hcurve value) by upload index, sorted
+    int32_t *val, *val_out;       // 0..n-1, and the upload indices in sorted order
+    int32_t *cnt;                 // molecules per block of the current sort
+    int32_t *newv;                // new upload index of each old one
+    int32_t *gtmp;                // global numbers, permuted
+    int32_t *glob;                // global number by upload index (the handle's)
+    void *tmp;                    // radix-sort scratch
+    size_t tmp_bytes;
+    FmSortScalars *ss;
+};
+// Hcurve for sort_flag 1 (x-fastest block numbers) or 2 (build_hilbert,
+// functions_lib.f90:2555-2604) over nb blocks per axis, into out[blocks].
+// Returns 0, or -1 with *why set.
+int sort_table(int flag, const int nb[3], int32_t *out, const char **why);
+// Radix-sort scratch bytes for n (key, value) pairs of end_bit key bits.
+size_t sort_scratch_bytes(int n, int end_bit);
+// The rebuild's sort_mols: counter, keys, stable sort, renumbering.  With
+// `gated` the kernels run only on a rebuild step.
+void launch_sort(const FmDev &d, const FmSortDev &s, int gated, cudaStream_t st);
+
 }  // namespace fm

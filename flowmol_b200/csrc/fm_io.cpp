@@ -336,7 +336,14 @@ extern "C" int fm_read_input(const char *path, fm_input *in)
     opt_i("POTENTIAL_FLAG", &in->potential_flag, 1);
     opt_i("PERIODIC", in->periodic, 3);
     opt_i("GLOBAL_NUMBERING", &in->global_numbering, 1);
-    opt_i("SORT_FLAG", &in->sort_flag, 1);
+    {  // SORT_FLAG: sort_flag, sort_freq, sortblocksize (setup_read_input.f90:818-827)
+        int32_t sf[3];
+        if (opt_i("SORT_FLAG", sf, 3)) {
+            in->sort_flag = sf[0];
+            in->sort_freq = sf[1];
+            in->sortblocksize = sf[2];
+        }
+    }
     opt_i("PRESSURE_OUTFLAG", &in->pressure_outflag, 1);
     opt_i("SLRC_FLAG", &in->sLRC_flag, 1);
     {
@@ -416,5 +423,10 @@ extern "C" int fm_read_input(const char *path, fm_input *in)
             if (cnt > 0) in->nthermo = cnt;
         }
     }
+    // GLOBAL_NUMBERING (setup_read_input.f90:835-847): polymers number their
+    // beads in the monomer data instead, and numbering cannot sort
+    if (in->potential_flag == 1) in->global_numbering = 0;
+    if (in->global_numbering == 1 && in->sort_flag != 0)
+        return iofail(FM_ERR_ARG, "Global number does not work with sort flag on");
     return FM_OK;
 }

@@ -241,15 +241,36 @@ FM_API int fm_linklist_deallocateall(fm_handle *h);
 /* sendmols, single-rank form: periodic wrap r >= L/2 -> r-L, r < -L/2 -> r+L
  * (messenger.serial.f90:961-1028; messenger.MPI.f90:1383-1424). */
 FM_API int fm_sendmols(fm_handle *h);
-/* sort_mols (linklist.f90:2744-2869): the reference re-orders r and v along a
- * Hilbert curve every sort_freq rebuilds for cache locality.  The device keeps
- * its molecules in cell order at every rebuild anyway, and state transfers use
- * upload order, so the order is invisible to the caller and this call only
- * validates the handle.  A run started from an input with SORT_FLAG != 0
- * therefore matches the reference run with SORT_FLAG 0: the caller's molecule
- * order never changes, and the FP64 sums are not taken in the order that the
- * reference's Hilbert renumbering would give (rounding-level differences). */
+/* SORT_FLAG (setup_read_input.f90:812-827): sort_flag 0 off, 1 blocks in
+ * x-fastest order, 2 blocks along a 3-D Hilbert curve; every sort_freq-th
+ * rebuild; blocks of sortblocksize^3 cells.  Builds the block table Hcurve
+ * (setup_set_parameters.f90:1140-1163) and resets the save variables of
+ * sort_mols (nrebuilds 1, safety factors 1.5 and 5).  Call after
+ * fm_upload_state.  Refused as the reference aborts: polymers, Mie, a
+ * sort_flag other than 0..2; also a subdomain handle (its molecules are named
+ * by global number, so their order carries nothing). */
+FM_API int fm_set_sort(fm_handle *h, int32_t sort_flag, int32_t sort_freq, int32_t sortblocksize);
+/* sort_mols (linklist.f90:2744-2869): on every sort_freq-th call, puts the
+ * molecules in the order of their sort blocks' Hcurve numbers, stable within
+ * a block; if a block holds more than ceiling((np/blocks) sf1 + sf2)
+ * molecules it keeps the order and grows sf1 by 0.1 and sf2 by 5.  The order
+ * is the one fm_download_state, fm_get_per_molecule and fm_get_pair_list
+ * report in (global numbers move with their molecules); the device's own
+ * layout stays in cell order.  The next cell sort orders each cell by the new
+ * numbering, so list order and FP64 summation order follow it as they follow
+ * the reference's array order.  Unlike the reference, a is permuted too (the
+ * reference recomputes it before reading it).  fm_step runs it on the device
+ * in each rebuild, after the periodic wrap.  With sort_flag 0 (the default)
+ * it does nothing. */
 FM_API int fm_sort_mols(fm_handle *h);
+/* Counters of sort_mols: sorts done, sorts skipped by an overflowing block,
+ * and its save variables nrebuilds, sf1, sf2.  Any output may be NULL. */
+FM_API int fm_get_sort_state(fm_handle *h, int64_t *sorts, int64_t *skipped, int32_t *nrebuilds, double *sf1,
+                             int32_t *sf2);
+/* Hcurve for nblocks sort blocks per axis, x fastest, values 1..blocks:
+ * sort_flag 1 numbers blocks in x-fastest order, 2 follows build_hilbert
+ * (functions_lib.f90:2555-2604).  Host only; cap >= nblocks[0]*[1]*[2]. */
+FM_API int fm_sort_table(int32_t sort_flag, const int32_t nblocks[3], int32_t *table, int64_t cap);
 /* assign_to_cell (linklist.f90:2645-2679) as a counting sort: histogram,
  * exclusive scan, scatter.  Molecules are also re-ordered by cell on the
  * device (invisible through fm_download_state). */
@@ -364,6 +385,7 @@ typedef struct fm_input {
     double thermostattemperature[2];
     double targetconc;           /* FENE_SOLUTION [5] */
     double eps_pp, eps_ps, eps_ss; /* SOLVENT_INFO [2-4] when solvent_flag is 1 */
+    int32_t sort_freq, sortblocksize; /* SORT_FLAG [2-3] (for fm_set_sort) */
 } fm_input;
 
 FM_API int fm_read_input(const char *path, fm_input *in);

@@ -1591,3 +1591,177 @@ long orc_bond_list(orc *s, int *owner, int *partner, int *code, long cap)
         }
     return n;
 }
+
+/* ---- sort_mols ----------------------------------------------------------- */
+
+/* hilbert3 of build_hilbert (functions_lib.f90:2609-2637) as the reference
+ * writes it: level n is eight copies of level n-1, the k-th copy mapped by the
+ * k-th entry of the array constructors for x, y and z.  Returns the point
+ * count (8^n), or 0 when allocation fails. */
+static size_t orc_hilbert3(int n, double **x, double **y, double **z)
+{
+    if (n <= 0) {
+        *x = calloc(1, sizeof(double)); *y = calloc(1, sizeof(double)); *z = calloc(1, sizeof(double));
+        if (!*x || !*y || !*z) return 0;
+        return 1;
+    }
+    double *xo, *yo, *zo;
+    size_t m = orc_hilbert3(n - 1, &xo, &yo, &zo);
+    if (!m) return 0;
+    *x = malloc(8 * m * sizeof(double)); *y = malloc(8 * m * sizeof(double)); *z = malloc(8 * m * sizeof(double));
+    if (!*x || !*y || !*z) { free(xo); free(yo); free(zo); return 0; }
+    double *X = *x, *Y = *y, *Z = *z;
+    for (size_t i = 0; i < m; i++) {
+        /* x = 0.5*(/ .5+zo, .5+yo, -.5+yo, -.5-xo, -.5-xo, -.5-yo, .5-yo, .5+zo /) */
+        X[0 * m + i] = 0.5 * (0.5 + zo[i]);  X[1 * m + i] = 0.5 * (0.5 + yo[i]);
+        X[2 * m + i] = 0.5 * (-0.5 + yo[i]); X[3 * m + i] = 0.5 * (-0.5 - xo[i]);
+        X[4 * m + i] = 0.5 * (-0.5 - xo[i]); X[5 * m + i] = 0.5 * (-0.5 - yo[i]);
+        X[6 * m + i] = 0.5 * (0.5 - yo[i]);  X[7 * m + i] = 0.5 * (0.5 + zo[i]);
+        /* y = 0.5*(/ .5+xo, .5+zo, .5+zo, .5+yo, -.5+yo, -.5-zo, -.5-zo, -.5-xo /) */
+        Y[0 * m + i] = 0.5 * (0.5 + xo[i]);  Y[1 * m + i] = 0.5 * (0.5 + zo[i]);
+        Y[2 * m + i] = 0.5 * (0.5 + zo[i]);  Y[3 * m + i] = 0.5 * (0.5 + yo[i]);
+        Y[4 * m + i] = 0.5 * (-0.5 + yo[i]); Y[5 * m + i] = 0.5 * (-0.5 - zo[i]);
+        Y[6 * m + i] = 0.5 * (-0.5 - zo[i]); Y[7 * m + i] = 0.5 * (-0.5 - xo[i]);
+        /* z = 0.5*(/ .5+yo, -.5+xo, -.5+xo, .5-zo, .5-zo, -.5+xo, -.5+xo, .5-yo /) */
+        Z[0 * m + i] = 0.5 * (0.5 + yo[i]);  Z[1 * m + i] = 0.5 * (-0.5 + xo[i]);
+        Z[2 * m + i] = 0.5 * (-0.5 + xo[i]); Z[3 * m + i] = 0.5 * (0.5 - zo[i]);
+        Z[4 * m + i] = 0.5 * (0.5 - zo[i]);  Z[5 * m + i] = 0.5 * (-0.5 + xo[i]);
+        Z[6 * m + i] = 0.5 * (-0.5 + xo[i]); Z[7 * m + i] = 0.5 * (0.5 - yo[i]);
+    }
+    free(xo); free(yo); free(zo);
+    return 8 * m;
+}
+
+/* Hcurve (setup_set_parameters.f90:1140-1163): sort_flag 1 numbers the
+ * blocks x fastest; sort_flag 2 is build_hilbert (functions_lib.f90:
+ * 2555-2604).  hc holds nb[0]*nb[1]*nb[2] values, x fastest.  Returns
+ * ORC_OK, ORC_ERR_PARAM (bad flag, a cell the curve missed, or more than 8
+ * levels) or ORC_ERR_ALLOC. */
+int orc_sort_table(int sort_flag, const int nb[3], int *hc)
+{
+    const long blocks = (long)nb[0] * nb[1] * nb[2];
+    if (sort_flag == 1) {
+        for (int k = 1; k <= nb[2]; k++)
+            for (int j = 1; j <= nb[1]; j++)
+                for (int i = 1; i <= nb[0]; i++)
+                    hc[(i - 1) + nb[0] * ((j - 1) + nb[1] * (k - 1))] = i + nb[0] * (j - 1) + nb[0] * nb[1] * (k - 1);
+        return ORC_OK;
+    }
+    if (sort_flag != 2) return ORC_ERR_PARAM;
+    int maxcells = nb[0];
+    if (nb[1] > maxcells) maxcells = nb[1];
+    if (nb[2] > maxcells) maxcells = nb[2];
+    int hindex = (int)ceil(log((double)maxcells) / log(2.0));
+    if (hindex > 8) return ORC_ERR_PARAM;
+    double *x, *y, *z;
+    size_t n = orc_hilbert3(hindex, &x, &y, &z);
+    if (!n) return ORC_ERR_ALLOC;
+    if (hindex - log((double)maxcells) / log(2.0) > 0.0001) maxcells = (int)ceil(pow(8.0, (double)hindex / 3.0));
+    double mn = x[0];
+    for (size_t i = 0; i < n; i++) {
+        if (x[i] < mn) mn = x[i];
+        if (y[i] < mn) mn = y[i];
+        if (z[i] < mn) mn = z[i];
+    }
+    const double shift = 0.00001 - mn;
+    for (long b = 0; b < blocks; b++) hc[b] = -666;
+    int m = 0;
+    for (size_t i = 0; i < n; i++) {
+        int icell = (int)ceil((x[i] + shift) * maxcells);
+        int jcell = (int)ceil((y[i] + shift) * maxcells);
+        int kcell = (int)ceil((z[i] + shift) * maxcells);
+        if (icell <= nb[0] && jcell <= nb[1] && kcell <= nb[2]) {
+            m = m + 1;
+            hc[(icell - 1) + nb[0] * ((jcell - 1) + nb[1] * (kcell - 1))] = m;
+        }
+    }
+    free(x); free(y); free(z);
+    for (long b = 0; b < blocks; b++)
+        if (hc[b] == -666) return ORC_ERR_PARAM;
+    return ORC_OK;
+}
+
+/* The save variables of sort_mols (linklist.f90:2758-2762). */
+typedef struct orc_sort_state {
+    int nrebuilds;  /* starts at 1 */
+    int sf2;        /* starts at 5 */
+    double sf1;     /* starts at 1.5 */
+} orc_sort_state;
+
+/* sort_mols (linklist.f90:2744-2869) on np molecules: r and v are (3, np)
+ * column-major and re-ordered in place, with glob (may be NULL) moved like
+ * tag.  hc is the table of orc_sort_table for the block grid nblocks =
+ * ceiling(domain / (sortblocksize * cellsidelength)).  *did is 0 when the
+ * rebuild counter or sort_flag 0 leaves the order alone, 1 when the molecules
+ * were sorted (perm[p] = old 0-based index of the molecule now at p) and 2
+ * when a block overflowed ave_molperblock (order unchanged, safety factors
+ * grown).  The reference's error_abort for polymers and Mie is the caller's
+ * business. */
+int orc_sort_mols(int np, double *r, double *v, int *glob, const double domain[3],
+                  const double cellsidelength[3], int sort_flag, int sort_freq, int sortblocksize,
+                  const int *hc, orc_sort_state *st, int *perm, int *did)
+{
+    *did = 0;
+    if (st->nrebuilds != sort_freq) {
+        st->nrebuilds = st->nrebuilds + 1;
+        return ORC_OK;
+    }
+    st->nrebuilds = 1;
+    if (sort_flag == 0) return ORC_OK;
+    if (sort_flag != 1 && sort_flag != 2) return ORC_ERR_PARAM;
+    double blocksidelength[3], halfdomain[3];
+    int nblocks[3];
+    for (int k = 0; k < 3; k++) {
+        blocksidelength[k] = sortblocksize * cellsidelength[k];
+        nblocks[k] = (int)ceil(domain[k] / blocksidelength[k]);
+        halfdomain[k] = 0.5 * domain[k];
+    }
+    const int blocks = nblocks[0] * nblocks[1] * nblocks[2];
+    int ave_molperblock = np / blocks;
+    ave_molperblock = (int)ceil(ave_molperblock * st->sf1 + st->sf2);
+    int *molperblock = calloc((size_t)blocks, sizeof(int));
+    int *blockof = malloc((size_t)(np > 0 ? np : 1) * sizeof(int));
+    if (!molperblock || !blockof) { free(molperblock); free(blockof); return ORC_ERR_ALLOC; }
+    for (int n = 0; n < np; n++) {
+        int ib[3];
+        for (int k = 0; k < 3; k++) ib[k] = (int)ceil((r[3 * (size_t)n + k] + halfdomain[k]) / blocksidelength[k]);
+        long lin = (ib[0] - 1) + (long)nblocks[0] * ((ib[1] - 1) + (long)nblocks[1] * (ib[2] - 1));
+        if (lin < 0) lin = 0;  /* a molecule on the lower face: see the CUDA path */
+        if (lin > blocks - 1) lin = blocks - 1;
+        int i = hc[lin];
+        molperblock[i - 1] = molperblock[i - 1] + 1;
+        if (molperblock[i - 1] > ave_molperblock) {
+            st->sf1 = st->sf1 + 0.1;
+            st->sf2 = st->sf2 + 5;
+            free(molperblock); free(blockof);
+            *did = 2;
+            return ORC_OK;
+        }
+        blockof[n] = i;
+    }
+    /* copy back block by block, each block in its molecules' old order */
+    int *start = malloc((size_t)blocks * sizeof(int));
+    double *r0 = malloc(3 * (size_t)np * sizeof(double) + 1), *v0 = malloc(3 * (size_t)np * sizeof(double) + 1);
+    int *g0 = glob ? malloc((size_t)np * sizeof(int) + 1) : NULL;
+    if (!start || !r0 || !v0 || (glob && !g0)) {
+        free(start); free(r0); free(v0); free(g0); free(molperblock); free(blockof);
+        return ORC_ERR_ALLOC;
+    }
+    memcpy(r0, r, 3 * (size_t)np * sizeof(double));
+    memcpy(v0, v, 3 * (size_t)np * sizeof(double));
+    if (glob) memcpy(g0, glob, (size_t)np * sizeof(int));
+    int pos = 0;
+    for (int b = 0; b < blocks; b++) { start[b] = pos; pos += molperblock[b]; }
+    for (int n = 0; n < np; n++) {
+        int p = start[blockof[n] - 1]++;
+        perm[p] = n;
+        for (int k = 0; k < 3; k++) {
+            r[3 * (size_t)p + k] = r0[3 * (size_t)n + k];
+            v[3 * (size_t)p + k] = v0[3 * (size_t)n + k];
+        }
+        if (glob) glob[p] = g0[n];
+    }
+    free(start); free(r0); free(v0); free(g0); free(molperblock); free(blockof);
+    *did = 1;
+    return ORC_OK;
+}

@@ -94,6 +94,9 @@ def lib():
         L.orc_pressure_average.argtypes = [C.c_void_p, d3, i3]
         L.orc_bond_list.restype = C.c_long
         L.orc_bond_list.argtypes = [C.c_void_p, i3, i3, i3, C.c_long]
+        L.orc_sort_table.argtypes = [C.c_int, i3, i3]
+        L.orc_sort_mols.argtypes = [C.c_int, d3, d3, i3, d3, d3, C.c_int, C.c_int, C.c_int, i3,
+                                    C.POINTER(SortState), i3, i3]
         _lib = L
     return _lib
 
@@ -113,6 +116,39 @@ class OracleError(RuntimeError):
 def _check(rc):
     if rc:
         raise OracleError(ORC_ERRORS.get(rc, f"error {rc}"))
+
+
+class SortState(C.Structure):
+    """The save variables of sort_mols (linklist.f90:2758-2762)."""
+    _fields_ = [("nrebuilds", C.c_int), ("sf2", C.c_int), ("sf1", C.c_double)]
+
+    def __init__(self):
+        super().__init__(1, 5, 1.5)
+
+
+def sort_table(sort_flag, nblocks):
+    """Hcurve over nblocks sort blocks per axis, flat and x fastest
+    (orc_sort_table)."""
+    nb = np.ascontiguousarray(nblocks, dtype=np.int32)
+    out = np.zeros(int(np.prod(nb)), np.int32)
+    _check(lib().orc_sort_table(int(sort_flag), _ip(nb), _ip(out)))
+    return out
+
+
+def sort_mols(r, v, glob, domain, cellsidelength, sort_flag, sort_freq, sortblocksize, state):
+    """One call of sort_mols on (n, 3) r and v and n global numbers.
+    Returns (r, v, glob, perm, did): did 0 = order kept by the counter, 1 =
+    sorted (perm[p] = old index now at p), 2 = a block overflowed."""
+    r = np.array(r, dtype=np.float64, order="C"); v = np.array(v, dtype=np.float64, order="C")
+    g = np.array(glob, dtype=np.int32)
+    n = r.shape[0]
+    nb = np.array([int(np.ceil(domain[k] / (sortblocksize * cellsidelength[k]))) for k in range(3)], np.int32)
+    hc = sort_table(sort_flag, nb) if sort_flag else np.zeros(1, np.int32)
+    perm = np.zeros(max(n, 1), np.int32); did = np.zeros(1, np.int32)
+    dom = np.ascontiguousarray(domain, dtype=np.float64); cs = np.ascontiguousarray(cellsidelength, dtype=np.float64)
+    _check(lib().orc_sort_mols(n, _dp(r), _dp(v), _ip(g), _dp(dom), _dp(cs), int(sort_flag), int(sort_freq),
+                               int(sortblocksize), _ip(hc), C.byref(state), _ip(perm), _ip(did)))
+    return r, v, g, (perm[:n] if did[0] == 1 else None), int(did[0])
 
 
 def global_domain(nunits, density):
