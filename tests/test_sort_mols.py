@@ -251,6 +251,29 @@ def test_fused_loop_sorts_like_the_mirror(liquid, monkeypatch, integration, forc
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("flag", [1, 2])
+def test_sort_of_molecules_on_the_lower_face_equals_oracle(liquid, flag):
+    """A molecule exactly at -L/2 gets block 0, outside Hcurve: the reference
+    reads the element before (iblk, jblk, kblk)'s column-major place, which
+    both paths reproduce, clamping an offset before the table's start."""
+    r, v, dom = liquid
+    r = r.copy()
+    r[0, 0] = -0.5 * dom[0]
+    r[1] = -0.5 * np.asarray(dom)
+    r[2, 1] = -0.5 * dom[1]
+    s = _system(r, v, dom)
+    s.set_sort(flag, 1, 1)
+    cs = O.cells(dom, 2.5, (0.3, 0.3, 0.3))[2]
+    r0, v0, _, g0 = s.download()
+    r1, v1, g1, _, did = O.sort_mols(r0, v0, g0, dom, cs, flag, 1, 1, O.SortState())
+    s.sort_mols()
+    r2, v2, _, g2 = s.download()
+    assert did == 1
+    assert np.array_equal(r2, r1) and np.array_equal(v2, v1) and np.array_equal(g2, g1)
+    s.close()
+
+
+@pytest.mark.gpu
 def test_step_graphs_carry_the_sort(liquid, monkeypatch):
     """With sorting on, the step graphs still capture the rebuild body (the
     sort kernels and the library radix sort inside the conditional node)
