@@ -464,7 +464,10 @@ FM_API int fm_engine_create(const fm_engine_params *p, fm_engine **out);
 FM_API int fm_engine_destroy(fm_engine *e);
 FM_API int fm_engine_set_stream(fm_engine *e, void *cuda_stream);
 /* Queues a job: r, v are (3, np) column-major; tag (np), rtether and slidev
- * ((3, np)) may be NULL.  The arrays are copied; returns the job id. */
+ * ((3, np)) may be NULL.  The arrays are copied; returns the job id.  A job
+ * keeps its molecules in submission order: sort_mols (fm_set_sort) is a
+ * single-system feature, so a job's results come back in the order it was
+ * submitted in, whatever the deck's SORT_FLAG. */
 FM_API int fm_engine_submit(fm_engine *e, const fm_job *job, const double *r, const double *v, const int32_t *tag,
                             const double *rtether, const double *slidev, int64_t *job_id);
 /* One admission point (retire finished jobs, admit queued ones that fit)
