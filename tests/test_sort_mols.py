@@ -217,19 +217,32 @@ def test_sort_counter_and_overflow_equal_oracle(liquid):
     s.close()
 
 
+FUSED_CASES = [
+    dict(integration_algorithm=1, force_list=3),
+    dict(integration_algorithm=0, force_list=3),
+    dict(integration_algorithm=1, force_list=0),
+    dict(integration_algorithm=1, force_list=3, force_path=api.FORCE_PATH_TILES),
+    dict(integration_algorithm=1, force_list=3, precision=api.PRECISION_FP32),
+    dict(integration_algorithm=1, force_list=3, rebuild_criteria=2),
+]
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("integration,force_list", [(1, 3), (0, 3), (1, 0)])
+@pytest.mark.parametrize("case", FUSED_CASES, ids=["vv", "lfv", "all_pairs", "tiles", "fp32", "crit2"])
 @pytest.mark.parametrize("graphs", ["1", "0"])
-def test_fused_loop_sorts_like_the_mirror(liquid, monkeypatch, integration, force_list, graphs):
+def test_fused_loop_sorts_like_the_mirror(liquid, monkeypatch, case, graphs):
     """The fused loop runs sort_mols inside its rebuild branch (in the step
     graphs' conditional body, or as gated launches with FM_STEP_GRAPHS=0):
     120 iterations end bit for bit where the subroutine mirror ends, with the
-    same numbering and the same number of sorts (sort_freq 2)."""
+    same numbering and the same number of sorts (sort_freq 2) -- leap-frog,
+    all pairs, the tiled force path, FP32 pair forces and the displacement
+    rebuild criterion included."""
     monkeypatch.setenv("FM_STEP_GRAPHS", graphs)
     r, v, dom = liquid
+    integration, force_list = case["integration_algorithm"], case["force_list"]
     out = []
     for fused in (False, True):
-        s = _system(r, v, dom, integration_algorithm=integration, force_list=force_list)
+        s = _system(r, v, dom, **case)
         s.set_sort(2, 2, 1)
         s.setup()
         if fused:
