@@ -370,7 +370,7 @@ def run_batched(api, torch, dev, nsteps, nrep=256):
 
 
 # Poisson arrivals at this fraction of the service rate probed with 48 jobs resident at once.
-ARRIVAL_FRACTION = 0.6
+ARRIVAL_FRACTION = 0.7
 
 
 def run_served(api, torch, dev, njobs, seed=0x466D6F6C + 5):
@@ -379,9 +379,9 @@ def run_served(api, torch, dev, njobs, seed=0x466D6F6C + 5):
     U(0.5, 2.0); the arrival rate is ARRIVAL_FRACTION x the service rate
     measured with 48 jobs resident at once.  Served jobs overlap less than the
     probe's, so each tick carries fewer molecules and its fixed launch cost
-    weighs more: 0.5x left the engine ~77% busy, 0.55x ~79%, 0.6x ~81%
-    (`gpu_busy_frac`: wall time inside graphs of ticks / total), each with a
-    bounded queue (p50 ~0.2 s, p99 ~0.5 s).  Latency = finish time -
+    weighs more: 0.5x left the engine ~77% busy, 0.55x ~79%, 0.6x 80-81%,
+    0.65x ~82% and 0.7x ~83% (`gpu_busy_frac`: wall time inside graphs of
+    ticks / total), each with a bounded queue (p50 ~0.2 s, p99 0.5-0.7 s).  Latency = finish time -
     scheduled arrival time."""
     from flowmol_b200 import couette
     rng = np.random.Generator(np.random.Philox(seed))
