@@ -109,7 +109,7 @@ struct fm_handle {
     FmDev rbd[4]{};
     int rbt[4] = {0, 0, 0, 0};    // lanes per molecule the force kernels were captured with
     bool rb_off = false;          // graphs unavailable here: per-kernel launches
-    cudaStream_t cap_st = nullptr, cap_st2 = nullptr;
+    cudaStream_t cap_st = nullptr, cap_st2 = nullptr, cap_st3 = nullptr;
     // sort_mols (fm_sort.cu): sort_flag 0 leaves the numbering alone
     int sort_flag = 0;
     fm::FmSortDev sdev{};
@@ -212,7 +212,8 @@ static void release(fm_handle *h)
     free_sort(h);
     if (h->cap_st) cudaStreamDestroy(h->cap_st);
     if (h->cap_st2) cudaStreamDestroy(h->cap_st2);
-    h->cap_st = h->cap_st2 = nullptr;
+    if (h->cap_st3) cudaStreamDestroy(h->cap_st3);
+    h->cap_st = h->cap_st2 = h->cap_st3 = nullptr;
     for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
     h->ev.clear();
     FmDev &d = h->d;
@@ -1063,6 +1064,40 @@ static void queue_rebuild_check(fm_handle *h, int it, int flip)
     }
 }
 
+// sort_mols inside the rebuild body being captured on h->cap_st2: the counter
+// kernel, then a nested IF node that it sets on the rebuilds that sort, whose
+// body (captured on h->cap_st3) holds the keys, the radix sort and the
+// renumbering.  The other rebuilds skip the radix sort entirely.
+static bool capture_sort(fm_handle *h)
+{
+    const FmDev &d = h->d;
+    cudaStreamCaptureStatus cst;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    if (!h->cap_st3 && cudaStreamCreateWithFlags(&h->cap_st3, cudaStreamNonBlocking) != cudaSuccess) return false;
+    if (cudaStreamGetCaptureInfo(h->cap_st2, &cst, nullptr, &g, nullptr, nullptr) != cudaSuccess || !g) return false;
+    cudaGraphConditionalHandle cond{};
+    if (cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault) != cudaSuccess) return false;
+    fm::launch_sort_gate_graph(d, h->sdev, cond, SORT_KERNELS - 1, h->cap_st2);
+    if (cudaStreamGetCaptureInfo(h->cap_st2, &cst, nullptr, nullptr, &deps, &nd) != cudaSuccess) return false;
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t ifn = nullptr;
+    if (cudaGraphAddNode(&ifn, g, deps, nd, &cp) != cudaSuccess) return false;
+    if (cudaStreamUpdateCaptureDependencies(h->cap_st2, &ifn, 1, cudaStreamSetCaptureDependencies) != cudaSuccess)
+        return false;
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    if (cudaStreamBeginCaptureToGraph(h->cap_st3, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) !=
+        cudaSuccess)
+        return false;
+    fm::launch_sort_body(d, h->sdev, 1, h->cap_st3);
+    return cudaStreamEndCapture(h->cap_st3, &body) == cudaSuccess;
+}
+
 // The rebuild branch of an iteration, appended to the graph being captured
 // on h->cap_st: k_decide_graph (the iteration from the device counter g_iter)
 // and an IF node whose body is the rebuild pipeline of queue_cells +
@@ -1079,7 +1114,7 @@ static bool capture_branch(fm_handle *h, int flip)
     if (cudaStreamGetCaptureInfo(h->cap_st, &cst, nullptr, &g, nullptr, nullptr) != cudaSuccess || !g) return false;
     cudaGraphConditionalHandle cond{};
     if (cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault) != cudaSuccess) return false;
-    const int body_kernels = 8 + (d.tile ? 1 : 0) + (d.angular ? 1 : 0) + (h->sort_flag ? SORT_KERNELS : 0);
+    const int body_kernels = 8 + (d.tile ? 1 : 0) + (d.angular ? 1 : 0) + (h->sort_flag ? 1 : 0);
     fm::launch_decide_graph(d, flip, p.rebuild_criteria, p.fixed_rebuild, h->half_min_delta, cond, body_kernels,
                             h->cap_st);
     if (cudaStreamGetCaptureInfo(h->cap_st, &cst, nullptr, nullptr, &deps, &nd) != cudaSuccess) return false;
@@ -1098,9 +1133,14 @@ static bool capture_branch(fm_handle *h, int flip)
         return false;
     fm::pdl_capture = true;  // the body's first kernel has no predecessor to overlap
     fm::launch_wrap_bin(d, 1, 1, 1, fm::ITER_DEVICE, h->cap_st2);
-    if (h->sort_flag) fm::launch_sort(d, h->sdev, 1, h->cap_st2);
-    fm::pdl_capture = false;
+    if (h->sort_flag && !capture_sort(h)) {
+        cudaGraph_t body_again = nullptr;  // the node's own graph: ends the capture, nothing to free
+        cudaStreamEndCapture(h->cap_st2, &body_again);
+        return false;
+    }
+    fm::pdl_capture = h->sort_flag != 0;  // no programmatic edge out of the sort's conditional node
     fm::launch_scan_cells(d, 1, h->cap_st2);
+    fm::pdl_capture = false;
     fm::launch_scatter(d, 1, h->cap_st2);
     fm::launch_reorder(d, 1, h->tpos, h->tuidx, h->cap_st2);
     if (d.tile) fm::launch_blk_seg(d, 1, fm::ITER_DEVICE, h->cap_st2);

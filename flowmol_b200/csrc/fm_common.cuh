@@ -322,5 +322,11 @@ size_t sort_scratch_bytes(int n, int end_bit);
 // The rebuild's sort_mols: counter, keys, stable sort, renumbering.  With
 // `gated` the kernels run only on a rebuild step.
 void launch_sort(const FmDev &d, const FmSortDev &s, int gated, cudaStream_t st);
+// The same split for the rebuild graph: the counter kernel, which sets `cond`
+// (a conditional node in the rebuild body) when this rebuild sorts and then
+// counts body_kernels more kernels, and the node's body.
+void launch_sort_gate_graph(const FmDev &d, const FmSortDev &s, cudaGraphConditionalHandle cond, int body_kernels,
+                            cudaStream_t st);
+void launch_sort_body(const FmDev &d, const FmSortDev &s, int gated, cudaStream_t st);
 
 }  // namespace fm

@@ -24,7 +24,11 @@
 //                 the overflow flag
 //   radix sort    (block, upload index) pairs: stable, so the molecules of a
 //                 block keep their order (CUB DeviceRadixSort, library code;
-//                 it runs on rebuild steps only)
+//                 its size is fixed at launch, so it cannot return early: in
+//                 the step graphs it sits with the kernels below in a nested
+//                 conditional node that k_sort_gate_graph opens only on the
+//                 rebuilds that sort; launched one by one it runs whenever
+//                 the gate does)
 //   k_sort_rank   new upload index of every old one; block counts cleared for
 //                 the next sort; an overflow grows the safety factors instead
 //   k_sort_apply  slot_of renumbered, global numbers permuted into scratch
@@ -56,22 +60,41 @@ __device__ __forceinline__ int sort_block(double r, double hd, double bsl)
     return (int)ceil(__ddiv_rn(__dadd_rn(r, hd), bsl));
 }
 
-__global__ void k_sort_gate(FmDev d, FmSortDev s, int gated)
+// The rebuild counter (linklist.f90:2766-2771) and ave_molperblock =
+// ceiling((np/blocks)*sf1 + sf2) (:2794-2796: an integer quotient, then one
+// multiply and one add in FP64).  Returns whether this rebuild sorts.
+__device__ bool sort_due(const FmDev &d, const FmSortDev &s)
 {
-    if (threadIdx.x != 0 || !sort_gate(d, gated)) return;
     FmSortScalars &q = *s.ss;
     q.due = 0;
-    if (q.nrebuilds != s.freq) {  // linklist.f90:2766-2771
+    if (q.nrebuilds != s.freq) {
         q.nrebuilds += 1;
-        return;
+        return false;
     }
     q.nrebuilds = 1;
-    // ave_molperblock = ceiling((np/blocks)*sf1 + sf2) (:2794-2796): an
-    // integer quotient, then one multiply and one add in FP64
     const int ave = d.n / s.blocks;
     q.ave = (int)ceil(__dadd_rn(__dmul_rn((double)ave, q.sf1), (double)q.sf2));
     q.overflow = 0;
     q.due = 1;
+    return true;
+}
+
+__global__ void k_sort_gate(FmDev d, FmSortDev s, int gated)
+{
+    if (threadIdx.x != 0 || !sort_gate(d, gated)) return;
+    sort_due(d, s);
+}
+
+// In the rebuild graph's body: opens the nested conditional node that holds
+// the rest of the sort only when this rebuild sorts (the condition's default
+// is 0 at every graph launch), and counts the kernels the node will run.
+__global__ void k_sort_gate_graph(FmDev d, FmSortDev s, cudaGraphConditionalHandle cond, int body_kernels)
+{
+    if (threadIdx.x != 0 || !sort_gate(d, 1)) return;
+    if (sort_due(d, s)) {
+        d.sc->graph_kernels += body_kernels;
+        cudaGraphSetConditional(cond, 1u);
+    }
 }
 
 __global__ void k_sort_keys(FmDev d, FmSortDev s, int gated)
@@ -232,16 +255,27 @@ size_t sort_scratch_bytes(int n, int end_bit)
     return bytes;
 }
 
-void launch_sort(const FmDev &d, const FmSortDev &s, int gated, cudaStream_t st)
+void launch_sort_body(const FmDev &d, const FmSortDev &s, int gated, cudaStream_t st)
 {
     const int g = grid_for(std::max(d.n, s.blocks));
-    k_sort_gate<<<1, 32, 0, st>>>(d, s, gated);
     k_sort_keys<<<g, 256, 0, st>>>(d, s, gated);
     size_t bytes = s.tmp_bytes;
     cub::DeviceRadixSort::SortPairs(s.tmp, bytes, s.key, s.key_out, s.val, s.val_out, d.n, 0, s.end_bit, st);
     k_sort_rank<<<g, 256, 0, st>>>(d, s, gated);
     k_sort_apply<<<g, 256, 0, st>>>(d, s, gated);
     k_sort_copy<<<g, 256, 0, st>>>(d, s, gated);
+}
+
+void launch_sort(const FmDev &d, const FmSortDev &s, int gated, cudaStream_t st)
+{
+    k_sort_gate<<<1, 32, 0, st>>>(d, s, gated);
+    launch_sort_body(d, s, gated, st);
+}
+
+void launch_sort_gate_graph(const FmDev &d, const FmSortDev &s, cudaGraphConditionalHandle cond, int body_kernels,
+                            cudaStream_t st)
+{
+    k_sort_gate_graph<<<1, 32, 0, st>>>(d, s, cond, body_kernels);
 }
 
 }  // namespace fm
